@@ -1,0 +1,302 @@
+"""Benchmark of the per-batch sorting hot path on B200.
+
+Workload (one step = one padded 60000-sample batch through the whole path:
+int16 ingest, highpass, whitening + drift, score GEMM, matching pursuit, PC
+features, records): 384-channel staggered probe, 400 templates, NT = 60000,
+linear drift of 5 um/min, FP32 path. Synthetic, seeded recording (no public
+dataset exists for this path). Metric: recording-seconds sorted per second.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+N > 1 runs one independent replica per GPU (the path has no exchange step);
+value = total recording-seconds of all ranks / max over ranks of device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+import torch
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+FS = 30000.0
+METRIC = 'rec-sec sorted/sec & p99 latency, 384ch; BF16 vs FP32 at >=0.99 spike agreement'
+N_BATCH_POOL = 6   # distinct device-resident batches the steps rotate over (276 MB int16 > L2)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument('--gpus', type=int, default=1)
+    p.add_argument('--steps', type=int, default=20)
+    p.add_argument('--warmup', type=int, default=3)
+    p.add_argument('--impl', default='b200', choices=['b200', 'reference'])
+    p.add_argument('--templates', type=int, default=400)
+    p.add_argument('--precision', default='fp32', choices=['fp32', 'bf16'])
+    p.add_argument('--no-cpu-baseline', action='store_true')
+    return p.parse_args()
+
+
+def workload(T, rank):
+    from livespikesorter_b200 import synth
+    setup, rec = synth.config(1, duration_s=(N_BATCH_POOL + 2) * 2.0, seed=17 + rank, T=T)
+    return setup, rec
+
+
+def batch_rows(rec, setup, ib):
+    NT, nt = setup.NT, setup.nt
+    b0 = ib * NT - nt
+    return np.ascontiguousarray(rec.raw[b0:b0 + NT + 2 * nt])
+
+
+def workload_desc(T, precision):
+    return {'workload': f'384-ch staggered probe, {T} templates, NT=60000 int16 batches (+-61 context), '
+                        f'drift 5 um/min, highpass+whitening+drift, score GEMM, matching pursuit, PC features; '
+                        f'{precision.upper()} path',
+            'channels': 384, 'templates': T, 'batch_samples': 60000, 'nt': 61, 'n_pcs': 6,
+            'nearest_chans': 10, 'precision': precision,
+            'l2': f'steps rotate over {N_BATCH_POOL} device-resident batches (276 MB int16) and each step '
+                  'streams >1 GB of intermediates, both larger than the 126 MB L2'}
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = ROOT / 'gpurun_out' / f'clocks_{os.getpid()}.csv'
+
+    def __enter__(self):
+        try:
+            self.path.parent.mkdir(exist_ok=True)
+            q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+                 'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+                 'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+            self.f = open(self.path, 'w')
+            self.proc = subprocess.Popen(['nvidia-smi', f'--id={self.index}', f'--query-gpu={q}',
+                                          '--format=csv,noheader,nounits', '-lms', '100'],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc or not self.path.exists():
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['unsampled']}
+        rows = [l.split(',') for l in self.path.read_text().strip().splitlines() if l.count(',') >= 8]
+        if not rows:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['unsampled']}
+        sm = [float(r[1]) for r in rows]
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if 'Active' in v and 'Not' not in v})
+        return {'sm_mhz': float(np.median(sm)), 'sm_max_mhz': float(rows[0][2]), 'reasons': reasons,
+                'samples': len(rows)}
+
+
+def algorithmic_work(setup, spikes_per_batch, T):
+    """Per-batch algorithmic FLOPs and bytes (the per-unit formulas of the
+    design notes, times one batch)."""
+    C, K, nt = setup.C, setup.K, setup.nt
+    N = setup.NT + 2 * nt
+    L2 = 2 * nt + 1
+    gemm_flops = 2.0 * T * C * K * N
+    mp_bytes = 4.0 * T * N + spikes_per_batch * 12.0 * T * L2
+    return gemm_flops, mp_bytes
+
+
+def run_b200(args):
+    from livespikesorter_b200.sorter import Sorter
+    rank = int(os.environ.get('RANK', 0))
+    world = int(os.environ.get('WORLD_SIZE', 1))
+    local = int(os.environ.get('LOCAL_RANK', 0))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=300))
+    T = args.templates
+    setup, rec = workload(T, rank)
+    s = Sorter.from_setup(setup, device=local, precision=args.precision)
+    s.set_profiling(True)
+    ids = list(range(1, N_BATCH_POOL + 1))
+    rows_h = [torch.from_numpy(batch_rows(rec, setup, ib)).pin_memory() for ib in ids]
+    rows_d = [r.cuda(local) for r in rows_h]
+    drifts = [setup.drift_matrix(rec.dshift[ib]) for ib in ids]
+    nb = rec.n_batches
+    stream = torch.cuda.current_stream(local)
+
+    def step(i, host):
+        j = i % len(ids)
+        s.set_drift(drifts[j])
+        return s.sort_batch(rows_h[j] if host else rows_d[j], ids[j], nb, on_device=not host)
+
+    def timed(K, W, host):
+        for i in range(W):
+            step(i, host)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(K + 1)]
+        stages, spikes, rounds = [], [], []
+        launches0 = s.stats()['launches']
+        ev[0].record(stream)
+        for i in range(K):
+            r = step(i, host)
+            ev[i + 1].record(stream)
+            stages.append(s.stage_times())
+            spikes.append(len(r['time']))
+            rounds.append(s.stats()['rounds'])
+        torch.cuda.synchronize()
+        per = np.array([ev[i].elapsed_time(ev[i + 1]) for i in range(K)])
+        tot = float(ev[0].elapsed_time(ev[K]))
+        if dist:
+            t = torch.tensor([tot], device=f'cuda:{local}')
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            tot = float(t.item())
+        return tot, per, stages, spikes, rounds, s.stats()['launches'] - launches0
+
+    K, W = args.steps, max(3, args.warmup)
+    with Clocks(local) as clk:
+        tot, per, stages, spikes, rounds, launches = timed(K, W, host=False)
+    clocks = clk.summary()
+    tot_h, per_h, stages_h, _, _, _ = timed(K, W, host=True)
+    rec_s = setup.NT / FS
+    value = world * K * rec_s / (tot / 1e3)
+    e2e = world * K * rec_s / (tot_h / 1e3)
+    # roofline of the dominant kernel, from the device-resident timed steps
+    mean_st = {k: float(np.mean([st[k] for st in stages])) for k in stages[0]}
+    kern = {k: v for k, v in mean_st.items() if k not in ('total_ms', 'h2d_ms', 'records_ms')}
+    top = max(kern, key=kern.get)
+    gemm_flops, mp_bytes = algorithmic_work(setup, float(np.mean(spikes)), T)
+    peaks = json.loads((ROOT / 'MEASURED_PEAKS.json').read_text()) if (ROOT / 'MEASURED_PEAKS.json').exists() else {}
+    hbm = peaks.get('hbm_gbs', 6650.0)
+    tfl = peaks.get('bf16_tflops', 1590.0)
+    src = 'measured' if peaks else 'fallback'
+    if top == 'mp_ms':
+        ach = mp_bytes / (mean_st['mp_ms'] / 1e3) / 1e9
+        roof = {'kernel': 'k_mp (matching pursuit)', 'bound': 'hbm', 'achieved': ach, 'peak': hbm, 'unit': 'GB/s',
+                'frac': ach / hbm, 'traffic': None, 'peak_source': src}
+    else:
+        ach = gemm_flops / (mean_st['score_ms'] / 1e3) / 1e12
+        roof = {'kernel': 'k_sgemm (score GEMM, FP32 SIMT)' if args.precision == 'fp32' else 'score GEMM',
+                'bound': 'tensor', 'achieved': ach, 'peak': tfl, 'unit': 'TFLOP/s', 'frac': ach / tfl,
+                'traffic': None, 'peak_source': src, 'top_stage': top}
+    h2d = int(rows_h[0].numel() * 2 + setup.C * setup.C * 4)
+    d2h = int(np.mean(spikes) * (8 + 4 + 4 + setup.nC * setup.K * 4) + 16)
+    out = {
+        'metric': METRIC, 'value': value, 'unit': 'rec-s/s', 'n_gpus': world, 'steps': K, 'warmup': W,
+        'ms_per_step': tot / K, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+        'dtype': 'f32' if args.precision == 'fp32' else 'bf16+f32', 'data': 'synthetic',
+        'config': workload_desc(T, args.precision) | {'parallelism': f'replicas x{world}'},
+        'e2e': {'value': e2e, 'unit': 'rec-s/s', 'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h,
+                'latency_ms_p50': float(np.percentile(per_h, 50)), 'latency_ms_p99': float(np.percentile(per_h, 99))},
+        'latency_ms_p50': float(np.percentile(per, 50)), 'latency_ms_p99': float(np.percentile(per, 99)),
+        'roofline': roof, 'gpu_launches': int(launches), 'clocks': clocks,
+        'stage_ms': mean_st, 'spikes_per_batch': float(np.mean(spikes)), 'rounds_per_batch': float(np.mean(rounds)),
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        out['cpu_baseline'] = cpu_baseline(setup, rec, budget_s=20.0)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
+def oracle_batch(setup, rec, ib, ns=None):
+    """The oracle's filter + run_matching + PC features on one batch."""
+    sys.path.insert(0, str(ROOT / 'oracle'))
+    import ks4_oracle as ko
+    X = ko.padded_batch(rec.raw, ib, setup.NT, setup.nt)
+    if ns is not None:
+        X = X[:, :ns + 2 * setup.nt]
+    X = ko.filter_batch(X, hp_filter=setup.hp_filter, whiten_mat=setup.Wrot,
+                        drift_M=setup.drift_matrix(rec.dshift[ib]))
+    st, amps, Xres = ko.run_matching(X, setup.U, setup.ctc, setup.wPCA, setup.Th, setup.nt)
+    ko.extract_batch(st, amps, Xres, setup.iCC, setup.iU, setup.Ucc, setup.wPCA, setup.nt, setup.nt0min, ib,
+                     setup.NT)
+    return len(st)
+
+
+def cpu_baseline(setup, rec, budget_s=20.0):
+    cores = os.cpu_count() or 1
+    torch.set_num_threads(cores)
+    oracle_batch(setup, rec, 1, ns=6000)  # warm-up
+    t0 = time.perf_counter()
+    n = 0
+    nb = 0
+    while True:
+        oracle_batch(setup, rec, 1 + nb % N_BATCH_POOL)
+        nb += 1
+        n = time.perf_counter() - t0
+        if n > budget_s or nb >= 3:
+            break
+    rate = nb * setup.NT / FS / n
+    return {'value': rate, 'unit': 'rec-s/s', 'cores': cores, 'kind': 'port',
+            'sample': f'{nb} full batches (60000 samples each) of the same workload through the CPU oracle '
+                      f'(torch {torch.__version__}, {cores} threads): filter + run_matching + PC features'}
+
+
+def run_reference(args):
+    """The reference's CPU implementation of the path (Kilosort4's torch
+    template matching, restated in the oracle because the reference is Python
+    and cannot travel), on the host cores, same workload and metric."""
+    rank = int(os.environ.get('RANK', 0))
+    if rank != 0:
+        return
+    T = args.templates
+    setup, rec = workload(T, 0)
+    cores = os.cpu_count() or 1
+    torch.set_num_threads(cores)
+    t0 = time.perf_counter()
+    oracle_batch(setup, rec, 1, ns=6000)
+    # size each step so that warmup + steps stay within ~3 minutes
+    t_small = time.perf_counter() - t0
+    est_full = t_small * 10
+    budget = 180.0 / max(1, args.steps + args.warmup)
+    ns = int(min(setup.NT, max(3000, setup.NT * budget / max(est_full, 1e-3))) // 1000 * 1000)
+    for i in range(args.warmup):
+        oracle_batch(setup, rec, 1 + i % N_BATCH_POOL, ns=ns)
+    times = []
+    for i in range(args.steps):
+        t = time.perf_counter()
+        oracle_batch(setup, rec, 1 + i % N_BATCH_POOL, ns=ns)
+        times.append(time.perf_counter() - t)
+    tot = float(np.sum(times))
+    value = args.steps * ns / FS / tot
+    cpu = {'value': value, 'unit': 'rec-s/s', 'cores': cores, 'kind': 'port',
+           'sample': f'each step: one {ns}-sample slice (+-61 context) of a 60000-sample batch through the '
+                     f'oracle filter + run_matching + PC features, torch CPU, {cores} threads'}
+    out = {'metric': METRIC, 'value': value, 'unit': 'rec-s/s', 'n_gpus': args.gpus, 'steps': args.steps,
+           'warmup': args.warmup, 'ms_per_step': tot / args.steps * 1e3, 'higher_is_better': True,
+           'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic', 'impl': 'reference',
+           'config': workload_desc(T, 'fp32') | {'parallelism': 'cpu'},
+           'cpu_baseline': cpu, 'e2e': {'value': value, 'unit': 'rec-s/s', 'h2d_bytes_per_step': 0,
+                                        'd2h_bytes_per_step': 0},
+           'latency_ms_p50': float(np.percentile(times, 50) * 1e3),
+           'latency_ms_p99': float(np.percentile(times, 99) * 1e3)}
+    print(json.dumps(out))
+
+
+if __name__ == '__main__':
+    a = parse()
+    if a.impl == 'reference':
+        run_reference(a)
+    else:
+        run_b200(a)

@@ -1,0 +1,183 @@
+/*
+ * lss.h - C ABI of the B200-native per-batch spike-sorting hot path.
+ *
+ * A drop-in for the sorting path of LiveSpikeSorter's V2 sorter
+ * (src/SpikeSorter/OnlineSpikesV2.{h,cu}) and of the Kilosort4 template
+ * matching it mirrors (kilosort/template_matching.py, kilosort/io.py).
+ * Plain C types only: pointers, sizes and status codes. No exception crosses
+ * this boundary and nothing here calls exit().
+ *
+ * Thread safety: one handle per probe stream; distinct handles may be used
+ * from distinct threads concurrently. A single handle is not re-entrant.
+ * Streams are passed as `void*` (a cudaStream_t; NULL = legacy default stream).
+ */
+#ifndef LSS_H_
+#define LSS_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes (replace _RUN_ERROR / _CUDA_CALL exceptions and loader exit(),
+ * src/Helpers/Utils.h:41-64, OnlineSpikesV2.cu:437-441). */
+#define LSS_OK            0
+#define LSS_ERR_ARG       1   /* invalid argument / unsupported value       */
+#define LSS_ERR_IO        2   /* file missing, unreadable or malformed .npy */
+#define LSS_ERR_SHAPE     3   /* tensor dtype or shape mismatch             */
+#define LSS_ERR_CUDA      4   /* CUDA runtime error                         */
+#define LSS_ERR_CAPACITY  5   /* spike or record buffer too small           */
+#define LSS_ERR_TIMEOUT   6   /* a bounded device-side wait gave up         */
+#define LSS_ERR_STATE     7   /* call out of order (e.g. no drift matrix)   */
+
+/* Score precision of the template-matching GEMM. */
+#define LSS_PREC_FP32          0  /* FP32 scores (parity path)                        */
+#define LSS_PREC_BF16_RECHECK  1  /* BF16 tcgen05 GEMM + FP32 recheck of near ties    */
+
+typedef struct lss_handle lss_handle;
+
+/* Shapes and hyper-parameters. Mirrors the sorter's members
+ * (OnlineSpikesV2.h:84-102) and the Kilosort ops entries it reads
+ * (misc.txt parsing at OnlineSpikesV2.cu:435-457). */
+typedef struct lss_config {
+    int32_t n_chan;        /* C: channels after chan_map                        */
+    int32_t n_chan_bin;    /* channels per raw int16 row (>= n_chan)            */
+    int32_t n_templates;   /* T: rows of Wall3 (unclu_T)                        */
+    int32_t n_pcs;         /* K: temporal basis size                            */
+    int32_t nt;            /* template length in samples (M)                    */
+    int32_t n_nearest;     /* nC: channels per PC feature                       */
+    int32_t batch_size;    /* NT: samples per batch (padded batch = NT + 2*nt)  */
+    int32_t nt0min;        /* trough alignment sample                           */
+    float   th_learned;    /* Th: score threshold is Th*Th                      */
+    int32_t max_rounds;    /* matching-pursuit round cap (Kilosort: 100)        */
+    int32_t max_spikes;    /* per-batch spike capacity (Kilosort: 100000)       */
+    int32_t do_car;        /* subtract the per-sample median across channels    */
+    int32_t invert_sign;   /* multiply raw data by -1                           */
+    int32_t precision;     /* LSS_PREC_*                                        */
+    int32_t device;        /* CUDA device ordinal                               */
+    int32_t hp_len;        /* taps in hp_filter (0 = no highpass)               */
+} lss_config;
+
+/* Host tensors, row-major, float32 unless noted. Kilosort export names
+ * (src/Python/run_online_spikes.py:548-576). The library copies them. */
+typedef struct lss_tensors {
+    const float*   wall3;      /* U          [T, K, C]                              */
+    const float*   wpca;       /* wPCA       [K, nt]                                */
+    const float*   ctc;        /* ctc        [T, T, 2*nt+1]  (ctc[i, j, l])         */
+    const float*   whitening;  /* Wrot       [C, C]                                 */
+    const float*   drift;      /* M          [C, C] or NULL (identity)              */
+    const float*   hp_filter;  /* hp_filter  [hp_len] or NULL                       */
+    const int64_t* iCC;        /* iCC        [nC, C]                                */
+    const int64_t* iU;         /* iU         [T]                                    */
+    const float*   Ucc;        /* Ucc        [nC, T, K]                             */
+    const int32_t* chan_map;   /* chan_map   [C] or NULL (identity)                 */
+    const float*   nm;         /* template energies [T] or NULL (computed)          */
+} lss_tensors;
+
+/* Caller-owned spike records of one batch (OnlineSpikesPayload's Times /
+ * Templates / Amplitudes, onlineSpikesPayload.h:8-48, plus Kilosort's tF).
+ * `count` is written on return; on LSS_ERR_CAPACITY it holds the required size. */
+typedef struct lss_records {
+    int64_t* time;         /* [capacity] absolute sample, Kilosort convention     */
+    int32_t* template_id;  /* [capacity]                                           */
+    float*   amplitude;    /* [capacity]                                           */
+    float*   pc;           /* [capacity, nC, K] or NULL                            */
+    int64_t  capacity;
+    int64_t  count;
+    int32_t  on_device;    /* 1: the four arrays are device pointers               */
+} lss_records;
+
+/* Construction. Replaces OnlineSpikesV2::OnlineSpikesV2 / initializeSorter /
+ * initializeStaticMemory (OnlineSpikesV2.cu:247-280, 321-352, 470-608): all
+ * device memory is allocated here, none per batch. */
+int  lss_create(const lss_config* cfg, const lss_tensors* tensors, lss_handle** out);
+
+/* Reads an LSS input directory (Wall3.npy, wPCA.npy, ctc.npy, whitening_mat.npy
+ * or whiteningMat.npy, drift_matrix.npy, hp_filter.npy, iCC.npy, iU.npy,
+ * Ucc.npy, channel_map.npy, misc.txt), honouring each .npy header's
+ * fortran_order flag (the reference's cnpy ignores it, cnpy.cpp:181-184, and
+ * drift_matrix.npy is written in Fortran order). `overrides` may be NULL;
+ * its non-zero fields replace values read from the directory. */
+int  lss_create_from_dir(const char* dir, const lss_config* overrides, lss_handle** out);
+
+void lss_destroy(lss_handle* h);
+
+/* Last error message of this handle, or of the calling thread's last failed
+ * create when h is NULL. */
+const char* lss_last_error(const lss_handle* h);
+
+/* Reads back the effective configuration. */
+int  lss_get_config(const lss_handle* h, lss_config* out);
+
+/* Per-batch drift interpolation matrix M [C, C] (host pointer); the filter
+ * applies (M @ Wrot) @ X as kilosort/io.py:782-789 does. NULL = identity. */
+int  lss_set_drift(lss_handle* h, const float* M);
+
+/* Ingest of one padded batch, kilosort/io.py:584-637 + 757-790:
+ * raw = the int16 rows [n_rows, n_chan_bin] that padded_batch_to_torch reads
+ * for batch `ibatch` of `n_batches` (device pointer if raw_on_device, else
+ * host), out X_dev = filtered, whitened, drift-corrected f32 [C, NT + 2*nt]
+ * (row stride NT + 2*nt). Replaces the preprocessing block of
+ * OnlineSpikesV2::runSpikeSorting (OnlineSpikesV2.cu:738-778). */
+int  lss_filter(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ibatch,
+                int64_t n_batches, int32_t raw_on_device, float* X_dev, void* stream);
+
+/* Template matching on a filtered batch, kilosort/template_matching.py:128-202
+ * (run_matching) and OnlineSpikesV2::kilosortMatchingPursuit
+ * (OnlineSpikesV2.h:56, OnlineSpikesV2.cu:873-971). X_dev f32 [C, N] (row
+ * stride N). Outputs (device pointers, run_matching order = round-major,
+ * time-minor): st_dev int64 [capacity, 2] (sample, template), amps_dev f32
+ * [capacity], xres_dev f32 [C, N] or NULL. *n_spikes = spikes found. */
+int  lss_match(lss_handle* h, const float* X_dev, int64_t N, int64_t* st_dev, float* amps_dev,
+               float* xres_dev, int64_t capacity, int64_t* n_spikes, void* stream);
+
+/* The matching-pursuit rounds alone on a given score field B_dev f32 [T, N]
+ * (template_matching.py:157-198), for parity checks of the rounds in isolation
+ * from the score GEMM. B_dev is not modified. */
+int  lss_match_scores(lss_handle* h, const float* B_dev, int64_t N, int64_t* st_dev,
+                      float* amps_dev, int64_t capacity, int64_t* n_spikes, void* stream);
+
+/* Score field B f32 [T, N] of a filtered batch (template_matching.py:145-146). */
+int  lss_scores(lss_handle* h, const float* X_dev, int64_t N, float* B_dev, void* stream);
+
+/* One batch end to end: ingest (a), scores (b), matching pursuit (c), PC
+ * features (d), time conversion and first-batch negative-time drop
+ * (template_matching.py:46-73). Records are in run_matching order. */
+int  lss_sort_batch(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ibatch,
+                    int64_t n_batches, int32_t raw_on_device, lss_records* out, void* stream);
+
+/* Statistics of the last lss_match / lss_sort_batch: rounds run, spikes,
+ * columns re-checked in FP32 (BF16 path). */
+typedef struct lss_stats {
+    int32_t rounds;
+    int64_t spikes;
+    int64_t recheck_columns;
+    int64_t recheck_flips;
+    int64_t launches;      /* kernels this handle has launched since creation */
+} lss_stats;
+int  lss_get_stats(const lss_handle* h, lss_stats* out);
+
+/* Per-stage device time of the last lss_sort_batch, from CUDA events recorded
+ * on the call's stream while profiling is on (the Timer scopes of
+ * OnlineSpikesV2.cu:719-964, whose print is disabled at Timer.h:15). */
+typedef struct lss_stage_times {
+    float h2d_ms;       /* raw rows host -> device                      */
+    float ingest_ms;    /* channel sums + mean + median CAR             */
+    float highpass_ms;  /* circular highpass                            */
+    float whiten_ms;    /* (M @ Wrot) @ X                               */
+    float project_ms;   /* temporal-basis projection                    */
+    float score_ms;     /* template score GEMM                          */
+    float mp_ms;        /* matching-pursuit rounds (+ count read-back)  */
+    float xres_ms;      /* residual                                     */
+    float feature_ms;   /* PC features                                  */
+    float records_ms;   /* record compaction + device -> host copies    */
+    float total_ms;
+} lss_stage_times;
+int  lss_set_profiling(lss_handle* h, int32_t on);
+int  lss_get_stage_times(const lss_handle* h, lss_stage_times* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LSS_H_ */

@@ -1,0 +1,102 @@
+"""ctypes binding of ``include/lss.h`` (the C ABI in ``liblss_b200.so``).
+
+Loading fails loudly when the library is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / 'liblss_b200.so'
+
+LSS_OK, LSS_ERR_ARG, LSS_ERR_IO, LSS_ERR_SHAPE, LSS_ERR_CUDA, LSS_ERR_CAPACITY, LSS_ERR_TIMEOUT, LSS_ERR_STATE = range(8)
+LSS_PREC_FP32, LSS_PREC_BF16_RECHECK = 0, 1
+
+# every entry point declared in include/lss.h
+EXPORTS = ('lss_create', 'lss_create_from_dir', 'lss_destroy', 'lss_last_error', 'lss_get_config',
+           'lss_set_drift', 'lss_filter', 'lss_match', 'lss_match_scores', 'lss_scores',
+           'lss_sort_batch', 'lss_get_stats', 'lss_set_profiling', 'lss_get_stage_times')
+
+
+class LssConfig(ct.Structure):
+    _fields_ = [('n_chan', ct.c_int32), ('n_chan_bin', ct.c_int32), ('n_templates', ct.c_int32),
+                ('n_pcs', ct.c_int32), ('nt', ct.c_int32), ('n_nearest', ct.c_int32),
+                ('batch_size', ct.c_int32), ('nt0min', ct.c_int32), ('th_learned', ct.c_float),
+                ('max_rounds', ct.c_int32), ('max_spikes', ct.c_int32), ('do_car', ct.c_int32),
+                ('invert_sign', ct.c_int32), ('precision', ct.c_int32), ('device', ct.c_int32),
+                ('hp_len', ct.c_int32)]
+
+
+class LssTensors(ct.Structure):
+    _fields_ = [('wall3', ct.c_void_p), ('wpca', ct.c_void_p), ('ctc', ct.c_void_p),
+                ('whitening', ct.c_void_p), ('drift', ct.c_void_p), ('hp_filter', ct.c_void_p),
+                ('iCC', ct.c_void_p), ('iU', ct.c_void_p), ('Ucc', ct.c_void_p),
+                ('chan_map', ct.c_void_p), ('nm', ct.c_void_p)]
+
+
+class LssRecords(ct.Structure):
+    _fields_ = [('time', ct.c_void_p), ('template_id', ct.c_void_p), ('amplitude', ct.c_void_p),
+                ('pc', ct.c_void_p), ('capacity', ct.c_int64), ('count', ct.c_int64),
+                ('on_device', ct.c_int32)]
+
+
+class LssStats(ct.Structure):
+    _fields_ = [('rounds', ct.c_int32), ('spikes', ct.c_int64), ('recheck_columns', ct.c_int64),
+                ('recheck_flips', ct.c_int64), ('launches', ct.c_int64)]
+
+
+STAGES = ('h2d_ms', 'ingest_ms', 'highpass_ms', 'whiten_ms', 'project_ms', 'score_ms', 'mp_ms', 'xres_ms',
+          'feature_ms', 'records_ms', 'total_ms')
+
+
+class LssStageTimes(ct.Structure):
+    _fields_ = [(n, ct.c_float) for n in STAGES]
+
+
+class LssError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f'lss error {code}: {msg}')
+        self.code = code
+
+
+_lib = None
+
+
+def load() -> ct.CDLL:
+    """Load ``liblss_b200.so`` (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(f'{LIB_PATH} is missing; run `python -m livespikesorter_b200.build` '
+                          '(the sorter has no CPU fallback)')
+    lib = ct.CDLL(str(LIB_PATH))
+    P, I64, I32 = ct.c_void_p, ct.c_int64, ct.c_int32
+    sig = {
+        'lss_create': ([ct.POINTER(LssConfig), ct.POINTER(LssTensors), ct.POINTER(P)], ct.c_int),
+        'lss_create_from_dir': ([ct.c_char_p, ct.POINTER(LssConfig), ct.POINTER(P)], ct.c_int),
+        'lss_destroy': ([P], None),
+        'lss_last_error': ([P], ct.c_char_p),
+        'lss_get_config': ([P, ct.POINTER(LssConfig)], ct.c_int),
+        'lss_set_drift': ([P, P], ct.c_int),
+        'lss_filter': ([P, P, I64, I64, I64, I32, P, P], ct.c_int),
+        'lss_match': ([P, P, I64, P, P, P, I64, ct.POINTER(I64), P], ct.c_int),
+        'lss_match_scores': ([P, P, I64, P, P, I64, ct.POINTER(I64), P], ct.c_int),
+        'lss_scores': ([P, P, I64, P, P], ct.c_int),
+        'lss_sort_batch': ([P, P, I64, I64, I64, I32, ct.POINTER(LssRecords), P], ct.c_int),
+        'lss_get_stats': ([P, ct.POINTER(LssStats)], ct.c_int),
+        'lss_set_profiling': ([P, I32], ct.c_int),
+        'lss_get_stage_times': ([P, ct.POINTER(LssStageTimes)], ct.c_int),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def check(rc: int, handle=None):
+    if rc != LSS_OK:
+        msg = load().lss_last_error(handle)
+        raise LssError(rc, msg.decode() if msg else '')

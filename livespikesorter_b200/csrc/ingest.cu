@@ -1,0 +1,207 @@
+// Ingest of one padded batch: int16 rows -> channel mean removal -> median
+// common-average reference -> circular highpass.
+//
+// Semantics follow kilosort/io.py:584-637 (padded_batch_to_torch) and
+// io.py:757-777 (BinaryFiltered.filter up to the whitening); the whitening and
+// drift GEMM runs in gemm_fp32.cu. LiveSpikeSorter's equivalents are
+// meanRemove / median_remove_kernel / highpassFilter
+// (myGPUhelpers.cu:98-118,471-534; OnlineSpikesV2.cu:976-1026).
+//
+// HBM layout: raw int16 [n_rows, ld_raw] (the file's interleaved rows), output
+// float [C, ldx] channel-major with time contiguous, so every later stage reads
+// 128-byte rows.
+#include "lss_kernels.cuh"
+
+namespace lss {
+
+__device__ __forceinline__ int64_t src_row(int64_t s, const IngestMap& m) {
+    int64_t j = s - m.lead;
+    if (j < 0) j = 0;
+    if (j >= m.nsamp) {
+        if (m.zero_tail) return -1;
+        j = m.nsamp - 1;
+    }
+    return j;
+}
+
+// Per-channel integer sums over the padded batch (exact: raw samples are
+// integers, so the mean is the correctly rounded quotient of an exact sum).
+// Grid: one CTA per 256 columns; threads stride over channels.
+__global__ void k_chan_sums(const int16_t* __restrict__ raw, int32_t ld_raw,
+                            const int32_t* __restrict__ chan_map, int32_t C, int64_t N,
+                            IngestMap map, long long* __restrict__ sums) {
+    const int64_t s0 = (int64_t)blockIdx.x * 256;
+    const int64_t s1 = min(N, s0 + 256);
+    for (int c = threadIdx.x; c < C; c += blockDim.x) {
+        const int ch = chan_map ? chan_map[c] : c;
+        int acc = 0;
+        for (int64_t s = s0; s < s1; ++s) {
+            const int64_t r = src_row(s, map);
+            if (r >= 0) acc += raw[r * ld_raw + ch];
+        }
+        atomicAdd((unsigned long long*)&sums[c], (unsigned long long)(long long)acc);
+    }
+}
+
+cudaError_t launch_chan_sums(const int16_t* raw, int32_t ld_raw, const int32_t* chan_map, int32_t C,
+                             int64_t N, IngestMap map, long long* sums, cudaStream_t s) {
+    cudaMemsetAsync(sums, 0, sizeof(long long) * C, s);
+    const int grid = (int)((N + 255) / 256);
+    k_chan_sums<<<grid, 256, 0, s>>>(raw, ld_raw, chan_map, C, N, map, sums);
+    return cudaGetLastError();
+}
+
+// Order-preserving float -> uint32 key.
+__device__ __forceinline__ uint32_t fkey(float f) {
+    uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float unkey(uint32_t k) {
+    uint32_t u = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+    return __uint_as_float(u);
+}
+
+// CAR tile: 32 time columns x C channels staged in shared memory. Each warp
+// finds the lower median (sorted index (C-1)/2, torch.median's choice) of a
+// column by a 32-step bitwise select on order-preserving keys, then the tile
+// is written back as 128-byte channel rows.
+constexpr int CAR_COLS = 32;
+__global__ void __launch_bounds__(256) k_car(const int16_t* __restrict__ raw, int32_t ld_raw,
+                                             const int32_t* __restrict__ chan_map, int32_t C,
+                                             int64_t N, IngestMap map, float sign,
+                                             const long long* __restrict__ sums, int do_car,
+                                             float* __restrict__ X1, int64_t ldx) {
+    extern __shared__ float sm[];
+    float* tile = sm;                                  // [C][CAR_COLS + 1]
+    float* mean = sm + (size_t)C * (CAR_COLS + 1);     // [C]
+    float* med = mean + C;                             // [CAR_COLS]
+    const int64_t s0 = (int64_t)blockIdx.x * CAR_COLS;
+    const int ncol = (int)min((int64_t)CAR_COLS, N - s0);
+    const double invN = 1.0 / (double)N;
+    for (int c = threadIdx.x; c < C; c += blockDim.x)
+        mean[c] = (float)((double)sign * (double)sums[c] * invN);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < C * CAR_COLS; idx += blockDim.x) {
+        const int c = idx % C, j = idx / C;
+        float v = 0.f;
+        if (j < ncol) {
+            const int64_t r = src_row(s0 + j, map);
+            const int ch = chan_map ? chan_map[c] : c;
+            const float x = (r >= 0) ? sign * (float)raw[r * ld_raw + ch] : 0.f;
+            v = __fsub_rn(x, mean[c]);
+        }
+        tile[c * (CAR_COLS + 1) + j] = v;
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (do_car) {
+        const uint32_t kth = (uint32_t)((C - 1) / 2);
+        for (int j = warp; j < ncol; j += blockDim.x >> 5) {
+            uint32_t res = 0;
+            for (int b = 31; b >= 0; --b) {
+                const uint32_t trial = res | ((1u << b) - 1u);
+                uint32_t cnt = 0;
+                for (int c = lane; c < C; c += 32) cnt += (fkey(tile[c * (CAR_COLS + 1) + j]) <= trial);
+                cnt = __reduce_add_sync(0xffffffffu, cnt);
+                if (cnt < kth + 1) res |= (1u << b);
+            }
+            if (lane == 0) med[j] = unkey(res);
+        }
+    } else if (threadIdx.x < CAR_COLS) {
+        med[threadIdx.x] = 0.f;
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < C * CAR_COLS; idx += blockDim.x) {
+        const int j = idx % CAR_COLS, c = idx / CAR_COLS;
+        if (j < ncol) {
+            const float v = tile[c * (CAR_COLS + 1) + j];
+            X1[(int64_t)c * ldx + s0 + j] = do_car ? __fsub_rn(v, med[j]) : v;
+        }
+    }
+}
+
+cudaError_t launch_car(const int16_t* raw, int32_t ld_raw, const int32_t* chan_map, int32_t C, int64_t N,
+                       IngestMap map, float sign, const long long* sums, int do_car, float* X1,
+                       int64_t ldx, cudaStream_t s) {
+    const size_t smem = sizeof(float) * ((size_t)C * (CAR_COLS + 1) + C + CAR_COLS);
+    static bool attr_done = false;
+    if (!attr_done) {
+        cudaFuncSetAttribute(k_car, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        attr_done = true;
+    }
+    const int grid = (int)((N + CAR_COLS - 1) / CAR_COLS);
+    k_car<<<grid, 256, smem, s>>>(raw, ld_raw, chan_map, C, N, map, sign, sums, do_car, X1, ldx);
+    return cudaGetLastError();
+}
+
+// Circular highpass: Xh[c, i] = sum_{d=-L..L} taps[d+L] * X1[c, (i+d) mod N].
+// This equals fftshift(real(ifft(fft(X) * conj(fft(h_N))))) of
+// kilosort/preprocessing.py:138-154 + io.py:771-774 with the impulse response
+// truncated where its tail mass is below 2^-30 of its L1 norm (the host picks
+// L; the tail then contributes less than the FP32 rounding of the transform).
+// CTA: one channel, HP_TILE outputs; thread: 8 consecutive outputs with a
+// sliding register window over the staged input.
+constexpr int HP_TILE = 1024;
+constexpr int HP_THREADS = HP_TILE / 8;
+__global__ void __launch_bounds__(HP_THREADS) k_highpass(const float* __restrict__ X1, int64_t ldx, int64_t N,
+                                                         const float* __restrict__ taps, int32_t L,
+                                                         float* __restrict__ Xh) {
+    extern __shared__ float sm[];
+    const int ntap = 2 * L + 1;
+    const int ntap_pad = (ntap + 7) & ~7;
+    float* tp = sm;                      // [ntap_pad] (zero padded)
+    float* xs = sm + ntap_pad;           // [HP_TILE + ntap_pad + 8]
+    const int c = blockIdx.y;
+    const int64_t i0 = (int64_t)blockIdx.x * HP_TILE;
+    const float* xrow = X1 + (int64_t)c * ldx;
+    for (int e = threadIdx.x; e < ntap_pad; e += blockDim.x) tp[e] = (e < ntap) ? taps[e] : 0.f;
+    const int nx = HP_TILE + ntap_pad + 8;
+    for (int p = threadIdx.x; p < nx; p += blockDim.x) {
+        int64_t g = i0 - L + p;
+        g %= N;
+        if (g < 0) g += N;
+        xs[p] = xrow[g];
+    }
+    __syncthreads();
+    float acc[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) acc[r] = 0.f;
+    const int o = threadIdx.x * 8;
+    float w[16];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) w[r] = xs[o + r];
+    for (int eb = 0; eb < ntap_pad; eb += 8) {
+#pragma unroll
+        for (int r = 0; r < 8; ++r) w[8 + r] = xs[o + eb + 8 + r];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const float t = tp[eb + u];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) acc[r] = fmaf(t, w[r + u], acc[r]);
+        }
+#pragma unroll
+        for (int r = 0; r < 8; ++r) w[r] = w[8 + r];
+    }
+    float* yrow = Xh + (int64_t)c * ldx;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const int64_t i = i0 + o + r;
+        if (i < N) yrow[i] = acc[r];
+    }
+}
+
+cudaError_t launch_highpass(const float* X1, int64_t ldx, int32_t C, int64_t N, const float* taps, int32_t L,
+                            float* Xh, cudaStream_t s) {
+    const int ntap_pad = ((2 * L + 1) + 7) & ~7;
+    const size_t smem = sizeof(float) * ((size_t)ntap_pad + HP_TILE + ntap_pad + 8);
+    static bool attr_done = false;
+    if (!attr_done) {
+        cudaFuncSetAttribute(k_highpass, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        attr_done = true;
+    }
+    dim3 grid((unsigned)((N + HP_TILE - 1) / HP_TILE), (unsigned)C);
+    k_highpass<<<grid, HP_THREADS, smem, s>>>(X1, ldx, N, taps, L, Xh);
+    return cudaGetLastError();
+}
+
+}  // namespace lss

@@ -1,0 +1,809 @@
+// C ABI of the sorter (include/lss.h): construction, device memory, and the
+// per-batch orchestration of the kernels.
+//
+// Mirrors OnlineSpikesV2 (src/SpikeSorter/OnlineSpikesV2.cu): the constructor
+// path (initializeSorter / allocateMemory / initializeStaticMemory,
+// :321-352, :380-422, :470-608) becomes lss_create, which allocates every
+// device buffer once; runSpikeSorting's per-batch body (:738-792) becomes
+// lss_filter + lss_match / lss_sort_batch. Kilosort semantics are followed
+// where LiveSpikeSorter departs from them (round cap 100, strict threshold,
+// exact-equality peak test, division by nm, [C, N] residual indexing).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/lss.h"
+#include "lss_kernels.cuh"
+#include "npy.h"
+
+using namespace lss;
+
+namespace {
+
+thread_local std::string g_create_err;
+
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaError_t alloc(size_t count) {
+        n = count;
+        return cudaMalloc(reinterpret_cast<void**>(&p), std::max<size_t>(count, 1) * sizeof(T));
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+    }
+};
+
+int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+}  // namespace
+
+struct lss_handle {
+    lss_config cfg{};
+    std::string err;
+    int C = 0, Cbin = 0, T = 0, K = 0, nt = 0, nC = 0, NT = 0, N = 0;
+    int64_t ld = 0;
+    int hpL = -1;  // FIR half length; -1 = no highpass
+    int mp_grid = 0;
+    std::vector<float> h_hp;
+    lss_stats stats{};
+    bool prof = false;
+    cudaEvent_t ev[11] = {};
+    lss_stage_times times{};
+
+    void mark(int i, cudaStream_t s) {
+        if (prof) cudaEventRecord(ev[i], s);
+    }
+
+    DevBuf<int16_t> raw;
+    DevBuf<int32_t> chan_map;
+    DevBuf<long long> sums;
+    DevBuf<float> taps, Mw, Wrot, Mdrift, X1, Xh, X, B0, Up, B, nm, ctcP, wave, wpca, Ucc, Xres, tF;
+    DevBuf<int64_t> iCC, iU;
+    DevBuf<float> cfmax;
+    DevBuf<int32_t> imax, blk_cnt, blk_x, blk_y, sp_x, sp_y, sp_round, round_start, counters, status;
+    DevBuf<float> sp_amp;
+    DevBuf<unsigned long long> colkey;
+    DevBuf<unsigned int> bar;
+    DevBuf<int64_t> rec_time, rec_count;
+    DevBuf<int32_t> rec_tmpl;
+    DevBuf<float> rec_amp, rec_pc;
+
+    int fail(int code, const std::string& m) {
+        err = m;
+        return code;
+    }
+    int cuda_fail(cudaError_t e, const char* where) {
+        err = std::string(where) + ": " + cudaGetErrorString(e);
+        return LSS_ERR_CUDA;
+    }
+    ~lss_handle() {
+        int dev = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess && dev != cfg.device) cudaSetDevice(cfg.device);
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+        raw.release(); chan_map.release(); sums.release(); taps.release(); Mw.release(); Wrot.release(); Mdrift.release();
+        X1.release(); Xh.release(); X.release(); B0.release(); Up.release(); B.release();
+        nm.release(); ctcP.release(); wave.release(); wpca.release(); Ucc.release(); Xres.release();
+        tF.release(); iCC.release(); iU.release(); cfmax.release(); imax.release(); blk_cnt.release();
+        blk_x.release(); blk_y.release(); sp_x.release(); sp_y.release(); sp_round.release();
+        round_start.release(); counters.release(); status.release(); sp_amp.release(); colkey.release();
+        bar.release(); rec_time.release(); rec_count.release(); rec_tmpl.release(); rec_amp.release();
+        rec_pc.release();
+    }
+};
+
+#define CK(call)                                                   \
+    do {                                                           \
+        cudaError_t e_ = (call);                                   \
+        if (e_ != cudaSuccess) return h->cuda_fail(e_, #call);     \
+    } while (0)
+
+// Circular-correlation taps of the highpass for a batch of N samples: the
+// impulse response is zero-padded or centre-cropped to N exactly as
+// fft_highpass does (kilosort/preprocessing.py:138-154), fftshift moves its
+// centre to lag 0, and the lags beyond L are dropped, L being the smallest
+// half-width whose discarded tail holds at most 2^-30 of the L1 mass.
+static int make_taps(const std::vector<float>& h, int64_t N, std::vector<float>& taps, std::string& err) {
+    const int64_t ft = (int64_t)h.size();
+    std::vector<double> g(N, 0.0);
+    if (ft < N) {
+        const int64_t pad = (N - ft) / 2;
+        for (int64_t m = 0; m < ft; ++m) g[pad + m] = h[m];
+    } else if (ft > N) {
+        const int64_t crop = (ft - N) / 2;
+        for (int64_t m = 0; m < N; ++m) g[m] = h[crop + m];
+    } else {
+        for (int64_t m = 0; m < N; ++m) g[m] = h[m];
+    }
+    const int64_t c = N / 2;
+    const int64_t dlo = -c, dhi = N - 1 - c;
+    auto hc = [&](int64_t d) -> double { return (d < dlo || d > dhi) ? 0.0 : g[d + c]; };
+    double total = 0.0;
+    for (int64_t m = 0; m < N; ++m) total += std::fabs(g[m]);
+    const double tol = std::ldexp(total, -30);
+    int64_t Lmax = std::max(-dlo, dhi);
+    // tail mass beyond L, scanning inwards from the outermost lags
+    double tail = 0.0;
+    int64_t L = Lmax;
+    while (L > 0) {
+        const double add = std::fabs(hc(L)) + std::fabs(hc(-L));
+        if (tail + add > tol) break;
+        tail += add;
+        --L;
+    }
+    const int64_t LCAP = 4096;
+    if (L > LCAP) {
+        err = "highpass impulse response does not decay within 4096 taps of its centre";
+        return -1;
+    }
+    taps.assign(2 * L + 1, 0.f);
+    for (int64_t d = -L; d <= L; ++d) {
+        // with an even N the lag +N/2 aliases -N/2; keep a single copy
+        if ((N % 2 == 0) && d == N / 2 && L >= N / 2) continue;
+        taps[d + L] = (float)hc(d);
+    }
+    return (int)L;
+}
+
+// Whitening with drift: Mw = M @ Wrot on the device (FP32, like the
+// reference's (M @ self.whiten_mat), kilosort/io.py:786), or Wrot when M is NULL.
+static int set_mixing(lss_handle* h, const float* M) {
+    const int C = h->C;
+    if (!M) {
+        CK(cudaMemcpy(h->Mw.p, h->Wrot.p, (size_t)C * C * sizeof(float), cudaMemcpyDeviceToDevice));
+        return LSS_OK;
+    }
+    CK(cudaMemcpy(h->Mdrift.p, M, (size_t)C * C * sizeof(float), cudaMemcpyHostToDevice));
+    CK(launch_sgemm(h->Mdrift.p, C, h->Wrot.p, C, h->Mw.p, C, C, C, C, 0));
+    h->stats.launches += 1;
+    return LSS_OK;
+}
+
+static int validate(const lss_config* c, std::string& err) {
+    if (!c) { err = "null config"; return LSS_ERR_ARG; }
+    if (c->n_chan <= 0 || c->n_templates <= 0 || c->n_pcs <= 0 || c->nt <= 0 || c->batch_size <= 0) {
+        err = "n_chan, n_templates, n_pcs, nt and batch_size must be positive";
+        return LSS_ERR_ARG;
+    }
+    if (c->n_pcs > 8) { err = "n_pcs > 8 is not supported"; return LSS_ERR_ARG; }
+    if (c->nt % 2 == 0) { err = "nt must be odd (conv1d with padding nt//2 keeps N columns only then)"; return LSS_ERR_ARG; }
+    if (c->nt > 255) { err = "nt > 255 is not supported"; return LSS_ERR_ARG; }
+    if (c->n_chan_bin < c->n_chan) { err = "n_chan_bin < n_chan"; return LSS_ERR_ARG; }
+    if (c->n_nearest < 0 || c->n_nearest > c->n_chan) { err = "n_nearest out of range"; return LSS_ERR_ARG; }
+    if (c->n_nearest * c->n_pcs > 1024) { err = "n_nearest * n_pcs > 1024"; return LSS_ERR_ARG; }
+    if (c->max_rounds <= 0 || c->max_rounds > 1000) { err = "max_rounds must be in 1..1000"; return LSS_ERR_ARG; }
+    if (c->max_spikes <= 0) { err = "max_spikes must be positive"; return LSS_ERR_ARG; }
+    if (c->precision != LSS_PREC_FP32 && c->precision != LSS_PREC_BF16_RECHECK) {
+        err = "unknown precision";
+        return LSS_ERR_ARG;
+    }
+    if (c->n_chan > 1024) { err = "n_chan > 1024 is not supported"; return LSS_ERR_ARG; }
+    if (!(c->th_learned > 0.f) || !std::isfinite(c->th_learned)) {
+        err = "th_learned must be positive and finite";
+        return LSS_ERR_ARG;
+    }
+    if (c->batch_size > (1 << 26)) { err = "batch_size too large"; return LSS_ERR_ARG; }
+    return LSS_OK;
+}
+
+extern "C" {
+
+int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
+    if (!out) { g_create_err = "null output pointer"; return LSS_ERR_ARG; }
+    *out = nullptr;
+    int rc = validate(cfg, g_create_err);
+    if (rc) return rc;
+    if (!t || !t->wall3 || !t->wpca || !t->ctc || !t->whitening) {
+        g_create_err = "wall3, wpca, ctc and whitening are required";
+        return LSS_ERR_ARG;
+    }
+    if (cfg->n_nearest > 0 && (!t->iCC || !t->iU || !t->Ucc)) {
+        g_create_err = "iCC, iU and Ucc are required when n_nearest > 0";
+        return LSS_ERR_ARG;
+    }
+    if (cfg->hp_len > 0 && !t->hp_filter) { g_create_err = "hp_len > 0 but hp_filter is NULL"; return LSS_ERR_ARG; }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        g_create_err = "no CUDA device available";
+        return LSS_ERR_CUDA;
+    }
+    if (cfg->device < 0 || cfg->device >= ndev) { g_create_err = "device ordinal out of range"; return LSS_ERR_ARG; }
+    cudaError_t ce = cudaSetDevice(cfg->device);
+    if (ce != cudaSuccess) { g_create_err = cudaGetErrorString(ce); return LSS_ERR_CUDA; }
+
+    std::unique_ptr<lss_handle> hp(new lss_handle());
+    lss_handle* h = hp.get();
+    h->cfg = *cfg;
+    h->C = cfg->n_chan; h->Cbin = cfg->n_chan_bin; h->T = cfg->n_templates; h->K = cfg->n_pcs;
+    h->nt = cfg->nt; h->nC = cfg->n_nearest; h->NT = cfg->batch_size;
+    h->N = h->NT + 2 * h->nt;
+    h->ld = round_up(h->N, 4);
+    const int C = h->C, T = h->T, K = h->K, nt = h->nt, nC = h->nC;
+    const int64_t ld = h->ld, L2 = 2 * nt + 1;
+
+    if (t->chan_map) {
+        for (int c = 0; c < C; ++c)
+            if (t->chan_map[c] < 0 || t->chan_map[c] >= h->Cbin) {
+                g_create_err = "chan_map entry out of range";
+                return LSS_ERR_ARG;
+            }
+    }
+    // template energies nm[t] = sum over (k, c) of U^2 (template_matching.py:141),
+    // the exact sum of the FP32 squares rounded once to FP32
+    std::vector<float> nmv(T);
+    for (int i = 0; i < T; ++i) {
+        if (t->nm) { nmv[i] = t->nm[i]; }
+        else {
+            double acc = 0.0;
+            for (int64_t e = 0; e < (int64_t)K * C; ++e) {
+                const float u = t->wall3[(int64_t)i * K * C + e];
+                acc += (double)(u * u);
+            }
+            nmv[i] = (float)acc;
+        }
+        if (!(nmv[i] > 0.f) || !std::isfinite(nmv[i])) {
+            g_create_err = "template " + std::to_string(i) + " has zero or non-finite energy";
+            return LSS_ERR_ARG;
+        }
+    }
+    if (t->iU) {
+        for (int i = 0; i < T; ++i)
+            if (t->iU[i] < 0 || t->iU[i] >= C) { g_create_err = "iU entry out of range"; return LSS_ERR_ARG; }
+    }
+    if (t->iCC && nC > 0) {
+        for (int64_t e = 0; e < (int64_t)nC * C; ++e)
+            if (t->iCC[e] < 0 || t->iCC[e] >= C) { g_create_err = "iCC entry out of range"; return LSS_ERR_ARG; }
+    }
+    // U_p[t, c*K + k] = U[t, k, c]; ctcP[j, i, l] = ctc[i, j, l];
+    // wave[t, c, m] = sum_k U[t, k, c] * wPCA[k, m] (run_online_spikes.py:539)
+    std::vector<float> up((size_t)T * C * K);
+    for (int i = 0; i < T; ++i)
+        for (int k = 0; k < K; ++k)
+            for (int c = 0; c < C; ++c)
+                up[((size_t)i * C + c) * K + k] = t->wall3[((size_t)i * K + k) * C + c];
+    std::vector<float> wave((size_t)T * C * nt);
+    for (int i = 0; i < T; ++i)
+        for (int c = 0; c < C; ++c)
+            for (int m = 0; m < nt; ++m) {
+                double acc = 0.0;
+                for (int k = 0; k < K; ++k)
+                    acc += (double)t->wall3[((size_t)i * K + k) * C + c] * (double)t->wpca[(size_t)k * nt + m];
+                wave[((size_t)i * C + c) * nt + m] = (float)acc;
+            }
+    if (cfg->hp_len > 0) {
+        h->h_hp.assign(t->hp_filter, t->hp_filter + cfg->hp_len);
+    }
+    std::vector<float> taps;
+    if (!h->h_hp.empty()) {
+        h->hpL = make_taps(h->h_hp, h->N, taps, g_create_err);
+        if (h->hpL < 0) return LSS_ERR_ARG;
+    }
+
+    h->mp_grid = mp_max_grid(cfg->device);
+    const int64_t cap = cfg->max_spikes;
+#define ALLOC(buf, cnt)                                                                    \
+    do {                                                                                   \
+        cudaError_t e_ = h->buf.alloc(cnt);                                                \
+        if (e_ != cudaSuccess) {                                                           \
+            g_create_err = std::string("cudaMalloc " #buf ": ") + cudaGetErrorString(e_);  \
+            return LSS_ERR_CUDA;                                                           \
+        }                                                                                  \
+    } while (0)
+    ALLOC(raw, (size_t)h->N * h->Cbin);
+    ALLOC(chan_map, C);
+    ALLOC(sums, C);
+    ALLOC(taps, std::max<size_t>(taps.size(), 1));
+    ALLOC(Mw, (size_t)C * C);
+    ALLOC(Wrot, (size_t)C * C);
+    ALLOC(Mdrift, (size_t)C * C);
+    ALLOC(X1, (size_t)C * ld);
+    ALLOC(Xh, (size_t)C * ld);
+    ALLOC(X, (size_t)C * ld);
+    ALLOC(B0, (size_t)C * K * ld);
+    ALLOC(Up, (size_t)T * C * K);
+    ALLOC(B, (size_t)T * ld);
+    ALLOC(nm, T);
+    ALLOC(ctcP, (size_t)T * T * L2);
+    ALLOC(wave, (size_t)T * C * nt);
+    ALLOC(wpca, (size_t)K * nt);
+    ALLOC(Ucc, (size_t)std::max(nC, 1) * T * K);
+    ALLOC(iCC, (size_t)std::max(nC, 1) * C);
+    ALLOC(iU, T);
+    ALLOC(Xres, (size_t)C * ld);
+    ALLOC(tF, (size_t)cap * std::max(nC * K, 1));
+    ALLOC(cfmax, ld);
+    ALLOC(imax, ld);
+    ALLOC(colkey, ld);
+    ALLOC(blk_cnt, 4096);
+    ALLOC(blk_x, ld);
+    ALLOC(blk_y, ld);
+    ALLOC(sp_x, cap);
+    ALLOC(sp_y, cap);
+    ALLOC(sp_amp, cap);
+    ALLOC(sp_round, cap);
+    ALLOC(round_start, cfg->max_rounds + 2);
+    ALLOC(counters, 4);
+    ALLOC(status, 1);
+    ALLOC(bar, 2);
+    ALLOC(rec_time, cap);
+    ALLOC(rec_tmpl, cap);
+    ALLOC(rec_amp, cap);
+    ALLOC(rec_pc, (size_t)cap * std::max(nC * K, 1));
+    ALLOC(rec_count, 1);
+#undef ALLOC
+
+    // ctc[i, j, l] -> ctcP[j, i, l], streamed through a host staging row
+    {
+        std::vector<float> row((size_t)T * L2);
+        for (int j = 0; j < T; ++j) {
+            for (int i = 0; i < T; ++i)
+                std::memcpy(&row[(size_t)i * L2], t->ctc + ((size_t)i * T + j) * L2, L2 * sizeof(float));
+            CK(cudaMemcpy(h->ctcP.p + (size_t)j * T * L2, row.data(), row.size() * sizeof(float),
+                          cudaMemcpyHostToDevice));
+        }
+    }
+    std::vector<int32_t> cmap(C);
+    for (int c = 0; c < C; ++c) cmap[c] = t->chan_map ? t->chan_map[c] : c;
+    CK(cudaMemcpy(h->chan_map.p, cmap.data(), C * sizeof(int32_t), cudaMemcpyHostToDevice));
+    if (!taps.empty()) CK(cudaMemcpy(h->taps.p, taps.data(), taps.size() * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->Up.p, up.data(), up.size() * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->nm.p, nmv.data(), T * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->wave.p, wave.data(), wave.size() * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->wpca.p, t->wpca, (size_t)K * nt * sizeof(float), cudaMemcpyHostToDevice));
+    if (nC > 0) {
+        CK(cudaMemcpy(h->Ucc.p, t->Ucc, (size_t)nC * T * K * sizeof(float), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h->iCC.p, t->iCC, (size_t)nC * C * sizeof(int64_t), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h->iU.p, t->iU, (size_t)T * sizeof(int64_t), cudaMemcpyHostToDevice));
+    }
+    CK(cudaMemset(h->colkey.p, 0, ld * sizeof(unsigned long long)));
+    CK(cudaMemcpy(h->Wrot.p, t->whitening, (size_t)C * C * sizeof(float), cudaMemcpyHostToDevice));
+    rc = set_mixing(h, t->drift);
+    if (rc) { g_create_err = h->err; return rc; }
+    CK(cudaDeviceSynchronize());
+    *out = hp.release();
+    return LSS_OK;
+}
+
+void lss_destroy(lss_handle* h) { delete h; }
+
+const char* lss_last_error(const lss_handle* h) { return h ? h->err.c_str() : g_create_err.c_str(); }
+
+int lss_get_config(const lss_handle* h, lss_config* out) {
+    if (!h || !out) return LSS_ERR_ARG;
+    *out = h->cfg;
+    return LSS_OK;
+}
+
+int lss_get_stats(const lss_handle* h, lss_stats* out) {
+    if (!h || !out) return LSS_ERR_ARG;
+    *out = h->stats;
+    return LSS_OK;
+}
+
+int lss_set_drift(lss_handle* h, const float* M) {
+    if (!h) return LSS_ERR_ARG;
+    CK(cudaSetDevice(h->cfg.device));
+    return set_mixing(h, M);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- stages
+static int run_filter(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ibatch, int64_t n_batches,
+                      int32_t raw_on_device, float* Xout, cudaStream_t s) {
+    if (!raw || n_rows <= 0) return h->fail(LSS_ERR_ARG, "empty raw batch");
+    if (ibatch < 0 || n_batches <= 0 || ibatch >= n_batches) return h->fail(LSS_ERR_ARG, "ibatch out of range");
+    const int64_t N = h->N;
+    IngestMap map{};
+    if (ibatch == 0) {
+        map.lead = h->nt;
+        map.nsamp = std::min<int64_t>(n_rows, h->NT + h->nt);
+        map.zero_tail = 1;
+    } else if (ibatch == n_batches - 1) {
+        map.lead = 0;
+        map.nsamp = std::min<int64_t>(n_rows, N);
+        map.zero_tail = 0;
+    } else {
+        if (n_rows < N)
+            return h->fail(LSS_ERR_SHAPE, "a middle batch needs NT + 2*nt rows (" + std::to_string(N) + ")");
+        map.lead = 0;
+        map.nsamp = N;
+        map.zero_tail = 0;
+    }
+    const int16_t* src = raw;
+    h->mark(0, s);
+    if (!raw_on_device) {
+        CK(cudaMemcpyAsync(h->raw.p, raw, (size_t)map.nsamp * h->Cbin * sizeof(int16_t), cudaMemcpyHostToDevice, s));
+        src = h->raw.p;
+    }
+    h->mark(1, s);
+    const float sign = h->cfg.invert_sign ? -1.f : 1.f;
+    CK(launch_chan_sums(src, h->Cbin, h->chan_map.p, h->C, N, map, h->sums.p, s));
+    CK(launch_car(src, h->Cbin, h->chan_map.p, h->C, N, map, sign, h->sums.p, h->cfg.do_car, h->X1.p, h->ld, s));
+    h->stats.launches += 2;
+    h->mark(2, s);
+    const float* pre = h->X1.p;
+    if (h->hpL >= 0) {
+        CK(launch_highpass(h->X1.p, h->ld, h->C, N, h->taps.p, h->hpL, h->Xh.p, s));
+        h->stats.launches += 1;
+        pre = h->Xh.p;
+    }
+    h->mark(3, s);
+    CK(launch_sgemm(h->Mw.p, h->C, pre, h->ld, Xout, h->ld, h->C, (int)N, h->C, s));
+    h->stats.launches += 1;
+    h->mark(4, s);
+    return LSS_OK;
+}
+
+static int run_scores(lss_handle* h, const float* X, int64_t ldx, int64_t N, float* B, cudaStream_t s) {
+    CK(launch_pca_proj(X, ldx, h->C, N, h->wpca.p, h->K, h->nt, h->B0.p, h->ld, s));
+    h->mark(5, s);
+    CK(launch_sgemm(h->Up.p, (int64_t)h->C * h->K, h->B0.p, h->ld, B, h->ld, h->T, (int)N, h->C * h->K, s));
+    h->stats.launches += 2;
+    h->mark(6, s);
+    return LSS_OK;
+}
+
+// Runs the rounds on h->B (already holding the score field); returns spikes.
+static int run_mp(lss_handle* h, int64_t N, int32_t* n_out, int32_t* rounds_out, cudaStream_t s) {
+    if (N <= 2 * h->nt) return h->fail(LSS_ERR_ARG, "batch shorter than 2*nt + 1 samples");
+    MPArgs a{};
+    a.B = h->B.p;
+    a.ldb = h->ld;
+    a.T = h->T;
+    a.N = (int)N;
+    a.nt = h->nt;
+    a.th2 = h->cfg.th_learned * h->cfg.th_learned;
+    a.nm = h->nm.p;
+    a.ctcP = h->ctcP.p;
+    a.cfmax = h->cfmax.p;
+    a.imax = h->imax.p;
+    a.colkey = h->colkey.p;
+    a.blk_cnt = h->blk_cnt.p;
+    a.blk_x = h->blk_x.p;
+    a.blk_y = h->blk_y.p;
+    a.sp_x = h->sp_x.p;
+    a.sp_y = h->sp_y.p;
+    a.sp_amp = h->sp_amp.p;
+    a.sp_round = h->sp_round.p;
+    a.round_start = h->round_start.p;
+    a.capacity = h->cfg.max_spikes;
+    a.max_rounds = h->cfg.max_rounds;
+    a.counters = h->counters.p;
+    a.status = h->status.p;
+    a.bar = h->bar.p;
+    const int G = h->mp_grid;
+    a.cols_per_blk = (int)((N + G - 1) / G);
+    a.rows_per_item = 64;
+    a.init_cols = 1;
+    CK(cudaMemsetAsync(h->status.p, 0, sizeof(int32_t), s));
+    CK(cudaMemsetAsync(h->counters.p, 0, 4 * sizeof(int32_t), s));
+    CK(cudaMemsetAsync(h->colkey.p, 0, h->ld * sizeof(unsigned long long), s));
+    CK(launch_mp(a, G, s));
+    h->stats.launches += 1;
+    int32_t hc[4], st = 0;
+    CK(cudaMemcpyAsync(hc, h->counters.p, sizeof(hc), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&st, h->status.p, sizeof(st), cudaMemcpyDeviceToHost, s));
+    h->mark(7, s);
+    CK(cudaStreamSynchronize(s));
+    if (st & STATUS_TIMEOUT) return h->fail(LSS_ERR_TIMEOUT, "matching pursuit grid barrier timed out");
+    if (st & STATUS_LIST) return h->fail(LSS_ERR_CAPACITY, "more than 32 peaks inside one 2*nt window");
+    if (st & STATUS_CAPACITY)
+        return h->fail(LSS_ERR_CAPACITY, "more than max_spikes spikes in one batch");
+    *n_out = hc[0];
+    *rounds_out = hc[1];
+    h->stats.rounds = hc[1];
+    h->stats.spikes = hc[0];
+    return LSS_OK;
+}
+
+static int run_xres(lss_handle* h, const float* X, int64_t ldx, int64_t N, int rounds, float* Xres,
+                    int64_t ldr, cudaStream_t s) {
+    (void)ldr;
+    CK(launch_xres(X, ldx, h->C, (int)N, h->nt, h->wave.p, h->sp_x.p, h->sp_y.p, h->sp_amp.p,
+                   h->round_start.p, h->counters.p, rounds, Xres, h->status.p, s));
+    h->stats.launches += 1;
+    return LSS_OK;
+}
+
+extern "C" {
+
+int lss_filter(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ibatch, int64_t n_batches,
+               int32_t raw_on_device, float* X_dev, void* stream) {
+    if (!h || !X_dev) return LSS_ERR_ARG;
+    CK(cudaSetDevice(h->cfg.device));
+    cudaStream_t s = (cudaStream_t)stream;
+    // the GEMM writes rows of stride ld; the caller's buffer has stride N
+    int rc = run_filter(h, raw, n_rows, ibatch, n_batches, raw_on_device, h->X.p, s);
+    if (rc) return rc;
+    CK(cudaMemcpy2DAsync(X_dev, h->N * sizeof(float), h->X.p, h->ld * sizeof(float), h->N * sizeof(float), h->C,
+                         cudaMemcpyDeviceToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    return LSS_OK;
+}
+
+int lss_scores(lss_handle* h, const float* X_dev, int64_t N, float* B_dev, void* stream) {
+    if (!h || !X_dev || !B_dev) return LSS_ERR_ARG;
+    if (N <= 0 || N > h->N) return h->fail(LSS_ERR_ARG, "N out of range");
+    CK(cudaSetDevice(h->cfg.device));
+    cudaStream_t s = (cudaStream_t)stream;
+    CK(cudaMemcpy2DAsync(h->X.p, h->ld * sizeof(float), X_dev, N * sizeof(float), N * sizeof(float), h->C,
+                         cudaMemcpyDeviceToDevice, s));
+    int rc = run_scores(h, h->X.p, h->ld, N, h->B.p, s);
+    if (rc) return rc;
+    CK(cudaMemcpy2DAsync(B_dev, N * sizeof(float), h->B.p, h->ld * sizeof(float), N * sizeof(float), h->T,
+                         cudaMemcpyDeviceToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    return LSS_OK;
+}
+
+static int match_common(lss_handle* h, int64_t N, const float* Xsrc, int64_t* st_dev, float* amps_dev,
+                        float* xres_dev, int64_t capacity, int64_t* n_spikes, cudaStream_t s) {
+    int32_t n = 0, rounds = 0;
+    int rc = run_mp(h, N, &n, &rounds, s);
+    if (rc) return rc;
+    if (n_spikes) *n_spikes = n;
+    if (n > capacity) return h->fail(LSS_ERR_CAPACITY, "output capacity smaller than the spike count");
+    if (st_dev && amps_dev && n > 0) {
+        CK(launch_st_out(h->sp_x.p, h->sp_y.p, h->sp_amp.p, n, st_dev, amps_dev, s));
+        h->stats.launches += 1;
+    }
+    if (xres_dev && Xsrc) {
+        rc = run_xres(h, Xsrc, h->ld, N, rounds, h->Xres.p, h->ld, s);
+        if (rc) return rc;
+        CK(cudaMemcpy2DAsync(xres_dev, N * sizeof(float), h->Xres.p, h->ld * sizeof(float), N * sizeof(float), h->C,
+                             cudaMemcpyDeviceToDevice, s));
+    }
+    int32_t st = 0;
+    CK(cudaMemcpyAsync(&st, h->status.p, sizeof(st), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (st & STATUS_LIST) return h->fail(LSS_ERR_CAPACITY, "residual tile touched by more than 1024 spikes");
+    return LSS_OK;
+}
+
+int lss_match(lss_handle* h, const float* X_dev, int64_t N, int64_t* st_dev, float* amps_dev, float* xres_dev,
+              int64_t capacity, int64_t* n_spikes, void* stream) {
+    if (!h || !X_dev) return LSS_ERR_ARG;
+    if (N <= 0 || N > h->N) return h->fail(LSS_ERR_ARG, "N out of range (1..NT+2nt)");
+    CK(cudaSetDevice(h->cfg.device));
+    cudaStream_t s = (cudaStream_t)stream;
+    CK(cudaMemcpy2DAsync(h->X.p, h->ld * sizeof(float), X_dev, N * sizeof(float), N * sizeof(float), h->C,
+                         cudaMemcpyDeviceToDevice, s));
+    int rc = run_scores(h, h->X.p, h->ld, N, h->B.p, s);
+    if (rc) return rc;
+    return match_common(h, N, h->X.p, st_dev, amps_dev, xres_dev, capacity, n_spikes, s);
+}
+
+int lss_match_scores(lss_handle* h, const float* B_dev, int64_t N, int64_t* st_dev, float* amps_dev,
+                     int64_t capacity, int64_t* n_spikes, void* stream) {
+    if (!h || !B_dev) return LSS_ERR_ARG;
+    if (N <= 0 || N > h->N) return h->fail(LSS_ERR_ARG, "N out of range (1..NT+2nt)");
+    CK(cudaSetDevice(h->cfg.device));
+    cudaStream_t s = (cudaStream_t)stream;
+    CK(cudaMemcpy2DAsync(h->B.p, h->ld * sizeof(float), B_dev, N * sizeof(float), N * sizeof(float), h->T,
+                         cudaMemcpyDeviceToDevice, s));
+    return match_common(h, N, nullptr, st_dev, amps_dev, nullptr, capacity, n_spikes, s);
+}
+
+int lss_sort_batch(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ibatch, int64_t n_batches,
+                   int32_t raw_on_device, lss_records* out, void* stream) {
+    if (!h || !out) return LSS_ERR_ARG;
+    if (!out->time || !out->template_id || !out->amplitude) return h->fail(LSS_ERR_ARG, "null record arrays");
+    CK(cudaSetDevice(h->cfg.device));
+    cudaStream_t s = (cudaStream_t)stream;
+    int rc = run_filter(h, raw, n_rows, ibatch, n_batches, raw_on_device, h->X.p, s);
+    if (rc) return rc;
+    rc = run_scores(h, h->X.p, h->ld, h->N, h->B.p, s);
+    if (rc) return rc;
+    int32_t n = 0, rounds = 0;
+    rc = run_mp(h, h->N, &n, &rounds, s);
+    if (rc) return rc;
+    const int feat = h->nC * h->K;
+    const bool want_pc = out->pc != nullptr && feat > 0;
+    if (want_pc && n > 0) {
+        rc = run_xres(h, h->X.p, h->ld, h->N, rounds, h->Xres.p, h->ld, s);
+        if (rc) return rc;
+        h->mark(8, s);
+        CK(launch_pc_features(h->Xres.p, h->ld, h->nt, h->K, h->nC, h->C, h->T, h->wpca.p, h->iCC.p, h->iU.p,
+                              h->Ucc.p, h->sp_x.p, h->sp_y.p, h->sp_amp.p, h->counters.p, n, h->tF.p, s));
+        h->stats.launches += 1;
+    } else {
+        h->mark(8, s);
+    }
+    h->mark(9, s);
+    const int64_t cap = out->capacity;
+    int64_t* d_time = out->on_device ? out->time : h->rec_time.p;
+    int32_t* d_tmpl = out->on_device ? out->template_id : h->rec_tmpl.p;
+    float* d_amp = out->on_device ? out->amplitude : h->rec_amp.p;
+    float* d_pc = want_pc ? (out->on_device ? out->pc : h->rec_pc.p) : nullptr;
+    const int64_t dcap = out->on_device ? cap : std::min<int64_t>(cap, h->cfg.max_spikes);
+    CK(launch_records(h->sp_x.p, h->sp_y.p, h->sp_amp.p, want_pc ? h->tF.p : nullptr, h->counters.p, n, feat,
+                      ibatch, h->nt, h->NT, h->cfg.nt0min, d_time, d_tmpl, d_amp, d_pc, dcap, h->rec_count.p, s));
+    h->stats.launches += 1;
+    int64_t count = 0;
+    int32_t st = 0;
+    CK(cudaMemcpyAsync(&count, h->rec_count.p, sizeof(count), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&st, h->status.p, sizeof(st), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (st & STATUS_LIST) return h->fail(LSS_ERR_CAPACITY, "residual tile touched by more than 1024 spikes");
+    out->count = count;
+    if (count > cap) return h->fail(LSS_ERR_CAPACITY, "record capacity smaller than the spike count");
+    if (!out->on_device && count > 0) {
+        CK(cudaMemcpyAsync(out->time, d_time, count * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(out->template_id, d_tmpl, count * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(out->amplitude, d_amp, count * sizeof(float), cudaMemcpyDeviceToHost, s));
+        if (want_pc)
+            CK(cudaMemcpyAsync(out->pc, d_pc, count * feat * sizeof(float), cudaMemcpyDeviceToHost, s));
+    }
+    h->mark(10, s);
+    CK(cudaStreamSynchronize(s));
+    if (h->prof) {
+        float* f = &h->times.h2d_ms;
+        for (int i = 0; i < 10; ++i) cudaEventElapsedTime(&f[i], h->ev[i], h->ev[i + 1]);
+        cudaEventElapsedTime(&h->times.total_ms, h->ev[0], h->ev[10]);
+    }
+    return LSS_OK;
+}
+
+int lss_set_profiling(lss_handle* h, int32_t on) {
+    if (!h) return LSS_ERR_ARG;
+    CK(cudaSetDevice(h->cfg.device));
+    if (on && !h->ev[0])
+        for (auto& e : h->ev) CK(cudaEventCreate(&e));
+    h->prof = on != 0;
+    return LSS_OK;
+}
+
+int lss_get_stage_times(const lss_handle* h, lss_stage_times* out) {
+    if (!h || !out) return LSS_ERR_ARG;
+    if (!h->prof) return LSS_ERR_STATE;
+    *out = h->times;
+    return LSS_OK;
+}
+
+// ---------------------------------------------------------------- directory
+static bool read_misc(const std::string& path, std::map<std::string, std::string>& kv) {
+    std::ifstream in(path);
+    if (!in) return false;
+    std::string line;
+    while (std::getline(in, line)) {
+        const size_t p = line.find(':');
+        if (p == std::string::npos) continue;
+        std::string v = line.substr(p + 1);
+        while (!v.empty() && (v.back() == '\r' || v.back() == ' ')) v.pop_back();
+        kv[line.substr(0, p)] = v;
+    }
+    return true;
+}
+
+int lss_create_from_dir(const char* dir, const lss_config* overrides, lss_handle** out) {
+    if (!dir || !out) { g_create_err = "null argument"; return LSS_ERR_ARG; }
+    std::string d(dir);
+    if (!d.empty() && d.back() != '/') d += '/';
+    std::string err;
+    auto load = [&](const char* name, NpyArray& a) -> bool {
+        if (!npy_load(d + name, a, err)) { g_create_err = err; return false; }
+        return true;
+    };
+    NpyArray aW, aP, aC, aWr, aDr, aHp, aICC, aIU, aUcc, aMap;
+    if (!load("Wall3.npy", aW) || !load("wPCA.npy", aP) || !load("ctc.npy", aC)) return LSS_ERR_IO;
+    if (!npy_load(d + "whitening_mat.npy", aWr, err) && !npy_load(d + "whiteningMat.npy", aWr, err)) {
+        g_create_err = "whitening_mat.npy / whiteningMat.npy: " + err;
+        return LSS_ERR_IO;
+    }
+    const bool have_drift = npy_load(d + "drift_matrix.npy", aDr, err);
+    const bool have_hp = npy_load(d + "hp_filter.npy", aHp, err);
+    const bool have_ext = npy_load(d + "iCC.npy", aICC, err) && npy_load(d + "iU.npy", aIU, err) &&
+                          npy_load(d + "Ucc.npy", aUcc, err);
+    const bool have_map = npy_load(d + "channel_map.npy", aMap, err) || npy_load(d + "channelMap.npy", aMap, err);
+    if (aW.shape.size() != 3 || aP.shape.size() != 2 || aC.shape.size() != 3 || aWr.shape.size() != 2) {
+        g_create_err = "Wall3 [T,K,C], wPCA [K,nt], ctc [T,T,2nt+1], whitening [C,C] expected";
+        return LSS_ERR_SHAPE;
+    }
+    lss_config c{};
+    c.n_templates = (int32_t)aW.shape[0];
+    c.n_pcs = (int32_t)aW.shape[1];
+    c.n_chan = (int32_t)aW.shape[2];
+    c.nt = (int32_t)aP.shape[1];
+    c.n_chan_bin = c.n_chan;
+    c.batch_size = 60000;
+    c.nt0min = 20;
+    c.th_learned = 8.f;
+    c.max_rounds = 100;
+    c.max_spikes = 100000;
+    c.do_car = 1;
+    c.n_nearest = have_ext ? (int32_t)aICC.shape[0] : 0;
+    std::map<std::string, std::string> kv;
+    if (read_misc(d + "misc.txt", kv)) {
+        if (kv.count("nt0min")) c.nt0min = std::stoi(kv["nt0min"]);
+        if (kv.count("Th_learned")) c.th_learned = std::stof(kv["Th_learned"]);
+        if (kv.count("numNearestChans") && have_ext && std::stoi(kv["numNearestChans"]) != c.n_nearest) {
+            g_create_err = "misc.txt numNearestChans disagrees with iCC.npy";
+            return LSS_ERR_SHAPE;
+        }
+    }
+    if (overrides) {
+        if (overrides->n_chan_bin) c.n_chan_bin = overrides->n_chan_bin;
+        if (overrides->batch_size) c.batch_size = overrides->batch_size;
+        if (overrides->nt0min) c.nt0min = overrides->nt0min;
+        if (overrides->th_learned != 0.f) c.th_learned = overrides->th_learned;
+        if (overrides->max_rounds) c.max_rounds = overrides->max_rounds;
+        if (overrides->max_spikes) c.max_spikes = overrides->max_spikes;
+        c.do_car = overrides->do_car;
+        c.invert_sign = overrides->invert_sign;
+        c.precision = overrides->precision;
+        c.device = overrides->device;
+    }
+    const int64_t T = c.n_templates, K = c.n_pcs, C = c.n_chan, nt = c.nt;
+    if (aP.shape[0] != K || aC.shape[0] != T || aC.shape[1] != T || aC.shape[2] != 2 * nt + 1 ||
+        aWr.shape[0] != C || aWr.shape[1] != C) {
+        g_create_err = "inconsistent shapes among Wall3, wPCA, ctc and whitening";
+        return LSS_ERR_SHAPE;
+    }
+    std::vector<float> W, P, Cc, Wr, Dr, Hp, Ucc;
+    std::vector<int64_t> iCC, iU, mp64;
+    if (!npy_as_f32(aW, W, err) || !npy_as_f32(aP, P, err) || !npy_as_f32(aC, Cc, err) || !npy_as_f32(aWr, Wr, err)) {
+        g_create_err = err;
+        return LSS_ERR_SHAPE;
+    }
+    if (have_drift) {
+        if (aDr.shape.size() != 2 || aDr.shape[0] != C || aDr.shape[1] != C) {
+            g_create_err = "drift_matrix.npy must be [C, C]";
+            return LSS_ERR_SHAPE;
+        }
+        if (!npy_as_f32(aDr, Dr, err)) { g_create_err = err; return LSS_ERR_SHAPE; }
+        // the file holds M.T (run_online_spikes.py:532); recover M
+        std::vector<float> M(Dr.size());
+        for (int64_t i = 0; i < C; ++i)
+            for (int64_t j = 0; j < C; ++j) M[i * C + j] = Dr[j * C + i];
+        Dr.swap(M);
+    }
+    if (have_hp) {
+        if (!npy_as_f32(aHp, Hp, err)) { g_create_err = err; return LSS_ERR_SHAPE; }
+        c.hp_len = (int32_t)Hp.size();
+    }
+    if (have_ext) {
+        if (!npy_as_i64(aICC, iCC, err) || !npy_as_i64(aIU, iU, err) || !npy_as_f32(aUcc, Ucc, err)) {
+            g_create_err = err;
+            return LSS_ERR_SHAPE;
+        }
+        if (aICC.shape.size() != 2 || aICC.shape[1] != C || (int64_t)iU.size() != T ||
+            (int64_t)Ucc.size() != (int64_t)c.n_nearest * T * K) {
+            g_create_err = "iCC [nC,C], iU [T], Ucc [nC,T,K] expected";
+            return LSS_ERR_SHAPE;
+        }
+    }
+    std::vector<int32_t> cmap;
+    if (have_map) {
+        if (!npy_as_i64(aMap, mp64, err)) { g_create_err = err; return LSS_ERR_SHAPE; }
+        if ((int64_t)mp64.size() != C) { g_create_err = "channel map must have C entries"; return LSS_ERR_SHAPE; }
+        cmap.assign(mp64.begin(), mp64.end());
+        for (auto v : cmap) c.n_chan_bin = std::max<int32_t>(c.n_chan_bin, v + 1);
+        if (overrides && overrides->n_chan_bin) c.n_chan_bin = overrides->n_chan_bin;
+    }
+    lss_tensors t{};
+    t.wall3 = W.data();
+    t.wpca = P.data();
+    t.ctc = Cc.data();
+    t.whitening = Wr.data();
+    t.drift = have_drift ? Dr.data() : nullptr;
+    t.hp_filter = have_hp ? Hp.data() : nullptr;
+    t.iCC = have_ext ? iCC.data() : nullptr;
+    t.iU = have_ext ? iU.data() : nullptr;
+    t.Ucc = have_ext ? Ucc.data() : nullptr;
+    t.chan_map = have_map ? cmap.data() : nullptr;
+    return lss_create(&c, &t, out);
+}
+
+}  // extern "C"

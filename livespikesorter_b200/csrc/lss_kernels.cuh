@@ -1,0 +1,86 @@
+// Internal declarations shared by the kernel translation units and the host
+// orchestration (lss_api.cpp). Launchers return cudaError_t of the launch.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace lss {
+
+// Where column s of the padded batch X [C, N] comes from in the raw rows
+// (kilosort/io.py:584-637): row = clamp(s - lead, 0, nsamp-1); columns at or
+// past lead + nsamp are zero when zero_tail (batch 0) and replicate the last
+// row otherwise (last batch).
+struct IngestMap {
+    int64_t lead;
+    int64_t nsamp;
+    int32_t zero_tail;
+};
+
+// ---- ingest (ingest.cu) ----
+cudaError_t launch_chan_sums(const int16_t* raw, int32_t ld_raw, const int32_t* chan_map, int32_t C,
+                             int64_t N, IngestMap map, long long* sums, cudaStream_t s);
+cudaError_t launch_car(const int16_t* raw, int32_t ld_raw, const int32_t* chan_map, int32_t C, int64_t N,
+                       IngestMap map, float sign, const long long* sums, int do_car, float* X1,
+                       int64_t ldx, cudaStream_t s);
+cudaError_t launch_highpass(const float* X1, int64_t ldx, int32_t C, int64_t N, const float* taps, int32_t L,
+                            float* Xh, cudaStream_t s);
+
+// ---- dense FP32 GEMM (gemm_fp32.cu): C[M,N] = A[M,K] @ B[K,N], row-major ----
+cudaError_t launch_sgemm(const float* A, int64_t lda, const float* B, int64_t ldb, float* Cm, int64_t ldc,
+                         int M, int N, int K, cudaStream_t s);
+
+// ---- temporal basis projection (score.cu): B0[c*K + k, s] ----
+cudaError_t launch_pca_proj(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
+                            int32_t nt, float* B0, int64_t ldb0, cudaStream_t s);
+
+// ---- matching pursuit (mp.cu) ----
+struct MPArgs {
+    float* B;                 // [T, ldb] score field, updated in place
+    int64_t ldb;
+    int32_t T, N, nt;
+    float th2;                // Th * Th
+    const float* nm;          // [T]
+    const float* ctcP;        // [T(j), T(i), 2nt+1] = ctc.permute(1,0,2)
+    float* cfmax;             // [N]
+    int32_t* imax;            // [N]
+    unsigned long long* colkey;  // [N], zero outside a round's update
+    int32_t* blk_cnt;         // [G]
+    int32_t* blk_x;           // [N] per-CTA peak columns (CTA b at b*W)
+    int32_t* blk_y;           // [N]
+    int32_t* sp_x;            // [capacity]
+    int32_t* sp_y;
+    float* sp_amp;
+    int32_t* sp_round;
+    int32_t* round_start;     // [max_rounds + 1]
+    int32_t capacity;
+    int32_t max_rounds;
+    int32_t* counters;        // [0]=spikes [1]=rounds
+    int32_t* status;          // error bits (LSS_STATUS_*)
+    unsigned int* bar;        // [2] grid barrier count / generation
+    int32_t cols_per_blk;     // W
+    int32_t rows_per_item;    // TB
+    int32_t init_cols;        // 1: compute column maxima of B before round 0
+};
+enum : int32_t { STATUS_TIMEOUT = 1, STATUS_CAPACITY = 2, STATUS_LIST = 4 };
+cudaError_t launch_mp(MPArgs a, int grid, cudaStream_t s);
+int mp_max_grid(int device);
+
+// ---- residual and PC features (features.cu); n = spikes of the batch ----
+cudaError_t launch_xres(const float* X, int64_t ldx, int32_t C, int32_t N, int32_t nt, const float* wave,
+                        const int32_t* sp_x, const int32_t* sp_y, const float* sp_amp,
+                        const int32_t* round_start, const int32_t* counters, int32_t rounds,
+                        float* Xres, int32_t* status, cudaStream_t s);
+cudaError_t launch_pc_features(const float* Xres, int64_t ldx, int32_t nt, int32_t K, int32_t nC,
+                               int32_t C, int32_t T, const float* wpca, const int64_t* iCC,
+                               const int64_t* iU, const float* Ucc, const int32_t* sp_x,
+                               const int32_t* sp_y, const float* sp_amp, const int32_t* counters,
+                               int32_t n, float* tF, cudaStream_t s);
+cudaError_t launch_records(const int32_t* sp_x, const int32_t* sp_y, const float* sp_amp, const float* tF,
+                           const int32_t* counters, int32_t n, int32_t feat_len, int64_t ibatch, int32_t nt,
+                           int32_t NT, int32_t nt0min, int64_t* out_time, int32_t* out_tmpl,
+                           float* out_amp, float* out_pc, int64_t capacity, int64_t* out_count,
+                           cudaStream_t s);
+cudaError_t launch_st_out(const int32_t* sp_x, const int32_t* sp_y, const float* sp_amp, int32_t n,
+                          int64_t* st, float* amps, cudaStream_t s);
+
+}  // namespace lss

@@ -1,0 +1,237 @@
+"""Torch-facing host API over the C ABI.
+
+``Sorter`` owns one ``lss_handle`` (one probe stream). ``run_matching`` keeps
+the signature and return types of ``kilosort/template_matching.py:128-202`` so
+it can stand in for it.
+
+All compute happens in ``liblss_b200.so`` on the GPU; tensors only carry
+device memory and the current CUDA stream across the boundary.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import LssConfig, LssRecords, LssStageTimes, LssStats, LssTensors, STAGES, check
+
+
+def _f32(x) -> torch.Tensor:
+    if isinstance(x, np.ndarray):
+        x = torch.from_numpy(x)
+    return x.detach().to('cpu', torch.float32).contiguous()
+
+
+def _i64(x) -> torch.Tensor:
+    if isinstance(x, np.ndarray):
+        x = torch.from_numpy(x)
+    return x.detach().to('cpu', torch.int64).contiguous()
+
+
+def _ptr(t):
+    return None if t is None else t.data_ptr()
+
+
+def _stream(device) -> int | None:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+class Sorter:
+    """One sorter handle: templates, ctc, whitening, filters and all device
+    workspaces live on ``device`` for the handle's lifetime."""
+
+    def __init__(self, *, U, wPCA, ctc, Wrot, hp_filter=None, drift=None, iCC=None, iU=None, Ucc=None,
+                 chan_map=None, nm=None, NT: int = 60000, nt0min: int = 20, Th: float = 8.0,
+                 n_chan_bin: int | None = None, max_rounds: int = 100, max_spikes: int = 100000,
+                 do_CAR: bool = True, invert_sign: bool = False, precision: str = 'fp32', device: int = 0):
+        self._lib = _lib.load()
+        U = _f32(U)
+        T, K, C = U.shape
+        wPCA = _f32(wPCA)
+        nt = wPCA.shape[1]
+        self._keep = dict(U=U, wPCA=wPCA, ctc=_f32(ctc), Wrot=_f32(Wrot),
+                          hp=None if hp_filter is None else _f32(hp_filter),
+                          drift=None if drift is None else _f32(drift),
+                          iCC=None if iCC is None else _i64(iCC), iU=None if iU is None else _i64(iU),
+                          Ucc=None if Ucc is None else _f32(Ucc),
+                          cmap=None if chan_map is None else torch.as_tensor(np.asarray(chan_map), dtype=torch.int32).contiguous(),
+                          nm=None if nm is None else _f32(nm))
+        k = self._keep
+        nC = 0 if k['iCC'] is None else k['iCC'].shape[0]
+        cfg = LssConfig(n_chan=C, n_chan_bin=n_chan_bin or C, n_templates=T, n_pcs=K, nt=nt, n_nearest=nC,
+                        batch_size=NT, nt0min=nt0min, th_learned=float(Th), max_rounds=max_rounds,
+                        max_spikes=max_spikes, do_car=int(do_CAR), invert_sign=int(invert_sign),
+                        precision={'fp32': 0, 'bf16': 1}[precision], device=device,
+                        hp_len=0 if k['hp'] is None else k['hp'].numel())
+        tens = LssTensors(wall3=_ptr(k['U']), wpca=_ptr(k['wPCA']), ctc=_ptr(k['ctc']), whitening=_ptr(k['Wrot']),
+                          drift=_ptr(k['drift']), hp_filter=_ptr(k['hp']), iCC=_ptr(k['iCC']), iU=_ptr(k['iU']),
+                          Ucc=_ptr(k['Ucc']), chan_map=_ptr(k['cmap']), nm=_ptr(k['nm']))
+        h = __import__('ctypes').c_void_p()
+        check(self._lib.lss_create(cfg, tens, h))
+        self._h = h
+        self._init_dims(device)
+        del self._keep
+
+    @classmethod
+    def from_dir(cls, path: str, **overrides) -> 'Sorter':
+        """Build from an LSS input directory (the files
+        ``src/Python/run_online_spikes.py:548-576`` writes)."""
+        import ctypes
+        self = cls.__new__(cls)
+        self._lib = _lib.load()
+        ov = LssConfig(n_chan_bin=overrides.get('n_chan_bin', 0), batch_size=overrides.get('NT', 0),
+                       nt0min=overrides.get('nt0min', 0), th_learned=float(overrides.get('Th', 0.0)),
+                       max_rounds=overrides.get('max_rounds', 0), max_spikes=overrides.get('max_spikes', 0),
+                       do_car=int(overrides.get('do_CAR', True)), invert_sign=int(overrides.get('invert_sign', False)),
+                       precision={'fp32': 0, 'bf16': 1}[overrides.get('precision', 'fp32')],
+                       device=overrides.get('device', 0))
+        h = ctypes.c_void_p()
+        check(self._lib.lss_create_from_dir(str(path).encode(), ov, h))
+        self._h = h
+        self._init_dims(ov.device)
+        return self
+
+    @classmethod
+    def from_setup(cls, setup, **kw) -> 'Sorter':
+        """Build from a ``synth.SortSetup``."""
+        return cls(U=setup.U, wPCA=setup.wPCA, ctc=setup.ctc, Wrot=setup.Wrot, hp_filter=setup.hp_filter,
+                   iCC=setup.iCC, iU=setup.iU, Ucc=setup.Ucc, NT=setup.NT, nt0min=setup.nt0min, Th=setup.Th, **kw)
+
+    def _init_dims(self, device):
+        cfg = LssConfig()
+        check(self._lib.lss_get_config(self._h, cfg), self._h)
+        self.cfg = cfg
+        self.device = torch.device('cuda', device)
+        self.C, self.T, self.K, self.nt = cfg.n_chan, cfg.n_templates, cfg.n_pcs, cfg.nt
+        self.nC, self.NT = cfg.n_nearest, cfg.batch_size
+        self.N = self.NT + 2 * self.nt
+
+    def close(self):
+        if getattr(self, '_h', None):
+            self._lib.lss_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        check(rc, self._h)
+
+    # ------------------------------------------------------------- stages
+    def set_drift(self, M):
+        """Drift interpolation matrix for the following batches (None = identity)."""
+        Mt = None if M is None else _f32(M)
+        self._check(self._lib.lss_set_drift(self._h, _ptr(Mt)))
+
+    def filter(self, raw, ibatch: int, n_batches: int) -> torch.Tensor:
+        """Padded, filtered, whitened batch ``[C, NT + 2nt]`` (kilosort/io.py:584-637, 757-790)."""
+        raw_t, on_dev = self._raw(raw)
+        X = torch.empty((self.C, self.N), device=self.device, dtype=torch.float32)
+        self._check(self._lib.lss_filter(self._h, raw_t.data_ptr(), raw_t.shape[0], ibatch, n_batches, on_dev,
+                                         X.data_ptr(), _stream(self.device)))
+        return X
+
+    def _raw(self, raw):
+        if isinstance(raw, np.ndarray):
+            raw = torch.from_numpy(np.ascontiguousarray(raw))
+        if raw.dtype != torch.int16 or raw.dim() != 2:
+            raise ValueError('raw must be an int16 [n_rows, n_chan_bin] array')
+        raw = raw.contiguous()
+        if raw.shape[1] != self.cfg.n_chan_bin:
+            raise ValueError(f'raw has {raw.shape[1]} channels, expected {self.cfg.n_chan_bin}')
+        return raw, int(raw.is_cuda)
+
+    def scores(self, X: torch.Tensor) -> torch.Tensor:
+        X = X.to(self.device, torch.float32).contiguous()
+        B = torch.empty((self.T, X.shape[1]), device=self.device, dtype=torch.float32)
+        self._check(self._lib.lss_scores(self._h, X.data_ptr(), X.shape[1], B.data_ptr(), _stream(self.device)))
+        return B
+
+    def match(self, X: torch.Tensor, return_xres: bool = True, capacity: int | None = None):
+        """``run_matching`` on a filtered batch: ``(st int64 [n,2], amps f32 [n,1], Xres [C,N])``."""
+        import ctypes
+        X = X.to(self.device, torch.float32).contiguous()
+        N = X.shape[1]
+        cap = capacity or self.cfg.max_spikes
+        st = torch.empty((cap, 2), device=self.device, dtype=torch.int64)
+        amps = torch.empty((cap, 1), device=self.device, dtype=torch.float32)
+        xres = torch.empty_like(X) if return_xres else None
+        n = ctypes.c_int64(0)
+        self._check(self._lib.lss_match(self._h, X.data_ptr(), N, st.data_ptr(), amps.data_ptr(),
+                                        _ptr(xres), cap, ctypes.byref(n), _stream(self.device)))
+        return st[:n.value], amps[:n.value], xres
+
+    def match_scores(self, B: torch.Tensor, capacity: int | None = None):
+        """The rounds alone on a given score field ``B [T, N]``: ``(st, amps)``."""
+        import ctypes
+        B = B.to(self.device, torch.float32).contiguous()
+        cap = capacity or self.cfg.max_spikes
+        st = torch.empty((cap, 2), device=self.device, dtype=torch.int64)
+        amps = torch.empty((cap, 1), device=self.device, dtype=torch.float32)
+        n = ctypes.c_int64(0)
+        self._check(self._lib.lss_match_scores(self._h, B.data_ptr(), B.shape[1], st.data_ptr(), amps.data_ptr(),
+                                               cap, ctypes.byref(n), _stream(self.device)))
+        return st[:n.value], amps[:n.value]
+
+    def sort_batch(self, raw, ibatch: int, n_batches: int, with_pc: bool = True, on_device: bool = False,
+                   capacity: int | None = None) -> dict:
+        """One batch end to end: records ``time, template, amplitude, pc [n, nC, K]``."""
+        raw_t, raw_dev = self._raw(raw)
+        cap = capacity or self.cfg.max_spikes
+        dev = self.device if on_device else 'cpu'
+        pin = (not on_device)
+        time = torch.empty(cap, dtype=torch.int64, device=dev, pin_memory=pin)
+        tmpl = torch.empty(cap, dtype=torch.int32, device=dev, pin_memory=pin)
+        amp = torch.empty(cap, dtype=torch.float32, device=dev, pin_memory=pin)
+        pc = torch.empty((cap, self.nC, self.K), dtype=torch.float32, device=dev, pin_memory=pin) \
+            if (with_pc and self.nC > 0) else None
+        rec = LssRecords(time=time.data_ptr(), template_id=tmpl.data_ptr(), amplitude=amp.data_ptr(),
+                         pc=_ptr(pc), capacity=cap, count=0, on_device=int(on_device))
+        self._check(self._lib.lss_sort_batch(self._h, raw_t.data_ptr(), raw_t.shape[0], ibatch, n_batches,
+                                             raw_dev, rec, _stream(self.device)))
+        n = rec.count
+        return dict(time=time[:n], template=tmpl[:n], amplitude=amp[:n], pc=None if pc is None else pc[:n])
+
+    def stats(self) -> dict:
+        s = LssStats()
+        self._check(self._lib.lss_get_stats(self._h, s))
+        return dict(rounds=s.rounds, spikes=s.spikes, recheck_columns=s.recheck_columns,
+                    recheck_flips=s.recheck_flips, launches=s.launches)
+
+    def set_profiling(self, on: bool = True):
+        self._check(self._lib.lss_set_profiling(self._h, int(on)))
+
+    def stage_times(self) -> dict:
+        t = LssStageTimes()
+        self._check(self._lib.lss_get_stage_times(self._h, t))
+        return {n: getattr(t, n) for n in STAGES}
+
+
+# ---------------------------------------------------------------- KS4 API
+_cache: dict = {}
+
+
+def _sorter_for(ops, U, ctc, N, device) -> Sorter:
+    dev = device.index if device.index is not None else torch.cuda.current_device()
+    key = (U.data_ptr(), tuple(U.shape), ctc.data_ptr(), ops['wPCA'].data_ptr(), float(ops['Th_learned']),
+           int(ops['nt']), N, dev)
+    s = _cache.get(key)
+    if s is None:
+        _cache.clear()
+        nt = int(ops['nt'])
+        C = U.shape[2]
+        s = Sorter(U=U, wPCA=ops['wPCA'], ctc=ctc, Wrot=torch.eye(C), NT=N - 2 * nt, Th=float(ops['Th_learned']),
+                   nt0min=int(ops.get('nt0min', 20)), device=dev)
+        _cache[key] = s
+    return s
+
+
+def run_matching(ops, X, U, ctc, device=torch.device('cuda')):
+    """Drop-in for ``kilosort.template_matching.run_matching`` (template_matching.py:128-202)."""
+    device = torch.device(device)
+    s = _sorter_for(ops, U, ctc, X.shape[1], device)
+    st, amps, Xres = s.match(X.to(s.device))
+    return st, amps, Xres

@@ -1,0 +1,302 @@
+"""CPU oracle for the per-batch spike-sorting hot path (TEST INFRASTRUCTURE ONLY).
+
+This module restates, in torch on the CPU, the Kilosort4 4.0.13 functions that
+LiveSpikeSorter's sorter mirrors, as vendored in the reference under
+``src/Python/run_online_spikes/Lib/site-packages/kilosort/``:
+
+* ``padded_batch``       <- ``io.py:584-637``        (BinaryRWFile.padded_batch_to_torch)
+* ``filter_batch``       <- ``io.py:757-790``        (BinaryFiltered.filter)
+* ``fft_highpass``       <- ``preprocessing.py:138-154``
+* ``get_highpass_filter``<- ``preprocessing.py:121-136``
+* ``whitening_*``        <- ``preprocessing.py:8-35``
+* ``get_drift_matrix``   <- ``preprocessing.py:44-69`` (nblocks == 1) and the
+                            ``iKxx`` precompute of ``datashift.py:215-219``
+* ``prepare_matching``   <- ``template_matching.py:110-121``
+* ``prepare_extract``    <- ``template_matching.py:20-26``
+* ``run_matching``       <- ``template_matching.py:128-202``
+* ``extract_batch``      <- ``template_matching.py:46-73`` (xfeat and time conversion)
+
+It is the checker, never the thing measured or shipped: only ``tests/``,
+``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` import it.
+The product path never routes through this file.
+
+Parity pin: ``tests/test_oracle_pin.py`` imports the vendored reference itself
+(when the reference tree is present) and checks that every function here returns
+bit-identical tensors on seeded inputs; ``tests/golden/`` holds fixtures that the
+reference produced (``tests/golden/make_golden.py``), including the reference's
+own known-answer case ``src/Python/conv1d_test.py:14-43``, so the pin also holds
+where the reference tree is absent.
+
+``dtype=torch.float64`` turns ``run_matching`` into the FP64 score oracle (the
+reference hard-codes float32 amplitudes at ``template_matching.py:151``; the
+FP64 mode keeps every intermediate in float64).
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+from torch.nn.functional import conv1d, max_pool1d
+from torch.fft import fft, ifft, fftshift
+
+
+# --------------------------------------------------------------------------
+# ingest: io.py:584-637 and io.py:757-790
+# --------------------------------------------------------------------------
+def padded_batch(raw: np.ndarray, ibatch: int, NT: int, nt: int,
+                 imin: int = 0, imax: int | None = None) -> torch.Tensor:
+    """``BinaryRWFile.padded_batch_to_torch`` (io.py:584-637) on an int16 array.
+
+    ``raw`` is the file's ``[n_samples, n_chan_bin]`` int16 matrix.  Returns
+    float32 ``[n_chan_bin, NT + 2*nt]`` with the reference's edge handling:
+    batch 0 replicates its first sample into the leading ``nt`` columns, the
+    last batch replicates its last sample to the end, and a short single batch
+    leaves zeros at the tail.
+    """
+    if imax is None:
+        imax = raw.shape[0]
+    n_samples = imax - imin
+    n_batches = int(np.ceil(n_samples / NT))
+    C = raw.shape[1]
+    if ibatch == 0:
+        bstart = imin
+        bend = imin + NT + nt
+    else:
+        bstart = imin + ibatch * NT - nt
+        bend = min(imax, bstart + NT + 2 * nt)
+    data = raw[bstart:bend].T
+    nsamp = data.shape[-1]
+    X = torch.zeros((C, NT + 2 * nt), dtype=torch.float32)
+    if ibatch == 0:
+        X[:, nt:nt + nsamp] = torch.from_numpy(np.ascontiguousarray(data)).float()
+        X[:, :nt] = X[:, nt:nt + 1]
+    elif ibatch == n_batches - 1:
+        X[:, :nsamp] = torch.from_numpy(np.ascontiguousarray(data)).float()
+        X[:, nsamp:] = X[:, nsamp - 1:nsamp]
+    else:
+        X[:] = torch.from_numpy(np.ascontiguousarray(data)).float()
+    return X
+
+
+def fft_highpass(hp_filter: torch.Tensor, NT: int) -> torch.Tensor:
+    """preprocessing.py:138-154: pad or crop the impulse response to NT, FFT it."""
+    ft = hp_filter.shape[0]
+    if ft < NT:
+        pad = (NT - ft) // 2
+        fhp = fft(torch.cat((torch.zeros(pad, dtype=hp_filter.dtype), hp_filter,
+                             torch.zeros(pad + (NT - pad * 2 - ft), dtype=hp_filter.dtype))))
+    elif ft > NT:
+        crop = (ft - NT) // 2
+        fhp = fft(hp_filter[crop:crop + NT])
+    else:
+        fhp = fft(hp_filter)
+    return fhp
+
+
+def filter_batch(X: torch.Tensor, chan_map=None, invert_sign=False, do_CAR=True,
+                 hp_filter: torch.Tensor | None = None,
+                 whiten_mat: torch.Tensor | None = None,
+                 drift_M: torch.Tensor | None = None) -> torch.Tensor:
+    """``BinaryFiltered.filter`` (io.py:757-790) without the artifact branch."""
+    if chan_map is not None:
+        X = X[torch.as_tensor(chan_map, dtype=torch.int64)]
+    if invert_sign:
+        X = X * -1
+    X = X - X.mean(1).unsqueeze(1)
+    if do_CAR:
+        X = X - torch.median(X, 0)[0]
+    if hp_filter is not None:
+        fwav = fft_highpass(hp_filter, NT=X.shape[1])
+        X = torch.real(ifft(fft(X) * torch.conj(fwav)))
+        X = fftshift(X, dim=-1)
+    if whiten_mat is not None:
+        if drift_M is not None:
+            X = (drift_M @ whiten_mat) @ X
+        else:
+            X = whiten_mat @ X
+    return X
+
+
+# --------------------------------------------------------------------------
+# one-time setup: preprocessing.py, datashift.py, template_matching.py
+# --------------------------------------------------------------------------
+def get_highpass_filter(fs=30000, cutoff=300) -> torch.Tensor:
+    """preprocessing.py:121-136: filtfilt impulse response of a 3rd-order Butterworth."""
+    from scipy.signal import butter, filtfilt
+    NT = 30122
+    b, a = butter(3, cutoff, fs=fs, btype='high')
+    x = np.zeros(NT)
+    x[NT // 2] = 1
+    return torch.from_numpy(filtfilt(b, a, x).copy()).float()
+
+
+def whitening_from_covariance(CC: torch.Tensor) -> torch.Tensor:
+    """preprocessing.py:8-17 (ZCA)."""
+    E, D, V = torch.linalg.svd(CC)
+    eps = 1e-6
+    return (E / (D + eps) ** .5) @ E.T
+
+
+def whitening_local(CC: torch.Tensor, xc, yc, nrange=32) -> torch.Tensor:
+    """preprocessing.py:19-35."""
+    Nchan = CC.shape[0]
+    Wrot = torch.zeros((Nchan, Nchan), dtype=CC.dtype)
+    for j in range(Nchan):
+        ds = (xc[j] - xc) ** 2 + (yc[j] - yc) ** 2
+        ix = np.argsort(ds)[:nrange]
+        wrot = whitening_from_covariance(CC[np.ix_(ix, ix)])
+        Wrot[j, ix] = wrot[0]
+    return Wrot
+
+
+def kernel2D(x, y, sig=1):
+    """datashift.py:176-179 (numpy)."""
+    ds = ((x[:, np.newaxis] - y) ** 2).sum(-1)
+    return np.exp(-ds / (2 * sig ** 2))
+
+
+def inv_kernel(xc, yc, sig_interp=20) -> torch.Tensor:
+    """datashift.py:213-219: ``iKxx`` for the drift interpolation."""
+    xp = np.vstack((xc, yc)).T
+    Kxx = torch.from_numpy(kernel2D(xp, xp, sig_interp))
+    return torch.linalg.inv(Kxx + 0.01 * torch.eye(Kxx.shape[0], dtype=Kxx.dtype))
+
+
+def get_drift_matrix(xc, yc, dshift, iKxx: torch.Tensor, sig_interp=20) -> torch.Tensor:
+    """preprocessing.py:44-69 with nblocks == 1 (scalar shift)."""
+    xp = np.vstack((xc, yc)).T
+    yp = xp.copy()
+    yp[:, 1] -= dshift
+    xp = torch.from_numpy(xp)
+    yp = torch.from_numpy(yp)
+    ds = ((yp.unsqueeze(1) - xp) ** 2).sum(-1)
+    Kyx = torch.exp(-ds / (2 * sig_interp ** 2))
+    return Kyx @ iKxx.to(Kyx.dtype)
+
+
+def prepare_matching(wPCA: torch.Tensor, U: torch.Tensor, nt: int) -> torch.Tensor:
+    """template_matching.py:110-121: ctc[i, j, l] template cross-correlations."""
+    W = wPCA.contiguous()
+    WtW = conv1d(W.reshape(-1, 1, nt), W.reshape(-1, 1, nt), padding=nt)
+    WtW = torch.flip(WtW, [2, ])
+    UtU = torch.einsum('ikl, jml -> ijkm', U, U)
+    return torch.einsum('ijkm, kml -> ijl', UtU, WtW)
+
+
+def prepare_extract(xc, yc, U: torch.Tensor, nC: int):
+    """template_matching.py:20-26: nearest-channel tables for PC features."""
+    ds = (xc - xc[:, np.newaxis]) ** 2 + (yc - yc[:, np.newaxis]) ** 2
+    iCC = torch.from_numpy(np.argsort(ds, 0)[:nC])
+    iU = torch.argmax((U ** 2).sum(1), -1)
+    Ucc = U[torch.arange(U.shape[0]), :, iCC[:, iU]]
+    return iCC, iU, Ucc
+
+
+# --------------------------------------------------------------------------
+# matching pursuit: template_matching.py:128-202
+# --------------------------------------------------------------------------
+def run_matching(X: torch.Tensor, U: torch.Tensor, ctc: torch.Tensor, wPCA: torch.Tensor,
+                 Th: float, nt: int, dtype=torch.float32, B: torch.Tensor | None = None,
+                 nm: torch.Tensor | None = None, max_rounds: int = 100,
+                 capacity: int = 100000, return_rounds=False):
+    """``run_matching`` restated (template_matching.py:128-202).
+
+    ``B`` optionally injects the score field (so the rounds can be checked in
+    isolation from the score GEMM's rounding); ``nm`` likewise injects the
+    template energies.  Returns ``(st int64 [n,2], amps [n,1], Xres [C,N])`` and,
+    with ``return_rounds``, the round index of every spike.
+    """
+    X = X.to(dtype)
+    U = U.to(dtype)
+    ctc = ctc.to(dtype)
+    W = wPCA.to(dtype).contiguous()
+    if nm is None:
+        nm = (U ** 2).sum(-1).sum(-1)
+    else:
+        nm = nm.to(dtype)
+    if B is None:
+        B = conv1d(X.unsqueeze(1), W.unsqueeze(1), padding=nt // 2)
+        B = torch.einsum('ijk, kjl -> il', U, B)
+    else:
+        B = B.to(dtype).clone()
+    trange = torch.arange(-nt, nt + 1)
+    tiwave = torch.arange(-(nt // 2), nt // 2 + 1)
+    st = torch.zeros((capacity, 2), dtype=torch.int64)
+    amps = torch.zeros((capacity, 1), dtype=dtype)
+    rounds = torch.zeros(capacity, dtype=torch.int64)
+    k = 0
+    Xres = X.clone()
+    for t in range(max_rounds):
+        Cf = torch.relu(B) ** 2 / nm.unsqueeze(-1)
+        Cf[:, :nt] = 0
+        Cf[:, -nt:] = 0
+        Cfmax, imax = torch.max(Cf, 0)
+        Cmax = max_pool1d(Cfmax.unsqueeze(0).unsqueeze(0), (2 * nt + 1), stride=1, padding=(nt))
+        cnd1 = Cmax[0, 0] > Th ** 2
+        cnd2 = torch.abs(Cmax[0, 0] - Cfmax) < 1e-9
+        xs = torch.nonzero(cnd1 * cnd2)
+        if len(xs) == 0:
+            break
+        iX = xs[:, :1]
+        iY = imax[iX]
+        nsp = len(iX)
+        st[k:k + nsp, 0] = iX[:, 0]
+        st[k:k + nsp, 1] = iY[:, 0]
+        amps[k:k + nsp] = B[iY, iX] / nm[iY]
+        rounds[k:k + nsp] = t
+        amp = amps[k:k + nsp]
+        k += nsp
+        n = 2
+        for j in range(n):
+            Xres[:, iX[j::n] + tiwave] -= amp[j::n] * torch.einsum('ijk, jl -> kil', U[iY[j::n, 0]], W)
+            B[:, iX[j::n] + trange] -= amp[j::n] * ctc[:, iY[j::n, 0], :]
+    if return_rounds:
+        return st[:k], amps[:k], Xres, rounds[:k]
+    return st[:k], amps[:k], Xres
+
+
+def score_field(X: torch.Tensor, U: torch.Tensor, wPCA: torch.Tensor, nt: int,
+                dtype=torch.float32) -> torch.Tensor:
+    """The score GEMM of template_matching.py:145-146: ``B[t, s]``."""
+    W = wPCA.to(dtype)
+    B0 = conv1d(X.to(dtype).unsqueeze(1), W.unsqueeze(1), padding=nt // 2)
+    return torch.einsum('ijk, kjl -> il', U.to(dtype), B0)
+
+
+def extract_batch(st: torch.Tensor, amps: torch.Tensor, Xres: torch.Tensor,
+                  iCC: torch.Tensor, iU: torch.Tensor, Ucc: torch.Tensor,
+                  wPCA: torch.Tensor, nt: int, nt0min: int, ibatch: int, NT: int):
+    """template_matching.py:46-73 for one batch: PC features and time conversion.
+
+    Returns ``(st3 float64 [n,3] (time, template, amplitude), tF [n, nC, K])``.
+    """
+    tiwave = torch.arange(-(nt // 2), nt // 2 + 1)
+    xfeat = Xres[iCC[:, iU[st[:, 1:2]]], st[:, :1] + tiwave] @ wPCA.T.to(Xres.dtype)
+    xfeat += amps * Ucc[:, st[:, 1]].to(Xres.dtype)
+    if ibatch == 0:
+        neg = (st[:, 0] - nt - nt // 2 + nt0min) < 0
+        st = st[~neg, :]
+        xfeat = xfeat[:, ~neg, :]
+        amps = amps[~neg, :]
+    stt = st.double()
+    out = np.zeros((len(st), 3), 'float64')
+    out[:, 0] = ((stt[:, 0] - nt) + ibatch * NT).numpy() - nt // 2 + nt0min
+    out[:, 1] = stt[:, 1].numpy()
+    out[:, 2] = amps[:, 0].double().numpy()
+    return out, xfeat.transpose(0, 1).contiguous()
+
+
+# --------------------------------------------------------------------------
+# diagnostics
+# --------------------------------------------------------------------------
+def margin_report(B: torch.Tensor, nm: torch.Tensor, Th: float, nt: int) -> dict:
+    """Round-1 decision margins of a score field (FP64): how close each column's
+    best template is to the threshold, to the runner-up template, and to the
+    largest other value in its pooling window.  Used to judge whether a spike
+    that differs between two FP32 evaluations sat on a near-tie."""
+    B = B.double()
+    Cf = torch.relu(B) ** 2 / nm.double().unsqueeze(-1)
+    Cf[:, :nt] = 0
+    Cf[:, -nt:] = 0
+    top2 = torch.topk(Cf, 2, dim=0).values
+    best, second = top2[0], top2[1]
+    return {'best': best, 'runner_up_gap': best - second, 'threshold_gap': best - Th ** 2}
