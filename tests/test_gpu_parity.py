@@ -34,17 +34,18 @@ def _sorter(g, p, **kw):
                   iCC=g['iCC'], iU=g['iU'], Ucc=g['Ucc'], NT=p['NT'], nt0min=p['nt0min'], Th=float(g['Th']), **kw)
 
 
-def _spike_set(st):
-    st = np.asarray(st)
-    return set(map(tuple, st[:, :2].astype(np.int64).tolist()))
-
-
 def _assert_same_spikes(st_a, amp_a, st_b, amp_b):
-    a = {tuple(r): float(v) for r, v in zip(np.asarray(st_a)[:, :2].astype(np.int64).tolist(), np.ravel(amp_a))}
-    b = {tuple(r): float(v) for r, v in zip(np.asarray(st_b)[:, :2].astype(np.int64).tolist(), np.ravel(amp_b))}
-    assert a.keys() == b.keys(), (sorted(a.keys() - b.keys())[:10], sorted(b.keys() - a.keys())[:10])
-    for k in a:
-        assert abs(a[k] - b[k]) <= AMP_RTOL * max(abs(b[k]), 1e-6), (k, a[k], b[k])
+    """Same (time, template) sequence in run_matching order (round-major,
+    time-minor; Kilosort may pick the same pair again in a later round), and
+    amplitudes within AMP_RTOL."""
+    ka = np.asarray(st_a)[:, :2].astype(np.int64)
+    kb = np.asarray(st_b)[:, :2].astype(np.int64)
+    assert ka.shape == kb.shape, (ka.shape, kb.shape)
+    bad = np.nonzero((ka != kb).any(1))[0]
+    assert len(bad) == 0, (bad[:5], ka[bad[:5]], kb[bad[:5]])
+    a = np.ravel(amp_a).astype(np.float64)
+    b = np.ravel(amp_b).astype(np.float64)
+    assert np.all(np.abs(a - b) <= AMP_RTOL * np.maximum(np.abs(b), 1e-6)), np.max(np.abs(a - b) / np.abs(b))
 
 
 def test_known_answer_case_scores():
@@ -132,14 +133,10 @@ def test_sort_batch_matches_reference_extract(on_device):
     times, tmpl, amp, pc = map(np.concatenate, (times, tmpl, amp, pc))
     ref = g['extract_st']
     ref_tf = g['extract_tF']
-    a = {(int(t), int(y)): i for i, (t, y) in enumerate(zip(times, tmpl))}
-    b = {(int(t), int(y)): i for i, (t, y) in enumerate(zip(ref[:, 0], ref[:, 1]))}
-    assert a.keys() == b.keys()
-    scale = np.abs(ref_tf).max()
-    for k, i in a.items():
-        j = b[k]
-        assert abs(amp[i] - ref[j, 2]) <= AMP_RTOL * abs(ref[j, 2])
-        assert np.abs(pc[i] - ref_tf[j]).max() <= 1e-3 * scale
+    ia = np.lexsort((amp, tmpl, times))
+    ib_ = np.lexsort((ref[:, 2], ref[:, 1], ref[:, 0]))
+    _assert_same_spikes(np.stack([times, tmpl], 1)[ia], amp[ia], ref[ib_, :2], ref[ib_, 2])
+    assert np.abs(pc[ia] - ref_tf[ib_]).max() <= 1e-3 * np.abs(ref_tf).max()
 
 
 def test_run_matching_drop_in():
@@ -223,8 +220,4 @@ def test_synthetic_config0_end_to_end():
     assert len(ref) > 300
     got = np.stack([r['time'].numpy(), r['template'].numpy()], 1)
     _assert_same_spikes(got, r['amplitude'].numpy(), ref[:, :2], ref[:, 2])
-    scale = np.abs(ref_tf).max()
-    order = {(int(t), int(y)): i for i, (t, y) in enumerate(ref[:, :2])}
-    pc = r['pc'].numpy()
-    for i, (t, y) in enumerate(got):
-        assert np.abs(pc[i] - ref_tf[order[(int(t), int(y))]]).max() <= 1e-3 * scale
+    assert np.abs(r['pc'].numpy() - ref_tf).max() <= 1e-3 * np.abs(ref_tf).max()
