@@ -98,7 +98,8 @@ int  lss_create(const lss_config* cfg, const lss_tensors* tensors, lss_handle** 
  * Ucc.npy, channel_map.npy, misc.txt), honouring each .npy header's
  * fortran_order flag (the reference's cnpy ignores it, cnpy.cpp:181-184, and
  * drift_matrix.npy is written in Fortran order). `overrides` may be NULL;
- * its non-zero fields replace values read from the directory. */
+ * otherwise its do_car, invert_sign, precision and device are used as given
+ * and its other non-zero fields replace values read from the directory. */
 int  lss_create_from_dir(const char* dir, const lss_config* overrides, lss_handle** out);
 
 void lss_destroy(lss_handle* h);
