@@ -139,6 +139,28 @@ int  lss_match(lss_handle* h, const float* X_dev, int64_t N, int64_t* st_dev, fl
 int  lss_match_scores(lss_handle* h, const float* B_dev, int64_t N, int64_t* st_dev,
                       float* amps_dev, int64_t capacity, int64_t* n_spikes, void* stream);
 
+/* The same matching-pursuit rounds for callers that cannot allocate device
+ * memory (an acquisition host that owns the GPU's memory, a process whose
+ * memory another allocator reserved up front, a real-time loop that must not
+ * take cudaMalloc's synchronisation). No counterpart in the reference.
+ * Allocates nothing: its working memory is a fixed array inside the library
+ * (about 1.6 MB, held on every GPU that loads the library until exit), sized
+ * for at most LSS_NOALLOC_MAX_SAMPLES columns; larger batches are rejected
+ * with LSS_ERR_ARG. Needs no handle; runs on the calling thread's current
+ * device. The first call on a device looks up the array's device address, so
+ * make that first call before any stream capture. All calls share the array:
+ * calls that overlap on the GPU race, so serialise them.
+ * B_dev f32 [T, ldb] is the score field and is updated in place;
+ * nm_dev f32 [T]; ctc_permuted_dev f32 [T, T, 2nt+1] = ctc.permute(1,0,2)
+ * (the reference's ctc_permuted.npy). Outputs: spike_x / spike_y / spike_amp
+ * (device, [capacity]) in run_matching order; *n_spikes and *n_rounds on the host. */
+#define LSS_NOALLOC_MAX_SAMPLES 65536
+int  lss_mp_rounds_noalloc(float* B_dev, int64_t ldb, int32_t n_templates, int32_t n_samples,
+                           int32_t nt, float th_learned, const float* nm_dev,
+                           const float* ctc_permuted_dev, int32_t max_rounds, int32_t capacity,
+                           int32_t* spike_x, int32_t* spike_y, float* spike_amp,
+                           int32_t* n_spikes, int32_t* n_rounds, void* stream);
+
 /* Score field B f32 [T, N] of a filtered batch (template_matching.py:145-146). */
 int  lss_scores(lss_handle* h, const float* X_dev, int64_t N, float* B_dev, void* stream);
 

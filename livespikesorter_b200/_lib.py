@@ -15,7 +15,8 @@ LSS_PREC_FP32, LSS_PREC_BF16_RECHECK = 0, 1
 # every entry point declared in include/lss.h
 EXPORTS = ('lss_create', 'lss_create_from_dir', 'lss_destroy', 'lss_last_error', 'lss_get_config',
            'lss_set_drift', 'lss_filter', 'lss_match', 'lss_match_scores', 'lss_scores',
-           'lss_sort_batch', 'lss_get_stats', 'lss_set_profiling', 'lss_get_stage_times')
+           'lss_sort_batch', 'lss_get_stats', 'lss_set_profiling', 'lss_get_stage_times',
+           'lss_mp_rounds_noalloc')
 
 
 class LssConfig(ct.Structure):
@@ -87,6 +88,8 @@ def load() -> ct.CDLL:
         'lss_get_stats': ([P, ct.POINTER(LssStats)], ct.c_int),
         'lss_set_profiling': ([P, I32], ct.c_int),
         'lss_get_stage_times': ([P, ct.POINTER(LssStageTimes)], ct.c_int),
+        'lss_mp_rounds_noalloc': ([P, I64, I32, I32, I32, ct.c_float, P, P, I32, I32, P, P, P,
+                                   ct.POINTER(I32), ct.POINTER(I32), P], ct.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

@@ -48,6 +48,10 @@ int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
 }  // namespace
 
+// Error text for entry points that have no handle (read back through
+// lss_last_error(NULL)).
+void lss::set_thread_error(const char* msg) { g_create_err = msg; }
+
 struct lss_handle {
     lss_config cfg{};
     std::string err;

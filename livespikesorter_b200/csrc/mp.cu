@@ -243,7 +243,7 @@ __global__ void __launch_bounds__(MP_THREADS, 1) k_mp(MPArgs a) {
                 a.sp_x[i] = x;
                 a.sp_y[i] = y;
                 a.sp_amp[i] = __fdiv_rn(__ldcg(a.B + (int64_t)y * a.ldb + x), __ldg(a.nm + y));
-                a.sp_round[i] = r;
+                if (a.sp_round) a.sp_round[i] = r;
             }
             if (b == 0 && tid == 0) a.round_start[r] = base;
             for (int s = lo + tid; s < hi; s += MP_THREADS)
@@ -364,4 +364,150 @@ cudaError_t launch_mp(MPArgs a, int grid, cudaStream_t s) {
     return cudaLaunchCooperativeKernel((void*)k_mp, dim3(grid), dim3(MP_THREADS), args, smem, s);
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the rounds (lss_mp_rounds_noalloc).
+//
+// Some callers cannot allocate device memory once they are running: a plugin
+// inside an acquisition host that owns the GPU's memory, a process whose
+// device memory is reserved up front by another allocator, or a real-time loop
+// that may not take cudaMalloc's implicit synchronisation. For them the
+// rounds' working memory (column maxima, update keys, per-CTA peak lists,
+// round offsets, counters and the grid barrier) lives in one fixed array
+// compiled into this library. Every GPU that loads the library holds the array
+// (about 1.6 MB) until the process exits. All calls share it, so calls whose
+// work overlaps on the GPU (two streams or two host threads at once) race and
+// must be serialised by the caller. Each call clears the parts that must start
+// at zero; the rest is fully written before it is read.
+// ---------------------------------------------------------------------------
+constexpr int NA_MAX_N = 65536;      // LSS_NOALLOC_MAX_SAMPLES
+constexpr int NA_MAX_GRID = 1024;
+constexpr int NA_MAX_ROUNDS = 1000;
+constexpr size_t na_align(size_t x) { return (x + 255) / 256 * 256; }
+constexpr size_t NA_OFF_CFMAX = 0;
+constexpr size_t NA_OFF_IMAX = na_align(NA_OFF_CFMAX + sizeof(float) * NA_MAX_N);
+constexpr size_t NA_OFF_COLKEY = na_align(NA_OFF_IMAX + sizeof(int32_t) * NA_MAX_N);
+constexpr size_t NA_OFF_BLKX = na_align(NA_OFF_COLKEY + sizeof(unsigned long long) * NA_MAX_N);
+constexpr size_t NA_OFF_BLKY = na_align(NA_OFF_BLKX + sizeof(int32_t) * NA_MAX_N);
+constexpr size_t NA_OFF_BLKCNT = na_align(NA_OFF_BLKY + sizeof(int32_t) * NA_MAX_N);
+constexpr size_t NA_OFF_RSTART = na_align(NA_OFF_BLKCNT + sizeof(int32_t) * NA_MAX_GRID);
+constexpr size_t NA_OFF_ZERO = na_align(NA_OFF_RSTART + sizeof(int32_t) * (NA_MAX_ROUNDS + 2));
+// zero-initialised tail: counters[4], status, pad, barrier[2]
+constexpr size_t NA_ZERO_BYTES = 256;
+constexpr size_t NA_BYTES = NA_OFF_ZERO + NA_ZERO_BYTES;
+
+static __device__ __align__(256) unsigned char g_mp_scratch[NA_BYTES];
+
 }  // namespace lss
+
+#include <mutex>
+
+#include "../../include/lss.h"
+
+namespace {
+std::mutex g_na_mutex;
+unsigned char* g_na_base[256] = {};  // device address of g_mp_scratch, per device ordinal
+}  // namespace
+
+extern "C" int lss_mp_rounds_noalloc(float* B_dev, int64_t ldb, int32_t n_templates, int32_t n_samples,
+                                     int32_t nt, float th_learned, const float* nm_dev,
+                                     const float* ctc_permuted_dev, int32_t max_rounds, int32_t capacity,
+                                     int32_t* spike_x, int32_t* spike_y, float* spike_amp, int32_t* n_spikes,
+                                     int32_t* n_rounds, void* stream) {
+    using namespace lss;
+    if (!B_dev || !nm_dev || !ctc_permuted_dev || !spike_x || !spike_y || !spike_amp || !n_spikes || !n_rounds) {
+        set_thread_error("lss_mp_rounds_noalloc: null pointer argument");
+        return LSS_ERR_ARG;
+    }
+    if (n_samples > NA_MAX_N) {
+        set_thread_error("lss_mp_rounds_noalloc: n_samples exceeds LSS_NOALLOC_MAX_SAMPLES (65536)");
+        return LSS_ERR_ARG;
+    }
+    if (n_templates <= 0 || nt <= 0 || nt % 2 == 0 || n_samples <= 2 * nt || ldb < n_samples) {
+        set_thread_error("lss_mp_rounds_noalloc: need n_templates > 0, odd nt, n_samples > 2*nt, ldb >= n_samples");
+        return LSS_ERR_ARG;
+    }
+    if (max_rounds <= 0 || max_rounds > NA_MAX_ROUNDS || capacity <= 0 || !(th_learned > 0.f)) {
+        set_thread_error("lss_mp_rounds_noalloc: need 0 < max_rounds <= 1000, capacity > 0, th_learned > 0");
+        return LSS_ERR_ARG;
+    }
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= 256) {
+        set_thread_error("lss_mp_rounds_noalloc: no current CUDA device");
+        return LSS_ERR_CUDA;
+    }
+    unsigned char* base = nullptr;
+    {
+        // one-time set-up per device: the device address of the scratch array
+        std::lock_guard<std::mutex> lock(g_na_mutex);
+        if (!g_na_base[dev]) {
+            void* p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_mp_scratch);
+            if (e != cudaSuccess) {
+                set_thread_error(cudaGetErrorString(e));
+                return LSS_ERR_CUDA;
+            }
+            g_na_base[dev] = static_cast<unsigned char*>(p);
+        }
+        base = g_na_base[dev];
+    }
+    const int G = mp_max_grid(dev);
+    if (G > NA_MAX_GRID) {
+        set_thread_error("lss_mp_rounds_noalloc: device has more SMs than the scratch supports");
+        return LSS_ERR_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    MPArgs a{};
+    a.B = B_dev;
+    a.ldb = ldb;
+    a.T = n_templates;
+    a.N = n_samples;
+    a.nt = nt;
+    a.th2 = th_learned * th_learned;
+    a.nm = nm_dev;
+    a.ctcP = ctc_permuted_dev;
+    a.cfmax = reinterpret_cast<float*>(base + NA_OFF_CFMAX);
+    a.imax = reinterpret_cast<int32_t*>(base + NA_OFF_IMAX);
+    a.colkey = reinterpret_cast<unsigned long long*>(base + NA_OFF_COLKEY);
+    a.blk_x = reinterpret_cast<int32_t*>(base + NA_OFF_BLKX);
+    a.blk_y = reinterpret_cast<int32_t*>(base + NA_OFF_BLKY);
+    a.blk_cnt = reinterpret_cast<int32_t*>(base + NA_OFF_BLKCNT);
+    a.round_start = reinterpret_cast<int32_t*>(base + NA_OFF_RSTART);
+    int32_t* zero = reinterpret_cast<int32_t*>(base + NA_OFF_ZERO);
+    a.counters = zero;           // [4]
+    a.status = zero + 4;         // [1]
+    a.bar = reinterpret_cast<unsigned int*>(zero + 8);  // [2]
+    a.sp_x = spike_x;
+    a.sp_y = spike_y;
+    a.sp_amp = spike_amp;
+    a.sp_round = nullptr;
+    a.capacity = capacity;
+    a.max_rounds = max_rounds;
+    a.cols_per_blk = (n_samples + G - 1) / G;
+    a.rows_per_item = 64;
+    a.init_cols = 1;
+    if ((e = cudaMemsetAsync(a.colkey, 0, sizeof(unsigned long long) * n_samples, s)) != cudaSuccess ||
+        (e = cudaMemsetAsync(zero, 0, NA_ZERO_BYTES, s)) != cudaSuccess ||
+        (e = launch_mp(a, G, s)) != cudaSuccess) {
+        set_thread_error(cudaGetErrorString(e));
+        return LSS_ERR_CUDA;
+    }
+    int32_t hc[8] = {0};
+    if ((e = cudaMemcpyAsync(hc, zero, sizeof(hc), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(s)) != cudaSuccess) {
+        set_thread_error(cudaGetErrorString(e));
+        return LSS_ERR_CUDA;
+    }
+    const int32_t st = hc[4];
+    *n_spikes = hc[0];
+    *n_rounds = hc[1];
+    if (st & STATUS_TIMEOUT) {
+        set_thread_error("lss_mp_rounds_noalloc: grid barrier timed out");
+        return LSS_ERR_TIMEOUT;
+    }
+    if (st & (STATUS_CAPACITY | STATUS_LIST)) {
+        set_thread_error("lss_mp_rounds_noalloc: more spikes than capacity, or a 2*nt window with over 32 peaks");
+        return LSS_ERR_CAPACITY;
+    }
+    return LSS_OK;
+}
