@@ -144,7 +144,7 @@ int  lss_match_scores(lss_handle* h, const float* B_dev, int64_t N, int64_t* st_
  * memory another allocator reserved up front, a real-time loop that must not
  * take cudaMalloc's synchronisation). No counterpart in the reference.
  * Allocates nothing: its working memory is a fixed array inside the library
- * (about 1.6 MB, held on every GPU that loads the library until exit), sized
+ * (about 2.3 MB, held on every GPU that loads the library until exit), sized
  * for at most LSS_NOALLOC_MAX_SAMPLES columns; larger batches are rejected
  * with LSS_ERR_ARG. Needs no handle; runs on the calling thread's current
  * device. The first call on a device looks up the array's device address, so

@@ -76,7 +76,7 @@ struct lss_handle {
     DevBuf<int64_t> iCC, iU;
     DevBuf<float> cfmax;
     DevBuf<int32_t> imax, blk_cnt, blk_x, blk_y, sp_x, sp_y, sp_round, round_start, counters, status;
-    DevBuf<float> sp_amp;
+    DevBuf<float> sp_amp, blk_amp;
     DevBuf<unsigned long long> colkey;
     DevBuf<unsigned int> bar;
     DevBuf<int64_t> rec_time, rec_count;
@@ -101,7 +101,7 @@ struct lss_handle {
         nm.release(); ctcP.release(); wave.release(); wpca.release(); Ucc.release(); Xres.release();
         tF.release(); iCC.release(); iU.release(); cfmax.release(); imax.release(); blk_cnt.release();
         blk_x.release(); blk_y.release(); sp_x.release(); sp_y.release(); sp_round.release();
-        round_start.release(); counters.release(); status.release(); sp_amp.release(); colkey.release();
+        round_start.release(); counters.release(); status.release(); sp_amp.release(); blk_amp.release(); colkey.release();
         bar.release(); rec_time.release(); rec_count.release(); rec_tmpl.release(); rec_amp.release();
         rec_pc.release();
     }
@@ -328,10 +328,11 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
     ALLOC(tF, (size_t)cap * std::max(nC * K, 1));
     ALLOC(cfmax, ld);
     ALLOC(imax, ld);
-    ALLOC(colkey, ld);
+    ALLOC(colkey, 2 * ld);
     ALLOC(blk_cnt, 4096);
     ALLOC(blk_x, ld);
     ALLOC(blk_y, ld);
+    ALLOC(blk_amp, ld);
     ALLOC(sp_x, cap);
     ALLOC(sp_y, cap);
     ALLOC(sp_amp, cap);
@@ -370,7 +371,7 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
         CK(cudaMemcpy(h->iCC.p, t->iCC, (size_t)nC * C * sizeof(int64_t), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(h->iU.p, t->iU, (size_t)T * sizeof(int64_t), cudaMemcpyHostToDevice));
     }
-    CK(cudaMemset(h->colkey.p, 0, ld * sizeof(unsigned long long)));
+    CK(cudaMemset(h->colkey.p, 0, 2 * ld * sizeof(unsigned long long)));
     CK(cudaMemcpy(h->Wrot.p, t->whitening, (size_t)C * C * sizeof(float), cudaMemcpyHostToDevice));
     rc = set_mixing(h, t->drift);
     if (rc) { g_create_err = h->err; return rc; }
@@ -474,9 +475,11 @@ static int run_mp(lss_handle* h, int64_t N, int32_t* n_out, int32_t* rounds_out,
     a.cfmax = h->cfmax.p;
     a.imax = h->imax.p;
     a.colkey = h->colkey.p;
+    a.ldk = h->ld;
     a.blk_cnt = h->blk_cnt.p;
     a.blk_x = h->blk_x.p;
     a.blk_y = h->blk_y.p;
+    a.blk_amp = h->blk_amp.p;
     a.sp_x = h->sp_x.p;
     a.sp_y = h->sp_y.p;
     a.sp_amp = h->sp_amp.p;
@@ -489,11 +492,10 @@ static int run_mp(lss_handle* h, int64_t N, int32_t* n_out, int32_t* rounds_out,
     a.bar = h->bar.p;
     const int G = h->mp_grid;
     a.cols_per_blk = (int)((N + G - 1) / G);
-    a.rows_per_item = 64;
     a.init_cols = 1;
     CK(cudaMemsetAsync(h->status.p, 0, sizeof(int32_t), s));
     CK(cudaMemsetAsync(h->counters.p, 0, 4 * sizeof(int32_t), s));
-    CK(cudaMemsetAsync(h->colkey.p, 0, h->ld * sizeof(unsigned long long), s));
+    CK(cudaMemsetAsync(h->colkey.p, 0, 2 * h->ld * sizeof(unsigned long long), s));
     CK(launch_mp(a, G, s));
     h->stats.launches += 1;
     int32_t hc[4], st = 0;

@@ -41,24 +41,25 @@ struct MPArgs {
     float th2;                // Th * Th
     const float* nm;          // [T]
     const float* ctcP;        // [T(j), T(i), 2nt+1] = ctc.permute(1,0,2)
-    float* cfmax;             // [N]
-    int32_t* imax;            // [N]
-    unsigned long long* colkey;  // [N], zero outside a round's update
-    int32_t* blk_cnt;         // [G]
-    int32_t* blk_x;           // [N] per-CTA peak columns (CTA b at b*W)
+    float* cfmax;             // [N] column maxima
+    int32_t* imax;            // [N] first argmax template of each column
+    unsigned long long* colkey;  // [2, ldk] update keys, alternating by round parity; zero at launch
+    int64_t ldk;
+    int32_t* blk_cnt;         // [G] peaks per CTA
+    int32_t* blk_x;           // [N] per-CTA peak lists (CTA b at b*W)
     int32_t* blk_y;           // [N]
-    int32_t* sp_x;            // [capacity]
+    float* blk_amp;           // [N]
+    int32_t* sp_x;            // [capacity] spikes in run_matching order
     int32_t* sp_y;
     float* sp_amp;
-    int32_t* sp_round;
-    int32_t* round_start;     // [max_rounds + 1]
+    int32_t* sp_round;        // may be null
+    int32_t* round_start;     // [max_rounds + 2]
     int32_t capacity;
     int32_t max_rounds;
     int32_t* counters;        // [0]=spikes [1]=rounds
-    int32_t* status;          // error bits (LSS_STATUS_*)
-    unsigned int* bar;        // [2] grid barrier count / generation
+    int32_t* status;          // error bits (STATUS_*)
+    unsigned int* bar;        // [2] grid barrier count / generation, zero at launch
     int32_t cols_per_blk;     // W
-    int32_t rows_per_item;    // TB
     int32_t init_cols;        // 1: compute column maxima of B before round 0
 };
 enum : int32_t { STATUS_TIMEOUT = 1, STATUS_CAPACITY = 2, STATUS_LIST = 4 };

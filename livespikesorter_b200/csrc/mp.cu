@@ -5,41 +5,48 @@
 // kilosortMatchingPursuit (OnlineSpikesV2.cu:873-971) with host round trips
 // every round; here the rounds never leave the device.
 //
-// One round r:
-//   P  (peak pick)  Cf = relu(B)^2 / nm with the first and last nt columns
+// One round r has two phases separated by grid barriers:
+//   P  (peaks)   Cf = relu(B)^2 / nm with the first and last nt columns
 //      zeroed; Cfmax, imax = max / first argmax over templates;
 //      Cmax = max_pool1d(Cfmax, 2nt+1, stride 1, pad nt);
 //      peaks = (Cmax > Th^2) & (|Cmax - Cfmax| < 1e-9), in time order.
-//      Each CTA owns W consecutive columns; column maxima are kept in
-//      cfmax/imax and refreshed from `colkey` where the previous round's
-//      update touched them.
-//   C0 (compact)    every CTA scans the per-CTA peak counts, writes its peaks
-//      at their global time-ordered slots with amp = B[y, x] / nm[y], and
-//      clears its columns' colkey.
-//   U  (update)     B[:, x + (-nt..nt)] -= amp * ctc[:, y, :] for the even
-//      spikes of the round, then for the odd ones. Every column is owned by
-//      the first spike whose window covers it; for each element the owner
-//      applies the last even spike's term and then the last odd spike's term,
-//      which is what the two index_put passes of the reference produce. The
-//      products and differences are single-rounded FP32 (__fmul_rn/__fsub_rn),
-//      so the score field stays bit-identical to the reference's given the same
-//      input field. The touched columns' new maxima go to colkey through a
-//      64-bit atomicMax on (Cf bits << 32 | ~t), i.e. larger score first and
-//      smaller template index on ties (torch.max's first-index rule).
-// A grid barrier separates the phases; it spins at most ~2 s before setting
-// STATUS_TIMEOUT and returning, so the kernel can never hang the device.
-// Everything another CTA writes during the kernel is read with ld.global.cg
-// (L2), never through the non-coherent L1.
+//      Each CTA owns W consecutive columns. Column maxima live in cfmax/imax
+//      and are refreshed from the update keys of the previous round. The CTA
+//      writes its peaks (column, template, amp = B[y, x] / nm[y]) in column
+//      order to its region of the per-CTA lists.
+//   U  (update)  every CTA prefix-sums the per-CTA peak counts, so the round's
+//      spikes have a global time order without another barrier. Then
+//      B[:, x + (-nt..nt)] -= amp * ctc[:, y, :] for the even spikes of the
+//      round, then for the odd ones. Every column is owned by the first spike
+//      whose window covers it; for each element the owner applies the last
+//      even spike's term and then the last odd spike's term, which is what the
+//      two index_put passes of the reference produce. Products and differences
+//      are single-rounded FP32 (__fmul_rn/__fsub_rn), so the score field stays
+//      bit-identical to the reference's given the same input field. The new
+//      column maxima go to the round's key buffer through a 64-bit atomicMax on
+//      (Cf bits << 32 | ~t): larger score first, smaller template index on ties
+//      (torch.max's first-index rule). The key buffers alternate by round
+//      parity; each CTA clears its columns of the buffer the next round writes.
+// Work items of U are (spike, block of template rows); a CTA runs four of
+// them at once in independent 128-thread groups (named barriers), each thread
+// owning one column and streaming its rows eight at a time.
+// The grid barrier spins at most ~2 s before setting STATUS_TIMEOUT and
+// returning, so the kernel can never hang the device. Everything another CTA
+// writes during the kernel is read with ld.global.cg (L2), never through the
+// non-coherent L1.
 #include "lss_kernels.cuh"
 
+#include <algorithm>
 #include <cfloat>
+#include <climits>
 
 namespace lss {
 
 constexpr int MP_THREADS = 512;
-constexpr int MP_COLS = 128;
-constexpr int MP_GROUPS = MP_THREADS / MP_COLS;
-constexpr int MP_LIST_MAX = 32;
+constexpr int MP_GROUPS = 4;                       // independent item groups per CTA
+constexpr int MP_GT = MP_THREADS / MP_GROUPS;      // threads (columns) per group
+constexpr int MP_LIST = 31;                        // spikes that may cover one owned window
+constexpr int MP_MAX_GRID = 1024;
 constexpr unsigned MP_SPIN_LIMIT = 1u << 24;
 
 __device__ __forceinline__ bool grid_sync(unsigned int* bar, int32_t* status) {
@@ -58,7 +65,8 @@ __device__ __forceinline__ bool grid_sync(unsigned int* bar, int32_t* status) {
         } else {
             unsigned int spins = 0;
             while (*vgen == gen) {
-                if ((++spins & 255u) == 0u && (*(volatile int32_t*)status & STATUS_TIMEOUT)) {
+                ++spins;
+                if ((spins & 255u) == 0u && (*(volatile int32_t*)status & STATUS_TIMEOUT)) {
                     ok = 0;
                     break;
                 }
@@ -67,7 +75,7 @@ __device__ __forceinline__ bool grid_sync(unsigned int* bar, int32_t* status) {
                     ok = 0;
                     break;
                 }
-                __nanosleep(128);
+                if (spins > 64) __nanosleep(32);
             }
         }
         __threadfence();
@@ -75,6 +83,10 @@ __device__ __forceinline__ bool grid_sync(unsigned int* bar, int32_t* status) {
     }
     __syncthreads();
     return s_ok != 0;
+}
+
+__device__ __forceinline__ void group_sync(int g) {
+    asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(MP_GT) : "memory");
 }
 
 __device__ __forceinline__ float cf_of(float b, float nmv) {
@@ -86,252 +98,293 @@ __device__ __forceinline__ unsigned long long pack_key(float cf, int t) {
     return ((unsigned long long)__float_as_uint(cf) << 32) | (unsigned long long)(0xFFFFFFFFu - (unsigned)t);
 }
 
-// Reduce (best, idx) over the MP_GROUPS row groups of a 128-column strip.
-// Returns the winner in the group-0 thread of each column.
-__device__ __forceinline__ void group_reduce(float& best, int& bi, float* sb, int* si) {
-    const int col = threadIdx.x % MP_COLS, g = threadIdx.x / MP_COLS;
-    sb[g * MP_COLS + col] = best;
-    si[g * MP_COLS + col] = bi;
-    __syncthreads();
-    if (g == 0) {
-#pragma unroll
-        for (int h = 1; h < MP_GROUPS; ++h) {
-            const float v = sb[h * MP_COLS + col];
-            const int ix = si[h * MP_COLS + col];
-            if (v > best || (v == best && ix < bi)) {
-                best = v;
-                bi = ix;
-            }
-        }
-    }
-    __syncthreads();
-}
-
 struct ListEnt {
     int x, y, par;
     float amp;
 };
 
+// Best Cf (first index on ties) of column s over rows [t0, t1), loads
+// issued eight rows at a time.
+__device__ __forceinline__ void column_best(const float* __restrict__ B, int64_t ldb, const float* __restrict__ nm,
+                                            int s, int t0, int t1, float& best, int& bi) {
+    int t = t0;
+    for (; t + 8 <= t1; t += 8) {
+        float v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = __ldcg(B + (int64_t)(t + u) * ldb + s);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const float cf = cf_of(v[u], __ldg(nm + t + u));
+            if (cf > best) {
+                best = cf;
+                bi = t + u;
+            }
+        }
+    }
+    for (; t < t1; ++t) {
+        const float cf = cf_of(__ldcg(B + (int64_t)t * ldb + s), __ldg(nm + t));
+        if (cf > best) {
+            best = cf;
+            bi = t;
+        }
+    }
+}
+
+// Inclusive warp scan.
+__device__ __forceinline__ int warp_inc_scan(int v, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += u;
+    }
+    return v;
+}
+
 __global__ void __launch_bounds__(MP_THREADS, 1) k_mp(MPArgs a) {
     extern __shared__ float smem[];
-    __shared__ float s_best[MP_THREADS];
-    __shared__ int s_idx[MP_THREADS];
-    __shared__ int s_scan[MP_THREADS];
-    __shared__ ListEnt s_list[MP_LIST_MAX];
-    __shared__ int s_nlist, s_total, s_off, s_cnt;
+    __shared__ int s_pref[MP_MAX_GRID + 1];
+    __shared__ int s_wcnt[MP_THREADS / 32];
+    __shared__ ListEnt s_list[MP_GROUPS][MP_LIST];
+    __shared__ int s_prevx[MP_GROUPS], s_nlist[MP_GROUPS];
+    __shared__ int s_cnt, s_total;
 
     const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
     const int N = a.N, T = a.T, nt = a.nt, L2 = 2 * nt + 1;
     const int W = a.cols_per_blk;
-    const int lo = b * W, hi = min(N, lo + W);
-    const int col = tid % MP_COLS, grp = tid / MP_COLS;
+    const int lo = min(N, b * W), hi = min(N, lo + W);
+    const int64_t ldk = a.ldk;
 
     // ---- initial column maxima of the score field
     if (a.init_cols) {
-        for (int c0 = lo; c0 < hi; c0 += MP_COLS) {
-            const int s = c0 + col;
+        for (int s = lo + tid; s < hi; s += MP_THREADS) {
+            const bool edge = (s < nt) || (s >= N - nt);
             float best = -1.f;
             int bi = 0;
-            const bool edge = (s < nt) || (s >= N - nt);
-            if (s < hi && !edge) {
-                for (int t = grp; t < T; t += MP_GROUPS) {
-                    const float cf = cf_of(__ldcg(a.B + (int64_t)t * a.ldb + s), __ldg(a.nm + t));
-                    if (cf > best) {
-                        best = cf;
-                        bi = t;
-                    }
-                }
-            }
-            group_reduce(best, bi, s_best, s_idx);
-            if (grp == 0 && s < hi) {
-                a.cfmax[s] = edge ? 0.f : best;
-                a.imax[s] = edge ? 0 : bi;
-            }
+            if (!edge) column_best(a.B, a.ldb, a.nm, s, 0, T, best, bi);
+            a.cfmax[s] = edge ? 0.f : best;
+            a.imax[s] = edge ? 0 : bi;
         }
     }
     if (!grid_sync(a.bar, a.status)) return;
 
-    float* vals = smem;  // [W + 2nt]
+    float* vals = smem;                                        // [W + 2nt]
+    int* ivals = reinterpret_cast<int*>(smem + W + 2 * nt);   // [W]
     int base = 0;
     int r = 0;
     for (; r < a.max_rounds; ++r) {
+        unsigned long long* kprev = a.colkey + (int64_t)((r + 1) & 1) * ldk;  // written last round
+        unsigned long long* knext = a.colkey + (int64_t)(r & 1) * ldk;        // written this round
+
         // ---- P: refresh owned maxima, stage the pooled window, pick peaks
         const int nv = (hi - lo) + 2 * nt;
         for (int p = tid; p < nv; p += MP_THREADS) {
             const int s = lo - nt + p;
             float v = -INFINITY;
             if (s >= 0 && s < N) {
-                const unsigned long long k = __ldcg(a.colkey + s);
+                const unsigned long long k = __ldcg(kprev + s);
+                const bool own = (s >= lo && s < hi);
                 if (k) {
                     v = __uint_as_float((unsigned)(k >> 32));
-                    if (s >= lo && s < hi) {
+                    if (own) {
+                        const int ix = (int)(0xFFFFFFFFu - (unsigned)(k & 0xFFFFFFFFull));
                         a.cfmax[s] = v;
-                        a.imax[s] = (int)(0xFFFFFFFFu - (unsigned)(k & 0xFFFFFFFFull));
+                        a.imax[s] = ix;
+                        ivals[s - lo] = ix;
                     }
                 } else {
                     v = __ldcg(a.cfmax + s);
+                    if (own) ivals[s - lo] = __ldcg(a.imax + s);
                 }
             }
             vals[p] = v;
         }
-        __syncthreads();
         if (tid == 0) s_cnt = 0;
         __syncthreads();
         for (int c0 = lo; c0 < hi; c0 += MP_THREADS) {
             const int s = c0 + tid;
-            int flag = 0;
+            bool flag = false;
             if (s < hi) {
                 const int p = s - lo + nt;
                 float cm = vals[p - nt];
                 for (int d = -nt + 1; d <= nt; ++d) cm = fmaxf(cm, vals[p + d]);
-                const float v = vals[p];
-                flag = (cm > a.th2) && (fabsf(__fsub_rn(cm, v)) < 1e-9f);
+                flag = (cm > a.th2) && (fabsf(__fsub_rn(cm, vals[p])) < 1e-9f);
             }
-            // ordered block compaction
-            s_scan[tid] = flag;
+            const unsigned bal = __ballot_sync(0xffffffffu, flag);
+            if (lane == 0) s_wcnt[warp] = __popc(bal);
             __syncthreads();
-            for (int off = 1; off < MP_THREADS; off <<= 1) {
-                const int v = (tid >= off) ? s_scan[tid - off] : 0;
-                __syncthreads();
-                s_scan[tid] += v;
-                __syncthreads();
+            if (warp == 0) {
+                const int c = (lane < MP_THREADS / 32) ? s_wcnt[lane] : 0;
+                const int inc = warp_inc_scan(c, lane);
+                if (lane < MP_THREADS / 32) s_wcnt[lane] = inc - c;  // exclusive
+                if (lane == MP_THREADS / 32 - 1) s_total = inc;
             }
+            __syncthreads();
             if (flag) {
-                const int k = s_cnt + s_scan[tid] - 1;
+                const int k = s_cnt + s_wcnt[warp] + __popc(bal & ((1u << lane) - 1u));
+                const int y = ivals[s - lo];
                 a.blk_x[lo + k] = s;
-                a.blk_y[lo + k] = __ldcg(a.imax + s);
+                a.blk_y[lo + k] = y;
+                a.blk_amp[lo + k] = __fdiv_rn(__ldcg(a.B + (int64_t)y * a.ldb + s), __ldg(a.nm + y));
             }
             __syncthreads();
-            if (tid == MP_THREADS - 1) s_cnt += s_scan[tid];
-            __syncthreads();
+            if (tid == 0) s_cnt += s_total;
         }
+        __syncthreads();
         if (tid == 0) a.blk_cnt[b] = s_cnt;
         if (!grid_sync(a.bar, a.status)) return;
 
-        // ---- C0: global time order, amplitudes, records
+        // ---- U: global order of the round's spikes, records, score update
         {
-            int v = 0;
-            for (int i = tid; i < G; i += MP_THREADS) v += (i < b) ? __ldcg(a.blk_cnt + i) : 0;
-            int tot = 0;
-            for (int i = tid; i < G; i += MP_THREADS) tot += __ldcg(a.blk_cnt + i);
-            s_scan[tid] = v;
-            s_best[tid] = __int_as_float(tot);
-            __syncthreads();
-            if (tid == 0) {
-                int o = 0, t2 = 0;
-                for (int i = 0; i < MP_THREADS; ++i) {
-                    o += s_scan[i];
-                    t2 += __float_as_int(s_best[i]);
+            int carry = 0;
+            for (int c0 = 0; c0 < G; c0 += MP_THREADS) {
+                const int i = c0 + tid;
+                const int c = (i < G) ? __ldcg(a.blk_cnt + i) : 0;
+                const int inc = warp_inc_scan(c, lane);
+                if (lane == 31) s_wcnt[warp] = inc;
+                __syncthreads();
+                if (warp == 0) {
+                    const int wc = (lane < MP_THREADS / 32) ? s_wcnt[lane] : 0;
+                    const int winc = warp_inc_scan(wc, lane);
+                    if (lane < MP_THREADS / 32) s_wcnt[lane] = winc - wc;
+                    if (lane == MP_THREADS / 32 - 1) s_total = winc;
                 }
-                s_off = o;
-                s_total = t2;
+                __syncthreads();
+                if (i < G) s_pref[i] = carry + s_wcnt[warp] + inc - c;
+                carry += s_total;
+                __syncthreads();
             }
+            if (tid == 0) s_pref[G] = carry;
             __syncthreads();
         }
-        const int total = s_total;
+        const int total = s_pref[G];
         if (total == 0) break;
         if (base + total > a.capacity) {
             if (tid == 0) atomicOr(a.status, STATUS_CAPACITY);
             break;
         }
         {
-            const int cnt = __ldcg(a.blk_cnt + b);
+            const int cnt = s_pref[b + 1] - s_pref[b];
             for (int k = tid; k < cnt; k += MP_THREADS) {
-                const int i = base + s_off + k;
-                const int x = __ldcg(a.blk_x + lo + k);
-                const int y = __ldcg(a.blk_y + lo + k);
-                a.sp_x[i] = x;
-                a.sp_y[i] = y;
-                a.sp_amp[i] = __fdiv_rn(__ldcg(a.B + (int64_t)y * a.ldb + x), __ldg(a.nm + y));
+                const int i = base + s_pref[b] + k;
+                a.sp_x[i] = __ldcg(a.blk_x + lo + k);
+                a.sp_y[i] = __ldcg(a.blk_y + lo + k);
+                a.sp_amp[i] = __ldcg(a.blk_amp + lo + k);
                 if (a.sp_round) a.sp_round[i] = r;
             }
             if (b == 0 && tid == 0) a.round_start[r] = base;
-            for (int s = lo + tid; s < hi; s += MP_THREADS)
-                if (__ldcg(a.colkey + s)) a.colkey[s] = 0ull;
+            for (int s = lo + tid; s < hi; s += MP_THREADS) kprev[s] = 0ull;  // next round's key buffer
         }
-        if (!grid_sync(a.bar, a.status)) return;
-
-        // ---- U: subtract the round's spikes from the score field
         {
-            const int tb_min = 16;
-            int nrb = (T + 63) / 64;
-            const int want = (2 * G + total - 1) / total;
-            if (want > nrb) nrb = want;
-            const int nrb_max = (T + tb_min - 1) / tb_min;
-            if (nrb > nrb_max) nrb = nrb_max;
+            // rows per item: enough items to fill every group, at least 8 rows
+            const int groups = G * MP_GROUPS;
+            int nrb = (2 * groups + total - 1) / total;
+            nrb = max(nrb, (T + 63) / 64);
+            nrb = min(nrb, (T + 7) / 8);
             const int tb = (T + nrb - 1) / nrb;
             const int items = total * nrb;
-            for (int it = b; it < items; it += G) {
+            const int g = tid / MP_GT, lt = tid % MP_GT;
+            for (int it = b * MP_GROUPS + g; it < items; it += groups) {
                 const int q = it / nrb, rb = it % nrb;
-                const int i = base + q;
-                const int xi = __ldcg(a.sp_x + i);
-                int lo_own = xi - nt;
-                if (q > 0) lo_own = max(lo_own, __ldcg(a.sp_x + i - 1) + nt + 1);
-                lo_own = max(lo_own, 0);
-                const int hi_own = min(xi + nt, N - 1);
-                if (tid == 0) {
-                    int n = 0;
-                    for (int j = i; j < base + total; ++j) {
-                        const int xj = __ldcg(a.sp_x + j);
-                        if (xj > xi + 2 * nt) break;
-                        if (n == MP_LIST_MAX) {
-                            atomicOr(a.status, STATUS_LIST);
-                            break;
+                if (lt < 32) {
+                    // lane 0: previous spike; lanes 1..31: spikes q, q+1, ...
+                    const int j = q - 1 + lt;
+                    int x = INT_MAX, y = 0;
+                    float amp = 0.f;
+                    if (j >= 0 && j < total) {
+                        int lo2 = 0, hi2 = G;  // region c with s_pref[c] <= j < s_pref[c+1]
+                        while (hi2 - lo2 > 1) {
+                            const int m = (lo2 + hi2) >> 1;
+                            if (s_pref[m] <= j) lo2 = m; else hi2 = m;
                         }
-                        s_list[n].x = xj;
-                        s_list[n].y = __ldcg(a.sp_y + j);
-                        s_list[n].amp = __ldcg(a.sp_amp + j);
-                        s_list[n].par = (j - base) & 1;
-                        ++n;
+                        const int idx = lo2 * W + (j - s_pref[lo2]);
+                        x = __ldcg(a.blk_x + idx);
+                        y = __ldcg(a.blk_y + idx);
+                        amp = __ldcg(a.blk_amp + idx);
                     }
-                    s_nlist = n;
+                    const int xi = __shfl_sync(0xffffffffu, x, 1);
+                    const bool ok = lt >= 1 && j < total && x <= xi + 2 * nt;
+                    const unsigned bal = __ballot_sync(0xffffffffu, ok);
+                    if (ok) s_list[g][lt - 1] = ListEnt{x, y, (j & 1), amp};
+                    if (lt == 0) {
+                        s_prevx[g] = (q > 0) ? x : INT_MIN / 2;
+                        s_nlist[g] = __popc(bal);
+                        if (__popc(bal) == MP_LIST && q + MP_LIST < total) atomicOr(a.status, STATUS_LIST);
+                    }
                 }
-                __syncthreads();
-                const int nl = s_nlist;
+                group_sync(g);
+                const int nl = s_nlist[g];
+                const int xi = s_list[g][0].x;
+                const int lo_own = max(max(xi - nt, s_prevx[g] + nt + 1), 0);
+                const int hi_own = min(xi + nt, N - 1);
                 const int t0 = rb * tb, t1 = min(T, t0 + tb);
-                for (int c0 = lo_own; c0 <= hi_own; c0 += MP_COLS) {
-                    const int s = c0 + col;
+                for (int c0 = lo_own; c0 <= hi_own; c0 += MP_GT) {
+                    const int s = c0 + lt;
+                    if (s > hi_own) continue;
+                    int e0 = -1, e1 = -1;
+                    for (int e = 0; e < nl; ++e) {
+                        if (s_list[g][e].x > s + nt) break;
+                        if (s_list[g][e].par) e1 = e; else e0 = e;
+                    }
+                    const float* c0p = nullptr;
+                    const float* c1p = nullptr;
+                    float a0 = 0.f, a1 = 0.f;
+                    if (e0 >= 0) {
+                        c0p = a.ctcP + (int64_t)s_list[g][e0].y * T * L2 + (s - s_list[g][e0].x + nt);
+                        a0 = s_list[g][e0].amp;
+                    }
+                    if (e1 >= 0) {
+                        c1p = a.ctcP + (int64_t)s_list[g][e1].y * T * L2 + (s - s_list[g][e1].x + nt);
+                        a1 = s_list[g][e1].amp;
+                    }
+                    const bool edge = (s < nt) || (s >= N - nt);
                     float best = -1.f;
                     int bi = 0;
-                    const bool active = s <= hi_own;
-                    const bool edge = (s < nt) || (s >= N - nt);
-                    if (active) {
-                        int e0 = -1, e1 = -1;
-                        for (int e = 0; e < nl; ++e) {
-                            if (s_list[e].x > s + nt) break;
-                            if (s_list[e].par) e1 = e; else e0 = e;
+                    float* bcol = a.B + s;
+                    int t = t0;
+                    for (; t + 8 <= t1; t += 8) {
+                        float v[8], w0[8], w1[8];
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) v[u] = __ldcg(bcol + (int64_t)(t + u) * a.ldb);
+                        if (c0p) {
+#pragma unroll
+                            for (int u = 0; u < 8; ++u) w0[u] = __ldg(c0p + (int64_t)(t + u) * L2);
                         }
-                        const float* c0p = nullptr;
-                        const float* c1p = nullptr;
-                        float a0 = 0.f, a1 = 0.f;
-                        if (e0 >= 0) {
-                            c0p = a.ctcP + (int64_t)s_list[e0].y * T * L2 + (s - s_list[e0].x + nt);
-                            a0 = s_list[e0].amp;
+                        if (c1p) {
+#pragma unroll
+                            for (int u = 0; u < 8; ++u) w1[u] = __ldg(c1p + (int64_t)(t + u) * L2);
                         }
-                        if (e1 >= 0) {
-                            c1p = a.ctcP + (int64_t)s_list[e1].y * T * L2 + (s - s_list[e1].x + nt);
-                            a1 = s_list[e1].amp;
-                        }
-                        for (int t = t0 + grp; t < t1; t += MP_GROUPS) {
-                            float* bp = a.B + (int64_t)t * a.ldb + s;
-                            float v = __ldcg(bp);
-                            if (c0p) v = __fsub_rn(v, __fmul_rn(a0, __ldg(c0p + (int64_t)t * L2)));
-                            if (c1p) v = __fsub_rn(v, __fmul_rn(a1, __ldg(c1p + (int64_t)t * L2)));
-                            __stcg(bp, v);
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) {
+                            float x = v[u];
+                            if (c0p) x = __fsub_rn(x, __fmul_rn(a0, w0[u]));
+                            if (c1p) x = __fsub_rn(x, __fmul_rn(a1, w1[u]));
+                            __stcg(bcol + (int64_t)(t + u) * a.ldb, x);
                             if (!edge) {
-                                const float cf = cf_of(v, __ldg(a.nm + t));
+                                const float cf = cf_of(x, __ldg(a.nm + t + u));
                                 if (cf > best) {
                                     best = cf;
-                                    bi = t;
+                                    bi = t + u;
                                 }
                             }
                         }
                     }
-                    group_reduce(best, bi, s_best, s_idx);
-                    if (grp == 0 && active && !edge && t1 > t0)
-                        atomicMax(a.colkey + s, pack_key(best, bi));
+                    for (; t < t1; ++t) {
+                        float x = __ldcg(bcol + (int64_t)t * a.ldb);
+                        if (c0p) x = __fsub_rn(x, __fmul_rn(a0, __ldg(c0p + (int64_t)t * L2)));
+                        if (c1p) x = __fsub_rn(x, __fmul_rn(a1, __ldg(c1p + (int64_t)t * L2)));
+                        __stcg(bcol + (int64_t)t * a.ldb, x);
+                        if (!edge) {
+                            const float cf = cf_of(x, __ldg(a.nm + t));
+                            if (cf > best) {
+                                best = cf;
+                                bi = t;
+                            }
+                        }
+                    }
+                    if (!edge && t1 > t0) atomicMax(knext + s, pack_key(best, bi));
                 }
-                __syncthreads();
+                group_sync(g);
             }
         }
         base += total;
@@ -350,11 +403,16 @@ int mp_max_grid(int device) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mp, MP_THREADS, 48 * 1024);
     if (occ < 1) occ = 1;
     if (occ > 1) occ = 1;
-    return sms * occ;
+    return std::min(sms * occ, MP_MAX_GRID);
+}
+
+size_t mp_smem_bytes(int cols_per_blk, int nt) {
+    return sizeof(float) * ((size_t)cols_per_blk + 2 * nt) + sizeof(int) * (size_t)cols_per_blk + 16;
 }
 
 cudaError_t launch_mp(MPArgs a, int grid, cudaStream_t s) {
-    const size_t smem = sizeof(float) * ((size_t)a.cols_per_blk + 2 * a.nt + 8);
+    if (grid > MP_MAX_GRID) return cudaErrorInvalidValue;
+    const size_t smem = mp_smem_bytes(a.cols_per_blk, a.nt);
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k_mp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
@@ -374,22 +432,22 @@ cudaError_t launch_mp(MPArgs a, int grid, cudaStream_t s) {
 // rounds' working memory (column maxima, update keys, per-CTA peak lists,
 // round offsets, counters and the grid barrier) lives in one fixed array
 // compiled into this library. Every GPU that loads the library holds the array
-// (about 1.6 MB) until the process exits. All calls share it, so calls whose
+// (about 2.3 MB) until the process exits. All calls share it, so calls whose
 // work overlaps on the GPU (two streams or two host threads at once) race and
 // must be serialised by the caller. Each call clears the parts that must start
 // at zero; the rest is fully written before it is read.
 // ---------------------------------------------------------------------------
 constexpr int NA_MAX_N = 65536;      // LSS_NOALLOC_MAX_SAMPLES
-constexpr int NA_MAX_GRID = 1024;
 constexpr int NA_MAX_ROUNDS = 1000;
 constexpr size_t na_align(size_t x) { return (x + 255) / 256 * 256; }
 constexpr size_t NA_OFF_CFMAX = 0;
 constexpr size_t NA_OFF_IMAX = na_align(NA_OFF_CFMAX + sizeof(float) * NA_MAX_N);
 constexpr size_t NA_OFF_COLKEY = na_align(NA_OFF_IMAX + sizeof(int32_t) * NA_MAX_N);
-constexpr size_t NA_OFF_BLKX = na_align(NA_OFF_COLKEY + sizeof(unsigned long long) * NA_MAX_N);
+constexpr size_t NA_OFF_BLKX = na_align(NA_OFF_COLKEY + 2 * sizeof(unsigned long long) * NA_MAX_N);
 constexpr size_t NA_OFF_BLKY = na_align(NA_OFF_BLKX + sizeof(int32_t) * NA_MAX_N);
-constexpr size_t NA_OFF_BLKCNT = na_align(NA_OFF_BLKY + sizeof(int32_t) * NA_MAX_N);
-constexpr size_t NA_OFF_RSTART = na_align(NA_OFF_BLKCNT + sizeof(int32_t) * NA_MAX_GRID);
+constexpr size_t NA_OFF_BLKAMP = na_align(NA_OFF_BLKY + sizeof(int32_t) * NA_MAX_N);
+constexpr size_t NA_OFF_BLKCNT = na_align(NA_OFF_BLKAMP + sizeof(float) * NA_MAX_N);
+constexpr size_t NA_OFF_RSTART = na_align(NA_OFF_BLKCNT + sizeof(int32_t) * MP_MAX_GRID);
 constexpr size_t NA_OFF_ZERO = na_align(NA_OFF_RSTART + sizeof(int32_t) * (NA_MAX_ROUNDS + 2));
 // zero-initialised tail: counters[4], status, pad, barrier[2]
 constexpr size_t NA_ZERO_BYTES = 256;
@@ -452,10 +510,6 @@ extern "C" int lss_mp_rounds_noalloc(float* B_dev, int64_t ldb, int32_t n_templa
         base = g_na_base[dev];
     }
     const int G = mp_max_grid(dev);
-    if (G > NA_MAX_GRID) {
-        set_thread_error("lss_mp_rounds_noalloc: device has more SMs than the scratch supports");
-        return LSS_ERR_ARG;
-    }
     cudaStream_t s = (cudaStream_t)stream;
     MPArgs a{};
     a.B = B_dev;
@@ -469,8 +523,10 @@ extern "C" int lss_mp_rounds_noalloc(float* B_dev, int64_t ldb, int32_t n_templa
     a.cfmax = reinterpret_cast<float*>(base + NA_OFF_CFMAX);
     a.imax = reinterpret_cast<int32_t*>(base + NA_OFF_IMAX);
     a.colkey = reinterpret_cast<unsigned long long*>(base + NA_OFF_COLKEY);
+    a.ldk = NA_MAX_N;
     a.blk_x = reinterpret_cast<int32_t*>(base + NA_OFF_BLKX);
     a.blk_y = reinterpret_cast<int32_t*>(base + NA_OFF_BLKY);
+    a.blk_amp = reinterpret_cast<float*>(base + NA_OFF_BLKAMP);
     a.blk_cnt = reinterpret_cast<int32_t*>(base + NA_OFF_BLKCNT);
     a.round_start = reinterpret_cast<int32_t*>(base + NA_OFF_RSTART);
     int32_t* zero = reinterpret_cast<int32_t*>(base + NA_OFF_ZERO);
@@ -484,9 +540,9 @@ extern "C" int lss_mp_rounds_noalloc(float* B_dev, int64_t ldb, int32_t n_templa
     a.capacity = capacity;
     a.max_rounds = max_rounds;
     a.cols_per_blk = (n_samples + G - 1) / G;
-    a.rows_per_item = 64;
     a.init_cols = 1;
     if ((e = cudaMemsetAsync(a.colkey, 0, sizeof(unsigned long long) * n_samples, s)) != cudaSuccess ||
+        (e = cudaMemsetAsync(a.colkey + NA_MAX_N, 0, sizeof(unsigned long long) * n_samples, s)) != cudaSuccess ||
         (e = cudaMemsetAsync(zero, 0, NA_ZERO_BYTES, s)) != cudaSuccess ||
         (e = launch_mp(a, G, s)) != cudaSuccess) {
         set_thread_error(cudaGetErrorString(e));
@@ -506,7 +562,7 @@ extern "C" int lss_mp_rounds_noalloc(float* B_dev, int64_t ldb, int32_t n_templa
         return LSS_ERR_TIMEOUT;
     }
     if (st & (STATUS_CAPACITY | STATUS_LIST)) {
-        set_thread_error("lss_mp_rounds_noalloc: more spikes than capacity, or a 2*nt window with over 32 peaks");
+        set_thread_error("lss_mp_rounds_noalloc: more spikes than capacity, or a 2*nt window with over 31 peaks");
         return LSS_ERR_CAPACITY;
     }
     return LSS_OK;
