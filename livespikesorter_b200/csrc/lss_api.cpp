@@ -8,6 +8,7 @@
 // lss_filter + lss_match / lss_sort_batch. Kilosort semantics are followed
 // where LiveSpikeSorter departs from them (round cap 100, strict threshold,
 // exact-equality peak test, division by nm, [C, N] residual indexing).
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -78,6 +79,9 @@ struct lss_handle {
     DevBuf<int32_t> imax, blk_cnt, blk_x, blk_y, sp_x, sp_y, sp_round, round_start, counters, status;
     DevBuf<float> sp_amp, blk_amp;
     DevBuf<unsigned long long> colkey;
+    DevBuf<__nv_bfloat16> B0T, Up16;   // BF16 path: transposed projection, templates
+    int CKpad = 0;
+    int sm_count = 0;
     DevBuf<unsigned int> bar;
     DevBuf<int64_t> rec_time, rec_count;
     DevBuf<int32_t> rec_tmpl;
@@ -103,7 +107,7 @@ struct lss_handle {
         blk_x.release(); blk_y.release(); sp_x.release(); sp_y.release(); sp_round.release();
         round_start.release(); counters.release(); status.release(); sp_amp.release(); blk_amp.release(); colkey.release();
         bar.release(); rec_time.release(); rec_count.release(); rec_tmpl.release(); rec_amp.release();
-        rec_pc.release();
+        rec_pc.release(); B0T.release(); Up16.release();
     }
 };
 
@@ -295,6 +299,8 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
     }
 
     h->mp_grid = mp_max_grid(cfg->device);
+    cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, cfg->device);
+    h->CKpad = (C * K + 63) / 64 * 64;
     const int64_t cap = cfg->max_spikes;
 #define ALLOC(buf, cnt)                                                                    \
     do {                                                                                   \
@@ -314,7 +320,19 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
     ALLOC(X1, (size_t)C * ld);
     ALLOC(Xh, (size_t)C * ld);
     ALLOC(X, (size_t)C * ld);
-    ALLOC(B0, (size_t)C * K * ld);
+    const bool bf16 = cfg->precision == LSS_PREC_BF16_RECHECK;
+    const TcPlan plan = tc_plan(T);
+    if (bf16 && plan.stages < 2) {
+        g_create_err = "too many templates for the tensor-core score GEMM's shared memory";
+        return LSS_ERR_ARG;
+    }
+    if (bf16) {
+        ALLOC(B0T, (size_t)h->N * h->CKpad);
+        ALLOC(Up16, (size_t)plan.Tpad * h->CKpad);
+        ALLOC(B0, 1);
+    } else {
+        ALLOC(B0, (size_t)C * K * ld);
+    }
     ALLOC(Up, (size_t)T * C * K);
     ALLOC(B, (size_t)T * ld);
     ALLOC(nm, T);
@@ -363,6 +381,14 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
     CK(cudaMemcpy(h->chan_map.p, cmap.data(), C * sizeof(int32_t), cudaMemcpyHostToDevice));
     if (!taps.empty()) CK(cudaMemcpy(h->taps.p, taps.data(), taps.size() * sizeof(float), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->Up.p, up.data(), up.size() * sizeof(float), cudaMemcpyHostToDevice));
+    if (bf16) {
+        // U_p in bf16, [Tpad, CKpad] with zero padding
+        std::vector<__nv_bfloat16> u16((size_t)plan.Tpad * h->CKpad, __float2bfloat16(0.f));
+        for (int i = 0; i < T; ++i)
+            for (int e = 0; e < C * K; ++e) u16[(size_t)i * h->CKpad + e] = __float2bfloat16(up[(size_t)i * C * K + e]);
+        CK(cudaMemcpy(h->Up16.p, u16.data(), u16.size() * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice));
+        CK(cudaMemset(h->B0T.p, 0, (size_t)h->N * h->CKpad * sizeof(__nv_bfloat16)));
+    }
     CK(cudaMemcpy(h->nm.p, nmv.data(), T * sizeof(float), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->wave.p, wave.data(), wave.size() * sizeof(float), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->wpca.p, t->wpca, (size_t)K * nt * sizeof(float), cudaMemcpyHostToDevice));
@@ -451,17 +477,33 @@ static int run_filter(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t
     return LSS_OK;
 }
 
-static int run_scores(lss_handle* h, const float* X, int64_t ldx, int64_t N, float* B, cudaStream_t s) {
+// Score field B [T, ld] of a filtered batch. The BF16 path also leaves the
+// column maxima of Cf in cfmax/imax (computed in the GEMM's epilogue), so the
+// rounds can skip their own first pass; *maxima_ready says which happened.
+static int run_scores(lss_handle* h, const float* X, int64_t ldx, int64_t N, float* B, cudaStream_t s,
+                      bool* maxima_ready = nullptr) {
+    if (h->cfg.precision == LSS_PREC_BF16_RECHECK) {
+        CK(launch_pca_proj_t(X, ldx, h->C, N, h->wpca.p, h->K, h->nt, h->B0T.p, h->CKpad, s));
+        h->mark(5, s);
+        CK(launch_score_tc(h->B0T.p, h->CKpad, (int)N, h->Up16.p, h->T, h->CKpad, h->nm.p, B, h->ld, h->cfmax.p,
+                           h->imax.p, h->nt, h->status.p, h->sm_count, s));
+        h->stats.launches += 2;
+        h->mark(6, s);
+        if (maxima_ready) *maxima_ready = true;
+        return LSS_OK;
+    }
     CK(launch_pca_proj(X, ldx, h->C, N, h->wpca.p, h->K, h->nt, h->B0.p, h->ld, s));
     h->mark(5, s);
     CK(launch_sgemm(h->Up.p, (int64_t)h->C * h->K, h->B0.p, h->ld, B, h->ld, h->T, (int)N, h->C * h->K, s));
     h->stats.launches += 2;
     h->mark(6, s);
+    if (maxima_ready) *maxima_ready = false;
     return LSS_OK;
 }
 
 // Runs the rounds on h->B (already holding the score field); returns spikes.
-static int run_mp(lss_handle* h, int64_t N, int32_t* n_out, int32_t* rounds_out, cudaStream_t s) {
+static int run_mp(lss_handle* h, int64_t N, int32_t* n_out, int32_t* rounds_out, cudaStream_t s,
+                  bool maxima_ready = false) {
     if (N <= 2 * h->nt) return h->fail(LSS_ERR_ARG, "batch shorter than 2*nt + 1 samples");
     MPArgs a{};
     a.B = h->B.p;
@@ -492,8 +534,8 @@ static int run_mp(lss_handle* h, int64_t N, int32_t* n_out, int32_t* rounds_out,
     a.bar = h->bar.p;
     const int G = h->mp_grid;
     a.cols_per_blk = (int)((N + G - 1) / G);
-    a.init_cols = 1;
-    CK(cudaMemsetAsync(h->status.p, 0, sizeof(int32_t), s));
+    a.init_cols = maxima_ready ? 0 : 1;
+    if (!maxima_ready) CK(cudaMemsetAsync(h->status.p, 0, sizeof(int32_t), s));
     CK(cudaMemsetAsync(h->counters.p, 0, 4 * sizeof(int32_t), s));
     CK(cudaMemsetAsync(h->colkey.p, 0, 2 * h->ld * sizeof(unsigned long long), s));
     CK(launch_mp(a, G, s));
@@ -546,18 +588,23 @@ int lss_scores(lss_handle* h, const float* X_dev, int64_t N, float* B_dev, void*
     cudaStream_t s = (cudaStream_t)stream;
     CK(cudaMemcpy2DAsync(h->X.p, h->ld * sizeof(float), X_dev, N * sizeof(float), N * sizeof(float), h->C,
                          cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemsetAsync(h->status.p, 0, sizeof(int32_t), s));
     int rc = run_scores(h, h->X.p, h->ld, N, h->B.p, s);
     if (rc) return rc;
     CK(cudaMemcpy2DAsync(B_dev, N * sizeof(float), h->B.p, h->ld * sizeof(float), N * sizeof(float), h->T,
                          cudaMemcpyDeviceToDevice, s));
+    int32_t st = 0;
+    CK(cudaMemcpyAsync(&st, h->status.p, sizeof(st), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    if (st & STATUS_TIMEOUT) return h->fail(LSS_ERR_TIMEOUT, "score GEMM pipeline wait timed out");
     return LSS_OK;
 }
 
 static int match_common(lss_handle* h, int64_t N, const float* Xsrc, int64_t* st_dev, float* amps_dev,
-                        float* xres_dev, int64_t capacity, int64_t* n_spikes, cudaStream_t s) {
+                        float* xres_dev, int64_t capacity, int64_t* n_spikes, cudaStream_t s,
+                        bool maxima_ready = false) {
     int32_t n = 0, rounds = 0;
-    int rc = run_mp(h, N, &n, &rounds, s);
+    int rc = run_mp(h, N, &n, &rounds, s, maxima_ready);
     if (rc) return rc;
     if (n_spikes) *n_spikes = n;
     if (n > capacity) return h->fail(LSS_ERR_CAPACITY, "output capacity smaller than the spike count");
@@ -586,9 +633,11 @@ int lss_match(lss_handle* h, const float* X_dev, int64_t N, int64_t* st_dev, flo
     cudaStream_t s = (cudaStream_t)stream;
     CK(cudaMemcpy2DAsync(h->X.p, h->ld * sizeof(float), X_dev, N * sizeof(float), N * sizeof(float), h->C,
                          cudaMemcpyDeviceToDevice, s));
-    int rc = run_scores(h, h->X.p, h->ld, N, h->B.p, s);
+    CK(cudaMemsetAsync(h->status.p, 0, sizeof(int32_t), s));
+    bool ready = false;
+    int rc = run_scores(h, h->X.p, h->ld, N, h->B.p, s, &ready);
     if (rc) return rc;
-    return match_common(h, N, h->X.p, st_dev, amps_dev, xres_dev, capacity, n_spikes, s);
+    return match_common(h, N, h->X.p, st_dev, amps_dev, xres_dev, capacity, n_spikes, s, ready);
 }
 
 int lss_match_scores(lss_handle* h, const float* B_dev, int64_t N, int64_t* st_dev, float* amps_dev,
@@ -599,6 +648,7 @@ int lss_match_scores(lss_handle* h, const float* B_dev, int64_t N, int64_t* st_d
     cudaStream_t s = (cudaStream_t)stream;
     CK(cudaMemcpy2DAsync(h->B.p, h->ld * sizeof(float), B_dev, N * sizeof(float), N * sizeof(float), h->T,
                          cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemsetAsync(h->status.p, 0, sizeof(int32_t), s));
     return match_common(h, N, nullptr, st_dev, amps_dev, nullptr, capacity, n_spikes, s);
 }
 
@@ -610,10 +660,12 @@ int lss_sort_batch(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ib
     cudaStream_t s = (cudaStream_t)stream;
     int rc = run_filter(h, raw, n_rows, ibatch, n_batches, raw_on_device, h->X.p, s);
     if (rc) return rc;
-    rc = run_scores(h, h->X.p, h->ld, h->N, h->B.p, s);
+    CK(cudaMemsetAsync(h->status.p, 0, sizeof(int32_t), s));
+    bool ready = false;
+    rc = run_scores(h, h->X.p, h->ld, h->N, h->B.p, s, &ready);
     if (rc) return rc;
     int32_t n = 0, rounds = 0;
-    rc = run_mp(h, h->N, &n, &rounds, s);
+    rc = run_mp(h, h->N, &n, &rounds, s, ready);
     if (rc) return rc;
     const int feat = h->nC * h->K;
     const bool want_pc = out->pc != nullptr && feat > 0;

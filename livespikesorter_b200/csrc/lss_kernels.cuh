@@ -1,6 +1,7 @@
 // Internal declarations shared by the kernel translation units and the host
 // orchestration (lss_api.cpp). Launchers return cudaError_t of the launch.
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -32,6 +33,25 @@ cudaError_t launch_sgemm(const float* A, int64_t lda, const float* B, int64_t ld
 // ---- temporal basis projection (score.cu): B0[c*K + k, s] ----
 cudaError_t launch_pca_proj(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
                             int32_t nt, float* B0, int64_t ldb0, cudaStream_t s);
+// transposed bf16 variant for the tensor-core GEMM: B0T[s, c*K + k], row stride ldk
+cudaError_t launch_pca_proj_t(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
+                              int32_t nt, __nv_bfloat16* B0T, int64_t ldk, cudaStream_t s);
+
+// ---- tensor-core score GEMM (tc_gemm.cu) ----
+struct TcPlan {
+    int Tpad;      // templates rounded up to 16 (the MMA's N granularity)
+    int box_rows;  // template rows per TMA box
+    int b_rows;    // template rows of one shared-memory stage
+    int stages;
+    int nacc;      // accumulator buffers in tensor memory
+    size_t smem;
+};
+TcPlan tc_plan(int T);
+// B[t, s] (row stride ldb) = sum_kk B0T[s, kk] * Up[t, kk] with B0T [N, ldk] and Up [Tpad, CKpad]
+// bf16, CKpad a multiple of 64; also writes the column maxima cfmax/imax of Cf.
+cudaError_t launch_score_tc(const __nv_bfloat16* B0T, int64_t ldk, int N, const __nv_bfloat16* Up, int T, int CKpad,
+                            const float* nm, float* Bout, int64_t ldb, float* cfmax, int32_t* imax, int nt,
+                            int32_t* status, int grid, cudaStream_t s);
 
 // ---- matching pursuit (mp.cu) ----
 struct MPArgs {

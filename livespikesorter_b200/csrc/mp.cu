@@ -103,31 +103,41 @@ struct ListEnt {
     float amp;
 };
 
-// Best Cf (first index on ties) of column s over rows [t0, t1), loads
-// issued eight rows at a time.
-__device__ __forceinline__ void column_best(const float* __restrict__ B, int64_t ldb, const float* __restrict__ nm,
-                                            int s, int t0, int t1, float& best, int& bi) {
-    int t = t0;
-    for (; t + 8 <= t1; t += 8) {
-        float v[8];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) v[u] = __ldcg(B + (int64_t)(t + u) * ldb + s);
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            const float cf = cf_of(v[u], __ldg(nm + t + u));
-            if (cf > best) {
-                best = cf;
-                bi = t + u;
-            }
-        }
-    }
-    for (; t < t1; ++t) {
-        const float cf = cf_of(__ldcg(B + (int64_t)t * ldb + s), __ldg(nm + t));
+// Running maximum of Cf = fl(fl(r*r) / nm) (r = relu(b)) with the first index
+// on ties. The correctly rounded quotient is formed only for candidates:
+// a = fl(fl(r*r) * fl(1/nm)) is within 3.01 ulp of it, so a < best*(1 - 8 ulp)
+// proves the exact value is below best (checked only while best is a normal
+// number, where the relative bounds hold).
+struct ColMax {
+    float best = -1.f;
+    float thr = -1.f;  // rounded-down best * (1 - 2^-21)
+    int bi = 0;
+    __device__ __forceinline__ void consider(float b, float nmv, float inv, int t) {
+        const float r = fmaxf(b, 0.f);
+        const float sq = __fmul_rn(r, r);
+        if (__fmul_rn(sq, inv) < thr) return;
+        const float cf = __fdiv_rn(sq, nmv);
         if (cf > best) {
             best = cf;
             bi = t;
+            thr = (cf >= 1e-30f) ? __fmul_rd(cf, 0.99999952316f) : -1.f;
         }
     }
+};
+
+// Best Cf of column s over rows [t0, t1), loads issued eight rows at a time.
+__device__ __forceinline__ void column_best(const float* __restrict__ B, int64_t ldb, const float* s_nm,
+                                            const float* s_inv, int s, int t0, int t1, ColMax& m) {
+    const float* bp = B + (int64_t)t0 * ldb + s;
+    int t = t0;
+    for (; t + 8 <= t1; t += 8, bp += 8 * ldb) {
+        float v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = __ldcg(bp + u * ldb);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) m.consider(v[u], s_nm[t + u], s_inv[t + u], t + u);
+    }
+    for (; t < t1; ++t, bp += ldb) m.consider(__ldcg(bp), s_nm[t], s_inv[t], t);
 }
 
 // Inclusive warp scan.
@@ -155,21 +165,28 @@ __global__ void __launch_bounds__(MP_THREADS, 1) k_mp(MPArgs a) {
     const int lo = min(N, b * W), hi = min(N, lo + W);
     const int64_t ldk = a.ldk;
 
+    float* vals = smem;                                        // [W + 2nt]
+    int* ivals = reinterpret_cast<int*>(smem + W + 2 * nt);   // [W]
+    float* s_nm = smem + 2 * W + 2 * nt;                       // [T]
+    float* s_inv = s_nm + T;                                   // [T]
+    for (int t = tid; t < T; t += MP_THREADS) {
+        const float v = __ldg(a.nm + t);
+        s_nm[t] = v;
+        s_inv[t] = __frcp_rn(v);
+    }
+    __syncthreads();
+
     // ---- initial column maxima of the score field
     if (a.init_cols) {
         for (int s = lo + tid; s < hi; s += MP_THREADS) {
             const bool edge = (s < nt) || (s >= N - nt);
-            float best = -1.f;
-            int bi = 0;
-            if (!edge) column_best(a.B, a.ldb, a.nm, s, 0, T, best, bi);
-            a.cfmax[s] = edge ? 0.f : best;
-            a.imax[s] = edge ? 0 : bi;
+            ColMax m;
+            if (!edge) column_best(a.B, a.ldb, s_nm, s_inv, s, 0, T, m);
+            a.cfmax[s] = edge ? 0.f : m.best;
+            a.imax[s] = edge ? 0 : m.bi;
         }
     }
     if (!grid_sync(a.bar, a.status)) return;
-
-    float* vals = smem;                                        // [W + 2nt]
-    int* ivals = reinterpret_cast<int*>(smem + W + 2 * nt);   // [W]
     int base = 0;
     int r = 0;
     for (; r < a.max_rounds; ++r) {
@@ -225,7 +242,7 @@ __global__ void __launch_bounds__(MP_THREADS, 1) k_mp(MPArgs a) {
                 const int y = ivals[s - lo];
                 a.blk_x[lo + k] = s;
                 a.blk_y[lo + k] = y;
-                a.blk_amp[lo + k] = __fdiv_rn(__ldcg(a.B + (int64_t)y * a.ldb + s), __ldg(a.nm + y));
+                a.blk_amp[lo + k] = __fdiv_rn(__ldcg(a.B + (int64_t)y * a.ldb + s), s_nm[y]);
             }
             __syncthreads();
             if (tid == 0) s_cnt += s_total;
@@ -338,51 +355,44 @@ __global__ void __launch_bounds__(MP_THREADS, 1) k_mp(MPArgs a) {
                         a1 = s_list[g][e1].amp;
                     }
                     const bool edge = (s < nt) || (s >= N - nt);
-                    float best = -1.f;
-                    int bi = 0;
-                    float* bcol = a.B + s;
+                    ColMax m;
+                    float* bp = a.B + (int64_t)t0 * a.ldb + s;
+                    const float* p0 = c0p ? c0p + (int64_t)t0 * L2 : nullptr;
+                    const float* p1 = c1p ? c1p + (int64_t)t0 * L2 : nullptr;
+                    const int64_t ldb = a.ldb;
                     int t = t0;
                     for (; t + 8 <= t1; t += 8) {
                         float v[8], w0[8], w1[8];
 #pragma unroll
-                        for (int u = 0; u < 8; ++u) v[u] = __ldcg(bcol + (int64_t)(t + u) * a.ldb);
-                        if (c0p) {
+                        for (int u = 0; u < 8; ++u) v[u] = __ldcg(bp + u * ldb);
+                        if (p0) {
 #pragma unroll
-                            for (int u = 0; u < 8; ++u) w0[u] = __ldg(c0p + (int64_t)(t + u) * L2);
+                            for (int u = 0; u < 8; ++u) w0[u] = __ldg(p0 + u * L2);
                         }
-                        if (c1p) {
+                        if (p1) {
 #pragma unroll
-                            for (int u = 0; u < 8; ++u) w1[u] = __ldg(c1p + (int64_t)(t + u) * L2);
+                            for (int u = 0; u < 8; ++u) w1[u] = __ldg(p1 + u * L2);
                         }
 #pragma unroll
                         for (int u = 0; u < 8; ++u) {
                             float x = v[u];
-                            if (c0p) x = __fsub_rn(x, __fmul_rn(a0, w0[u]));
-                            if (c1p) x = __fsub_rn(x, __fmul_rn(a1, w1[u]));
-                            __stcg(bcol + (int64_t)(t + u) * a.ldb, x);
-                            if (!edge) {
-                                const float cf = cf_of(x, __ldg(a.nm + t + u));
-                                if (cf > best) {
-                                    best = cf;
-                                    bi = t + u;
-                                }
-                            }
+                            if (p0) x = __fsub_rn(x, __fmul_rn(a0, w0[u]));
+                            if (p1) x = __fsub_rn(x, __fmul_rn(a1, w1[u]));
+                            __stcg(bp + u * ldb, x);
+                            if (!edge) m.consider(x, s_nm[t + u], s_inv[t + u], t + u);
                         }
+                        bp += 8 * ldb;
+                        if (p0) p0 += 8 * L2;
+                        if (p1) p1 += 8 * L2;
                     }
-                    for (; t < t1; ++t) {
-                        float x = __ldcg(bcol + (int64_t)t * a.ldb);
-                        if (c0p) x = __fsub_rn(x, __fmul_rn(a0, __ldg(c0p + (int64_t)t * L2)));
-                        if (c1p) x = __fsub_rn(x, __fmul_rn(a1, __ldg(c1p + (int64_t)t * L2)));
-                        __stcg(bcol + (int64_t)t * a.ldb, x);
-                        if (!edge) {
-                            const float cf = cf_of(x, __ldg(a.nm + t));
-                            if (cf > best) {
-                                best = cf;
-                                bi = t;
-                            }
-                        }
+                    for (; t < t1; ++t, bp += ldb) {
+                        float x = __ldcg(bp);
+                        if (p0) { x = __fsub_rn(x, __fmul_rn(a0, __ldg(p0))); p0 += L2; }
+                        if (p1) { x = __fsub_rn(x, __fmul_rn(a1, __ldg(p1))); p1 += L2; }
+                        __stcg(bp, x);
+                        if (!edge) m.consider(x, s_nm[t], s_inv[t], t);
                     }
-                    if (!edge && t1 > t0) atomicMax(knext + s, pack_key(best, bi));
+                    if (!edge && t1 > t0) atomicMax(knext + s, pack_key(m.best, m.bi));
                 }
                 group_sync(g);
             }
@@ -406,13 +416,14 @@ int mp_max_grid(int device) {
     return std::min(sms * occ, MP_MAX_GRID);
 }
 
-size_t mp_smem_bytes(int cols_per_blk, int nt) {
-    return sizeof(float) * ((size_t)cols_per_blk + 2 * nt) + sizeof(int) * (size_t)cols_per_blk + 16;
+size_t mp_smem_bytes(int cols_per_blk, int nt, int T) {
+    return sizeof(float) * ((size_t)cols_per_blk + 2 * nt) + sizeof(int) * (size_t)cols_per_blk +
+           sizeof(float) * 2 * (size_t)T + 16;
 }
 
 cudaError_t launch_mp(MPArgs a, int grid, cudaStream_t s) {
     if (grid > MP_MAX_GRID) return cudaErrorInvalidValue;
-    const size_t smem = mp_smem_bytes(a.cols_per_blk, a.nt);
+    const size_t smem = mp_smem_bytes(a.cols_per_blk, a.nt, a.T);
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k_mp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;

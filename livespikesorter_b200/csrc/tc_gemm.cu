@@ -1,0 +1,446 @@
+// Template scores on the 5th-generation tensor cores (tcgen05), BF16 inputs,
+// FP32 accumulation in tensor memory:
+//   B[t, s] = sum_kk B0T[s, kk] * U_p[t, kk]      (kk = c*K + k)
+// i.e. einsum('ijk,kjl->il', U, conv1d(X, wPCA)) of
+// kilosort/template_matching.py:145-146 (cross_correlation_kernel,
+// myGPUhelpers.cu:262-336, in the reference).
+//
+// Shape: samples are the MMA's M (128 per tile, one TMEM lane each), templates
+// its N (up to 512 TMEM columns per pass; several passes when T > 512), the
+// (channel, component) pairs its K (64 per pipeline stage = one 128-byte
+// swizzle row of bf16). Both operands are K-major, loaded by TMA with 128B
+// swizzle into a multi-stage shared-memory ring guarded by mbarriers.
+//
+// Warp roles (192 threads): warp 0 issues TMA, warp 1 owns TMEM and issues the
+// MMAs (one elected lane), warps 2-5 drain the accumulator: each thread owns
+// one sample (TMEM lane), so the stores of B[t, s] for a fixed template are
+// 128-byte coalesced across a warp, and the same thread forms the column
+// maximum of Cf = relu(B)^2 / nm over all templates (the matching pursuit's
+// first Cfmax / imax), exactly as the rounds' kernel does.
+//
+// Every mbarrier wait is bounded; on expiry the CTA raises an abort flag,
+// drains what it issued and frees its tensor memory before returning.
+#include "lss_kernels.cuh"
+
+#include <cuda.h>
+
+#include <algorithm>
+#include <cstdio>
+
+namespace lss {
+namespace tc {
+
+constexpr int BM = 128;               // samples per tile
+constexpr int BK = 64;                // bf16 per k-block (128 bytes)
+constexpr int MAX_NP = 512;           // templates per pass (TMEM columns)
+constexpr int THREADS = 192;
+constexpr uint32_t WAIT_LIMIT = 1u << 24;
+constexpr uint32_t A_BYTES = BM * BK * 2;  // 16 KB
+
+struct Args {
+    int N, T, Tpad, KB;
+    int box_rows, nbox_max, stages, b_rows;
+    int nacc;                 // accumulator buffers in TMEM (2 when a pass fits in 256 columns)
+    float* Bout;
+    int64_t ldb;
+    const float* nm;
+    float* cfmax;
+    int32_t* imax;
+    int nt;
+    int32_t* status;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t globaltimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait (about 2 s of wall time); false when the CTA is aborting or
+// the budget expired (then the abort flag and STATUS_TIMEOUT are raised).
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag,
+                                          int32_t* status) {
+    const uint64_t t0 = globaltimer();
+    for (uint32_t i = 0;; ++i) {
+        if (mbar_try(bar, parity)) return true;
+        if ((i & 255u) == 255u) {
+            if (*abort_flag) return false;
+            if (globaltimer() - t0 > 2000000000ull) break;
+        }
+    }
+    *abort_flag = 1;
+    atomicOr(status, STATUS_TIMEOUT);
+    return false;
+}
+
+// Wait (bounded, no abort check) for a phase that is known to complete.
+__device__ __forceinline__ void mbar_drain(uint32_t bar, uint32_t parity) {
+    const uint64_t t0 = globaltimer();
+    while (!mbar_try(bar, parity) && globaltimer() - t0 < 2000000000ull) {
+    }
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+// K-major operand, 128B swizzle: rows of 128 bytes, 8-row atoms 1024 bytes apart.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+// kind::f16 instruction descriptor: BF16 x BF16 -> F32, both K-major, M = 128.
+__device__ __forceinline__ uint32_t idesc_bf16(int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// Running column maximum of Cf with the rounds kernel's exact rule.
+struct ColMax {
+    float best = -1.f;
+    float thr = -1.f;
+    int bi = 0;
+    __device__ __forceinline__ void consider(float b, float nmv, float inv, int t) {
+        const float r = fmaxf(b, 0.f);
+        const float sq = __fmul_rn(r, r);
+        if (__fmul_rn(sq, inv) < thr) return;
+        const float cf = __fdiv_rn(sq, nmv);
+        if (cf > best) {
+            best = cf;
+            bi = t;
+            thr = (cf >= 1e-30f) ? __fmul_rd(cf, 0.99999952316f) : -1.f;
+        }
+    }
+};
+
+__global__ void __launch_bounds__(THREADS, 1)
+    k_score_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Args a) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const uint32_t stage_bytes = A_BYTES + (uint32_t)a.b_rows * 128u;
+    uint8_t* tail = smem + (size_t)a.stages * stage_bytes;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(tail);  // full[S], empty[S], acc_full[2], acc_empty[2], drain
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * a.stages + 5);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    float* s_nm = reinterpret_cast<float*>(tmem_slot + 4);
+    float* s_inv = s_nm + a.Tpad;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t s0 = smem_u32(smem);
+    auto full_bar = [&](int s) { return smem_u32(bars + s); };
+    auto empty_bar = [&](int s) { return smem_u32(bars + a.stages + s); };
+    auto accf_bar = [&](int i) { return smem_u32(bars + 2 * a.stages + i); };
+    auto acce_bar = [&](int i) { return smem_u32(bars + 2 * a.stages + 2 + i); };
+    const uint32_t drain_bar = smem_u32(bars + 2 * a.stages + 4);
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < a.stages; ++s) {
+            mbar_init(full_bar(s), 1);
+            mbar_init(empty_bar(s), 1);
+        }
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(accf_bar(i), 1);
+            mbar_init(acce_bar(i), 4);
+        }
+        mbar_init(drain_bar, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int t = threadIdx.x; t < a.Tpad; t += THREADS) {
+        const float v = (t < a.T) ? a.nm[t] : 1.f;
+        s_nm[t] = v;
+        s_inv[t] = __frcp_rn(v);
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(MAX_NP)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    const int ntiles = (a.N + BM - 1) / BM;
+    const int npass = (a.Tpad + MAX_NP - 1) / MAX_NP;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---------------- TMA producer
+            int stage = 0;
+            uint32_t ph = 0;
+            uint32_t last_ph[8];
+            bool pending[8] = {false, false, false, false, false, false, false, false};
+            bool ok = true;
+            for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+                for (int p = 0; p < npass && ok; ++p) {
+                    const int np = min(MAX_NP, a.Tpad - p * MAX_NP);
+                    const int nbox = (np + a.box_rows - 1) / a.box_rows;
+                    const uint32_t bytes = A_BYTES + (uint32_t)nbox * a.box_rows * 128u;
+                    for (int kb = 0; kb < a.KB; ++kb) {
+                        if (!mbar_wait(empty_bar(stage), ph ^ 1u, abort_flag, a.status)) { ok = false; break; }
+                        const uint32_t sa = s0 + stage * stage_bytes;
+                        mbar_expect_tx(full_bar(stage), bytes);
+                        tma_load_2d(sa, &tmA, kb * BK, tile * BM, full_bar(stage));
+                        for (int bx = 0; bx < nbox; ++bx)
+                            tma_load_2d(sa + A_BYTES + bx * a.box_rows * 128u, &tmB, kb * BK,
+                                        p * MAX_NP + bx * a.box_rows, full_bar(stage));
+                        last_ph[stage] = ph;
+                        pending[stage] = true;
+                        if (++stage == a.stages) { stage = 0; ph ^= 1u; }
+                    }
+                }
+            }
+            if (!ok) {
+                // aborting: let every load this thread issued land before the CTA exits
+                for (int s = 0; s < a.stages; ++s)
+                    if (pending[s]) mbar_drain(full_bar(s), last_ph[s]);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---------------- MMA issuer
+            int stage = 0;
+            uint32_t ph = 0;
+            uint32_t acc_ph[2] = {0, 0};
+            int acc = 0;
+            bool ok = true;
+            for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+                for (int p = 0; p < npass && ok; ++p) {
+                    const int np = min(MAX_NP, a.Tpad - p * MAX_NP);
+                    if (!mbar_wait(acce_bar(acc), acc_ph[acc] ^ 1u, abort_flag, a.status)) { ok = false; break; }
+                    fence_after();
+                    const uint32_t dcol = tmem + (uint32_t)(acc * 256);
+                    for (int kb = 0; kb < a.KB; ++kb) {
+                        if (!mbar_wait(full_bar(stage), ph, abort_flag, a.status)) { ok = false; break; }
+                        fence_after();
+                        const uint32_t sa = s0 + stage * stage_bytes;
+                        const uint32_t sb = sa + A_BYTES;
+#pragma unroll
+                        for (int ks = 0; ks < BK / 16; ++ks) {
+                            const uint64_t ad = sw128_desc(sa + ks * 32);
+                            for (int c = 0; c < np; c += 256) {
+                                const int n = min(256, np - c);
+                                const uint64_t bd = sw128_desc(sb + (uint32_t)c * 128u + ks * 32);
+                                mma_bf16(dcol + (uint32_t)c, ad, bd, idesc_bf16(n), (kb | ks) != 0);
+                            }
+                        }
+                        mma_commit(empty_bar(stage));
+                        if (++stage == a.stages) { stage = 0; ph ^= 1u; }
+                    }
+                    if (!ok) break;
+                    mma_commit(accf_bar(acc));
+                    acc_ph[acc] ^= 1u;
+                    acc = (acc + 1) % a.nacc;
+                }
+            }
+            if (!ok) {
+                *abort_flag = 1;
+                // aborting: wait for every MMA already issued before the memory is released
+                mma_commit(drain_bar);
+                mbar_drain(drain_bar, 0);
+            }
+        }
+    } else {
+        // ---------------- epilogue: warps 2..5, one sample per thread
+        const int q = warp & 3;  // TMEM lane quarter this warp may access
+        const int row = q * 32 + lane;
+        uint32_t acc_ph[2] = {0, 0};
+        int acc = 0;
+        bool ok = true;
+        for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+            const int n = tile * BM + row;
+            const bool valid = n < a.N;
+            const bool edge = (n < a.nt) || (n >= a.N - a.nt);
+            ColMax m;
+            for (int p = 0; p < npass; ++p) {
+                const int np = min(MAX_NP, a.Tpad - p * MAX_NP);
+                if (!mbar_wait(accf_bar(acc), acc_ph[acc], abort_flag, a.status)) { ok = false; break; }
+                fence_after();
+                const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * 256);
+                for (int c = 0; c < np; c += 16) {
+                    uint32_t r[16];
+                    tmem_ld16(tbase + (uint32_t)c, r);
+                    const int t0 = p * MAX_NP + c;
+                    if (valid) {
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) {
+                            const int t = t0 + j;
+                            if (t < a.T) {
+                                const float v = __uint_as_float(r[j]);
+                                a.Bout[(int64_t)t * a.ldb + n] = v;
+                                if (!edge) m.consider(v, s_nm[t], s_inv[t], t);
+                            }
+                        }
+                    }
+                }
+                fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(acce_bar(acc));
+                acc_ph[acc] ^= 1u;
+                acc = (acc + 1) % a.nacc;
+            }
+            if (ok && valid) {
+                a.cfmax[n] = edge ? 0.f : m.best;
+                a.imax[n] = edge ? 0 : m.bi;
+            }
+        }
+    }
+    fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(MAX_NP) : "memory");
+    }
+}
+
+}  // namespace tc
+
+// ---------------------------------------------------------------- host side
+typedef CUresult (*PFN_encodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                    CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static PFN_encodeTiled get_encode() {
+    static PFN_encodeTiled fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_encodeTiled>(p);
+    }
+    return fn;
+}
+
+// 2-D bf16 tensor [rows, cols] (cols contiguous, row pitch in elements), box [box_rows, 64].
+static bool make_map(CUtensorMap* m, const void* base, int64_t rows, int64_t cols, int64_t pitch, int box_rows) {
+    PFN_encodeTiled enc = get_encode();
+    if (!enc) return false;
+    if ((reinterpret_cast<uintptr_t>(base) & 15) || ((pitch * 2) & 15) || box_rows < 8 || box_rows > 256 ||
+        (box_rows & 7))
+        return false;
+    cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)(pitch * 2)};
+    cuuint32_t box[2] = {64u, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1u, 1u};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+TcPlan tc_plan(int T) {
+    TcPlan p{};
+    p.Tpad = (T + 15) / 16 * 16;
+    const int np0 = std::min(tc::MAX_NP, p.Tpad);
+    if (np0 <= 256) {
+        p.box_rows = np0;
+    } else {
+        p.box_rows = ((np0 + 1) / 2 + 7) / 8 * 8;
+    }
+    // largest pass rounded up to whole boxes
+    int b_rows = 0;
+    for (int off = 0; off < p.Tpad; off += tc::MAX_NP) {
+        const int np = std::min(tc::MAX_NP, p.Tpad - off);
+        b_rows = std::max(b_rows, (np + p.box_rows - 1) / p.box_rows * p.box_rows);
+    }
+    p.b_rows = b_rows;
+    const size_t stage = tc::A_BYTES + (size_t)b_rows * 128;
+    const size_t budget = 220 * 1024 - 1024 - 64 - 8 * (size_t)p.Tpad;
+    p.stages = (int)std::min<size_t>(4, budget / stage);
+    p.nacc = (np0 <= 256) ? 2 : 1;
+    p.smem = 1024 + (size_t)p.stages * stage + 8 * (2 * p.stages + 5) + 16 + 8 * (size_t)p.Tpad;
+    return p;
+}
+
+cudaError_t launch_score_tc(const __nv_bfloat16* B0T, int64_t ldk, int N, const __nv_bfloat16* Up, int T, int CKpad,
+                            const float* nm, float* Bout, int64_t ldb, float* cfmax, int32_t* imax, int nt,
+                            int32_t* status, int grid, cudaStream_t s) {
+    const TcPlan p = tc_plan(T);
+    if (p.stages < 2 || CKpad % tc::BK) return cudaErrorInvalidValue;
+    CUtensorMap ma, mb;
+    if (!make_map(&ma, B0T, N, CKpad, ldk, tc::BM) || !make_map(&mb, Up, p.Tpad, CKpad, CKpad, p.box_rows))
+        return cudaErrorInvalidValue;
+    tc::Args a{};
+    a.N = N;
+    a.T = T;
+    a.Tpad = p.Tpad;
+    a.KB = CKpad / tc::BK;
+    a.box_rows = p.box_rows;
+    a.stages = p.stages;
+    a.b_rows = p.b_rows;
+    a.nacc = p.nacc;
+    a.Bout = Bout;
+    a.ldb = ldb;
+    a.nm = nm;
+    a.cfmax = cfmax;
+    a.imax = imax;
+    a.nt = nt;
+    a.status = status;
+    cudaError_t e = cudaFuncSetAttribute(tc::k_score_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
+    if (e != cudaSuccess) return e;
+    const int ntiles = (N + tc::BM - 1) / tc::BM;
+    tc::k_score_tc<<<std::min(grid, ntiles), tc::THREADS, p.smem, s>>>(ma, mb, a);
+    return cudaGetLastError();
+}
+
+}  // namespace lss
