@@ -73,13 +73,14 @@ struct lss_handle {
     DevBuf<int16_t> raw;
     DevBuf<int32_t> chan_map;
     DevBuf<long long> sums;
-    DevBuf<float> taps, Mw, Wrot, Mdrift, X1, Xh, X, B0, Up, B, nm, ctcP, wave, wpca, Ucc, Xres, tF;
+    DevBuf<float> taps, Mw, Wrot, Mdrift, X1, Xh, X, B, nm, ctcP, wave, wpca, Ucc, Xres, tF;
     DevBuf<int64_t> iCC, iU;
     DevBuf<float> cfmax;
     DevBuf<int32_t> imax, blk_cnt, blk_x, blk_y, sp_x, sp_y, sp_round, round_start, counters, status;
     DevBuf<float> sp_amp, blk_amp;
     DevBuf<unsigned long long> colkey;
     DevBuf<__nv_bfloat16> B0T, Up16;   // BF16 path: transposed projection, templates
+    DevBuf<float> B0T_hi, B0T_lo, Up_hi, Up_lo;  // FP32 path (3xTF32): tf32 hi/lo splits
     int CKpad = 0;
     int sm_count = 0;
     DevBuf<unsigned int> bar;
@@ -101,13 +102,14 @@ struct lss_handle {
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
         raw.release(); chan_map.release(); sums.release(); taps.release(); Mw.release(); Wrot.release(); Mdrift.release();
-        X1.release(); Xh.release(); X.release(); B0.release(); Up.release(); B.release();
+        X1.release(); Xh.release(); X.release(); B.release();
         nm.release(); ctcP.release(); wave.release(); wpca.release(); Ucc.release(); Xres.release();
         tF.release(); iCC.release(); iU.release(); cfmax.release(); imax.release(); blk_cnt.release();
         blk_x.release(); blk_y.release(); sp_x.release(); sp_y.release(); sp_round.release();
         round_start.release(); counters.release(); status.release(); sp_amp.release(); blk_amp.release(); colkey.release();
         bar.release(); rec_time.release(); rec_count.release(); rec_tmpl.release(); rec_amp.release();
         rec_pc.release(); B0T.release(); Up16.release();
+        B0T_hi.release(); B0T_lo.release(); Up_hi.release(); Up_lo.release();
     }
 };
 
@@ -321,19 +323,20 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
     ALLOC(Xh, (size_t)C * ld);
     ALLOC(X, (size_t)C * ld);
     const bool bf16 = cfg->precision == LSS_PREC_BF16_RECHECK;
-    const TcPlan plan = tc_plan(T);
-    if (bf16 && plan.stages < 2) {
+    const TcPlan plan = tc_plan(T, !bf16);
+    if (plan.stages < 2) {
         g_create_err = "too many templates for the tensor-core score GEMM's shared memory";
         return LSS_ERR_ARG;
     }
     if (bf16) {
         ALLOC(B0T, (size_t)h->N * h->CKpad);
         ALLOC(Up16, (size_t)plan.Tpad * h->CKpad);
-        ALLOC(B0, 1);
     } else {
-        ALLOC(B0, (size_t)C * K * ld);
+        ALLOC(B0T_hi, (size_t)h->N * h->CKpad);
+        ALLOC(B0T_lo, (size_t)h->N * h->CKpad);
+        ALLOC(Up_hi, (size_t)plan.Tpad * h->CKpad);
+        ALLOC(Up_lo, (size_t)plan.Tpad * h->CKpad);
     }
-    ALLOC(Up, (size_t)T * C * K);
     ALLOC(B, (size_t)T * ld);
     ALLOC(nm, T);
     ALLOC(ctcP, (size_t)T * T * L2);
@@ -380,7 +383,6 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
     for (int c = 0; c < C; ++c) cmap[c] = t->chan_map ? t->chan_map[c] : c;
     CK(cudaMemcpy(h->chan_map.p, cmap.data(), C * sizeof(int32_t), cudaMemcpyHostToDevice));
     if (!taps.empty()) CK(cudaMemcpy(h->taps.p, taps.data(), taps.size() * sizeof(float), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(h->Up.p, up.data(), up.size() * sizeof(float), cudaMemcpyHostToDevice));
     if (bf16) {
         // U_p in bf16, [Tpad, CKpad] with zero padding
         std::vector<__nv_bfloat16> u16((size_t)plan.Tpad * h->CKpad, __float2bfloat16(0.f));
@@ -388,6 +390,24 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
             for (int e = 0; e < C * K; ++e) u16[(size_t)i * h->CKpad + e] = __float2bfloat16(up[(size_t)i * C * K + e]);
         CK(cudaMemcpy(h->Up16.p, u16.data(), u16.size() * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice));
         CK(cudaMemset(h->B0T.p, 0, (size_t)h->N * h->CKpad * sizeof(__nv_bfloat16)));
+    } else {
+        // U_p split into tf32 hi (round half away, like cvt.rna.tf32.f32) and lo = x - hi
+        std::vector<float> hi((size_t)plan.Tpad * h->CKpad, 0.f), lo(hi.size(), 0.f);
+        for (int i = 0; i < T; ++i)
+            for (int e = 0; e < C * K; ++e) {
+                const float x = up[(size_t)i * C * K + e];
+                uint32_t u;
+                std::memcpy(&u, &x, 4);
+                if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x1000u) & 0xffffe000u;
+                float xh;
+                std::memcpy(&xh, &u, 4);
+                hi[(size_t)i * h->CKpad + e] = xh;
+                lo[(size_t)i * h->CKpad + e] = x - xh;
+            }
+        CK(cudaMemcpy(h->Up_hi.p, hi.data(), hi.size() * sizeof(float), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h->Up_lo.p, lo.data(), lo.size() * sizeof(float), cudaMemcpyHostToDevice));
+        CK(cudaMemset(h->B0T_hi.p, 0, (size_t)h->N * h->CKpad * sizeof(float)));
+        CK(cudaMemset(h->B0T_lo.p, 0, (size_t)h->N * h->CKpad * sizeof(float)));
     }
     CK(cudaMemcpy(h->nm.p, nmv.data(), T * sizeof(float), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->wave.p, wave.data(), wave.size() * sizeof(float), cudaMemcpyHostToDevice));
@@ -492,12 +512,13 @@ static int run_scores(lss_handle* h, const float* X, int64_t ldx, int64_t N, flo
         if (maxima_ready) *maxima_ready = true;
         return LSS_OK;
     }
-    CK(launch_pca_proj(X, ldx, h->C, N, h->wpca.p, h->K, h->nt, h->B0.p, h->ld, s));
+    CK(launch_pca_proj_t_tf32(X, ldx, h->C, N, h->wpca.p, h->K, h->nt, h->B0T_hi.p, h->B0T_lo.p, h->CKpad, s));
     h->mark(5, s);
-    CK(launch_sgemm(h->Up.p, (int64_t)h->C * h->K, h->B0.p, h->ld, B, h->ld, h->T, (int)N, h->C * h->K, s));
+    CK(launch_score_tc_tf32x3(h->B0T_hi.p, h->B0T_lo.p, h->CKpad, (int)N, h->Up_hi.p, h->Up_lo.p, h->T, h->CKpad,
+                              h->nm.p, B, h->ld, h->cfmax.p, h->imax.p, h->nt, h->status.p, h->sm_count, s));
     h->stats.launches += 2;
     h->mark(6, s);
-    if (maxima_ready) *maxima_ready = false;
+    if (maxima_ready) *maxima_ready = true;
     return LSS_OK;
 }
 

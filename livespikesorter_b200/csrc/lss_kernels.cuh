@@ -45,13 +45,21 @@ struct TcPlan {
     int stages;
     int nacc;      // accumulator buffers in tensor memory
     size_t smem;
+    int kblock;    // K elements per pipeline stage
 };
-TcPlan tc_plan(int T);
+TcPlan tc_plan(int T, bool tf32);
 // B[t, s] (row stride ldb) = sum_kk B0T[s, kk] * Up[t, kk] with B0T [N, ldk] and Up [Tpad, CKpad]
 // bf16, CKpad a multiple of 64; also writes the column maxima cfmax/imax of Cf.
 cudaError_t launch_score_tc(const __nv_bfloat16* B0T, int64_t ldk, int N, const __nv_bfloat16* Up, int T, int CKpad,
                             const float* nm, float* Bout, int64_t ldb, float* cfmax, int32_t* imax, int nt,
                             int32_t* status, int grid, cudaStream_t s);
+// FP32-class variant (3xTF32): operands split into tf32 hi + lo parts stored as fp32.
+cudaError_t launch_score_tc_tf32x3(const float* B0T_hi, const float* B0T_lo, int64_t ldk, int N, const float* Up_hi,
+                                   const float* Up_lo, int T, int CKpad, const float* nm, float* Bout, int64_t ldb,
+                                   float* cfmax, int32_t* imax, int nt, int32_t* status, int grid, cudaStream_t s);
+// transposed projection split into tf32 hi/lo parts (fp32 containers) for the 3xTF32 GEMM
+cudaError_t launch_pca_proj_t_tf32(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
+                                   int32_t nt, float* hi, float* lo, int64_t ldk, cudaStream_t s);
 
 // ---- matching pursuit (mp.cu) ----
 struct MPArgs {

@@ -101,42 +101,48 @@ cudaError_t launch_pca_proj(const float* X, int64_t ldx, int32_t C, int64_t N, c
 
 // ---------------------------------------------------------------------------
 // Transposed projection for the tensor-core score GEMM:
-//   B0T[s, c*K + k] = bf16( sum_m wPCA[k, m] * X[c, s + m - nt/2] )
-// rows = samples (the GEMM's M), columns = (channel, component) (its K),
-// row stride ldk (a multiple of 64, the pad columns stay zero). CTA: 64
-// samples x 64 channels; the bf16 tile is staged in shared memory and written
-// as 2*64*K-byte row segments.
+//   B0T[s, c*K + k] = sum_m wPCA[k, m] * X[c, s + m - nt/2]
+// rows = samples (the GEMM's M), columns = (channel, component) (its K), row
+// stride ldk (a multiple of the GEMM's k-block; pad columns stay zero). The
+// BF16 path stores bf16; the FP32 path stores the tf32 split hi = rna(x),
+// lo = x - hi (exact in fp32) in two fp32 arrays. CTA: 64 samples x PC
+// channels, staged in shared memory and written as contiguous row segments.
 // ---------------------------------------------------------------------------
 constexpr int PT_S = 64;    // samples per CTA
-constexpr int PT_C = 64;    // channels per CTA
 
-template <int KPC>
+__device__ __forceinline__ float tf32_rna(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+template <int KPC, int PC, bool TF32>
 __global__ void __launch_bounds__(256) k_pca_proj_t(const float* __restrict__ X, int64_t ldx, int32_t C, int64_t N,
-                                                    const float* __restrict__ wpca, int32_t nt,
-                                                    __nv_bfloat16* __restrict__ B0T, int64_t ldk) {
+                                                    const float* __restrict__ wpca, int32_t nt, void* __restrict__ out0,
+                                                    float* __restrict__ out_lo, int64_t ldk) {
     extern __shared__ float sm[];
     const int ntp = (nt + 7) & ~7;
     const int xw = PT_S + ntp + 8;                 // staged samples per channel row
     float* ws = sm;                                // [KPC][ntp]
-    float* xs = ws + KPC * ntp;                    // [PT_C][xw]
-    __nv_bfloat16* out = reinterpret_cast<__nv_bfloat16*>(xs + PT_C * xw);  // [PT_S][PT_C*KPC]
+    float* xs = ws + KPC * ntp;                    // [PC][xw]
+    float* stage = xs + PC * xw;                   // [PT_S][PC*KPC]
     const int64_t s0 = (int64_t)blockIdx.x * PT_S;
-    const int c0 = blockIdx.y * PT_C;
-    const int nc = min(PT_C, C - c0);
+    const int c0 = blockIdx.y * PC;
+    const int nc = min(PC, C - c0);
     const int half = nt / 2;
     for (int e = threadIdx.x; e < KPC * ntp; e += blockDim.x) {
         const int k = e / ntp, m = e % ntp;
         ws[e] = (m < nt) ? wpca[k * nt + m] : 0.f;
     }
-    for (int e = threadIdx.x; e < PT_C * xw; e += blockDim.x) {
+    for (int e = threadIdx.x; e < PC * xw; e += blockDim.x) {
         const int c = e / xw, p = e % xw;
         const int64_t g = s0 - half + p;
         xs[e] = (c < nc && g >= 0 && g < N) ? X[(int64_t)(c0 + c) * ldx + g] : 0.f;
     }
     __syncthreads();
     // task = (channel, 8-sample group)
-    for (int task = threadIdx.x; task < PT_C * (PT_S / 8); task += blockDim.x) {
-        const int c = task % PT_C, sg = task / PT_C;
+    for (int task = threadIdx.x; task < PC * (PT_S / 8); task += blockDim.x) {
+        const int c = task % PC, sg = task / PC;
         const float* xr = xs + c * xw + sg * 8;
         float acc[KPC][8];
 #pragma unroll
@@ -164,43 +170,63 @@ __global__ void __launch_bounds__(256) k_pca_proj_t(const float* __restrict__ X,
 #pragma unroll
         for (int r = 0; r < 8; ++r)
 #pragma unroll
-            for (int k = 0; k < KPC; ++k) out[(sg * 8 + r) * (PT_C * KPC) + c * KPC + k] = __float2bfloat16_rn(acc[k][r]);
+            for (int k = 0; k < KPC; ++k) stage[(sg * 8 + r) * (PC * KPC) + c * KPC + k] = acc[k][r];
     }
     __syncthreads();
-    // row segments: PT_S rows of nc*KPC bf16 each
+    // row segments: PT_S rows of nc*KPC values each
     const int seg = nc * KPC;
     for (int e = threadIdx.x; e < PT_S * seg; e += blockDim.x) {
         const int r = e / seg, j = e % seg;
         const int64_t s = s0 + r;
-        if (s < N) B0T[s * ldk + (int64_t)c0 * KPC + j] = out[r * (PT_C * KPC) + j];
+        if (s >= N) continue;
+        const float v = stage[r * (PC * KPC) + j];
+        const int64_t o = s * ldk + (int64_t)c0 * KPC + j;
+        if (TF32) {
+            const float hi = tf32_rna(v);
+            static_cast<float*>(out0)[o] = hi;
+            out_lo[o] = __fsub_rn(v, hi);
+        } else {
+            static_cast<__nv_bfloat16*>(out0)[o] = __float2bfloat16_rn(v);
+        }
     }
 }
 
-template <int KPC>
+template <int KPC, bool TF32>
 static cudaError_t launch_pjt(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t nt,
-                              __nv_bfloat16* B0T, int64_t ldk, cudaStream_t s) {
+                              void* out0, float* out_lo, int64_t ldk, cudaStream_t s) {
+    constexpr int PC = 64;
     const int ntp = (nt + 7) & ~7;
-    const size_t smem = sizeof(float) * ((size_t)KPC * ntp + (size_t)PT_C * (PT_S + ntp + 8)) +
-                        sizeof(__nv_bfloat16) * (size_t)PT_S * PT_C * KPC;
-    cudaFuncSetAttribute(k_pca_proj_t<KPC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    dim3 grid((unsigned)((N + PT_S - 1) / PT_S), (unsigned)((C + PT_C - 1) / PT_C));
-    k_pca_proj_t<KPC><<<grid, 256, smem, s>>>(X, ldx, C, N, wpca, nt, B0T, ldk);
+    const size_t smem = sizeof(float) * ((size_t)KPC * ntp + (size_t)PC * (PT_S + ntp + 8) + (size_t)PT_S * PC * KPC);
+    cudaFuncSetAttribute(k_pca_proj_t<KPC, PC, TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    dim3 grid((unsigned)((N + PT_S - 1) / PT_S), (unsigned)((C + PC - 1) / PC));
+    k_pca_proj_t<KPC, PC, TF32><<<grid, 256, smem, s>>>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk);
     return cudaGetLastError();
+}
+
+template <bool TF32>
+static cudaError_t pjt_dispatch(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
+                                int32_t nt, void* out0, float* out_lo, int64_t ldk, cudaStream_t s) {
+    switch (K) {
+        case 1: return launch_pjt<1, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, s);
+        case 2: return launch_pjt<2, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, s);
+        case 3: return launch_pjt<3, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, s);
+        case 4: return launch_pjt<4, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, s);
+        case 5: return launch_pjt<5, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, s);
+        case 6: return launch_pjt<6, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, s);
+        case 7: return launch_pjt<7, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, s);
+        case 8: return launch_pjt<8, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, s);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 cudaError_t launch_pca_proj_t(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
                               int32_t nt, __nv_bfloat16* B0T, int64_t ldk, cudaStream_t s) {
-    switch (K) {
-        case 1: return launch_pjt<1>(X, ldx, C, N, wpca, nt, B0T, ldk, s);
-        case 2: return launch_pjt<2>(X, ldx, C, N, wpca, nt, B0T, ldk, s);
-        case 3: return launch_pjt<3>(X, ldx, C, N, wpca, nt, B0T, ldk, s);
-        case 4: return launch_pjt<4>(X, ldx, C, N, wpca, nt, B0T, ldk, s);
-        case 5: return launch_pjt<5>(X, ldx, C, N, wpca, nt, B0T, ldk, s);
-        case 6: return launch_pjt<6>(X, ldx, C, N, wpca, nt, B0T, ldk, s);
-        case 7: return launch_pjt<7>(X, ldx, C, N, wpca, nt, B0T, ldk, s);
-        case 8: return launch_pjt<8>(X, ldx, C, N, wpca, nt, B0T, ldk, s);
-        default: return cudaErrorInvalidValue;
-    }
+    return pjt_dispatch<false>(X, ldx, C, N, wpca, K, nt, B0T, nullptr, ldk, s);
+}
+
+cudaError_t launch_pca_proj_t_tf32(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
+                                   int32_t nt, float* hi, float* lo, int64_t ldk, cudaStream_t s) {
+    return pjt_dispatch<true>(X, ldx, C, N, wpca, K, nt, hi, lo, ldk, s);
 }
 
 }  // namespace lss

@@ -31,11 +31,24 @@ namespace lss {
 namespace tc {
 
 constexpr int BM = 128;               // samples per tile
-constexpr int BK = 64;                // bf16 per k-block (128 bytes)
 constexpr int MAX_NP = 512;           // templates per pass (TMEM columns)
 constexpr int THREADS = 192;
-constexpr uint32_t WAIT_LIMIT = 1u << 24;
-constexpr uint32_t A_BYTES = BM * BK * 2;  // 16 KB
+
+// Element kinds of the score GEMM.
+//  BF16 : one MMA term, 128-byte rows (64 bf16 per k-block), 128B swizzle.
+//  TF32x3: FP32-class accuracy from tf32 splits x = hi + lo:
+//         D += A_hi B_hi + A_hi B_lo + A_lo B_hi, 64-byte rows (16 floats per
+//         k-block), 64B swizzle; A and B each have a hi and a lo tile.
+template <bool TF32>
+struct Kind {
+    static constexpr uint32_t ROW = TF32 ? 64u : 128u;       // bytes per operand row in a stage
+    static constexpr int BKE = TF32 ? 16 : 64;               // elements per k-block
+    static constexpr int SUB = 2 * (TF32 ? 1 : 2);           // 32-byte MMA K steps per k-block
+    static constexpr int PARTS = TF32 ? 2 : 1;               // hi (+ lo) tiles per operand
+    static constexpr uint32_t A_TILE = BM * ROW;             // bytes of one A tile
+    static constexpr uint32_t ATOM = 8 * ROW;                // swizzle atom (8 rows)
+    static constexpr uint64_t LAYOUT = TF32 ? 4 : 2;         // UMMA layout: SWIZZLE_64B / SWIZZLE_128B
+};
 
 struct Args {
     int N, T, Tpad, KB;
@@ -115,25 +128,40 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
         : "memory");
 }
 
-// K-major operand, 128B swizzle: rows of 128 bytes, 8-row atoms 1024 bytes apart.
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
-    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
-           ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+// K-major operand with swizzled rows: 8-row atoms of ATOM bytes.
+template <bool TF32>
+__device__ __forceinline__ uint64_t operand_desc(uint32_t addr) {
+    using KD = Kind<TF32>;
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(KD::ATOM >> 4) << 32) |
+           ((uint64_t)1 << 46) | (KD::LAYOUT << 61);
 }
 
-// kind::f16 instruction descriptor: BF16 x BF16 -> F32, both K-major, M = 128.
-__device__ __forceinline__ uint32_t idesc_bf16(int n) {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+// Instruction descriptor: F32 accumulator, BF16 (1) or TF32 (2) operands,
+// both K-major, M = 128.
+template <bool TF32>
+__device__ __forceinline__ uint32_t instr_desc(int n) {
+    const uint32_t fmt = TF32 ? 2u : 1u;
+    return (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
 }
 
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                         uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-        ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
-        : "memory");
+template <bool TF32>
+__device__ __forceinline__ void mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                    uint32_t accumulate) {
+    if constexpr (TF32) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
+            ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+            : "memory");
+    } else {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+            ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+            : "memory");
+    }
 }
 
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
@@ -171,11 +199,17 @@ struct ColMax {
     }
 };
 
+// Stage layout: [A_hi | A_lo] [B_hi rows | B_lo rows] (lo tiles only for TF32x3).
+template <bool TF32>
 __global__ void __launch_bounds__(THREADS, 1)
-    k_score_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Args a) {
+    k_score_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmAlo,
+               const __grid_constant__ CUtensorMap tmB, const __grid_constant__ CUtensorMap tmBlo, Args a) {
+    using KD = Kind<TF32>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    const uint32_t stage_bytes = A_BYTES + (uint32_t)a.b_rows * 128u;
+    const uint32_t a_bytes = KD::PARTS * KD::A_TILE;
+    const uint32_t b_part = (uint32_t)a.b_rows * KD::ROW;
+    const uint32_t stage_bytes = a_bytes + KD::PARTS * b_part;
     uint8_t* tail = smem + (size_t)a.stages * stage_bytes;
     uint64_t* bars = reinterpret_cast<uint64_t*>(tail);  // full[S], empty[S], acc_full[2], acc_empty[2], drain
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * a.stages + 5);
@@ -235,15 +269,20 @@ __global__ void __launch_bounds__(THREADS, 1)
                 for (int p = 0; p < npass && ok; ++p) {
                     const int np = min(MAX_NP, a.Tpad - p * MAX_NP);
                     const int nbox = (np + a.box_rows - 1) / a.box_rows;
-                    const uint32_t bytes = A_BYTES + (uint32_t)nbox * a.box_rows * 128u;
+                    const uint32_t bytes = KD::PARTS * (KD::A_TILE + (uint32_t)nbox * a.box_rows * KD::ROW);
                     for (int kb = 0; kb < a.KB; ++kb) {
                         if (!mbar_wait(empty_bar(stage), ph ^ 1u, abort_flag, a.status)) { ok = false; break; }
                         const uint32_t sa = s0 + stage * stage_bytes;
+                        const uint32_t sb = sa + a_bytes;
+                        const int kx = kb * KD::BKE;
                         mbar_expect_tx(full_bar(stage), bytes);
-                        tma_load_2d(sa, &tmA, kb * BK, tile * BM, full_bar(stage));
-                        for (int bx = 0; bx < nbox; ++bx)
-                            tma_load_2d(sa + A_BYTES + bx * a.box_rows * 128u, &tmB, kb * BK,
-                                        p * MAX_NP + bx * a.box_rows, full_bar(stage));
+                        tma_load_2d(sa, &tmA, kx, tile * BM, full_bar(stage));
+                        if (TF32) tma_load_2d(sa + KD::A_TILE, &tmAlo, kx, tile * BM, full_bar(stage));
+                        for (int bx = 0; bx < nbox; ++bx) {
+                            const int row = p * MAX_NP + bx * a.box_rows;
+                            tma_load_2d(sb + bx * a.box_rows * KD::ROW, &tmB, kx, row, full_bar(stage));
+                            if (TF32) tma_load_2d(sb + b_part + bx * a.box_rows * KD::ROW, &tmBlo, kx, row, full_bar(stage));
+                        }
                         last_ph[stage] = ph;
                         pending[stage] = true;
                         if (++stage == a.stages) { stage = 0; ph ^= 1u; }
@@ -274,14 +313,25 @@ __global__ void __launch_bounds__(THREADS, 1)
                         if (!mbar_wait(full_bar(stage), ph, abort_flag, a.status)) { ok = false; break; }
                         fence_after();
                         const uint32_t sa = s0 + stage * stage_bytes;
-                        const uint32_t sb = sa + A_BYTES;
+                        const uint32_t sb = sa + a_bytes;
 #pragma unroll
-                        for (int ks = 0; ks < BK / 16; ++ks) {
-                            const uint64_t ad = sw128_desc(sa + ks * 32);
+                        for (int ks = 0; ks < KD::SUB; ++ks) {
+                            const uint32_t ko = ks * 32;
+                            const uint64_t ad = operand_desc<TF32>(sa + ko);
                             for (int c = 0; c < np; c += 256) {
                                 const int n = min(256, np - c);
-                                const uint64_t bd = sw128_desc(sb + (uint32_t)c * 128u + ks * 32);
-                                mma_bf16(dcol + (uint32_t)c, ad, bd, idesc_bf16(n), (kb | ks) != 0);
+                                const uint32_t idesc = instr_desc<TF32>(n);
+                                const uint64_t bd = operand_desc<TF32>(sb + (uint32_t)c * KD::ROW + ko);
+                                const uint32_t acc_on = (kb | ks) != 0;
+                                if (TF32) {
+                                    const uint64_t adl = operand_desc<TF32>(sa + KD::A_TILE + ko);
+                                    const uint64_t bdl = operand_desc<TF32>(sb + b_part + (uint32_t)c * KD::ROW + ko);
+                                    mma<TF32>(dcol + (uint32_t)c, adl, bd, idesc, acc_on);   // A_lo B_hi
+                                    mma<TF32>(dcol + (uint32_t)c, ad, bdl, idesc, 1u);      // A_hi B_lo
+                                    mma<TF32>(dcol + (uint32_t)c, ad, bd, idesc, 1u);       // A_hi B_hi
+                                } else {
+                                    mma<TF32>(dcol + (uint32_t)c, ad, bd, idesc, acc_on);
+                                }
                             }
                         }
                         mma_commit(empty_bar(stage));
@@ -372,59 +422,70 @@ static PFN_encodeTiled get_encode() {
     return fn;
 }
 
-// 2-D bf16 tensor [rows, cols] (cols contiguous, row pitch in elements), box [box_rows, 64].
-static bool make_map(CUtensorMap* m, const void* base, int64_t rows, int64_t cols, int64_t pitch, int box_rows) {
+// 2-D tensor [rows, cols] (cols contiguous, row pitch in elements) of bf16 or
+// fp32, box [box_rows, one swizzled row] with 128B (bf16) or 64B (fp32) swizzle.
+static bool make_map(CUtensorMap* m, const void* base, int64_t rows, int64_t cols, int64_t pitch, int box_rows,
+                     bool f32) {
     PFN_encodeTiled enc = get_encode();
     if (!enc) return false;
-    if ((reinterpret_cast<uintptr_t>(base) & 15) || ((pitch * 2) & 15) || box_rows < 8 || box_rows > 256 ||
+    const int64_t esz = f32 ? 4 : 2;
+    if ((reinterpret_cast<uintptr_t>(base) & 15) || ((pitch * esz) & 15) || box_rows < 8 || box_rows > 256 ||
         (box_rows & 7))
         return false;
     cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)(pitch * 2)};
-    cuuint32_t box[2] = {64u, (cuuint32_t)box_rows};
+    cuuint64_t strides[1] = {(cuuint64_t)(pitch * esz)};
+    cuuint32_t box[2] = {f32 ? 16u : 64u, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1u, 1u};
-    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
-               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+    return enc(m, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base),
+               dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               f32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-TcPlan tc_plan(int T) {
+TcPlan tc_plan(int T, bool tf32) {
     TcPlan p{};
     p.Tpad = (T + 15) / 16 * 16;
     const int np0 = std::min(tc::MAX_NP, p.Tpad);
-    if (np0 <= 256) {
-        p.box_rows = np0;
-    } else {
-        p.box_rows = ((np0 + 1) / 2 + 7) / 8 * 8;
-    }
-    // largest pass rounded up to whole boxes
-    int b_rows = 0;
+    p.box_rows = (np0 <= 256) ? np0 : ((np0 + 1) / 2 + 7) / 8 * 8;
+    int b_rows = 0;  // largest pass rounded up to whole boxes
     for (int off = 0; off < p.Tpad; off += tc::MAX_NP) {
         const int np = std::min(tc::MAX_NP, p.Tpad - off);
         b_rows = std::max(b_rows, (np + p.box_rows - 1) / p.box_rows * p.box_rows);
     }
     p.b_rows = b_rows;
-    const size_t stage = tc::A_BYTES + (size_t)b_rows * 128;
-    const size_t budget = 220 * 1024 - 1024 - 64 - 8 * (size_t)p.Tpad;
+    const size_t row = tf32 ? 64 : 128, parts = tf32 ? 2 : 1;
+    const size_t stage = parts * (tc::BM * row + (size_t)b_rows * row);
+    const size_t tail = 8 * (2 * 4 + 5) + 16 + 8 * (size_t)p.Tpad;
+    const size_t budget = 227 * 1024 - 1024 - tail;
     p.stages = (int)std::min<size_t>(4, budget / stage);
     p.nacc = (np0 <= 256) ? 2 : 1;
     p.smem = 1024 + (size_t)p.stages * stage + 8 * (2 * p.stages + 5) + 16 + 8 * (size_t)p.Tpad;
+    p.kblock = tf32 ? 16 : 64;
     return p;
 }
 
-cudaError_t launch_score_tc(const __nv_bfloat16* B0T, int64_t ldk, int N, const __nv_bfloat16* Up, int T, int CKpad,
-                            const float* nm, float* Bout, int64_t ldb, float* cfmax, int32_t* imax, int nt,
-                            int32_t* status, int grid, cudaStream_t s) {
-    const TcPlan p = tc_plan(T);
-    if (p.stages < 2 || CKpad % tc::BK) return cudaErrorInvalidValue;
-    CUtensorMap ma, mb;
-    if (!make_map(&ma, B0T, N, CKpad, ldk, tc::BM) || !make_map(&mb, Up, p.Tpad, CKpad, CKpad, p.box_rows))
+template <bool TF32>
+static cudaError_t launch_tc(const void* A, const void* Alo, int64_t ldk, int N, const void* Bm, const void* Blo, int T,
+                             int CKpad, const float* nm, float* Bout, int64_t ldb, float* cfmax, int32_t* imax, int nt,
+                             int32_t* status, int grid, cudaStream_t s) {
+    const TcPlan p = tc_plan(T, TF32);
+    if (p.stages < 2 || CKpad % p.kblock) return cudaErrorInvalidValue;
+    CUtensorMap ma, malo, mb, mblo;
+    if (!make_map(&ma, A, N, CKpad, ldk, tc::BM, TF32) || !make_map(&mb, Bm, p.Tpad, CKpad, CKpad, p.box_rows, TF32))
         return cudaErrorInvalidValue;
+    if (TF32) {
+        if (!make_map(&malo, Alo, N, CKpad, ldk, tc::BM, true) ||
+            !make_map(&mblo, Blo, p.Tpad, CKpad, CKpad, p.box_rows, true))
+            return cudaErrorInvalidValue;
+    } else {
+        malo = ma;
+        mblo = mb;
+    }
     tc::Args a{};
     a.N = N;
     a.T = T;
     a.Tpad = p.Tpad;
-    a.KB = CKpad / tc::BK;
+    a.KB = CKpad / p.kblock;
     a.box_rows = p.box_rows;
     a.stages = p.stages;
     a.b_rows = p.b_rows;
@@ -436,11 +497,24 @@ cudaError_t launch_score_tc(const __nv_bfloat16* B0T, int64_t ldk, int N, const 
     a.imax = imax;
     a.nt = nt;
     a.status = status;
-    cudaError_t e = cudaFuncSetAttribute(tc::k_score_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
+    cudaError_t e = cudaFuncSetAttribute(tc::k_score_tc<TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
     if (e != cudaSuccess) return e;
     const int ntiles = (N + tc::BM - 1) / tc::BM;
-    tc::k_score_tc<<<std::min(grid, ntiles), tc::THREADS, p.smem, s>>>(ma, mb, a);
+    tc::k_score_tc<TF32><<<std::min(grid, ntiles), tc::THREADS, p.smem, s>>>(ma, malo, mb, mblo, a);
     return cudaGetLastError();
+}
+
+cudaError_t launch_score_tc(const __nv_bfloat16* B0T, int64_t ldk, int N, const __nv_bfloat16* Up, int T, int CKpad,
+                            const float* nm, float* Bout, int64_t ldb, float* cfmax, int32_t* imax, int nt,
+                            int32_t* status, int grid, cudaStream_t s) {
+    return launch_tc<false>(B0T, nullptr, ldk, N, Up, nullptr, T, CKpad, nm, Bout, ldb, cfmax, imax, nt, status, grid, s);
+}
+
+cudaError_t launch_score_tc_tf32x3(const float* B0T_hi, const float* B0T_lo, int64_t ldk, int N, const float* Up_hi,
+                                   const float* Up_lo, int T, int CKpad, const float* nm, float* Bout, int64_t ldb,
+                                   float* cfmax, int32_t* imax, int nt, int32_t* status, int grid, cudaStream_t s) {
+    return launch_tc<true>(B0T_hi, B0T_lo, ldk, N, Up_hi, Up_lo, T, CKpad, nm, Bout, ldb, cfmax, imax, nt, status, grid,
+                           s);
 }
 
 }  // namespace lss
