@@ -11,6 +11,8 @@
 //   times of batch 0 (template_matching.py:53-68), in run_matching order.
 #include "lss_kernels.cuh"
 
+#include <algorithm>
+
 namespace lss {
 
 constexpr int XR_COLS = 128;
@@ -139,60 +141,74 @@ cudaError_t launch_pc_features(const float* Xres, int64_t ldx, int32_t nt, int32
     return cudaGetLastError();
 }
 
-// Single-CTA ordered compaction of the batch's spikes into caller records.
-__global__ void __launch_bounds__(1024) k_records(const int32_t* __restrict__ sp_x,
-                                                  const int32_t* __restrict__ sp_y,
-                                                  const float* __restrict__ sp_amp,
-                                                  const float* __restrict__ tF, int32_t n, int32_t feat_len,
-                                                  int64_t ibatch, int32_t nt, int32_t NT, int32_t nt0min,
-                                                  int64_t* out_time, int32_t* out_tmpl, float* out_amp,
-                                                  float* out_pc, int64_t capacity, int64_t* out_count) {
-    __shared__ int scan[1024];
-    __shared__ int64_t s_base;
+// Records: one CTA computes every kept spike's output slot with ballot scans
+// (only batch 0 drops spikes, those aligned before the recording start), then
+// a grid writes the slots and their PC features in parallel.
+__global__ void __launch_bounds__(1024) k_records_scan(const int32_t* __restrict__ sp_x, int32_t n, int64_t ibatch,
+                                                       int32_t nt, int32_t nt0min, int32_t* __restrict__ slot,
+                                                       int64_t* out_count) {
+    __shared__ int wsum[32];
+    __shared__ int s_base;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) s_base = 0;
     __syncthreads();
     for (int c0 = 0; c0 < n; c0 += 1024) {
         const int i = c0 + threadIdx.x;
-        int keep = 0;
-        int64_t t = 0;
-        if (i < n) {
-            const int x = sp_x[i];
-            keep = !(ibatch == 0 && (x - nt - nt / 2 + nt0min) < 0);
-            t = (int64_t)(x - nt) + ibatch * (int64_t)NT - nt / 2 + nt0min;
-        }
-        scan[threadIdx.x] = keep;
+        bool keep = false;
+        if (i < n) keep = !(ibatch == 0 && (sp_x[i] - nt - nt / 2 + nt0min) < 0);
+        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0) wsum[warp] = __popc(bal);
         __syncthreads();
-        for (int off = 1; off < 1024; off <<= 1) {
-            const int v = (threadIdx.x >= off) ? scan[threadIdx.x - off] : 0;
-            __syncthreads();
-            scan[threadIdx.x] += v;
-            __syncthreads();
-        }
-        if (keep) {
-            const int64_t o = s_base + scan[threadIdx.x] - 1;
-            if (o < capacity) {
-                out_time[o] = t;
-                out_tmpl[o] = sp_y[i];
-                out_amp[o] = sp_amp[i];
-                if (out_pc && tF)
-                    for (int f = 0; f < feat_len; ++f) out_pc[o * feat_len + f] = tF[(int64_t)i * feat_len + f];
+        if (warp == 0) {
+            const int c = wsum[lane];
+            int inc = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int u = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o) inc += u;
             }
+            wsum[lane] = inc - c;
         }
         __syncthreads();
-        if (threadIdx.x == 1023) s_base += scan[1023];
+        if (i < n) slot[i] = keep ? s_base + wsum[warp] + __popc(bal & ((1u << lane) - 1u)) : -1;
+        __syncthreads();
+        if (threadIdx.x == 1023) s_base += wsum[31] + __popc(bal);
         __syncthreads();
     }
     if (threadIdx.x == 0) *out_count = s_base;
 }
 
+__global__ void k_records_write(const int32_t* __restrict__ sp_x, const int32_t* __restrict__ sp_y,
+                                const float* __restrict__ sp_amp, const float* __restrict__ tF,
+                                const int32_t* __restrict__ slot, int32_t n, int32_t feat_len, int64_t ibatch,
+                                int32_t nt, int32_t NT, int32_t nt0min, int64_t* out_time, int32_t* out_tmpl,
+                                float* out_amp, float* out_pc, int64_t capacity) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int row = 3 + feat_len;  // time, template, amplitude, features
+    const int64_t i = e / row;
+    const int f = (int)(e % row);
+    if (i >= n) return;
+    const int o = slot[i];
+    if (o < 0 || o >= capacity) return;
+    if (f == 0) out_time[o] = (int64_t)(sp_x[i] - nt) + ibatch * (int64_t)NT - nt / 2 + nt0min;
+    else if (f == 1) out_tmpl[o] = sp_y[i];
+    else if (f == 2) out_amp[o] = sp_amp[i];
+    else if (out_pc && tF) out_pc[(int64_t)o * feat_len + (f - 3)] = tF[i * feat_len + (f - 3)];
+}
+
 cudaError_t launch_records(const int32_t* sp_x, const int32_t* sp_y, const float* sp_amp, const float* tF,
-                           const int32_t* counters, int32_t n, int32_t feat_len, int64_t ibatch, int32_t nt,
+                           int32_t* slot, int32_t n, int32_t feat_len, int64_t ibatch, int32_t nt,
                            int32_t NT, int32_t nt0min, int64_t* out_time, int32_t* out_tmpl,
                            float* out_amp, float* out_pc, int64_t capacity, int64_t* out_count,
                            cudaStream_t s) {
-    (void)counters;
-    k_records<<<1, 1024, 0, s>>>(sp_x, sp_y, sp_amp, tF, n, feat_len, ibatch, nt, NT, nt0min, out_time,
-                                 out_tmpl, out_amp, out_pc, capacity, out_count);
+    k_records_scan<<<1, 1024, 0, s>>>(sp_x, n, ibatch, nt, nt0min, slot, out_count);
+    const int64_t total = (int64_t)n * (3 + (tF ? feat_len : 0));
+    if (total > 0) {
+        k_records_write<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(sp_x, sp_y, sp_amp, tF, slot, n,
+                                                                        tF ? feat_len : 0, ibatch, nt, NT, nt0min,
+                                                                        out_time, out_tmpl, out_amp,
+                                                                        tF ? out_pc : nullptr, capacity);
+    }
     return cudaGetLastError();
 }
 
@@ -209,6 +225,209 @@ cudaError_t launch_st_out(const int32_t* sp_x, const int32_t* sp_y, const float*
                           int64_t* st, float* amps, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
     k_st_out<<<(n + 255) / 256, 256, 0, s>>>(sp_x, sp_y, sp_amp, n, st, amps);
+    return cudaGetLastError();
+}
+
+
+
+// ---------------------------------------------------------------------------
+// PC features without a residual array (used by lss_sort_batch, where the
+// whitening is folded into the templates). With Xh the highpassed batch and
+// Mw = M @ Wrot, Kilosort's
+//   xfeat[i, j, k] = sum_m Xres[ch, x_i + m - nt/2] * wPCA[k, m] + amp_i * Ucc[j, y_i, k]
+// (template_matching.py:50-51, ch = iCC[j, iU[y_i]]) is evaluated as
+//   sum_c' Mw[ch, c'] * sum_m wPCA[k, m] Xh[c', x_i + m - nt/2]
+//   - sum_{spikes i', |x_i - x_i'| < nt} amp_i' * sum_k' U[y_i', k', ch] * R[k, k', x_i - x_i']
+//   + amp_i * Ucc[j, y_i, k]
+// with R[k, k', d] = sum_m wPCA[k, m] wPCA[k', m + d] (the waveform of spike i'
+// projected on the basis at lag d). Same linear algebra, different order.
+// One CTA per spike; channels are staged 64 at a time.
+// ---------------------------------------------------------------------------
+constexpr int FT_CH = 64;
+constexpr int FT_LIST = 512;
+constexpr int FT_NQ = 32;  // neighbours per staged chunk
+
+__global__ void __launch_bounds__(256) k_pc_features_folded(
+    const float* __restrict__ Xh, int64_t ldx, int32_t C, int32_t nt, int32_t K, int32_t nC, int32_t T,
+    const float* __restrict__ wpca, const float* __restrict__ Mw, const float* __restrict__ U,
+    const float* __restrict__ R, const int64_t* __restrict__ iCC, const int64_t* __restrict__ iU,
+    const float* __restrict__ Ucc, const int32_t* __restrict__ sp_x, const int32_t* __restrict__ sp_y,
+    const float* __restrict__ sp_amp, const int32_t* __restrict__ round_start, int32_t rounds,
+    float* __restrict__ tF, int32_t* status, const float* __restrict__ Phi, const float* __restrict__ Plo,
+    int64_t ldp) {
+    extern __shared__ float sm[];
+    const int ntp = nt + 1;
+    float* ws = sm;                          // [K][nt]
+    float* xs = ws + K * nt;                 // [FT_CH][ntp]
+    float* pc = xs + FT_CH * ntp;            // [FT_CH][K]
+    float* mw = pc + FT_CH * K;              // [nC][FT_CH]
+    // the projection-row path reuses the front of the buffer (see below)
+    const int front = max(K * nt + FT_CH * ntp + FT_CH * K + nC * FT_CH, C * K + nC * C + 4 * nC * K);
+    float* acc = sm + front;                 // [nC*K]
+    __shared__ int s_ch[64];
+    __shared__ int l_x[FT_LIST], l_y[FT_LIST];
+    __shared__ float l_a[FT_LIST];
+    __shared__ int s_n;
+    __shared__ int s_cnt[256];
+    const int i = blockIdx.x;
+    const int x = sp_x[i], y = sp_y[i];
+    const int h = nt / 2;
+    for (int e = threadIdx.x; e < K * nt; e += blockDim.x) ws[e] = wpca[e];
+    if (threadIdx.x < nC) s_ch[threadIdx.x] = (int)iCC[(int64_t)threadIdx.x * C + iU[y]];
+    for (int e = threadIdx.x; e < nC * K; e += blockDim.x) acc[e] = 0.f;
+    if (threadIdx.x == 0) s_n = 0;
+    __syncthreads();
+    // neighbours (any round, round order) whose waveform window overlaps this
+    // spike's window; rounds are scanned blockDim.x at a time
+    for (int rb = 0; rb < rounds; rb += blockDim.x) {
+        const int r = rb + threadIdx.x;
+        int lo = 0, cnt = 0;
+        if (r < rounds) {
+            const int b = round_start[r + 1];
+            int hi2 = b;
+            lo = round_start[r];
+            while (lo < hi2) {
+                const int m = (lo + hi2) >> 1;
+                if (sp_x[m] <= x - nt) lo = m + 1; else hi2 = m;
+            }
+            int e = lo;
+            while (e < b && sp_x[e] < x + nt) ++e;
+            cnt = e - lo;
+        }
+        s_cnt[threadIdx.x] = cnt;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int o = s_n;
+            for (int q = 0; q < (int)blockDim.x; ++q) {
+                const int c = s_cnt[q];
+                s_cnt[q] = o;
+                o += c;
+            }
+            s_n = o;
+        }
+        __syncthreads();
+        for (int q = 0; q < cnt; ++q) {
+            const int slot = s_cnt[threadIdx.x] + q;
+            if (slot < FT_LIST) {
+                l_x[slot] = sp_x[lo + q];
+                l_y[slot] = sp_y[lo + q];
+                l_a[slot] = sp_amp[lo + q];
+            }
+        }
+        __syncthreads();
+    }
+    if (Phi) {
+        // the spike's projection row P[x, :] = hi + lo and the nC rows of Mw,
+        // then each (j, k) dot product split over 4 threads, combined in order
+        float* prow = sm;                  // [C*K]
+        float* mwr = prow + C * K;         // [nC][C]
+        float* red = mwr + nC * C;         // [4*nC*K]
+        __syncthreads();
+        const int64_t o = (int64_t)x * ldp;
+        for (int e = threadIdx.x; e < C * K; e += blockDim.x) prow[e] = __fadd_rn(Phi[o + e], Plo[o + e]);
+        for (int e = threadIdx.x; e < nC * C; e += blockDim.x) {
+            const int j = e / C, c = e % C;
+            mwr[e] = Mw[(int64_t)s_ch[j] * C + c];
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < 4 * nC * K; e += blockDim.x) {
+            const int f = e >> 2, part = e & 3;
+            const int j = f / K, k = f % K;
+            float v = 0.f;
+            for (int c = part; c < C; c += 4) v = fmaf(mwr[j * C + c], prow[c * K + k], v);
+            red[e] = v;
+        }
+        __syncthreads();
+        for (int f = threadIdx.x; f < nC * K; f += blockDim.x)
+            acc[f] = __fadd_rn(__fadd_rn(red[4 * f], red[4 * f + 1]), __fadd_rn(red[4 * f + 2], red[4 * f + 3]));
+    }
+    for (int c0 = 0; c0 < (Phi ? 0 : C); c0 += FT_CH) {
+        const int nc = min(FT_CH, C - c0);
+        __syncthreads();
+        if (Phi) {
+            // projection row of the score GEMM: P[x, c*K + k] = hi + lo
+            const int64_t o = (int64_t)x * ldp + (int64_t)c0 * K;
+            for (int e = threadIdx.x; e < nc * K; e += blockDim.x) pc[e] = __fadd_rn(Phi[o + e], Plo[o + e]);
+        } else {
+            for (int e = threadIdx.x; e < nc * nt; e += blockDim.x) {
+                const int c = e / nt, m = e % nt;
+                xs[c * ntp + m] = Xh[(int64_t)(c0 + c) * ldx + x - h + m];
+            }
+        }
+        for (int e = threadIdx.x; e < nC * nc; e += blockDim.x) {
+            const int j = e / nc, c = e % nc;
+            mw[j * FT_CH + c] = Mw[(int64_t)s_ch[j] * C + c0 + c];
+        }
+        __syncthreads();
+        if (!Phi) {
+            for (int e = threadIdx.x; e < nc * K; e += blockDim.x) {
+                const int c = e / K, k = e % K;
+                float p = 0.f;
+                for (int m = 0; m < nt; ++m) p = fmaf(ws[k * nt + m], xs[c * ntp + m], p);
+                pc[c * K + k] = p;
+            }
+            __syncthreads();
+        }
+        for (int e = threadIdx.x; e < nC * K; e += blockDim.x) {
+            const int j = e / K, k = e % K;
+            float v = acc[e];
+            for (int c = 0; c < nc; ++c) v = fmaf(mw[j * FT_CH + c], pc[c * K + k], v);
+            acc[e] = v;
+        }
+    }
+    __syncthreads();
+    const int nl = min(s_n, FT_LIST);
+    if (threadIdx.x == 0 && s_n > FT_LIST) atomicOr(status, STATUS_LIST);
+    // neighbours' projected waveforms, FT_NQ at a time:
+    //   contrib[q][j][k] = sum_k' U[y_q, k', ch_j] * R[k, k', x - x_q]
+    // all loads of a chunk are independent, then each (j, k) sums its column
+    // over q in list order
+    float* contrib = acc + nC * K;  // [FT_NQ][nC*K]
+    const int F = nC * K;
+    const int nd = 2 * nt - 1;
+    float v = 0.f;
+    const int e_own = threadIdx.x;  // (j, k) owned by this thread when < F
+    if (e_own < F) v = acc[e_own];
+    for (int q0 = 0; q0 < nl; q0 += FT_NQ) {
+        const int nq = min(FT_NQ, nl - q0);
+        __syncthreads();
+        for (int task = threadIdx.x; task < nq * F; task += blockDim.x) {
+            const int q = task / F, f = task % F;
+            const int j = f / K, k = f % K;
+            const int d = x - l_x[q0 + q];
+            const float* rk = R + ((int64_t)k * K) * nd + (d + nt - 1);
+            const float* uy = U + (int64_t)l_y[q0 + q] * K * C + s_ch[j];
+            float sub = 0.f;
+            for (int kk = 0; kk < K; ++kk) sub = fmaf(__ldg(uy + (int64_t)kk * C), __ldg(rk + (int64_t)kk * nd), sub);
+            contrib[q * F + f] = sub;
+        }
+        __syncthreads();
+        if (e_own < F)
+            for (int q = 0; q < nq; ++q) v = __fsub_rn(v, __fmul_rn(l_a[q0 + q], contrib[q * F + e_own]));
+    }
+    if (e_own < F) {
+        const int j = e_own / K, k = e_own % K;
+        v = __fadd_rn(v, __fmul_rn(sp_amp[i], Ucc[((int64_t)j * T + y) * K + k]));
+        tF[(int64_t)i * F + e_own] = v;
+    }
+}
+
+cudaError_t launch_pc_features_folded(const float* Xh, int64_t ldx, int32_t C, int32_t nt, int32_t K, int32_t nC,
+                                      int32_t T, const float* wpca, const float* Mw, const float* U, const float* R,
+                                      const int64_t* iCC, const int64_t* iU, const float* Ucc, const int32_t* sp_x,
+                                      const int32_t* sp_y, const float* sp_amp, const int32_t* round_start,
+                                      int32_t rounds, int32_t n, float* tF, int32_t* status, const float* Phi,
+                                      const float* Plo, int64_t ldp, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    if (nC * K > 256) return cudaErrorInvalidValue;  // one (j, k) per thread
+    const size_t front = std::max<size_t>((size_t)K * nt + (size_t)FT_CH * (nt + 1) + (size_t)FT_CH * K +
+                                              (size_t)nC * FT_CH,
+                                          (size_t)C * K + (size_t)nC * C + 4 * (size_t)nC * K);
+    const size_t smem = sizeof(float) * (front + (size_t)nC * K + (size_t)FT_NQ * nC * K);
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(k_pc_features_folded, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_pc_features_folded<<<n, 256, smem, s>>>(Xh, ldx, C, nt, K, nC, T, wpca, Mw, U, R, iCC, iU, Ucc, sp_x, sp_y,
+                                              sp_amp, round_start, rounds, tF, status, Phi, Plo, ldp);
     return cudaGetLastError();
 }
 

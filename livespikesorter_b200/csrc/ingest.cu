@@ -63,9 +63,11 @@ __device__ __forceinline__ float unkey(uint32_t k) {
 
 // CAR tile: 32 time columns x C channels staged in shared memory. Each warp
 // finds the lower median (sorted index (C-1)/2, torch.median's choice) of a
-// column by a 32-step bitwise select on order-preserving keys, then the tile
-// is written back as 128-byte channel rows.
+// column by a 32-step bitwise select on order-preserving keys held in
+// registers (NQ = keys per lane >= C/32; padding keys are the largest value),
+// then the tile is written back as 128-byte channel rows.
 constexpr int CAR_COLS = 32;
+template <int NQ>
 __global__ void __launch_bounds__(256) k_car(const int16_t* __restrict__ raw, int32_t ld_raw,
                                              const int32_t* __restrict__ chan_map, int32_t C,
                                              int64_t N, IngestMap map, float sign,
@@ -97,11 +99,18 @@ __global__ void __launch_bounds__(256) k_car(const int16_t* __restrict__ raw, in
     if (do_car) {
         const uint32_t kth = (uint32_t)((C - 1) / 2);
         for (int j = warp; j < ncol; j += blockDim.x >> 5) {
+            uint32_t key[NQ];
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) {
+                const int c = lane + 32 * q;
+                key[q] = (c < C) ? fkey(tile[c * (CAR_COLS + 1) + j]) : 0xFFFFFFFFu;
+            }
             uint32_t res = 0;
             for (int b = 31; b >= 0; --b) {
                 const uint32_t trial = res | ((1u << b) - 1u);
                 uint32_t cnt = 0;
-                for (int c = lane; c < C; c += 32) cnt += (fkey(tile[c * (CAR_COLS + 1) + j]) <= trial);
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) cnt += (key[q] <= trial);
                 cnt = __reduce_add_sync(0xffffffffu, cnt);
                 if (cnt < kth + 1) res |= (1u << b);
             }
@@ -120,18 +129,28 @@ __global__ void __launch_bounds__(256) k_car(const int16_t* __restrict__ raw, in
     }
 }
 
+template <int NQ>
+static cudaError_t launch_car_t(const int16_t* raw, int32_t ld_raw, const int32_t* chan_map, int32_t C, int64_t N,
+                                IngestMap map, float sign, const long long* sums, int do_car, float* X1, int64_t ldx,
+                                cudaStream_t s) {
+    const size_t smem = sizeof(float) * ((size_t)C * (CAR_COLS + 1) + C + CAR_COLS);
+    cudaFuncSetAttribute(k_car<NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    const int grid = (int)((N + CAR_COLS - 1) / CAR_COLS);
+    k_car<NQ><<<grid, 256, smem, s>>>(raw, ld_raw, chan_map, C, N, map, sign, sums, do_car, X1, ldx);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_car(const int16_t* raw, int32_t ld_raw, const int32_t* chan_map, int32_t C, int64_t N,
                        IngestMap map, float sign, const long long* sums, int do_car, float* X1,
                        int64_t ldx, cudaStream_t s) {
-    const size_t smem = sizeof(float) * ((size_t)C * (CAR_COLS + 1) + C + CAR_COLS);
-    static bool attr_done = false;
-    if (!attr_done) {
-        cudaFuncSetAttribute(k_car, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        attr_done = true;
-    }
-    const int grid = (int)((N + CAR_COLS - 1) / CAR_COLS);
-    k_car<<<grid, 256, smem, s>>>(raw, ld_raw, chan_map, C, N, map, sign, sums, do_car, X1, ldx);
-    return cudaGetLastError();
+    const int nq = (C + 31) / 32;
+    if (nq <= 2) return launch_car_t<2>(raw, ld_raw, chan_map, C, N, map, sign, sums, do_car, X1, ldx, s);
+    if (nq <= 4) return launch_car_t<4>(raw, ld_raw, chan_map, C, N, map, sign, sums, do_car, X1, ldx, s);
+    if (nq <= 8) return launch_car_t<8>(raw, ld_raw, chan_map, C, N, map, sign, sums, do_car, X1, ldx, s);
+    if (nq <= 12) return launch_car_t<12>(raw, ld_raw, chan_map, C, N, map, sign, sums, do_car, X1, ldx, s);
+    if (nq <= 16) return launch_car_t<16>(raw, ld_raw, chan_map, C, N, map, sign, sums, do_car, X1, ldx, s);
+    if (nq <= 24) return launch_car_t<24>(raw, ld_raw, chan_map, C, N, map, sign, sums, do_car, X1, ldx, s);
+    return launch_car_t<32>(raw, ld_raw, chan_map, C, N, map, sign, sums, do_car, X1, ldx, s);
 }
 
 // Circular highpass: Xh[c, i] = sum_{d=-L..L} taps[d+L] * X1[c, (i+d) mod N].

@@ -21,7 +21,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/lss.h"
+#include "lss.h"
 #include "lss_kernels.cuh"
 #include "npy.h"
 
@@ -81,11 +81,14 @@ struct lss_handle {
     DevBuf<unsigned long long> colkey;
     DevBuf<__nv_bfloat16> B0T, Up16;   // BF16 path: transposed projection, templates
     DevBuf<float> B0T_hi, B0T_lo, Up_hi, Up_lo;  // FP32 path (3xTF32): tf32 hi/lo splits
+    DevBuf<__nv_bfloat16> Uw16;                  // templates with the whitening folded in (BF16 path)
+    DevBuf<float> Uw_hi, Uw_lo;                  // ... (FP32 path)
+    DevBuf<float> U, R;                          // U [T,K,C]; R [K,K,2nt-1] basis lag correlations
     int CKpad = 0;
     int sm_count = 0;
     DevBuf<unsigned int> bar;
     DevBuf<int64_t> rec_time, rec_count;
-    DevBuf<int32_t> rec_tmpl;
+    DevBuf<int32_t> rec_tmpl, rec_slot;
     DevBuf<float> rec_amp, rec_pc;
 
     int fail(int code, const std::string& m) {
@@ -107,9 +110,10 @@ struct lss_handle {
         tF.release(); iCC.release(); iU.release(); cfmax.release(); imax.release(); blk_cnt.release();
         blk_x.release(); blk_y.release(); sp_x.release(); sp_y.release(); sp_round.release();
         round_start.release(); counters.release(); status.release(); sp_amp.release(); blk_amp.release(); colkey.release();
-        bar.release(); rec_time.release(); rec_count.release(); rec_tmpl.release(); rec_amp.release();
+        bar.release(); rec_time.release(); rec_count.release(); rec_tmpl.release(); rec_slot.release(); rec_amp.release();
         rec_pc.release(); B0T.release(); Up16.release();
         B0T_hi.release(); B0T_lo.release(); Up_hi.release(); Up_lo.release();
+        Uw16.release(); Uw_hi.release(); Uw_lo.release(); U.release(); R.release();
     }
 };
 
@@ -172,10 +176,15 @@ static int set_mixing(lss_handle* h, const float* M) {
     const int C = h->C;
     if (!M) {
         CK(cudaMemcpy(h->Mw.p, h->Wrot.p, (size_t)C * C * sizeof(float), cudaMemcpyDeviceToDevice));
-        return LSS_OK;
+    } else {
+        CK(cudaMemcpy(h->Mdrift.p, M, (size_t)C * C * sizeof(float), cudaMemcpyHostToDevice));
+        CK(launch_sgemm(h->Mdrift.p, C, h->Wrot.p, C, h->Mw.p, C, C, C, C, 0));
+        h->stats.launches += 1;
     }
-    CK(cudaMemcpy(h->Mdrift.p, M, (size_t)C * C * sizeof(float), cudaMemcpyHostToDevice));
-    CK(launch_sgemm(h->Mdrift.p, C, h->Wrot.p, C, h->Mw.p, C, C, C, C, 0));
+    // templates with the whitening folded in, for lss_sort_batch
+    const bool bf16 = h->cfg.precision == LSS_PREC_BF16_RECHECK;
+    CK(launch_build_uw(h->U.p, h->Mw.p, h->T, h->K, C, h->CKpad, bf16 ? h->Uw16.p : nullptr,
+                       bf16 ? nullptr : h->Uw_hi.p, bf16 ? nullptr : h->Uw_lo.p, 0));
     h->stats.launches += 1;
     return LSS_OK;
 }
@@ -191,7 +200,7 @@ static int validate(const lss_config* c, std::string& err) {
     if (c->nt > 255) { err = "nt > 255 is not supported"; return LSS_ERR_ARG; }
     if (c->n_chan_bin < c->n_chan) { err = "n_chan_bin < n_chan"; return LSS_ERR_ARG; }
     if (c->n_nearest < 0 || c->n_nearest > c->n_chan) { err = "n_nearest out of range"; return LSS_ERR_ARG; }
-    if (c->n_nearest * c->n_pcs > 1024) { err = "n_nearest * n_pcs > 1024"; return LSS_ERR_ARG; }
+    if (c->n_nearest * c->n_pcs > 256) { err = "n_nearest * n_pcs > 256"; return LSS_ERR_ARG; }
     if (c->max_rounds <= 0 || c->max_rounds > 1000) { err = "max_rounds must be in 1..1000"; return LSS_ERR_ARG; }
     if (c->max_spikes <= 0) { err = "max_spikes must be positive"; return LSS_ERR_ARG; }
     if (c->precision != LSS_PREC_FP32 && c->precision != LSS_PREC_BF16_RECHECK) {
@@ -331,12 +340,17 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
     if (bf16) {
         ALLOC(B0T, (size_t)h->N * h->CKpad);
         ALLOC(Up16, (size_t)plan.Tpad * h->CKpad);
+        ALLOC(Uw16, (size_t)plan.Tpad * h->CKpad);
     } else {
         ALLOC(B0T_hi, (size_t)h->N * h->CKpad);
         ALLOC(B0T_lo, (size_t)h->N * h->CKpad);
         ALLOC(Up_hi, (size_t)plan.Tpad * h->CKpad);
         ALLOC(Up_lo, (size_t)plan.Tpad * h->CKpad);
+        ALLOC(Uw_hi, (size_t)plan.Tpad * h->CKpad);
+        ALLOC(Uw_lo, (size_t)plan.Tpad * h->CKpad);
     }
+    ALLOC(U, (size_t)T * K * C);
+    ALLOC(R, (size_t)K * K * (2 * nt - 1));
     ALLOC(B, (size_t)T * ld);
     ALLOC(nm, T);
     ALLOC(ctcP, (size_t)T * T * L2);
@@ -364,6 +378,7 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
     ALLOC(bar, 2);
     ALLOC(rec_time, cap);
     ALLOC(rec_tmpl, cap);
+    ALLOC(rec_slot, cap);
     ALLOC(rec_amp, cap);
     ALLOC(rec_pc, (size_t)cap * std::max(nC * K, 1));
     ALLOC(rec_count, 1);
@@ -412,6 +427,28 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
     CK(cudaMemcpy(h->nm.p, nmv.data(), T * sizeof(float), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->wave.p, wave.data(), wave.size() * sizeof(float), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->wpca.p, t->wpca, (size_t)K * nt * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->U.p, t->wall3, (size_t)T * K * C * sizeof(float), cudaMemcpyHostToDevice));
+    {
+        // R[k, k', d] = sum_m wPCA[k, m] * wPCA[k', m + d], d = -(nt-1) .. nt-1
+        const int nd = 2 * nt - 1;
+        std::vector<float> r((size_t)K * K * nd);
+        for (int k = 0; k < K; ++k)
+            for (int k2 = 0; k2 < K; ++k2)
+                for (int d = -(nt - 1); d <= nt - 1; ++d) {
+                    double acc = 0.0;
+                    for (int m = 0; m < nt; ++m)
+                        if (m + d >= 0 && m + d < nt)
+                            acc += (double)t->wpca[(size_t)k * nt + m] * t->wpca[(size_t)k2 * nt + m + d];
+                    r[((size_t)k * K + k2) * nd + (d + nt - 1)] = (float)acc;
+                }
+        CK(cudaMemcpy(h->R.p, r.data(), r.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    if (bf16) {
+        CK(cudaMemset(h->Uw16.p, 0, (size_t)plan.Tpad * h->CKpad * sizeof(__nv_bfloat16)));
+    } else {
+        CK(cudaMemset(h->Uw_hi.p, 0, (size_t)plan.Tpad * h->CKpad * sizeof(float)));
+        CK(cudaMemset(h->Uw_lo.p, 0, (size_t)plan.Tpad * h->CKpad * sizeof(float)));
+    }
     if (nC > 0) {
         CK(cudaMemcpy(h->Ucc.p, t->Ucc, (size_t)nC * T * K * sizeof(float), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(h->iCC.p, t->iCC, (size_t)nC * C * sizeof(int64_t), cudaMemcpyHostToDevice));
@@ -451,8 +488,10 @@ int lss_set_drift(lss_handle* h, const float* M) {
 }  // extern "C"
 
 // ---------------------------------------------------------------- stages
+// Ingest of one padded batch. Xout (may be null) receives the whitened,
+// drift-corrected batch; *pre_out the highpassed batch before whitening.
 static int run_filter(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ibatch, int64_t n_batches,
-                      int32_t raw_on_device, float* Xout, cudaStream_t s) {
+                      int32_t raw_on_device, float* Xout, cudaStream_t s, const float** pre_out = nullptr) {
     if (!raw || n_rows <= 0) return h->fail(LSS_ERR_ARG, "empty raw batch");
     if (ibatch < 0 || n_batches <= 0 || ibatch >= n_batches) return h->fail(LSS_ERR_ARG, "ibatch out of range");
     const int64_t N = h->N;
@@ -491,22 +530,22 @@ static int run_filter(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t
         pre = h->Xh.p;
     }
     h->mark(3, s);
-    CK(launch_sgemm(h->Mw.p, h->C, pre, h->ld, Xout, h->ld, h->C, (int)N, h->C, s));
-    h->stats.launches += 1;
+    if (Xout) {
+        CK(launch_sgemm(h->Mw.p, h->C, pre, h->ld, Xout, h->ld, h->C, (int)N, h->C, s));
+        h->stats.launches += 1;
+    }
     h->mark(4, s);
+    if (pre_out) *pre_out = pre;
     return LSS_OK;
 }
 
-// Score field B [T, ld] of a filtered batch. The BF16 path also leaves the
-// column maxima of Cf in cfmax/imax (computed in the GEMM's epilogue), so the
-// rounds can skip their own first pass; *maxima_ready says which happened.
 static int run_scores(lss_handle* h, const float* X, int64_t ldx, int64_t N, float* B, cudaStream_t s,
-                      bool* maxima_ready = nullptr) {
+                      bool* maxima_ready = nullptr, bool folded = false) {
     if (h->cfg.precision == LSS_PREC_BF16_RECHECK) {
         CK(launch_pca_proj_t(X, ldx, h->C, N, h->wpca.p, h->K, h->nt, h->B0T.p, h->CKpad, s));
         h->mark(5, s);
-        CK(launch_score_tc(h->B0T.p, h->CKpad, (int)N, h->Up16.p, h->T, h->CKpad, h->nm.p, B, h->ld, h->cfmax.p,
-                           h->imax.p, h->nt, h->status.p, h->sm_count, s));
+        CK(launch_score_tc(h->B0T.p, h->CKpad, (int)N, folded ? h->Uw16.p : h->Up16.p, h->T, h->CKpad, h->nm.p, B,
+                           h->ld, h->cfmax.p, h->imax.p, h->nt, h->status.p, h->sm_count, s));
         h->stats.launches += 2;
         h->mark(6, s);
         if (maxima_ready) *maxima_ready = true;
@@ -514,8 +553,9 @@ static int run_scores(lss_handle* h, const float* X, int64_t ldx, int64_t N, flo
     }
     CK(launch_pca_proj_t_tf32(X, ldx, h->C, N, h->wpca.p, h->K, h->nt, h->B0T_hi.p, h->B0T_lo.p, h->CKpad, s));
     h->mark(5, s);
-    CK(launch_score_tc_tf32x3(h->B0T_hi.p, h->B0T_lo.p, h->CKpad, (int)N, h->Up_hi.p, h->Up_lo.p, h->T, h->CKpad,
-                              h->nm.p, B, h->ld, h->cfmax.p, h->imax.p, h->nt, h->status.p, h->sm_count, s));
+    CK(launch_score_tc_tf32x3(h->B0T_hi.p, h->B0T_lo.p, h->CKpad, (int)N, folded ? h->Uw_hi.p : h->Up_hi.p,
+                              folded ? h->Uw_lo.p : h->Up_lo.p, h->T, h->CKpad, h->nm.p, B, h->ld, h->cfmax.p,
+                              h->imax.p, h->nt, h->status.p, h->sm_count, s));
     h->stats.launches += 2;
     h->mark(6, s);
     if (maxima_ready) *maxima_ready = true;
@@ -679,26 +719,28 @@ int lss_sort_batch(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ib
     if (!out->time || !out->template_id || !out->amplitude) return h->fail(LSS_ERR_ARG, "null record arrays");
     CK(cudaSetDevice(h->cfg.device));
     cudaStream_t s = (cudaStream_t)stream;
-    int rc = run_filter(h, raw, n_rows, ibatch, n_batches, raw_on_device, h->X.p, s);
+    // the whitening / drift matrix is folded into the templates (set_mixing), so
+    // the scores come from the highpassed batch directly
+    const float* Xh = nullptr;
+    int rc = run_filter(h, raw, n_rows, ibatch, n_batches, raw_on_device, nullptr, s, &Xh);
     if (rc) return rc;
     CK(cudaMemsetAsync(h->status.p, 0, sizeof(int32_t), s));
     bool ready = false;
-    rc = run_scores(h, h->X.p, h->ld, h->N, h->B.p, s, &ready);
+    rc = run_scores(h, Xh, h->ld, h->N, h->B.p, s, &ready, /*folded=*/true);
     if (rc) return rc;
     int32_t n = 0, rounds = 0;
     rc = run_mp(h, h->N, &n, &rounds, s, ready);
     if (rc) return rc;
     const int feat = h->nC * h->K;
     const bool want_pc = out->pc != nullptr && feat > 0;
+    const bool bf16 = h->cfg.precision == LSS_PREC_BF16_RECHECK;
+    h->mark(8, s);
     if (want_pc && n > 0) {
-        rc = run_xres(h, h->X.p, h->ld, h->N, rounds, h->Xres.p, h->ld, s);
-        if (rc) return rc;
-        h->mark(8, s);
-        CK(launch_pc_features(h->Xres.p, h->ld, h->nt, h->K, h->nC, h->C, h->T, h->wpca.p, h->iCC.p, h->iU.p,
-                              h->Ucc.p, h->sp_x.p, h->sp_y.p, h->sp_amp.p, h->counters.p, n, h->tF.p, s));
+        CK(launch_pc_features_folded(Xh, h->ld, h->C, h->nt, h->K, h->nC, h->T, h->wpca.p, h->Mw.p, h->U.p, h->R.p,
+                                     h->iCC.p, h->iU.p, h->Ucc.p, h->sp_x.p, h->sp_y.p, h->sp_amp.p,
+                                     h->round_start.p, rounds, n, h->tF.p, h->status.p,
+                                     bf16 ? nullptr : h->B0T_hi.p, bf16 ? nullptr : h->B0T_lo.p, h->CKpad, s));
         h->stats.launches += 1;
-    } else {
-        h->mark(8, s);
     }
     h->mark(9, s);
     const int64_t cap = out->capacity;
@@ -707,9 +749,9 @@ int lss_sort_batch(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ib
     float* d_amp = out->on_device ? out->amplitude : h->rec_amp.p;
     float* d_pc = want_pc ? (out->on_device ? out->pc : h->rec_pc.p) : nullptr;
     const int64_t dcap = out->on_device ? cap : std::min<int64_t>(cap, h->cfg.max_spikes);
-    CK(launch_records(h->sp_x.p, h->sp_y.p, h->sp_amp.p, want_pc ? h->tF.p : nullptr, h->counters.p, n, feat,
+    CK(launch_records(h->sp_x.p, h->sp_y.p, h->sp_amp.p, want_pc ? h->tF.p : nullptr, h->rec_slot.p, n, feat,
                       ibatch, h->nt, h->NT, h->cfg.nt0min, d_time, d_tmpl, d_amp, d_pc, dcap, h->rec_count.p, s));
-    h->stats.launches += 1;
+    h->stats.launches += (n > 0) ? 2 : 1;
     int64_t count = 0;
     int32_t st = 0;
     CK(cudaMemcpyAsync(&count, h->rec_count.p, sizeof(count), cudaMemcpyDeviceToHost, s));

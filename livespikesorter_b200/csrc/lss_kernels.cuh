@@ -61,6 +61,10 @@ cudaError_t launch_score_tc_tf32x3(const float* B0T_hi, const float* B0T_lo, int
 cudaError_t launch_pca_proj_t_tf32(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
                                    int32_t nt, float* hi, float* lo, int64_t ldk, cudaStream_t s);
 
+// U_w[t, c'*K + k] = sum_c U[t,k,c] Mw[c,c'] in GEMM layout: bf16 (out16) or tf32 hi/lo
+cudaError_t launch_build_uw(const float* U, const float* Mw, int32_t T, int32_t K, int32_t C, int64_t ldk,
+                            __nv_bfloat16* out16, float* hi, float* lo, cudaStream_t s);
+
 // ---- matching pursuit (mp.cu) ----
 struct MPArgs {
     float* B;                 // [T, ldb] score field, updated in place
@@ -105,11 +109,20 @@ cudaError_t launch_pc_features(const float* Xres, int64_t ldx, int32_t nt, int32
                                const int64_t* iU, const float* Ucc, const int32_t* sp_x,
                                const int32_t* sp_y, const float* sp_amp, const int32_t* counters,
                                int32_t n, float* tF, cudaStream_t s);
+// slot: scratch [n] for the output position of each spike
 cudaError_t launch_records(const int32_t* sp_x, const int32_t* sp_y, const float* sp_amp, const float* tF,
-                           const int32_t* counters, int32_t n, int32_t feat_len, int64_t ibatch, int32_t nt,
+                           int32_t* slot, int32_t n, int32_t feat_len, int64_t ibatch, int32_t nt,
                            int32_t NT, int32_t nt0min, int64_t* out_time, int32_t* out_tmpl,
                            float* out_amp, float* out_pc, int64_t capacity, int64_t* out_count,
                            cudaStream_t s);
+// PC features from the highpassed batch (or, when Phi is given, the projection rows
+// P = Phi + Plo [N, ldp] of the score GEMM) and the folded whitening (no residual array)
+cudaError_t launch_pc_features_folded(const float* Xh, int64_t ldx, int32_t C, int32_t nt, int32_t K, int32_t nC,
+                                      int32_t T, const float* wpca, const float* Mw, const float* U, const float* R,
+                                      const int64_t* iCC, const int64_t* iU, const float* Ucc, const int32_t* sp_x,
+                                      const int32_t* sp_y, const float* sp_amp, const int32_t* round_start,
+                                      int32_t rounds, int32_t n, float* tF, int32_t* status, const float* Phi,
+                                      const float* Plo, int64_t ldp, cudaStream_t s);
 cudaError_t launch_st_out(const int32_t* sp_x, const int32_t* sp_y, const float* sp_amp, int32_t n,
                           int64_t* st, float* amps, cudaStream_t s);
 

@@ -85,6 +85,33 @@ __device__ __forceinline__ bool grid_sync(unsigned int* bar, int32_t* status) {
     return s_ok != 0;
 }
 
+// L2 residency: the score field is read-modify-written every round and fits
+// in L2 for a few hundred templates, while each spike's ctc slice is read once
+// per spike, so the field is kept (evict_last) and ctc streamed (evict_first).
+__device__ __forceinline__ uint64_t policy_keep() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t policy_stream() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ float ld_keep(const float* a, uint64_t pol) {
+    float v;
+    asm volatile("ld.global.cg.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ void st_keep(float* a, float v, uint64_t pol) {
+    asm volatile("st.global.cg.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(a), "f"(v), "l"(pol) : "memory");
+}
+__device__ __forceinline__ float ld_stream(const float* a, uint64_t pol) {
+    float v;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
+    return v;
+}
+
 __device__ __forceinline__ void group_sync(int g) {
     asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(MP_GT) : "memory");
 }
@@ -356,6 +383,7 @@ __global__ void __launch_bounds__(MP_THREADS, 1) k_mp(MPArgs a) {
                     }
                     const bool edge = (s < nt) || (s >= N - nt);
                     ColMax m;
+                    const uint64_t pk = policy_keep(), ps = policy_stream();
                     float* bp = a.B + (int64_t)t0 * a.ldb + s;
                     const float* p0 = c0p ? c0p + (int64_t)t0 * L2 : nullptr;
                     const float* p1 = c1p ? c1p + (int64_t)t0 * L2 : nullptr;
@@ -364,21 +392,21 @@ __global__ void __launch_bounds__(MP_THREADS, 1) k_mp(MPArgs a) {
                     for (; t + 8 <= t1; t += 8) {
                         float v[8], w0[8], w1[8];
 #pragma unroll
-                        for (int u = 0; u < 8; ++u) v[u] = __ldcg(bp + u * ldb);
+                        for (int u = 0; u < 8; ++u) v[u] = ld_keep(bp + u * ldb, pk);
                         if (p0) {
 #pragma unroll
-                            for (int u = 0; u < 8; ++u) w0[u] = __ldg(p0 + u * L2);
+                            for (int u = 0; u < 8; ++u) w0[u] = ld_stream(p0 + u * L2, ps);
                         }
                         if (p1) {
 #pragma unroll
-                            for (int u = 0; u < 8; ++u) w1[u] = __ldg(p1 + u * L2);
+                            for (int u = 0; u < 8; ++u) w1[u] = ld_stream(p1 + u * L2, ps);
                         }
 #pragma unroll
                         for (int u = 0; u < 8; ++u) {
                             float x = v[u];
                             if (p0) x = __fsub_rn(x, __fmul_rn(a0, w0[u]));
                             if (p1) x = __fsub_rn(x, __fmul_rn(a1, w1[u]));
-                            __stcg(bp + u * ldb, x);
+                            st_keep(bp + u * ldb, x, pk);
                             if (!edge) m.consider(x, s_nm[t + u], s_inv[t + u], t + u);
                         }
                         bp += 8 * ldb;
@@ -386,10 +414,10 @@ __global__ void __launch_bounds__(MP_THREADS, 1) k_mp(MPArgs a) {
                         if (p1) p1 += 8 * L2;
                     }
                     for (; t < t1; ++t, bp += ldb) {
-                        float x = __ldcg(bp);
-                        if (p0) { x = __fsub_rn(x, __fmul_rn(a0, __ldg(p0))); p0 += L2; }
-                        if (p1) { x = __fsub_rn(x, __fmul_rn(a1, __ldg(p1))); p1 += L2; }
-                        __stcg(bp, x);
+                        float x = ld_keep(bp, pk);
+                        if (p0) { x = __fsub_rn(x, __fmul_rn(a0, ld_stream(p0, ps))); p0 += L2; }
+                        if (p1) { x = __fsub_rn(x, __fmul_rn(a1, ld_stream(p1, ps))); p1 += L2; }
+                        st_keep(bp, x, pk);
                         if (!edge) m.consider(x, s_nm[t], s_inv[t], t);
                     }
                     if (!edge && t1 > t0) atomicMax(knext + s, pack_key(m.best, m.bi));
@@ -470,7 +498,7 @@ static __device__ __align__(256) unsigned char g_mp_scratch[NA_BYTES];
 
 #include <mutex>
 
-#include "../../include/lss.h"
+#include "lss.h"
 
 namespace {
 std::mutex g_na_mutex;

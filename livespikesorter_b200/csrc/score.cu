@@ -116,16 +116,19 @@ __device__ __forceinline__ float tf32_rna(float x) {
     return __uint_as_float(r);
 }
 
+// Thread = (channel, 8-sample group) with the channel fastest across a warp,
+// so the K values a thread writes per sample land next to its neighbours'
+// and a warp writes 32*K contiguous outputs per sample row.
 template <int KPC, int PC, bool TF32>
 __global__ void __launch_bounds__(256) k_pca_proj_t(const float* __restrict__ X, int64_t ldx, int32_t C, int64_t N,
                                                     const float* __restrict__ wpca, int32_t nt, void* __restrict__ out0,
                                                     float* __restrict__ out_lo, int64_t ldk) {
     extern __shared__ float sm[];
     const int ntp = (nt + 7) & ~7;
-    const int xw = PT_S + ntp + 8;                 // staged samples per channel row
+    const int xw = PT_S + ntp + 9;                 // staged samples per channel row (odd: no bank conflicts)
     float* ws = sm;                                // [KPC][ntp]
     float* xs = ws + KPC * ntp;                    // [PC][xw]
-    float* stage = xs + PC * xw;                   // [PT_S][PC*KPC]
+    float* stage = xs + PC * xw + ((PC * xw) & 3 ? 4 - ((PC * xw) & 3) : 0);  // [PT_S][PC*KPC], 16-byte aligned
     const int64_t s0 = (int64_t)blockIdx.x * PT_S;
     const int c0 = blockIdx.y * PC;
     const int nc = min(PC, C - c0);
@@ -140,9 +143,9 @@ __global__ void __launch_bounds__(256) k_pca_proj_t(const float* __restrict__ X,
         xs[e] = (c < nc && g >= 0 && g < N) ? X[(int64_t)(c0 + c) * ldx + g] : 0.f;
     }
     __syncthreads();
-    // task = (channel, 8-sample group)
     for (int task = threadIdx.x; task < PC * (PT_S / 8); task += blockDim.x) {
         const int c = task % PC, sg = task / PC;
+        if (c >= nc) continue;
         const float* xr = xs + c * xw + sg * 8;
         float acc[KPC][8];
 #pragma unroll
@@ -173,10 +176,33 @@ __global__ void __launch_bounds__(256) k_pca_proj_t(const float* __restrict__ X,
             for (int k = 0; k < KPC; ++k) stage[(sg * 8 + r) * (PC * KPC) + c * KPC + k] = acc[k][r];
     }
     __syncthreads();
-    // row segments: PT_S rows of nc*KPC values each
+    // rows of nc*KPC outputs, written as 16-byte vectors (ldk and c0*KPC are
+    // multiples of 4, so every vector is aligned)
     const int seg = nc * KPC;
-    for (int e = threadIdx.x; e < PT_S * seg; e += blockDim.x) {
-        const int r = e / seg, j = e % seg;
+    const int nv4 = seg / 4;
+    for (int e = threadIdx.x; e < PT_S * nv4; e += blockDim.x) {
+        const int r = e / nv4, q = e % nv4;
+        const int64_t s = s0 + r;
+        if (s >= N) continue;
+        const float4 v = *reinterpret_cast<const float4*>(stage + r * (PC * KPC) + 4 * q);
+        const int64_t o = s * ldk + (int64_t)c0 * KPC + 4 * q;
+        if (TF32) {
+            const float4 hi = make_float4(tf32_rna(v.x), tf32_rna(v.y), tf32_rna(v.z), tf32_rna(v.w));
+            const float4 lo = make_float4(__fsub_rn(v.x, hi.x), __fsub_rn(v.y, hi.y), __fsub_rn(v.z, hi.z),
+                                          __fsub_rn(v.w, hi.w));
+            *reinterpret_cast<float4*>(static_cast<float*>(out0) + o) = hi;
+            *reinterpret_cast<float4*>(out_lo + o) = lo;
+        } else {
+            __nv_bfloat16* d = static_cast<__nv_bfloat16*>(out0) + o;
+            d[0] = __float2bfloat16_rn(v.x);
+            d[1] = __float2bfloat16_rn(v.y);
+            d[2] = __float2bfloat16_rn(v.z);
+            d[3] = __float2bfloat16_rn(v.w);
+        }
+    }
+    // tail (seg not a multiple of 4)
+    for (int e = threadIdx.x; e < PT_S * (seg - 4 * nv4); e += blockDim.x) {
+        const int r = e / (seg - 4 * nv4), j = 4 * nv4 + e % (seg - 4 * nv4);
         const int64_t s = s0 + r;
         if (s >= N) continue;
         const float v = stage[r * (PC * KPC) + j];
@@ -194,10 +220,11 @@ __global__ void __launch_bounds__(256) k_pca_proj_t(const float* __restrict__ X,
 template <int KPC, bool TF32>
 static cudaError_t launch_pjt(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t nt,
                               void* out0, float* out_lo, int64_t ldk, cudaStream_t s) {
-    constexpr int PC = 64;
+    constexpr int PC = 32;
     const int ntp = (nt + 7) & ~7;
-    const size_t smem = sizeof(float) * ((size_t)KPC * ntp + (size_t)PC * (PT_S + ntp + 8) + (size_t)PT_S * PC * KPC);
-    cudaFuncSetAttribute(k_pca_proj_t<KPC, PC, TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const size_t smem = sizeof(float) * ((size_t)KPC * ntp + (size_t)PC * (PT_S + ntp + 9) + 4 + (size_t)PT_S * PC * KPC);
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(k_pca_proj_t<KPC, PC, TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     dim3 grid((unsigned)((N + PT_S - 1) / PT_S), (unsigned)((C + PC - 1) / PC));
     k_pca_proj_t<KPC, PC, TF32><<<grid, 256, smem, s>>>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk);
     return cudaGetLastError();
@@ -227,6 +254,38 @@ cudaError_t launch_pca_proj_t(const float* X, int64_t ldx, int32_t C, int64_t N,
 cudaError_t launch_pca_proj_t_tf32(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
                                    int32_t nt, float* hi, float* lo, int64_t ldk, cudaStream_t s) {
     return pjt_dispatch<true>(X, ldx, C, N, wpca, K, nt, hi, lo, ldk, s);
+}
+
+// Templates with the whitening folded in, in the score GEMM's layout:
+//   U_w[t, c'*K + k] = sum_c U[t, k, c] * Mw[c, c']       (Mw = M @ Wrot)
+// so that sum_kk U_w[t, kk] * P[s, kk] over the projection P of the
+// un-whitened batch equals the score of the whitened batch. Stored as bf16
+// (BF16 path) or as a tf32 hi/lo split (FP32 path), rows [Tpad, ldk].
+__global__ void k_build_uw(const float* __restrict__ U, const float* __restrict__ Mw, int32_t T, int32_t K,
+                           int32_t C, int64_t ldk, __nv_bfloat16* __restrict__ out16, float* __restrict__ hi,
+                           float* __restrict__ lo) {
+    const int cp = blockIdx.x * blockDim.x + threadIdx.x;
+    const int tk = blockIdx.y;  // t * K + k
+    if (cp >= C) return;
+    const float* u = U + (int64_t)tk * C;  // U[t, k, :]
+    float acc = 0.f;
+    for (int c = 0; c < C; ++c) acc = fmaf(u[c], Mw[(int64_t)c * C + cp], acc);
+    const int t = tk / K, k = tk % K;
+    const int64_t o = (int64_t)t * ldk + (int64_t)cp * K + k;
+    if (out16) {
+        out16[o] = __float2bfloat16_rn(acc);
+    } else {
+        const float h = tf32_rna(acc);
+        hi[o] = h;
+        lo[o] = __fsub_rn(acc, h);
+    }
+}
+
+cudaError_t launch_build_uw(const float* U, const float* Mw, int32_t T, int32_t K, int32_t C, int64_t ldk,
+                            __nv_bfloat16* out16, float* hi, float* lo, cudaStream_t s) {
+    dim3 grid((unsigned)((C + 127) / 128), (unsigned)(T * K));
+    k_build_uw<<<grid, 128, 0, s>>>(U, Mw, T, K, C, ldk, out16, hi, lo);
+    return cudaGetLastError();
 }
 
 }  // namespace lss

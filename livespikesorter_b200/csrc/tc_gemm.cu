@@ -181,6 +181,10 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
+__device__ __forceinline__ void st_keep(float* a, float v, uint64_t pol) {
+    asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(a), "f"(v), "l"(pol) : "memory");
+}
+
 // Running column maximum of Cf with the rounds kernel's exact rule.
 struct ColMax {
     float best = -1.f;
@@ -353,6 +357,9 @@ __global__ void __launch_bounds__(THREADS, 1)
     } else {
         // ---------------- epilogue: warps 2..5, one sample per thread
         const int q = warp & 3;  // TMEM lane quarter this warp may access
+        // the score field is re-read by the matching pursuit right after: keep it in L2
+        uint64_t pol;
+        asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
         const int row = q * 32 + lane;
         uint32_t acc_ph[2] = {0, 0};
         int acc = 0;
@@ -377,7 +384,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                             const int t = t0 + j;
                             if (t < a.T) {
                                 const float v = __uint_as_float(r[j]);
-                                a.Bout[(int64_t)t * a.ldb + n] = v;
+                                st_keep(a.Bout + (int64_t)t * a.ldb + n, v, pol);
                                 if (!edge) m.consider(v, s_nm[t], s_inv[t], t);
                             }
                         }
