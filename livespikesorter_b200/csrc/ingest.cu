@@ -223,4 +223,99 @@ cudaError_t launch_highpass(const float* X1, int64_t ldx, int32_t C, int64_t N, 
     return cudaGetLastError();
 }
 
+
+
+// ---------------------------------------------------------------------------
+// The same circular highpass by overlap-save FFT convolution (used when the
+// truncated impulse response has L <= 1024). One CTA filters two channels at
+// once as the real and imaginary parts of a 4096-point complex signal (the
+// filter is real, so both come out of one transform): the block x[start-L ..
+// start-L+4096) (indices mod N) is transformed by a radix-4 Stockham FFT in
+// shared memory, multiplied by H = conj(FFT(g)) where g holds the taps wrapped
+// around index 0 (a circular correlation), and transformed back; its outputs
+// L .. 4096-L-1 are exact (their taps never wrap inside the block).
+// ---------------------------------------------------------------------------
+constexpr int HF = 4096;
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(__fsub_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)),
+                       __fadd_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
+}
+
+// Forward FFT of src (HF points) into src, using dst as the ping-pong buffer
+// (HF = 4^6: an even number of radix-4 stages ends back in src).
+__device__ __forceinline__ void fft4096(float2* src, float2* dst, const float2* __restrict__ tw) {
+    float2* a = src;
+    float2* b = dst;
+    for (int L = 1; L < HF; L *= 4) {
+        const int step = HF / (4 * L);
+        for (int j = threadIdx.x; j < HF / 4; j += blockDim.x) {
+            const int k = j % L, m = j / L;
+            const float2 w1 = __ldg(tw + k * step);
+            const float2 w2 = __ldg(tw + ((2 * k * step) & (HF - 1)));
+            const float2 w3 = __ldg(tw + ((3 * k * step) & (HF - 1)));
+            const float2 a0 = a[j];
+            const float2 a1 = cmul(a[j + HF / 4], w1);
+            const float2 a2 = cmul(a[j + HF / 2], w2);
+            const float2 a3 = cmul(a[j + 3 * HF / 4], w3);
+            const float2 s02 = make_float2(a0.x + a2.x, a0.y + a2.y), d02 = make_float2(a0.x - a2.x, a0.y - a2.y);
+            const float2 s13 = make_float2(a1.x + a3.x, a1.y + a3.y), d13 = make_float2(a1.x - a3.x, a1.y - a3.y);
+            const int base = m * 4 * L + k;
+            b[base] = make_float2(s02.x + s13.x, s02.y + s13.y);
+            b[base + L] = make_float2(d02.x + d13.y, d02.y - d13.x);       // d02 - i*d13
+            b[base + 2 * L] = make_float2(s02.x - s13.x, s02.y - s13.y);
+            b[base + 3 * L] = make_float2(d02.x - d13.y, d02.y + d13.x);   // d02 + i*d13
+        }
+        __syncthreads();
+        float2* t = a;
+        a = b;
+        b = t;
+    }
+}
+
+__global__ void __launch_bounds__(512) k_highpass_fft(const float* __restrict__ X1, int64_t ldx, int32_t C, int64_t N,
+                                                      int32_t L, const float2* __restrict__ H,
+                                                      const float2* __restrict__ tw, float* __restrict__ Xh) {
+    extern __shared__ float2 fbuf[];
+    float2* A = fbuf;
+    float2* Bb = fbuf + HF;
+    const int c1 = 2 * blockIdx.y, c2 = c1 + 1;
+    const bool two = c2 < C;
+    const int64_t start = (int64_t)blockIdx.x * (HF - 2 * L);
+    const float* x1 = X1 + (int64_t)c1 * ldx;
+    const float* x2 = X1 + (int64_t)(two ? c2 : c1) * ldx;
+    for (int n = threadIdx.x; n < HF; n += blockDim.x) {
+        int64_t g = (start - L + n) % N;
+        if (g < 0) g += N;
+        A[n] = make_float2(x1[g], two ? x2[g] : 0.f);
+    }
+    __syncthreads();
+    fft4096(A, Bb, tw);
+    // conj(Z * H): the second forward transform then gives conj(F * y)
+    for (int n = threadIdx.x; n < HF; n += blockDim.x) {
+        const float2 z = cmul(A[n], __ldg(H + n));
+        A[n] = make_float2(z.x, -z.y);
+    }
+    __syncthreads();
+    fft4096(A, Bb, tw);
+    const float inv = 1.f / (float)HF;
+    for (int n = L + threadIdx.x; n < HF - L; n += blockDim.x) {
+        const int64_t i = start + (n - L);
+        if (i >= N) break;
+        const float2 r = A[n];
+        Xh[(int64_t)c1 * ldx + i] = r.x * inv;
+        if (two) Xh[(int64_t)c2 * ldx + i] = -r.y * inv;
+    }
+}
+
+cudaError_t launch_highpass_fft(const float* X1, int64_t ldx, int32_t C, int64_t N, int32_t L, const float2* H,
+                                const float2* tw, float* Xh, cudaStream_t s) {
+    if (L > 1024) return cudaErrorInvalidValue;
+    const size_t smem = 2 * HF * sizeof(float2);
+    cudaFuncSetAttribute(k_highpass_fft, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    dim3 grid((unsigned)((N + (HF - 2 * L) - 1) / (HF - 2 * L)), (unsigned)((C + 1) / 2));
+    k_highpass_fft<<<grid, 512, smem, s>>>(X1, ldx, C, N, L, H, tw, Xh);
+    return cudaGetLastError();
+}
+
 }  // namespace lss

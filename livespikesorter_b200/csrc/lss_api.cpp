@@ -13,6 +13,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <complex>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -84,6 +85,7 @@ struct lss_handle {
     DevBuf<__nv_bfloat16> Uw16;                  // templates with the whitening folded in (BF16 path)
     DevBuf<float> Uw_hi, Uw_lo;                  // ... (FP32 path)
     DevBuf<float> U, R;                          // U [T,K,C]; R [K,K,2nt-1] basis lag correlations
+    DevBuf<float2> hpH, hpTw;                    // highpass spectrum and twiddles (FFT form)
     int CKpad = 0;
     int sm_count = 0;
     DevBuf<unsigned int> bar;
@@ -113,7 +115,7 @@ struct lss_handle {
         bar.release(); rec_time.release(); rec_count.release(); rec_tmpl.release(); rec_slot.release(); rec_amp.release();
         rec_pc.release(); B0T.release(); Up16.release();
         B0T_hi.release(); B0T_lo.release(); Up_hi.release(); Up_lo.release();
-        Uw16.release(); Uw_hi.release(); Uw_lo.release(); U.release(); R.release();
+        Uw16.release(); Uw_hi.release(); Uw_lo.release(); U.release(); R.release(); hpH.release(); hpTw.release();
     }
 };
 
@@ -172,6 +174,27 @@ static int make_taps(const std::vector<float>& h, int64_t N, std::vector<float>&
 
 // Whitening with drift: Mw = M @ Wrot on the device (FP32, like the
 // reference's (M @ self.whiten_mat), kilosort/io.py:786), or Wrot when M is NULL.
+// In-place forward DFT (radix-2, double precision), exp(-2 pi i k n / n).
+static void fft_double(std::vector<std::complex<double>>& a) {
+    const size_t n = a.size();
+    for (size_t i = 1, j = 0; i < n; ++i) {
+        size_t bit = n >> 1;
+        for (; j & bit; bit >>= 1) j ^= bit;
+        j ^= bit;
+        if (i < j) std::swap(a[i], a[j]);
+    }
+    for (size_t len = 2; len <= n; len <<= 1) {
+        const double ang = -2.0 * M_PI / (double)len;
+        for (size_t i = 0; i < n; i += len)
+            for (size_t k = 0; k < len / 2; ++k) {
+                const std::complex<double> w(std::cos(ang * k), std::sin(ang * k));
+                const std::complex<double> u = a[i + k], v = a[i + k + len / 2] * w;
+                a[i + k] = u + v;
+                a[i + k + len / 2] = u - v;
+            }
+    }
+}
+
 static int set_mixing(lss_handle* h, const float* M) {
     const int C = h->C;
     if (!M) {
@@ -350,6 +373,11 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
         ALLOC(Uw_lo, (size_t)plan.Tpad * h->CKpad);
     }
     ALLOC(U, (size_t)T * K * C);
+    const bool hp_fft = h->hpL >= 0 && h->hpL <= 1024;
+    if (hp_fft) {
+        ALLOC(hpH, 4096);
+        ALLOC(hpTw, 4096);
+    }
     ALLOC(R, (size_t)K * K * (2 * nt - 1));
     ALLOC(B, (size_t)T * ld);
     ALLOC(nm, T);
@@ -428,6 +456,25 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
     CK(cudaMemcpy(h->wave.p, wave.data(), wave.size() * sizeof(float), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->wpca.p, t->wpca, (size_t)K * nt * sizeof(float), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->U.p, t->wall3, (size_t)T * K * C * sizeof(float), cudaMemcpyHostToDevice));
+    if (hp_fft) {
+        // g = taps wrapped around index 0 (circular correlation), H = conj(FFT(g))
+        const int F = 4096, L = h->hpL;
+        std::vector<std::complex<double>> g(F, 0.0);
+        g[0] = taps[L];
+        for (int d = 1; d <= L; ++d) {
+            g[d] = taps[L + d];
+            g[F - d] = taps[L - d];
+        }
+        fft_double(g);
+        std::vector<float2> hv(F), tv(F);
+        for (int k = 0; k < F; ++k) {
+            hv[k] = make_float2((float)g[k].real(), (float)-g[k].imag());
+            const double ang = -2.0 * M_PI * k / F;
+            tv[k] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+        }
+        CK(cudaMemcpy(h->hpH.p, hv.data(), F * sizeof(float2), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h->hpTw.p, tv.data(), F * sizeof(float2), cudaMemcpyHostToDevice));
+    }
     {
         // R[k, k', d] = sum_m wPCA[k, m] * wPCA[k', m + d], d = -(nt-1) .. nt-1
         const int nd = 2 * nt - 1;
@@ -525,7 +572,10 @@ static int run_filter(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t
     h->mark(2, s);
     const float* pre = h->X1.p;
     if (h->hpL >= 0) {
-        CK(launch_highpass(h->X1.p, h->ld, h->C, N, h->taps.p, h->hpL, h->Xh.p, s));
+        if (h->hpH.p)
+            CK(launch_highpass_fft(h->X1.p, h->ld, h->C, N, h->hpL, h->hpH.p, h->hpTw.p, h->Xh.p, s));
+        else
+            CK(launch_highpass(h->X1.p, h->ld, h->C, N, h->taps.p, h->hpL, h->Xh.p, s));
         h->stats.launches += 1;
         pre = h->Xh.p;
     }

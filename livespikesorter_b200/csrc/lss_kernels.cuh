@@ -25,6 +25,9 @@ cudaError_t launch_car(const int16_t* raw, int32_t ld_raw, const int32_t* chan_m
                        int64_t ldx, cudaStream_t s);
 cudaError_t launch_highpass(const float* X1, int64_t ldx, int32_t C, int64_t N, const float* taps, int32_t L,
                             float* Xh, cudaStream_t s);
+// overlap-save FFT form (L <= 1024): H = conj(FFT_4096(taps wrapped around 0)), tw[k] = exp(-2 pi i k / 4096)
+cudaError_t launch_highpass_fft(const float* X1, int64_t ldx, int32_t C, int64_t N, int32_t L, const float2* H,
+                                const float2* tw, float* Xh, cudaStream_t s);
 
 // ---- dense FP32 GEMM (gemm_fp32.cu): C[M,N] = A[M,K] @ B[K,N], row-major ----
 cudaError_t launch_sgemm(const float* A, int64_t lda, const float* B, int64_t ldb, float* Cm, int64_t ldc,

@@ -325,27 +325,39 @@ __global__ void __launch_bounds__(MP_THREADS, 1) k_mp(MPArgs a) {
             int nrb = (2 * groups + total - 1) / total;
             nrb = max(nrb, (T + 63) / 64);
             nrb = min(nrb, (T + 7) / 8);
-            const int tb = (T + nrb - 1) / nrb;
+            const int tb = ((T + nrb - 1) / nrb + 7) & ~7;  // whole 8-row batches
+            nrb = (T + tb - 1) / tb;
             const int items = total * nrb;
             const int g = tid / MP_GT, lt = tid % MP_GT;
+            // warp 0 of the group gathers the spike list of an item: lane 0 the
+            // previous spike, lanes 1..31 spikes q, q+1, ...; the loads for the
+            // next item are issued before the current item's rows are streamed
+            auto fetch = [&](int it2, int& x, int& y, float& amp) {
+                const int j = it2 / nrb - 1 + lt;
+                x = INT_MAX;
+                y = 0;
+                amp = 0.f;
+                if (it2 < items && j >= 0 && j < total) {
+                    int lo2 = 0, hi2 = G;  // region c with s_pref[c] <= j < s_pref[c+1]
+                    while (hi2 - lo2 > 1) {
+                        const int m = (lo2 + hi2) >> 1;
+                        if (s_pref[m] <= j) lo2 = m; else hi2 = m;
+                    }
+                    const int idx = lo2 * W + (j - s_pref[lo2]);
+                    x = __ldcg(a.blk_x + idx);
+                    y = __ldcg(a.blk_y + idx);
+                    amp = __ldcg(a.blk_amp + idx);
+                }
+            };
+            int fx = 0, fy = 0;
+            float fa = 0.f;
+            if (lt < 32) fetch(b * MP_GROUPS + g, fx, fy, fa);
             for (int it = b * MP_GROUPS + g; it < items; it += groups) {
                 const int q = it / nrb, rb = it % nrb;
                 if (lt < 32) {
-                    // lane 0: previous spike; lanes 1..31: spikes q, q+1, ...
                     const int j = q - 1 + lt;
-                    int x = INT_MAX, y = 0;
-                    float amp = 0.f;
-                    if (j >= 0 && j < total) {
-                        int lo2 = 0, hi2 = G;  // region c with s_pref[c] <= j < s_pref[c+1]
-                        while (hi2 - lo2 > 1) {
-                            const int m = (lo2 + hi2) >> 1;
-                            if (s_pref[m] <= j) lo2 = m; else hi2 = m;
-                        }
-                        const int idx = lo2 * W + (j - s_pref[lo2]);
-                        x = __ldcg(a.blk_x + idx);
-                        y = __ldcg(a.blk_y + idx);
-                        amp = __ldcg(a.blk_amp + idx);
-                    }
+                    const int x = fx, y = fy;
+                    const float amp = fa;
                     const int xi = __shfl_sync(0xffffffffu, x, 1);
                     const bool ok = lt >= 1 && j < total && x <= xi + 2 * nt;
                     const unsigned bal = __ballot_sync(0xffffffffu, ok);
@@ -355,6 +367,7 @@ __global__ void __launch_bounds__(MP_THREADS, 1) k_mp(MPArgs a) {
                         s_nlist[g] = __popc(bal);
                         if (__popc(bal) == MP_LIST && q + MP_LIST < total) atomicOr(a.status, STATUS_LIST);
                     }
+                    fetch(it + groups, fx, fy, fa);
                 }
                 group_sync(g);
                 const int nl = s_nlist[g];
