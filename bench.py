@@ -194,7 +194,8 @@ def run_b200(args):
                 'frac': ach / hbm, 'traffic': None, 'peak_source': src}
     else:
         ach = gemm_flops / (mean_st['score_ms'] / 1e3) / 1e12
-        roof = {'kernel': 'k_sgemm (score GEMM, FP32 SIMT)' if args.precision == 'fp32' else 'score GEMM',
+        roof = {'kernel': 'k_score_tc (tcgen05 3xTF32 score GEMM)' if args.precision == 'fp32'
+                else 'k_score_tc (tcgen05 BF16 score GEMM)',
                 'bound': 'tensor', 'achieved': ach, 'peak': tfl, 'unit': 'TFLOP/s', 'frac': ach / tfl,
                 'traffic': None, 'peak_source': src, 'top_stage': top}
     h2d = int(rows_h[0].numel() * 2 + setup.C * setup.C * 4)
@@ -210,6 +211,8 @@ def run_b200(args):
         'roofline': roof, 'gpu_launches': int(launches), 'clocks': clocks,
         'stage_ms': mean_st, 'spikes_per_batch': float(np.mean(spikes)), 'rounds_per_batch': float(np.mean(rounds)),
     }
+    if args.precision == 'bf16':
+        out['bf16'] = bf16_report(s, setup, local, rows_d, drifts, ids, nb)
     if rank == 0 and not args.no_cpu_baseline:
         out['cpu_baseline'] = cpu_baseline(setup, rec, budget_s=20.0)
     if dist:
@@ -217,6 +220,33 @@ def run_b200(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(out))
+
+
+def bf16_report(s16, setup, local, rows_d, drifts, ids, nb):
+    """Untimed: the BF16 path's re-check statistics and its spike agreement
+    with the FP32 path over the batch pool ((time, template) pairs)."""
+    from livespikesorter_b200.sorter import Sorter
+    s32 = Sorter.from_setup(setup, device=local)
+    near = rescored = flips = common = n32 = n16 = 0
+    for j, ib in enumerate(ids):
+        s16.set_drift(drifts[j])
+        s32.set_drift(drifts[j])
+        r16 = s16.sort_batch(rows_d[j], ib, nb, on_device=True)
+        st = s16.stats()
+        near += st['recheck_columns']
+        rescored += st['recheck_rescored']
+        flips += st['recheck_flips']
+        r32 = s32.sort_batch(rows_d[j], ib, nb, on_device=True)
+        a = set(zip(r32['time'].tolist(), r32['template'].tolist()))
+        b = set(zip(r16['time'].tolist(), r16['template'].tolist()))
+        common += len(a & b)
+        n32 += len(a)
+        n16 += len(b)
+    nbat = len(ids)
+    return {'agreement_vs_fp32': common / max(n32, n16, 1), 'spikes_fp32': n32, 'spikes_bf16': n16,
+            'common': common, 'recheck_near_columns_per_batch': near / nbat,
+            'recheck_rescored_columns_per_batch': rescored / nbat, 'recheck_flips_per_batch': flips / nbat,
+            'batch_samples': setup.NT}
 
 
 def oracle_batch(setup, rec, ib, ns=None):

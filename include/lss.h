@@ -170,14 +170,17 @@ int  lss_scores(lss_handle* h, const float* X_dev, int64_t N, float* B_dev, void
 int  lss_sort_batch(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ibatch,
                     int64_t n_batches, int32_t raw_on_device, lss_records* out, void* stream);
 
-/* Statistics of the last lss_match / lss_sort_batch: rounds run, spikes,
- * columns re-checked in FP32 (BF16 path). */
+/* Statistics of the last lss_match / lss_sort_batch: rounds run and spikes;
+ * for the BF16 path, of the last scoring: columns whose decisions lay within
+ * the re-check margin, decisions (best template or threshold side) the FP32
+ * re-check changed, and columns re-scored in FP32 (whole 64-sample tiles). */
 typedef struct lss_stats {
     int32_t rounds;
     int64_t spikes;
     int64_t recheck_columns;
     int64_t recheck_flips;
     int64_t launches;      /* kernels this handle has launched since creation */
+    int64_t recheck_rescored;
 } lss_stats;
 int  lss_get_stats(const lss_handle* h, lss_stats* out);
 

@@ -86,6 +86,12 @@ struct lss_handle {
     DevBuf<float> Uw_hi, Uw_lo;                  // ... (FP32 path)
     DevBuf<float> U, R;                          // U [T,K,C]; R [K,K,2nt-1] basis lag correlations
     DevBuf<float2> hpH, hpTw;                    // highpass spectrum and twiddles (FFT form)
+    DevBuf<float> cf2, pre_cf, Pc_hi, Pc_lo;     // BF16 re-check: runner-up Cf, saved maxima, gathered projection
+    DevBuf<int32_t> rc_tiles, pre_im, rc_count;  // ... listed tiles, saved argmax, [tiles, flips, near columns]
+    int32_t* rc_host = nullptr;                  // pinned copy of rc_count (read by lss_get_stats)
+    cudaEvent_t rc_ev = nullptr;                 // recorded after that copy
+    bool rc_pending = false;
+    int64_t last_scored = 0;                     // samples of the last BF16 scoring
     int CKpad = 0;
     int sm_count = 0;
     DevBuf<unsigned int> bar;
@@ -116,6 +122,10 @@ struct lss_handle {
         rec_pc.release(); B0T.release(); Up16.release();
         B0T_hi.release(); B0T_lo.release(); Up_hi.release(); Up_lo.release();
         Uw16.release(); Uw_hi.release(); Uw_lo.release(); U.release(); R.release(); hpH.release(); hpTw.release();
+        cf2.release(); pre_cf.release(); Pc_hi.release(); Pc_lo.release(); rc_tiles.release(); pre_im.release();
+        rc_count.release();
+        if (rc_ev) cudaEventDestroy(rc_ev);
+        if (rc_host) cudaFreeHost(rc_host);
     }
 };
 
@@ -206,9 +216,12 @@ static int set_mixing(lss_handle* h, const float* M) {
     }
     // templates with the whitening folded in, for lss_sort_batch
     const bool bf16 = h->cfg.precision == LSS_PREC_BF16_RECHECK;
-    CK(launch_build_uw(h->U.p, h->Mw.p, h->T, h->K, C, h->CKpad, bf16 ? h->Uw16.p : nullptr,
-                       bf16 ? nullptr : h->Uw_hi.p, bf16 ? nullptr : h->Uw_lo.p, 0));
+    CK(launch_build_uw(h->U.p, h->Mw.p, h->T, h->K, C, h->CKpad, nullptr, h->Uw_hi.p, h->Uw_lo.p, 0));
     h->stats.launches += 1;
+    if (bf16) {
+        CK(launch_build_uw(h->U.p, h->Mw.p, h->T, h->K, C, h->CKpad, h->Uw16.p, nullptr, nullptr, 0));
+        h->stats.launches += 1;
+    }
     return LSS_OK;
 }
 
@@ -361,17 +374,41 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
         return LSS_ERR_ARG;
     }
     if (bf16) {
+        if (tc_plan(T, true).stages < 2) {
+            g_create_err = "too many templates for the FP32 re-check GEMM's shared memory";
+            return LSS_ERR_ARG;
+        }
         ALLOC(B0T, (size_t)h->N * h->CKpad);
         ALLOC(Up16, (size_t)plan.Tpad * h->CKpad);
         ALLOC(Uw16, (size_t)plan.Tpad * h->CKpad);
+        // FP32 re-check of near decisions: gathered projection rows, bookkeeping
+        const size_t rc_rows = (size_t)(h->N + RECHECK_TILE - 1) / RECHECK_TILE * RECHECK_TILE;
+        ALLOC(Pc_hi, rc_rows * h->CKpad);
+        ALLOC(Pc_lo, rc_rows * h->CKpad);
+        ALLOC(cf2, ld);
+        ALLOC(pre_cf, rc_rows);
+        ALLOC(pre_im, rc_rows);
+        ALLOC(rc_tiles, rc_rows / RECHECK_TILE);
+        ALLOC(rc_count, 4);
+        if (cudaMallocHost(&h->rc_host, 4 * sizeof(int32_t)) != cudaSuccess) {
+            g_create_err = "pinned host allocation failed";
+            return LSS_ERR_CUDA;
+        }
+        memset(h->rc_host, 0, 4 * sizeof(int32_t));
+        if (cudaEventCreateWithFlags(&h->rc_ev, cudaEventDisableTiming) != cudaSuccess) {
+            g_create_err = "event creation failed";
+            return LSS_ERR_CUDA;
+        }
     } else {
         ALLOC(B0T_hi, (size_t)h->N * h->CKpad);
         ALLOC(B0T_lo, (size_t)h->N * h->CKpad);
-        ALLOC(Up_hi, (size_t)plan.Tpad * h->CKpad);
-        ALLOC(Up_lo, (size_t)plan.Tpad * h->CKpad);
-        ALLOC(Uw_hi, (size_t)plan.Tpad * h->CKpad);
-        ALLOC(Uw_lo, (size_t)plan.Tpad * h->CKpad);
     }
+    // tf32 template splits: the FP32 path's scores, and the BF16 path's re-check
+    const int Tpad32 = tc_plan(T, true).Tpad;
+    ALLOC(Up_hi, (size_t)Tpad32 * h->CKpad);
+    ALLOC(Up_lo, (size_t)Tpad32 * h->CKpad);
+    ALLOC(Uw_hi, (size_t)Tpad32 * h->CKpad);
+    ALLOC(Uw_lo, (size_t)Tpad32 * h->CKpad);
     ALLOC(U, (size_t)T * K * C);
     const bool hp_fft = h->hpL >= 0 && h->hpL <= 1024;
     if (hp_fft) {
@@ -433,9 +470,13 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
             for (int e = 0; e < C * K; ++e) u16[(size_t)i * h->CKpad + e] = __float2bfloat16(up[(size_t)i * C * K + e]);
         CK(cudaMemcpy(h->Up16.p, u16.data(), u16.size() * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice));
         CK(cudaMemset(h->B0T.p, 0, (size_t)h->N * h->CKpad * sizeof(__nv_bfloat16)));
-    } else {
+        const size_t rc_bytes = (size_t)(h->N + RECHECK_TILE - 1) / RECHECK_TILE * RECHECK_TILE * h->CKpad * sizeof(float);
+        CK(cudaMemset(h->Pc_hi.p, 0, rc_bytes));
+        CK(cudaMemset(h->Pc_lo.p, 0, rc_bytes));
+    }
+    {
         // U_p split into tf32 hi (round half away, like cvt.rna.tf32.f32) and lo = x - hi
-        std::vector<float> hi((size_t)plan.Tpad * h->CKpad, 0.f), lo(hi.size(), 0.f);
+        std::vector<float> hi((size_t)Tpad32 * h->CKpad, 0.f), lo(hi.size(), 0.f);
         for (int i = 0; i < T; ++i)
             for (int e = 0; e < C * K; ++e) {
                 const float x = up[(size_t)i * C * K + e];
@@ -449,8 +490,10 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
             }
         CK(cudaMemcpy(h->Up_hi.p, hi.data(), hi.size() * sizeof(float), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(h->Up_lo.p, lo.data(), lo.size() * sizeof(float), cudaMemcpyHostToDevice));
-        CK(cudaMemset(h->B0T_hi.p, 0, (size_t)h->N * h->CKpad * sizeof(float)));
-        CK(cudaMemset(h->B0T_lo.p, 0, (size_t)h->N * h->CKpad * sizeof(float)));
+        if (!bf16) {
+            CK(cudaMemset(h->B0T_hi.p, 0, (size_t)h->N * h->CKpad * sizeof(float)));
+            CK(cudaMemset(h->B0T_lo.p, 0, (size_t)h->N * h->CKpad * sizeof(float)));
+        }
     }
     CK(cudaMemcpy(h->nm.p, nmv.data(), T * sizeof(float), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->wave.p, wave.data(), wave.size() * sizeof(float), cudaMemcpyHostToDevice));
@@ -490,12 +533,9 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
                 }
         CK(cudaMemcpy(h->R.p, r.data(), r.size() * sizeof(float), cudaMemcpyHostToDevice));
     }
-    if (bf16) {
-        CK(cudaMemset(h->Uw16.p, 0, (size_t)plan.Tpad * h->CKpad * sizeof(__nv_bfloat16)));
-    } else {
-        CK(cudaMemset(h->Uw_hi.p, 0, (size_t)plan.Tpad * h->CKpad * sizeof(float)));
-        CK(cudaMemset(h->Uw_lo.p, 0, (size_t)plan.Tpad * h->CKpad * sizeof(float)));
-    }
+    if (bf16) CK(cudaMemset(h->Uw16.p, 0, (size_t)plan.Tpad * h->CKpad * sizeof(__nv_bfloat16)));
+    CK(cudaMemset(h->Uw_hi.p, 0, (size_t)Tpad32 * h->CKpad * sizeof(float)));
+    CK(cudaMemset(h->Uw_lo.p, 0, (size_t)Tpad32 * h->CKpad * sizeof(float)));
     if (nC > 0) {
         CK(cudaMemcpy(h->Ucc.p, t->Ucc, (size_t)nC * T * K * sizeof(float), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(h->iCC.p, t->iCC, (size_t)nC * C * sizeof(int64_t), cudaMemcpyHostToDevice));
@@ -523,6 +563,17 @@ int lss_get_config(const lss_handle* h, lss_config* out) {
 int lss_get_stats(const lss_handle* h, lss_stats* out) {
     if (!h || !out) return LSS_ERR_ARG;
     *out = h->stats;
+    if (h->rc_pending) {
+        // re-check counts of the last BF16 scoring, copied back asynchronously
+        const cudaError_t e = cudaEventSynchronize(h->rc_ev);
+        if (e != cudaSuccess) {
+            lss::set_thread_error((std::string("lss_get_stats: ") + cudaGetErrorString(e)).c_str());
+            return LSS_ERR_CUDA;
+        }
+        out->recheck_columns = h->rc_host[2];
+        out->recheck_flips = h->rc_host[1];
+        out->recheck_rescored = std::min<int64_t>((int64_t)h->rc_host[0] * RECHECK_TILE, h->last_scored);
+    }
     return LSS_OK;
 }
 
@@ -594,9 +645,33 @@ static int run_scores(lss_handle* h, const float* X, int64_t ldx, int64_t N, flo
     if (h->cfg.precision == LSS_PREC_BF16_RECHECK) {
         CK(launch_pca_proj_t(X, ldx, h->C, N, h->wpca.p, h->K, h->nt, h->B0T.p, h->CKpad, s));
         h->mark(5, s);
+        TcExtra ex;
+        ex.cf2 = h->cf2.p;
         CK(launch_score_tc(h->B0T.p, h->CKpad, (int)N, folded ? h->Uw16.p : h->Up16.p, h->T, h->CKpad, h->nm.p, B,
-                           h->ld, h->cfmax.p, h->imax.p, h->nt, h->status.p, h->sm_count, s));
-        h->stats.launches += 2;
+                           h->ld, h->cfmax.p, h->imax.p, h->nt, h->status.p, h->sm_count, s, ex));
+        // FP32 re-check of the tiles holding columns whose decisions lie within
+        // the margin; the tile list and its length stay on the device
+        const float th2 = h->cfg.th_learned * h->cfg.th_learned;
+        CK(launch_recheck_select(h->cfmax.p, h->cf2.p, h->imax.p, (int)N, h->nt, th2, h->rc_tiles.p, h->pre_cf.p,
+                                 h->pre_im.p, h->rc_count.p, s));
+        CK(launch_pca_proj_tiles_tf32(X, ldx, h->C, N, h->wpca.p, h->K, h->nt, h->rc_tiles.p, h->rc_count.p,
+                                      h->Pc_hi.p, h->Pc_lo.p, h->CKpad, s));
+        TcExtra ex2;
+        ex2.rowmap = h->rc_tiles.p;
+        ex2.map_rows = RECHECK_TILE;
+        ex2.count_dev = h->rc_count.p;
+        ex2.ncols = (int)N;
+        const int max_rows = (int)((N + RECHECK_TILE - 1) / RECHECK_TILE * RECHECK_TILE);
+        CK(launch_score_tc_tf32x3(h->Pc_hi.p, h->Pc_lo.p, h->CKpad, max_rows, folded ? h->Uw_hi.p : h->Up_hi.p,
+                                  folded ? h->Uw_lo.p : h->Up_lo.p, h->T, h->CKpad, h->nm.p, B, h->ld, h->cfmax.p,
+                                  h->imax.p, h->nt, h->status.p, h->sm_count, s, ex2));
+        CK(launch_recheck_flips(h->cfmax.p, h->imax.p, h->rc_tiles.p, h->pre_cf.p, h->pre_im.p, h->rc_count.p, (int)N,
+                                th2, s));
+        CK(cudaMemcpyAsync(h->rc_host, h->rc_count.p, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        CK(cudaEventRecord(h->rc_ev, s));
+        h->rc_pending = true;
+        h->last_scored = N;
+        h->stats.launches += 6;
         h->mark(6, s);
         if (maxima_ready) *maxima_ready = true;
         return LSS_OK;

@@ -51,15 +51,26 @@ struct TcPlan {
     int kblock;    // K elements per pipeline stage
 };
 TcPlan tc_plan(int T, bool tf32);
+// Optional epilogue behaviour of the score GEMM.
+struct TcExtra {
+    // GEMM row r scores sample rowmap[r / map_rows] * map_rows + r % map_rows
+    // (re-check tiles); rows beyond count_dev[0] * map_rows are skipped
+    const int32_t* rowmap = nullptr;
+    int map_rows = 1;
+    const int32_t* count_dev = nullptr;
+    int ncols = 0;                    // batch samples when rowmap is set
+    float* cf2 = nullptr;             // runner-up Cf per sample
+};
 // B[t, s] (row stride ldb) = sum_kk B0T[s, kk] * Up[t, kk] with B0T [N, ldk] and Up [Tpad, CKpad]
 // bf16, CKpad a multiple of 64; also writes the column maxima cfmax/imax of Cf.
 cudaError_t launch_score_tc(const __nv_bfloat16* B0T, int64_t ldk, int N, const __nv_bfloat16* Up, int T, int CKpad,
                             const float* nm, float* Bout, int64_t ldb, float* cfmax, int32_t* imax, int nt,
-                            int32_t* status, int grid, cudaStream_t s);
+                            int32_t* status, int grid, cudaStream_t s, const TcExtra& ex = TcExtra());
 // FP32-class variant (3xTF32): operands split into tf32 hi + lo parts stored as fp32.
 cudaError_t launch_score_tc_tf32x3(const float* B0T_hi, const float* B0T_lo, int64_t ldk, int N, const float* Up_hi,
                                    const float* Up_lo, int T, int CKpad, const float* nm, float* Bout, int64_t ldb,
-                                   float* cfmax, int32_t* imax, int nt, int32_t* status, int grid, cudaStream_t s);
+                                   float* cfmax, int32_t* imax, int nt, int32_t* status, int grid, cudaStream_t s,
+                                   const TcExtra& ex = TcExtra());
 // transposed projection split into tf32 hi/lo parts (fp32 containers) for the 3xTF32 GEMM
 cudaError_t launch_pca_proj_t_tf32(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
                                    int32_t nt, float* hi, float* lo, int64_t ldk, cudaStream_t s);
@@ -67,6 +78,18 @@ cudaError_t launch_pca_proj_t_tf32(const float* X, int64_t ldx, int32_t C, int64
 // U_w[t, c'*K + k] = sum_c U[t,k,c] Mw[c,c'] in GEMM layout: bf16 (out16) or tf32 hi/lo
 cudaError_t launch_build_uw(const float* U, const float* Mw, int32_t T, int32_t K, int32_t C, int64_t ldk,
                             __nv_bfloat16* out16, float* hi, float* lo, cudaStream_t s);
+
+// FP32 re-check of the BF16 path (score.cu)
+constexpr int RECHECK_TILE = 64;  // samples per re-check tile (= projection CTA width)
+cudaError_t launch_recheck_select(const float* cfmax, const float* cf2, const int32_t* imax, int32_t N, int32_t nt,
+                                  float th2, int32_t* tiles, float* pre_cf, int32_t* pre_im, int32_t* count,
+                                  cudaStream_t s);
+// projection of the listed sample tiles into rows x*RECHECK_TILE.. (tf32 hi/lo), as launch_pca_proj_t_tf32
+cudaError_t launch_pca_proj_tiles_tf32(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
+                                       int32_t nt, const int32_t* tiles, const int32_t* ntiles, float* hi, float* lo,
+                                       int64_t ldk, cudaStream_t s);
+cudaError_t launch_recheck_flips(const float* cfmax, const int32_t* imax, const int32_t* tiles, const float* pre_cf,
+                                 const int32_t* pre_im, int32_t* count, int32_t N, float th2, cudaStream_t s);
 
 // ---- matching pursuit (mp.cu) ----
 struct MPArgs {

@@ -122,14 +122,18 @@ __device__ __forceinline__ float tf32_rna(float x) {
 template <int KPC, int PC, bool TF32>
 __global__ void __launch_bounds__(256) k_pca_proj_t(const float* __restrict__ X, int64_t ldx, int32_t C, int64_t N,
                                                     const float* __restrict__ wpca, int32_t nt, void* __restrict__ out0,
-                                                    float* __restrict__ out_lo, int64_t ldk) {
+                                                    float* __restrict__ out_lo, int64_t ldk,
+                                                    const int32_t* __restrict__ tiles, const int32_t* __restrict__ ntiles) {
     extern __shared__ float sm[];
+    // tiles != null: CTA x projects sample tile tiles[x] into output rows x*PT_S.. (the first *ntiles entries)
+    if (tiles && (int)blockIdx.x >= *ntiles) return;
+    const int64_t s0 = tiles ? (int64_t)tiles[blockIdx.x] * PT_S : (int64_t)blockIdx.x * PT_S;
+    const int64_t o0 = (int64_t)blockIdx.x * PT_S;
     const int ntp = (nt + 7) & ~7;
     const int xw = PT_S + ntp + 9;                 // staged samples per channel row (odd: no bank conflicts)
     float* ws = sm;                                // [KPC][ntp]
     float* xs = ws + KPC * ntp;                    // [PC][xw]
     float* stage = xs + PC * xw + ((PC * xw) & 3 ? 4 - ((PC * xw) & 3) : 0);  // [PT_S][PC*KPC], 16-byte aligned
-    const int64_t s0 = (int64_t)blockIdx.x * PT_S;
     const int c0 = blockIdx.y * PC;
     const int nc = min(PC, C - c0);
     const int half = nt / 2;
@@ -185,7 +189,7 @@ __global__ void __launch_bounds__(256) k_pca_proj_t(const float* __restrict__ X,
         const int64_t s = s0 + r;
         if (s >= N) continue;
         const float4 v = *reinterpret_cast<const float4*>(stage + r * (PC * KPC) + 4 * q);
-        const int64_t o = s * ldk + (int64_t)c0 * KPC + 4 * q;
+        const int64_t o = (o0 + r) * ldk + (int64_t)c0 * KPC + 4 * q;
         if (TF32) {
             const float4 hi = make_float4(tf32_rna(v.x), tf32_rna(v.y), tf32_rna(v.z), tf32_rna(v.w));
             const float4 lo = make_float4(__fsub_rn(v.x, hi.x), __fsub_rn(v.y, hi.y), __fsub_rn(v.z, hi.z),
@@ -206,7 +210,7 @@ __global__ void __launch_bounds__(256) k_pca_proj_t(const float* __restrict__ X,
         const int64_t s = s0 + r;
         if (s >= N) continue;
         const float v = stage[r * (PC * KPC) + j];
-        const int64_t o = s * ldk + (int64_t)c0 * KPC + j;
+        const int64_t o = (o0 + r) * ldk + (int64_t)c0 * KPC + j;
         if (TF32) {
             const float hi = tf32_rna(v);
             static_cast<float*>(out0)[o] = hi;
@@ -219,41 +223,49 @@ __global__ void __launch_bounds__(256) k_pca_proj_t(const float* __restrict__ X,
 
 template <int KPC, bool TF32>
 static cudaError_t launch_pjt(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t nt,
-                              void* out0, float* out_lo, int64_t ldk, cudaStream_t s) {
+                              void* out0, float* out_lo, int64_t ldk, const int32_t* tiles, const int32_t* ntiles,
+                              cudaStream_t s) {
     constexpr int PC = 32;
     const int ntp = (nt + 7) & ~7;
     const size_t smem = sizeof(float) * ((size_t)KPC * ntp + (size_t)PC * (PT_S + ntp + 9) + 4 + (size_t)PT_S * PC * KPC);
     if (smem > 48 * 1024)
         cudaFuncSetAttribute(k_pca_proj_t<KPC, PC, TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     dim3 grid((unsigned)((N + PT_S - 1) / PT_S), (unsigned)((C + PC - 1) / PC));
-    k_pca_proj_t<KPC, PC, TF32><<<grid, 256, smem, s>>>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk);
+    k_pca_proj_t<KPC, PC, TF32><<<grid, 256, smem, s>>>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles);
     return cudaGetLastError();
 }
 
 template <bool TF32>
 static cudaError_t pjt_dispatch(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
-                                int32_t nt, void* out0, float* out_lo, int64_t ldk, cudaStream_t s) {
+                                int32_t nt, void* out0, float* out_lo, int64_t ldk, const int32_t* tiles,
+                                const int32_t* ntiles, cudaStream_t s) {
     switch (K) {
-        case 1: return launch_pjt<1, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, s);
-        case 2: return launch_pjt<2, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, s);
-        case 3: return launch_pjt<3, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, s);
-        case 4: return launch_pjt<4, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, s);
-        case 5: return launch_pjt<5, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, s);
-        case 6: return launch_pjt<6, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, s);
-        case 7: return launch_pjt<7, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, s);
-        case 8: return launch_pjt<8, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, s);
+        case 1: return launch_pjt<1, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles, s);
+        case 2: return launch_pjt<2, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles, s);
+        case 3: return launch_pjt<3, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles, s);
+        case 4: return launch_pjt<4, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles, s);
+        case 5: return launch_pjt<5, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles, s);
+        case 6: return launch_pjt<6, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles, s);
+        case 7: return launch_pjt<7, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles, s);
+        case 8: return launch_pjt<8, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles, s);
         default: return cudaErrorInvalidValue;
     }
 }
 
 cudaError_t launch_pca_proj_t(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
                               int32_t nt, __nv_bfloat16* B0T, int64_t ldk, cudaStream_t s) {
-    return pjt_dispatch<false>(X, ldx, C, N, wpca, K, nt, B0T, nullptr, ldk, s);
+    return pjt_dispatch<false>(X, ldx, C, N, wpca, K, nt, B0T, nullptr, ldk, nullptr, nullptr, s);
 }
 
 cudaError_t launch_pca_proj_t_tf32(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
                                    int32_t nt, float* hi, float* lo, int64_t ldk, cudaStream_t s) {
-    return pjt_dispatch<true>(X, ldx, C, N, wpca, K, nt, hi, lo, ldk, s);
+    return pjt_dispatch<true>(X, ldx, C, N, wpca, K, nt, hi, lo, ldk, nullptr, nullptr, s);
+}
+
+cudaError_t launch_pca_proj_tiles_tf32(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
+                                       int32_t nt, const int32_t* tiles, const int32_t* ntiles, float* hi, float* lo,
+                                       int64_t ldk, cudaStream_t s) {
+    return pjt_dispatch<true>(X, ldx, C, N, wpca, K, nt, hi, lo, ldk, tiles, ntiles, s);
 }
 
 // Templates with the whitening folded in, in the score GEMM's layout:
@@ -285,6 +297,120 @@ cudaError_t launch_build_uw(const float* U, const float* Mw, int32_t T, int32_t 
                             __nv_bfloat16* out16, float* hi, float* lo, cudaStream_t s) {
     dim3 grid((unsigned)((C + 127) / 128), (unsigned)(T * K));
     k_build_uw<<<grid, 128, 0, s>>>(U, Mw, T, K, C, ldk, out16, hi, lo);
+    return cudaGetLastError();
+}
+
+
+
+// ---------------------------------------------------------------------------
+// FP32 re-check of the BF16 path's near decisions (first round).
+//
+// A column s needs its FP32 score when its BF16 maximum Cf could be above the
+// threshold (best >= Th^2 (1 - m)) and a decision taken on it lies within the
+// relative margin m = 1/16:
+//   * the threshold itself: |best - Th^2| <= m Th^2;
+//   * the runner-up template: second >= best (1 - m);
+//   * the peak test: best is within m of the window maximum and another column
+//     of the window is within m of best.
+// (BF16 rounding of both GEMM operands moves Cf by about 1% at the scores
+// spikes have, so m is several times the error.) Selection works on 64-sample
+// tiles (the projection's CTA width): a tile holding any such column is listed,
+// projected in FP32 by the FP32 path's own projection kernel, split into tf32
+// hi/lo and re-scored by the 3xTF32 GEMM through the tile list, which
+// overwrites the tile's scores and column maxima with the FP32 path's values.
+// Counts stay on the device: count[0] = listed tiles, count[1] = flips,
+// count[2] = near-decision columns.
+// ---------------------------------------------------------------------------
+constexpr float RECHECK_MARGIN = 1.f / 16.f;
+constexpr int RS_TILE = 256;
+static_assert(RECHECK_TILE == PT_S, "re-check tiles are projection CTA tiles");
+static_assert(RS_TILE % RECHECK_TILE == 0, "selection CTAs cover whole re-check tiles");
+
+__global__ void __launch_bounds__(RS_TILE) k_recheck_select(const float* __restrict__ cfmax, const float* __restrict__ cf2,
+                                                            const int32_t* __restrict__ imax, int32_t N, int32_t nt,
+                                                            float th2, int32_t* __restrict__ tiles,
+                                                            float* __restrict__ pre_cf, int32_t* __restrict__ pre_im,
+                                                            int32_t* __restrict__ count) {
+    constexpr int NTL = RS_TILE / RECHECK_TILE;
+    __shared__ float v[RS_TILE + 2 * 256];
+    __shared__ int flag[NTL], slot[NTL];
+    const int s0 = blockIdx.x * RS_TILE;
+    for (int p = threadIdx.x; p < RS_TILE + 2 * nt; p += blockDim.x) {
+        const int s = s0 - nt + p;
+        v[p] = (s >= 0 && s < N) ? cfmax[s] : -1.f;
+    }
+    if (threadIdx.x < NTL) flag[threadIdx.x] = 0;
+    __syncthreads();
+    const int s = s0 + threadIdx.x;
+    const float best = v[threadIdx.x + nt];
+    bool sel = false;
+    if (s < N) {
+        const float m = RECHECK_MARGIN;
+        if (best >= th2 * (1.f - m)) {
+            float wmax = best, other = -1.f;
+            for (int d = -nt; d <= nt; ++d) {
+                if (d == 0) continue;
+                const float u = v[threadIdx.x + nt + d];
+                wmax = fmaxf(wmax, u);
+                other = fmaxf(other, u);
+            }
+            const bool near_thr = fabsf(best - th2) <= m * th2;
+            const bool near_tmpl = cf2[s] >= best * (1.f - m);
+            const bool near_peak = best >= wmax * (1.f - m) && other >= best * (1.f - m);
+            sel = near_thr || near_tmpl || near_peak;
+        }
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, sel);
+    if (bal) {
+        if ((threadIdx.x & 31) == 0) atomicAdd(count + 2, __popc(bal));
+        flag[threadIdx.x / RECHECK_TILE] = 1;
+    }
+    __syncthreads();
+    if (threadIdx.x < NTL) {
+        int sl = -1;
+        if (flag[threadIdx.x]) {
+            sl = atomicAdd(count, 1);
+            tiles[sl] = s0 / RECHECK_TILE + threadIdx.x;
+        }
+        slot[threadIdx.x] = sl;
+    }
+    __syncthreads();
+    const int sl = slot[threadIdx.x / RECHECK_TILE];
+    if (sl >= 0) {
+        const int64_t r = (int64_t)sl * RECHECK_TILE + threadIdx.x % RECHECK_TILE;
+        pre_cf[r] = (s < N) ? best : 0.f;
+        pre_im[r] = (s < N) ? imax[s] : 0;
+    }
+}
+
+cudaError_t launch_recheck_select(const float* cfmax, const float* cf2, const int32_t* imax, int32_t N, int32_t nt,
+                                  float th2, int32_t* tiles, float* pre_cf, int32_t* pre_im, int32_t* count,
+                                  cudaStream_t s) {
+    if (nt > 256) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(count, 0, 4 * sizeof(int32_t), s);
+    if (e != cudaSuccess) return e;
+    k_recheck_select<<<(N + RS_TILE - 1) / RS_TILE, RS_TILE, 0, s>>>(cfmax, cf2, imax, N, nt, th2, tiles, pre_cf,
+                                                                    pre_im, count);
+    return cudaGetLastError();
+}
+
+// Decisions the FP32 re-check changed: the best template, or the side of the
+// threshold the column maximum falls on.
+__global__ void k_recheck_flips(const float* __restrict__ cfmax, const int32_t* __restrict__ imax,
+                                const int32_t* __restrict__ tiles, const float* __restrict__ pre_cf,
+                                const int32_t* __restrict__ pre_im, const int32_t* __restrict__ count, int32_t N,
+                                float th2, int32_t* flips) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= count[0] * RECHECK_TILE) return;
+    const int s = tiles[r / RECHECK_TILE] * RECHECK_TILE + r % RECHECK_TILE;
+    if (s >= N) return;
+    if (imax[s] != pre_im[r] || ((cfmax[s] > th2) != (pre_cf[r] > th2))) atomicAdd(flips, 1);
+}
+
+cudaError_t launch_recheck_flips(const float* cfmax, const int32_t* imax, const int32_t* tiles, const float* pre_cf,
+                                 const int32_t* pre_im, int32_t* count, int32_t N, float th2, cudaStream_t s) {
+    const int rows = (N + RECHECK_TILE - 1) / RECHECK_TILE * RECHECK_TILE;
+    k_recheck_flips<<<(rows + 255) / 256, 256, 0, s>>>(cfmax, imax, tiles, pre_cf, pre_im, count, N, th2, count + 1);
     return cudaGetLastError();
 }
 

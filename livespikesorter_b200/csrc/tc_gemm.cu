@@ -61,6 +61,11 @@ struct Args {
     int32_t* imax;
     int nt;
     int32_t* status;
+    const int32_t* rowmap;    // GEMM row r scores sample rowmap[r / map_rows] * map_rows + r % map_rows (null: r)
+    int map_rows;
+    const int32_t* count_dev; // rows = min(N, count_dev[0] * map_rows) (null: N)
+    int ncols;                // samples in the batch (edge columns are the first/last nt)
+    float* cf2;               // runner-up Cf of each column (null: not tracked)
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -185,20 +190,30 @@ __device__ __forceinline__ void st_keep(float* a, float v, uint64_t pol) {
     asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(a), "f"(v), "l"(pol) : "memory");
 }
 
-// Running column maximum of Cf with the rounds kernel's exact rule.
+// Running column maximum of Cf with the rounds kernel's exact rule, plus the
+// runner-up (to within the 3-ulp reciprocal approximation) when asked for.
 struct ColMax {
     float best = -1.f;
     float thr = -1.f;
+    float second = -1.f;
     int bi = 0;
+    template <bool SECOND>
     __device__ __forceinline__ void consider(float b, float nmv, float inv, int t) {
         const float r = fmaxf(b, 0.f);
         const float sq = __fmul_rn(r, r);
-        if (__fmul_rn(sq, inv) < thr) return;
+        const float approx = __fmul_rn(sq, inv);
+        if (approx < thr) {
+            if (SECOND) second = fmaxf(second, approx);
+            return;
+        }
         const float cf = __fdiv_rn(sq, nmv);
         if (cf > best) {
+            if (SECOND) second = fmaxf(second, best);
             best = cf;
             bi = t;
             thr = (cf >= 1e-30f) ? __fmul_rd(cf, 0.99999952316f) : -1.f;
+        } else if (SECOND) {
+            second = fmaxf(second, cf);
         }
     }
 };
@@ -258,7 +273,8 @@ __global__ void __launch_bounds__(THREADS, 1)
     fence_after();
     const uint32_t tmem = *tmem_slot;
 
-    const int ntiles = (a.N + BM - 1) / BM;
+    const int rows = a.count_dev ? min(a.N, a.count_dev[0] * a.map_rows) : a.N;
+    const int ntiles = (rows + BM - 1) / BM;
     const int npass = (a.Tpad + MAX_NP - 1) / MAX_NP;
 
     if (warp == 0) {
@@ -365,9 +381,11 @@ __global__ void __launch_bounds__(THREADS, 1)
         int acc = 0;
         bool ok = true;
         for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-            const int n = tile * BM + row;
-            const bool valid = n < a.N;
-            const bool edge = (n < a.nt) || (n >= a.N - a.nt);
+            const int gr = tile * BM + row;
+            const int n = (a.rowmap && gr < rows) ? a.rowmap[gr / a.map_rows] * a.map_rows + gr % a.map_rows : gr;
+            const bool valid = gr < rows && n < a.ncols;
+            const bool edge = (n < a.nt) || (n >= a.ncols - a.nt);
+            const bool second = a.cf2 != nullptr;
             ColMax m;
             for (int p = 0; p < npass; ++p) {
                 const int np = min(MAX_NP, a.Tpad - p * MAX_NP);
@@ -385,7 +403,10 @@ __global__ void __launch_bounds__(THREADS, 1)
                             if (t < a.T) {
                                 const float v = __uint_as_float(r[j]);
                                 st_keep(a.Bout + (int64_t)t * a.ldb + n, v, pol);
-                                if (!edge) m.consider(v, s_nm[t], s_inv[t], t);
+                                if (!edge) {
+                                    if (second) m.consider<true>(v, s_nm[t], s_inv[t], t);
+                                    else m.consider<false>(v, s_nm[t], s_inv[t], t);
+                                }
                             }
                         }
                     }
@@ -399,6 +420,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             if (ok && valid) {
                 a.cfmax[n] = edge ? 0.f : m.best;
                 a.imax[n] = edge ? 0 : m.bi;
+                if (second) a.cf2[n] = edge ? 0.f : m.second;
             }
         }
     }
@@ -474,7 +496,7 @@ TcPlan tc_plan(int T, bool tf32) {
 template <bool TF32>
 static cudaError_t launch_tc(const void* A, const void* Alo, int64_t ldk, int N, const void* Bm, const void* Blo, int T,
                              int CKpad, const float* nm, float* Bout, int64_t ldb, float* cfmax, int32_t* imax, int nt,
-                             int32_t* status, int grid, cudaStream_t s) {
+                             int32_t* status, int grid, cudaStream_t s, const TcExtra& ex) {
     const TcPlan p = tc_plan(T, TF32);
     if (p.stages < 2 || CKpad % p.kblock) return cudaErrorInvalidValue;
     CUtensorMap ma, malo, mb, mblo;
@@ -504,6 +526,11 @@ static cudaError_t launch_tc(const void* A, const void* Alo, int64_t ldk, int N,
     a.imax = imax;
     a.nt = nt;
     a.status = status;
+    a.rowmap = ex.rowmap;
+    a.map_rows = ex.map_rows;
+    a.count_dev = ex.count_dev;
+    a.ncols = ex.rowmap ? ex.ncols : N;
+    a.cf2 = ex.cf2;
     cudaError_t e = cudaFuncSetAttribute(tc::k_score_tc<TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
     if (e != cudaSuccess) return e;
     const int ntiles = (N + tc::BM - 1) / tc::BM;
@@ -513,15 +540,17 @@ static cudaError_t launch_tc(const void* A, const void* Alo, int64_t ldk, int N,
 
 cudaError_t launch_score_tc(const __nv_bfloat16* B0T, int64_t ldk, int N, const __nv_bfloat16* Up, int T, int CKpad,
                             const float* nm, float* Bout, int64_t ldb, float* cfmax, int32_t* imax, int nt,
-                            int32_t* status, int grid, cudaStream_t s) {
-    return launch_tc<false>(B0T, nullptr, ldk, N, Up, nullptr, T, CKpad, nm, Bout, ldb, cfmax, imax, nt, status, grid, s);
+                            int32_t* status, int grid, cudaStream_t s, const TcExtra& ex) {
+    return launch_tc<false>(B0T, nullptr, ldk, N, Up, nullptr, T, CKpad, nm, Bout, ldb, cfmax, imax, nt, status, grid, s,
+                            ex);
 }
 
 cudaError_t launch_score_tc_tf32x3(const float* B0T_hi, const float* B0T_lo, int64_t ldk, int N, const float* Up_hi,
                                    const float* Up_lo, int T, int CKpad, const float* nm, float* Bout, int64_t ldb,
-                                   float* cfmax, int32_t* imax, int nt, int32_t* status, int grid, cudaStream_t s) {
+                                   float* cfmax, int32_t* imax, int nt, int32_t* status, int grid, cudaStream_t s,
+                                   const TcExtra& ex) {
     return launch_tc<true>(B0T_hi, B0T_lo, ldk, N, Up_hi, Up_lo, T, CKpad, nm, Bout, ldb, cfmax, imax, nt, status, grid,
-                           s);
+                           s, ex);
 }
 
 }  // namespace lss

@@ -199,7 +199,7 @@ class Sorter:
         s = LssStats()
         self._check(self._lib.lss_get_stats(self._h, s))
         return dict(rounds=s.rounds, spikes=s.spikes, recheck_columns=s.recheck_columns,
-                    recheck_flips=s.recheck_flips, launches=s.launches)
+                    recheck_flips=s.recheck_flips, recheck_rescored=s.recheck_rescored, launches=s.launches)
 
     def set_profiling(self, on: bool = True):
         self._check(self._lib.lss_set_profiling(self._h, int(on)))

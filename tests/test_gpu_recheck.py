@@ -1,0 +1,88 @@
+"""FP32 re-check of the BF16 score path.
+
+The BF16 GEMM tracks each column's best and runner-up Cf. Columns whose
+decision lies within the re-check margin (best Cf near Th^2, runner-up
+template near the best, or a neighbour within +-nt near the column's value)
+mark their 64-sample tile; marked tiles are projected by the FP32 path's own
+projection kernel and rescored by its 3xTF32 GEMM through the tile list. Their
+scores must then be bit-identical to the FP32 path, and the sorted spikes must
+agree with the FP32 path on all but a small fraction.
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+
+def _fixture():
+    g = np.load(GOLDEN / 'ks4_extract_c32_t12.npz')
+    C, T, NT, nt, nt0min, nC, K, nb = [int(v) for v in g['params']]
+    kw = dict(U=g['U'], wPCA=g['wPCA'], ctc=g['ctc'], Wrot=g['Wrot'], hp_filter=g['hp_filter'], iCC=g['iCC'],
+              iU=g['iU'], Ucc=g['Ucc'], NT=NT, nt0min=nt0min, Th=float(g['Th']))
+    return g, kw
+
+
+def test_rechecked_columns_equal_fp32_scores():
+    from livespikesorter_b200.sorter import Sorter
+    g, kw = _fixture()
+    X = torch.from_numpy(g['X_1']).cuda()
+    s32 = Sorter(**kw)
+    s16 = Sorter(precision='bf16', **kw)
+    B32 = s32.scores(X)
+    B16 = s16.scores(X)
+    st = s16.stats()
+    assert 0 < st['recheck_columns'] <= st['recheck_rescored']
+    same = (B16 == B32).all(dim=0)
+    # every re-scored column is bit-identical to the FP32 path (a column the
+    # BF16 GEMM got exactly right by chance only adds to the count)
+    assert int(same.sum()) >= st['recheck_rescored']
+    # columns whose FP32 decision sits at the threshold are among them
+    nt = int(g['params'][3])
+    nm = (torch.from_numpy(g['U']).double() ** 2).sum((1, 2)).cuda()
+    cf = (torch.relu(B32.double()) ** 2 / nm[:, None]).max(0).values
+    cf[:nt] = 0
+    cf[-nt:] = 0
+    th2 = kw['Th'] ** 2
+    near = (cf - th2).abs() <= th2 / 64
+    assert bool(same[near].all())
+
+
+def test_bf16_recheck_sort_batch_agrees_with_fp32():
+    from livespikesorter_b200.sorter import Sorter
+    g, kw = _fixture()
+    NT, nt, nb = kw['NT'], int(g['params'][3]), int(g['params'][7])
+    s32 = Sorter(**kw)
+    s16 = Sorter(precision='bf16', **kw)
+    for ib in range(nb):
+        rows = g['raw'][0:NT + nt] if ib == 0 else g['raw'][ib * NT - nt: ib * NT + NT + nt]
+        r32 = s32.sort_batch(rows, ib, nb)
+        r16 = s16.sort_batch(rows, ib, nb)
+        a = set(zip(r32['time'].tolist(), r32['template'].tolist()))
+        b = set(zip(r16['time'].tolist(), r16['template'].tolist()))
+        assert len(a) > 0
+        assert len(a & b) >= 0.99 * max(len(a), len(b)), (ib, len(a), len(b), len(a & b))
+
+
+def test_bf16_recheck_agreement_on_synthetic_recording():
+    from livespikesorter_b200 import synth
+    from livespikesorter_b200.sorter import Sorter
+    setup, rec = synth.config(1, duration_s=4.0, seed=17, T=400)
+    s32 = Sorter.from_setup(setup)
+    s16 = Sorter.from_setup(setup, precision='bf16')
+    NT, nt = setup.NT, setup.nt
+    ib = 1
+    rows = np.ascontiguousarray(rec.raw[ib * NT - nt: ib * NT + NT + nt])
+    M = setup.drift_matrix(rec.dshift[ib])
+    s32.set_drift(M)
+    s16.set_drift(M)
+    r32 = s32.sort_batch(rows, ib, rec.n_batches)
+    r16 = s16.sort_batch(rows, ib, rec.n_batches)
+    st = s16.stats()
+    a = set(zip(r32['time'].tolist(), r32['template'].tolist()))
+    b = set(zip(r16['time'].tolist(), r16['template'].tolist()))
+    assert len(a) > 1000
+    assert st['recheck_columns'] > 0
+    assert len(a & b) >= 0.99 * max(len(a), len(b)), (len(a), len(b), len(a & b), st)
