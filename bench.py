@@ -191,7 +191,10 @@ def run_b200(args):
     if top == 'mp_ms':
         ach = mp_bytes / (mean_st['mp_ms'] / 1e3) / 1e9
         roof = {'kernel': 'k_mp (matching pursuit)', 'bound': 'hbm', 'achieved': ach, 'peak': hbm, 'unit': 'GB/s',
-                'frac': ach / hbm, 'traffic': None, 'peak_source': src}
+                'frac': ach / hbm, 'traffic': profile_traffic('k_mp_384ch_400t.md') if T == 400 else None,
+                'traffic_source': 'ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of this workload '
+                                  '(profiles/k_mp_384ch_400t.md)',
+                'algorithmic_bytes': mp_bytes, 'peak_source': src}
     else:
         ach = gemm_flops / (mean_st['score_ms'] / 1e3) / 1e12
         roof = {'kernel': 'k_score_tc (tcgen05 3xTF32 score GEMM)' if args.precision == 'fp32'
@@ -220,6 +223,17 @@ def run_b200(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(out))
+
+
+def profile_traffic(name):
+    """DRAM bytes per launch recorded in a committed ncu summary (None if absent)."""
+    f = ROOT / 'profiles' / name
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.startswith('dram_bytes_per_launch:'):
+            return int(line.split(':')[1])
+    return None
 
 
 def bf16_report(s16, setup, local, rows_d, drifts, ids, nb):

@@ -108,39 +108,6 @@ cudaError_t launch_xres(const float* X, int64_t ldx, int32_t C, int32_t N, int32
     return cudaGetLastError();
 }
 
-// One CTA per spike; thread (j, k) computes one feature.
-__global__ void k_pc_features(const float* __restrict__ Xres, int64_t ldx, int32_t nt, int32_t K, int32_t nC,
-                              int32_t C, int32_t T, const float* __restrict__ wpca,
-                              const int64_t* __restrict__ iCC, const int64_t* __restrict__ iU,
-                              const float* __restrict__ Ucc, const int32_t* __restrict__ sp_x,
-                              const int32_t* __restrict__ sp_y, const float* __restrict__ sp_amp,
-                              float* __restrict__ tF) {
-    const int i = blockIdx.x;
-    const int f = threadIdx.x;
-    if (f >= nC * K) return;
-    const int j = f / K, k = f % K;
-    const int x = sp_x[i], y = sp_y[i];
-    const int64_t ch = iCC[(int64_t)j * C + iU[y]];
-    const float* xr = Xres + ch * ldx + (x - nt / 2);
-    const float* w = wpca + (int64_t)k * nt;
-    float acc = 0.f;
-    for (int m = 0; m < nt; ++m) acc = fmaf(xr[m], w[m], acc);
-    const float off = __fmul_rn(sp_amp[i], Ucc[((int64_t)j * T + y) * K + k]);
-    tF[(int64_t)i * nC * K + f] = __fadd_rn(acc, off);
-}
-
-cudaError_t launch_pc_features(const float* Xres, int64_t ldx, int32_t nt, int32_t K, int32_t nC,
-                               int32_t C, int32_t T, const float* wpca, const int64_t* iCC,
-                               const int64_t* iU, const float* Ucc, const int32_t* sp_x,
-                               const int32_t* sp_y, const float* sp_amp, const int32_t* counters,
-                               int32_t n, float* tF, cudaStream_t s) {
-    (void)counters;
-    if (n <= 0) return cudaSuccess;
-    const int threads = ((nC * K + 31) / 32) * 32;
-    k_pc_features<<<n, threads, 0, s>>>(Xres, ldx, nt, K, nC, C, T, wpca, iCC, iU, Ucc, sp_x, sp_y, sp_amp, tF);
-    return cudaGetLastError();
-}
-
 // Records: one CTA computes every kept spike's output slot with ballot scans
 // (only batch 0 drops spikes, those aligned before the recording start), then
 // a grid writes the slots and their PC features in parallel.

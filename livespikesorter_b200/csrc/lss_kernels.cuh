@@ -33,9 +33,7 @@ cudaError_t launch_highpass_fft(const float* X1, int64_t ldx, int32_t C, int64_t
 cudaError_t launch_sgemm(const float* A, int64_t lda, const float* B, int64_t ldb, float* Cm, int64_t ldc,
                          int M, int N, int K, cudaStream_t s);
 
-// ---- temporal basis projection (score.cu): B0[c*K + k, s] ----
-cudaError_t launch_pca_proj(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
-                            int32_t nt, float* B0, int64_t ldb0, cudaStream_t s);
+// ---- temporal basis projection (score.cu) ----
 // transposed bf16 variant for the tensor-core GEMM: B0T[s, c*K + k], row stride ldk
 cudaError_t launch_pca_proj_t(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
                               int32_t nt, __nv_bfloat16* B0T, int64_t ldk, cudaStream_t s);
@@ -130,11 +128,6 @@ cudaError_t launch_xres(const float* X, int64_t ldx, int32_t C, int32_t N, int32
                         const int32_t* sp_x, const int32_t* sp_y, const float* sp_amp,
                         const int32_t* round_start, const int32_t* counters, int32_t rounds,
                         float* Xres, int32_t* status, cudaStream_t s);
-cudaError_t launch_pc_features(const float* Xres, int64_t ldx, int32_t nt, int32_t K, int32_t nC,
-                               int32_t C, int32_t T, const float* wpca, const int64_t* iCC,
-                               const int64_t* iU, const float* Ucc, const int32_t* sp_x,
-                               const int32_t* sp_y, const float* sp_amp, const int32_t* counters,
-                               int32_t n, float* tF, cudaStream_t s);
 // slot: scratch [n] for the output position of each spike
 cudaError_t launch_records(const int32_t* sp_x, const int32_t* sp_y, const float* sp_amp, const float* tF,
                            int32_t* slot, int32_t n, int32_t feat_len, int64_t ibatch, int32_t nt,

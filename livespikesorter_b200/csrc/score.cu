@@ -4,100 +4,11 @@
 // kilosort/template_matching.py:145 (conv1d kernel, myGPUhelpers.cu:355-399).
 // The row order (c, k) lets the score GEMM contract over c*K + k with the
 // template matrix permuted once at set-up to U_p[t, c*K + k] = U[t, k, c].
-//
-// CTA: one channel, PJ_TILE outputs for all K components; thread: 8
-// consecutive samples x K components with a sliding register window (one
-// shared load of X per 8*K FMAs).
 #include "lss_kernels.cuh"
 
 #include <cuda_bf16.h>
 
 namespace lss {
-
-constexpr int PJ_TILE = 1024;
-constexpr int PJ_THREADS = PJ_TILE / 8;
-
-template <int KPC>
-__global__ void __launch_bounds__(PJ_THREADS) k_pca_proj(const float* __restrict__ X, int64_t ldx, int64_t N,
-                                                         const float* __restrict__ wpca, int32_t nt,
-                                                         float* __restrict__ B0, int64_t ldb0) {
-    extern __shared__ float sm[];
-    const int ntp = (nt + 7) & ~7;
-    float* ws = sm;                  // [KPC][ntp]
-    float* xs = sm + KPC * ntp;      // [PJ_TILE + ntp + 8]
-    const int c = blockIdx.y;
-    const int64_t s0 = (int64_t)blockIdx.x * PJ_TILE;
-    const int half = nt / 2;
-    for (int e = threadIdx.x; e < KPC * ntp; e += blockDim.x) {
-        const int k = e / ntp, m = e % ntp;
-        ws[e] = (m < nt) ? wpca[k * nt + m] : 0.f;
-    }
-    const float* xrow = X + (int64_t)c * ldx;
-    const int nx = PJ_TILE + ntp + 8;
-    for (int p = threadIdx.x; p < nx; p += blockDim.x) {
-        const int64_t g = s0 - half + p;
-        xs[p] = (g >= 0 && g < N) ? xrow[g] : 0.f;
-    }
-    __syncthreads();
-    float acc[KPC][8];
-#pragma unroll
-    for (int k = 0; k < KPC; ++k)
-#pragma unroll
-        for (int r = 0; r < 8; ++r) acc[k][r] = 0.f;
-    const int o = threadIdx.x * 8;
-    float w[16];
-#pragma unroll
-    for (int r = 0; r < 8; ++r) w[r] = xs[o + r];
-    for (int mb = 0; mb < ntp; mb += 8) {
-#pragma unroll
-        for (int r = 0; r < 8; ++r) w[8 + r] = xs[o + mb + 8 + r];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-#pragma unroll
-            for (int k = 0; k < KPC; ++k) {
-                const float t = ws[k * ntp + mb + u];
-#pragma unroll
-                for (int r = 0; r < 8; ++r) acc[k][r] = fmaf(t, w[r + u], acc[k][r]);
-            }
-        }
-#pragma unroll
-        for (int r = 0; r < 8; ++r) w[r] = w[8 + r];
-    }
-#pragma unroll
-    for (int k = 0; k < KPC; ++k) {
-        float* row = B0 + ((int64_t)c * KPC + k) * ldb0;
-#pragma unroll
-        for (int r = 0; r < 8; ++r) {
-            const int64_t s = s0 + o + r;
-            if (s < N) row[s] = acc[k][r];
-        }
-    }
-}
-
-template <int KPC>
-static cudaError_t launch_pj(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t nt,
-                             float* B0, int64_t ldb0, cudaStream_t s) {
-    const int ntp = (nt + 7) & ~7;
-    const size_t smem = sizeof(float) * ((size_t)KPC * ntp + PJ_TILE + ntp + 8);
-    dim3 grid((unsigned)((N + PJ_TILE - 1) / PJ_TILE), (unsigned)C);
-    k_pca_proj<KPC><<<grid, PJ_THREADS, smem, s>>>(X, ldx, N, wpca, nt, B0, ldb0);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_pca_proj(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
-                            int32_t nt, float* B0, int64_t ldb0, cudaStream_t s) {
-    switch (K) {
-        case 1: return launch_pj<1>(X, ldx, C, N, wpca, nt, B0, ldb0, s);
-        case 2: return launch_pj<2>(X, ldx, C, N, wpca, nt, B0, ldb0, s);
-        case 3: return launch_pj<3>(X, ldx, C, N, wpca, nt, B0, ldb0, s);
-        case 4: return launch_pj<4>(X, ldx, C, N, wpca, nt, B0, ldb0, s);
-        case 5: return launch_pj<5>(X, ldx, C, N, wpca, nt, B0, ldb0, s);
-        case 6: return launch_pj<6>(X, ldx, C, N, wpca, nt, B0, ldb0, s);
-        case 7: return launch_pj<7>(X, ldx, C, N, wpca, nt, B0, ldb0, s);
-        case 8: return launch_pj<8>(X, ldx, C, N, wpca, nt, B0, ldb0, s);
-        default: return cudaErrorInvalidValue;
-    }
-}
 
 // ---------------------------------------------------------------------------
 // Transposed projection for the tensor-core score GEMM:
