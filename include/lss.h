@@ -30,6 +30,7 @@ extern "C" {
 #define LSS_ERR_CAPACITY  5   /* spike or record buffer too small           */
 #define LSS_ERR_TIMEOUT   6   /* a bounded device-side wait gave up         */
 #define LSS_ERR_STATE     7   /* call out of order (e.g. no drift matrix)   */
+#define LSS_ERR_BUSY      8   /* no probe slot or device memory free now    */
 
 /* Score precision of the template-matching GEMM. */
 #define LSS_PREC_FP32          0  /* FP32 scores (parity path)                        */
@@ -202,6 +203,59 @@ typedef struct lss_stage_times {
 } lss_stage_times;
 int  lss_set_profiling(lss_handle* h, int32_t on);
 int  lss_get_stage_times(const lss_handle* h, lss_stage_times* out);
+
+/* ------------------------------------------------------------------------
+ * Streaming serving loop. No counterpart in the reference as an API: there
+ * each probe runs its own OnlineSpikesV2 object on its own thread
+ * (main.cpp:77-85), whose runSpikeSorting loop (OnlineSpikesV2.cu:632-820)
+ * fetches the latest window from the acquisition socket, sorts it with
+ * synchronous copies and writes spikeOutput.txt.
+ *
+ * Here one server owns a device and admits probe streams while device memory
+ * and probe slots allow (LSS_ERR_BUSY otherwise: retry after a release). Each
+ * probe has its own sorter handle (its own templates and T), CUDA stream,
+ * device ring of raw int16 rows and one CUDA graph, captured at admission,
+ * that sorts one batch of cfg->batch_size (= NT) samples end to end with no
+ * host synchronisation. Probes' graphs run concurrently on the device.
+ *
+ * Stream batch b (b = 0, 1, ...) is launched as soon as its NT-sample block
+ * has arrived: its window is stream rows [b*NT - 2nt, (b+1)*NT) (rows before
+ * the stream start replicate row 0) and it sorts samples [b*NT - nt,
+ * (b+1)*NT - nt), i.e. Kilosort's batch semantics on the stream delayed by nt
+ * samples, so no batch waits for the next block. Record times are stream
+ * samples in Kilosort's convention (trough-aligned: + nt0min - nt/2);
+ * negative times are dropped. Results land in pinned host memory written by
+ * the device; arrival-to-emit latency is measured from the arrival time given
+ * to lss_server_push for the block's last row to the host callback that runs
+ * when the batch's work has finished.
+ * ---------------------------------------------------------------------- */
+typedef struct lss_server lss_server;
+
+int  lss_server_create(int32_t device, int64_t memory_budget_bytes, int32_t max_probes, lss_server** out);
+void lss_server_destroy(lss_server* s);
+/* Admits a probe: creates its handle from (cfg, t), applies the drift matrix
+ * M [C, C] when given, allocates its ring (`depth` batches in flight) and
+ * result ring (`capacity` records per batch) and captures its graph.
+ * LSS_ERR_BUSY when no slot is free or the handle would exceed the budget. */
+int  lss_server_admit(lss_server* s, const lss_config* cfg, const lss_tensors* t, const float* drift_M,
+                      int32_t depth, int64_t capacity, int32_t* probe);
+/* Appends n_rows raw int16 rows [n_rows, n_chan_bin] (host) to the probe's
+ * stream; every completed NT-row block launches its batch. arrival_ns: host
+ * CLOCK_MONOTONIC time the rows arrived (<= 0: now). Blocks only when `depth`
+ * batches are already in flight. */
+int  lss_server_push(lss_server* s, int32_t probe, const int16_t* rows, int64_t n_rows, int64_t arrival_ns);
+/* Oldest finished batch's records into `out` (host arrays); *batch = its
+ * index, or -1 when none is finished (wait = 0) or none is in flight. */
+int  lss_server_poll(lss_server* s, int32_t probe, lss_records* out, int64_t* batch, int32_t wait);
+/* Waits for the probe's batches, frees its memory and slot. Finished batches
+ * not yet polled are dropped. */
+int  lss_server_release(lss_server* s, int32_t probe);
+/* Replaces the probe's drift matrix after its in-flight batches finish. */
+int  lss_server_set_drift(lss_server* s, int32_t probe, const float* drift_M);
+/* Arrival-to-emit latency percentiles (ms) over the probe's polled batches. */
+int  lss_server_latency(lss_server* s, int32_t probe, double* p50_ms, double* p99_ms, int64_t* batches);
+/* Device memory held by admitted probes and the budget, in bytes. */
+int  lss_server_memory(lss_server* s, int64_t* used, int64_t* budget);
 
 #ifdef __cplusplus
 }

@@ -9,14 +9,17 @@ from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / 'liblss_b200.so'
 
-LSS_OK, LSS_ERR_ARG, LSS_ERR_IO, LSS_ERR_SHAPE, LSS_ERR_CUDA, LSS_ERR_CAPACITY, LSS_ERR_TIMEOUT, LSS_ERR_STATE = range(8)
+(LSS_OK, LSS_ERR_ARG, LSS_ERR_IO, LSS_ERR_SHAPE, LSS_ERR_CUDA, LSS_ERR_CAPACITY, LSS_ERR_TIMEOUT, LSS_ERR_STATE,
+ LSS_ERR_BUSY) = range(9)
 LSS_PREC_FP32, LSS_PREC_BF16_RECHECK = 0, 1
 
 # every entry point declared in include/lss.h
 EXPORTS = ('lss_create', 'lss_create_from_dir', 'lss_destroy', 'lss_last_error', 'lss_get_config',
            'lss_set_drift', 'lss_filter', 'lss_match', 'lss_match_scores', 'lss_scores',
            'lss_sort_batch', 'lss_get_stats', 'lss_set_profiling', 'lss_get_stage_times',
-           'lss_mp_rounds_noalloc')
+           'lss_mp_rounds_noalloc', 'lss_server_create', 'lss_server_destroy', 'lss_server_admit',
+           'lss_server_push', 'lss_server_poll', 'lss_server_release', 'lss_server_set_drift',
+           'lss_server_latency', 'lss_server_memory')
 
 
 class LssConfig(ct.Structure):
@@ -90,6 +93,17 @@ def load() -> ct.CDLL:
         'lss_get_stage_times': ([P, ct.POINTER(LssStageTimes)], ct.c_int),
         'lss_mp_rounds_noalloc': ([P, I64, I32, I32, I32, ct.c_float, P, P, I32, I32, P, P, P,
                                    ct.POINTER(I32), ct.POINTER(I32), P], ct.c_int),
+        'lss_server_create': ([I32, I64, I32, ct.POINTER(P)], ct.c_int),
+        'lss_server_destroy': ([P], None),
+        'lss_server_admit': ([P, ct.POINTER(LssConfig), ct.POINTER(LssTensors), P, I32, I64, ct.POINTER(I32)],
+                             ct.c_int),
+        'lss_server_push': ([P, I32, P, I64, I64], ct.c_int),
+        'lss_server_poll': ([P, I32, ct.POINTER(LssRecords), ct.POINTER(I64), I32], ct.c_int),
+        'lss_server_release': ([P, I32], ct.c_int),
+        'lss_server_set_drift': ([P, I32, P], ct.c_int),
+        'lss_server_latency': ([P, I32, ct.POINTER(ct.c_double), ct.POINTER(ct.c_double), ct.POINTER(I64)],
+                               ct.c_int),
+        'lss_server_memory': ([P, ct.POINTER(I64), ct.POINTER(I64)], ct.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

@@ -109,20 +109,32 @@ cudaError_t launch_xres(const float* X, int64_t ldx, int32_t C, int32_t N, int32
 }
 
 // Records: one CTA computes every kept spike's output slot with ballot scans
-// (only batch 0 drops spikes, those aligned before the recording start), then
-// a grid writes the slots and their PC features in parallel.
-__global__ void __launch_bounds__(1024) k_records_scan(const int32_t* __restrict__ sp_x, int32_t n, int64_t ibatch,
-                                                       int32_t nt, int32_t nt0min, int32_t* __restrict__ slot,
-                                                       int64_t* out_count) {
+// (spikes aligned before the recording start are dropped, which only happens
+// in the first batch), then a grid writes the slots and their PC features.
+//
+// Record time t = (x - nt) + ibatch * NT + shift - nt/2 + nt0min
+// (template_matching.py:54-59; shift = 0 for Kilosort's batches). With
+// rc.counters the spike count is read from the device, with rc.ibatch_dev the
+// batch index too, and with rc.slots > 0 batch b writes slot b % slots of
+// output arrays that hold `slots` batches of `capacity` records each (the
+// streaming loop's result rings).
+__device__ __forceinline__ int64_t rec_time(int x, int64_t ibatch, const RecordClock& rc) {
+    return (int64_t)(x - rc.nt) + ibatch * (int64_t)rc.NT + rc.shift - rc.nt / 2 + rc.nt0min;
+}
+
+__global__ void __launch_bounds__(1024) k_records_scan(const int32_t* __restrict__ sp_x, int32_t n, RecordClock rc,
+                                                       int32_t* __restrict__ slot, int64_t* out_count) {
     __shared__ int wsum[32];
     __shared__ int s_base;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (rc.counters) n = rc.counters[0];
+    const int64_t ibatch = rc.ibatch_dev ? *rc.ibatch_dev : rc.ibatch;
     if (threadIdx.x == 0) s_base = 0;
     __syncthreads();
     for (int c0 = 0; c0 < n; c0 += 1024) {
         const int i = c0 + threadIdx.x;
         bool keep = false;
-        if (i < n) keep = !(ibatch == 0 && (sp_x[i] - nt - nt / 2 + nt0min) < 0);
+        if (i < n) keep = rec_time(sp_x[i], ibatch, rc) >= 0;
         const unsigned bal = __ballot_sync(0xffffffffu, keep);
         if (lane == 0) wsum[warp] = __popc(bal);
         __syncthreads();
@@ -142,39 +154,45 @@ __global__ void __launch_bounds__(1024) k_records_scan(const int32_t* __restrict
         if (threadIdx.x == 1023) s_base += wsum[31] + __popc(bal);
         __syncthreads();
     }
-    if (threadIdx.x == 0) *out_count = s_base;
+    if (threadIdx.x == 0) out_count[rc.slots > 0 ? ibatch % rc.slots : 0] = s_base;
 }
 
 __global__ void k_records_write(const int32_t* __restrict__ sp_x, const int32_t* __restrict__ sp_y,
                                 const float* __restrict__ sp_amp, const float* __restrict__ tF,
-                                const int32_t* __restrict__ slot, int32_t n, int32_t feat_len, int64_t ibatch,
-                                int32_t nt, int32_t NT, int32_t nt0min, int64_t* out_time, int32_t* out_tmpl,
-                                float* out_amp, float* out_pc, int64_t capacity) {
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+                                const int32_t* __restrict__ slot, int32_t n, int32_t feat_len, RecordClock rc,
+                                int64_t* out_time, int32_t* out_tmpl, float* out_amp, float* out_pc,
+                                int64_t capacity) {
+    if (rc.counters) n = rc.counters[0];
+    const int64_t ibatch = rc.ibatch_dev ? *rc.ibatch_dev : rc.ibatch;
+    const int64_t base = rc.slots > 0 ? (ibatch % rc.slots) * capacity : 0;
     const int row = 3 + feat_len;  // time, template, amplitude, features
-    const int64_t i = e / row;
-    const int f = (int)(e % row);
-    if (i >= n) return;
-    const int o = slot[i];
-    if (o < 0 || o >= capacity) return;
-    if (f == 0) out_time[o] = (int64_t)(sp_x[i] - nt) + ibatch * (int64_t)NT - nt / 2 + nt0min;
-    else if (f == 1) out_tmpl[o] = sp_y[i];
-    else if (f == 2) out_amp[o] = sp_amp[i];
-    else if (out_pc && tF) out_pc[(int64_t)o * feat_len + (f - 3)] = tF[i * feat_len + (f - 3)];
+    const int64_t total = (int64_t)n * row;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = e / row;
+        const int f = (int)(e % row);
+        const int o = slot[i];
+        if (o < 0 || o >= capacity) continue;
+        const int64_t q = base + o;
+        if (f == 0) out_time[q] = rec_time(sp_x[i], ibatch, rc);
+        else if (f == 1) out_tmpl[q] = sp_y[i];
+        else if (f == 2) out_amp[q] = sp_amp[i];
+        else if (out_pc && tF) out_pc[q * feat_len + (f - 3)] = tF[i * feat_len + (f - 3)];
+    }
 }
 
 cudaError_t launch_records(const int32_t* sp_x, const int32_t* sp_y, const float* sp_amp, const float* tF,
-                           int32_t* slot, int32_t n, int32_t feat_len, int64_t ibatch, int32_t nt,
-                           int32_t NT, int32_t nt0min, int64_t* out_time, int32_t* out_tmpl,
-                           float* out_amp, float* out_pc, int64_t capacity, int64_t* out_count,
+                           int32_t* slot, int32_t n, int32_t feat_len, const RecordClock& rc, int64_t* out_time,
+                           int32_t* out_tmpl, float* out_amp, float* out_pc, int64_t capacity, int64_t* out_count,
                            cudaStream_t s) {
-    k_records_scan<<<1, 1024, 0, s>>>(sp_x, n, ibatch, nt, nt0min, slot, out_count);
+    // n: the spike count, or (rc.counters != null) an upper bound that sizes the write grid
+    k_records_scan<<<1, 1024, 0, s>>>(sp_x, n, rc, slot, out_count);
     const int64_t total = (int64_t)n * (3 + (tF ? feat_len : 0));
     if (total > 0) {
-        k_records_write<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(sp_x, sp_y, sp_amp, tF, slot, n,
-                                                                        tF ? feat_len : 0, ibatch, nt, NT, nt0min,
-                                                                        out_time, out_tmpl, out_amp,
-                                                                        tF ? out_pc : nullptr, capacity);
+        const int64_t blocks = std::min<int64_t>((total + 255) / 256, rc.counters ? 1184 : INT32_MAX);
+        k_records_write<<<(unsigned)blocks, 256, 0, s>>>(sp_x, sp_y, sp_amp, tF, slot, n, tF ? feat_len : 0, rc,
+                                                         out_time, out_tmpl, out_amp, tF ? out_pc : nullptr,
+                                                         capacity);
     }
     return cudaGetLastError();
 }
@@ -214,14 +232,13 @@ constexpr int FT_CH = 64;
 constexpr int FT_LIST = 512;
 constexpr int FT_NQ = 32;  // neighbours per staged chunk
 
-__global__ void __launch_bounds__(256) k_pc_features_folded(
-    const float* __restrict__ Xh, int64_t ldx, int32_t C, int32_t nt, int32_t K, int32_t nC, int32_t T,
-    const float* __restrict__ wpca, const float* __restrict__ Mw, const float* __restrict__ U,
+__device__ __forceinline__ void pc_features_one(
+    int i, int rounds, const float* __restrict__ Xh, int64_t ldx, int32_t C, int32_t nt, int32_t K, int32_t nC,
+    int32_t T, const float* __restrict__ wpca, const float* __restrict__ Mw, const float* __restrict__ U,
     const float* __restrict__ R, const int64_t* __restrict__ iCC, const int64_t* __restrict__ iU,
     const float* __restrict__ Ucc, const int32_t* __restrict__ sp_x, const int32_t* __restrict__ sp_y,
-    const float* __restrict__ sp_amp, const int32_t* __restrict__ round_start, int32_t rounds,
-    float* __restrict__ tF, int32_t* status, const float* __restrict__ Phi, const float* __restrict__ Plo,
-    int64_t ldp) {
+    const float* __restrict__ sp_amp, const int32_t* __restrict__ round_start, float* __restrict__ tF,
+    int32_t* status, const float* __restrict__ Phi, const float* __restrict__ Plo, int64_t ldp) {
     extern __shared__ float sm[];
     const int ntp = nt + 1;
     float* ws = sm;                          // [K][nt]
@@ -236,7 +253,6 @@ __global__ void __launch_bounds__(256) k_pc_features_folded(
     __shared__ float l_a[FT_LIST];
     __shared__ int s_n;
     __shared__ int s_cnt[256];
-    const int i = blockIdx.x;
     const int x = sp_x[i], y = sp_y[i];
     const int h = nt / 2;
     for (int e = threadIdx.x; e < K * nt; e += blockDim.x) ws[e] = wpca[e];
@@ -379,12 +395,35 @@ __global__ void __launch_bounds__(256) k_pc_features_folded(
     }
 }
 
+// CTA per spike, grid-stride over the spikes; with counters != null the spike
+// and round counts are read from the matching pursuit's device counters
+// (graph-captured batches, whose launch does not know them).
+__global__ void __launch_bounds__(256) k_pc_features_folded(
+    const float* __restrict__ Xh, int64_t ldx, int32_t C, int32_t nt, int32_t K, int32_t nC, int32_t T,
+    const float* __restrict__ wpca, const float* __restrict__ Mw, const float* __restrict__ U,
+    const float* __restrict__ R, const int64_t* __restrict__ iCC, const int64_t* __restrict__ iU,
+    const float* __restrict__ Ucc, const int32_t* __restrict__ sp_x, const int32_t* __restrict__ sp_y,
+    const float* __restrict__ sp_amp, const int32_t* __restrict__ round_start, int32_t rounds, int32_t n,
+    const int32_t* __restrict__ counters, float* __restrict__ tF, int32_t* status, const float* __restrict__ Phi,
+    const float* __restrict__ Plo, int64_t ldp) {
+    if (counters) {
+        n = counters[0];
+        rounds = counters[1];
+    }
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+        pc_features_one(i, rounds, Xh, ldx, C, nt, K, nC, T, wpca, Mw, U, R, iCC, iU, Ucc, sp_x, sp_y, sp_amp,
+                        round_start, tF, status, Phi, Plo, ldp);
+        __syncthreads();
+    }
+}
+
 cudaError_t launch_pc_features_folded(const float* Xh, int64_t ldx, int32_t C, int32_t nt, int32_t K, int32_t nC,
                                       int32_t T, const float* wpca, const float* Mw, const float* U, const float* R,
                                       const int64_t* iCC, const int64_t* iU, const float* Ucc, const int32_t* sp_x,
                                       const int32_t* sp_y, const float* sp_amp, const int32_t* round_start,
-                                      int32_t rounds, int32_t n, float* tF, int32_t* status, const float* Phi,
-                                      const float* Plo, int64_t ldp, cudaStream_t s) {
+                                      int32_t rounds, int32_t n, const int32_t* counters, float* tF,
+                                      int32_t* status, const float* Phi, const float* Plo, int64_t ldp,
+                                      cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
     if (nC * K > 256) return cudaErrorInvalidValue;  // one (j, k) per thread
     const size_t front = std::max<size_t>((size_t)K * nt + (size_t)FT_CH * (nt + 1) + (size_t)FT_CH * K +
@@ -393,8 +432,9 @@ cudaError_t launch_pc_features_folded(const float* Xh, int64_t ldx, int32_t C, i
     const size_t smem = sizeof(float) * (front + (size_t)nC * K + (size_t)FT_NQ * nC * K);
     if (smem > 48 * 1024)
         cudaFuncSetAttribute(k_pc_features_folded, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // n: the spike count, or (counters != null) the grid size
     k_pc_features_folded<<<n, 256, smem, s>>>(Xh, ldx, C, nt, K, nC, T, wpca, Mw, U, R, iCC, iU, Ucc, sp_x, sp_y,
-                                              sp_amp, round_start, rounds, tF, status, Phi, Plo, ldp);
+                                              sp_amp, round_start, rounds, n, counters, tF, status, Phi, Plo, ldp);
     return cudaGetLastError();
 }
 

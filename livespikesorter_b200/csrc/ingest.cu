@@ -14,7 +14,11 @@
 
 namespace lss {
 
-__device__ __forceinline__ int64_t src_row(int64_t s, const IngestMap& m) {
+__device__ __forceinline__ int64_t src_row(int64_t s, const IngestMap& m, int64_t base) {
+    if (m.base_dev) {
+        const int64_t r = base + s;
+        return r < 0 ? 0 : r % m.ring_rows;
+    }
     int64_t j = s - m.lead;
     if (j < 0) j = 0;
     if (j >= m.nsamp) {
@@ -32,11 +36,12 @@ __global__ void k_chan_sums(const int16_t* __restrict__ raw, int32_t ld_raw,
                             IngestMap map, long long* __restrict__ sums) {
     const int64_t s0 = (int64_t)blockIdx.x * 256;
     const int64_t s1 = min(N, s0 + 256);
+    const int64_t base = map.base_dev ? *map.base_dev : 0;
     for (int c = threadIdx.x; c < C; c += blockDim.x) {
         const int ch = chan_map ? chan_map[c] : c;
         int acc = 0;
         for (int64_t s = s0; s < s1; ++s) {
-            const int64_t r = src_row(s, map);
+            const int64_t r = src_row(s, map, base);
             if (r >= 0) acc += raw[r * ld_raw + ch];
         }
         atomicAdd((unsigned long long*)&sums[c], (unsigned long long)(long long)acc);
@@ -80,6 +85,7 @@ __global__ void __launch_bounds__(256) k_car(const int16_t* __restrict__ raw, in
     const int64_t s0 = (int64_t)blockIdx.x * CAR_COLS;
     const int ncol = (int)min((int64_t)CAR_COLS, N - s0);
     const double invN = 1.0 / (double)N;
+    const int64_t base = map.base_dev ? *map.base_dev : 0;
     for (int c = threadIdx.x; c < C; c += blockDim.x)
         mean[c] = (float)((double)sign * (double)sums[c] * invN);
     __syncthreads();
@@ -87,7 +93,7 @@ __global__ void __launch_bounds__(256) k_car(const int16_t* __restrict__ raw, in
         const int c = idx % C, j = idx / C;
         float v = 0.f;
         if (j < ncol) {
-            const int64_t r = src_row(s0 + j, map);
+            const int64_t r = src_row(s0 + j, map, base);
             const int ch = chan_map ? chan_map[c] : c;
             const float x = (r >= 0) ? sign * (float)raw[r * ld_raw + ch] : 0.f;
             v = __fsub_rn(x, mean[c]);

@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "lss.h"
+#include "lss_handle.h"
 #include "lss_kernels.cuh"
 #include "npy.h"
 
@@ -32,108 +33,12 @@ namespace {
 
 thread_local std::string g_create_err;
 
-template <typename T>
-struct DevBuf {
-    T* p = nullptr;
-    size_t n = 0;
-    cudaError_t alloc(size_t count) {
-        n = count;
-        return cudaMalloc(reinterpret_cast<void**>(&p), std::max<size_t>(count, 1) * sizeof(T));
-    }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-    }
-};
-
-int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
-
 }  // namespace
 
 // Error text for entry points that have no handle (read back through
 // lss_last_error(NULL)).
 void lss::set_thread_error(const char* msg) { g_create_err = msg; }
 
-struct lss_handle {
-    lss_config cfg{};
-    std::string err;
-    int C = 0, Cbin = 0, T = 0, K = 0, nt = 0, nC = 0, NT = 0, N = 0;
-    int64_t ld = 0;
-    int hpL = -1;  // FIR half length; -1 = no highpass
-    int mp_grid = 0;
-    std::vector<float> h_hp;
-    lss_stats stats{};
-    bool prof = false;
-    cudaEvent_t ev[11] = {};
-    lss_stage_times times{};
-
-    void mark(int i, cudaStream_t s) {
-        if (prof) cudaEventRecord(ev[i], s);
-    }
-
-    DevBuf<int16_t> raw;
-    DevBuf<int32_t> chan_map;
-    DevBuf<long long> sums;
-    DevBuf<float> taps, Mw, Wrot, Mdrift, X1, Xh, X, B, nm, ctcP, wave, wpca, Ucc, Xres, tF;
-    DevBuf<int64_t> iCC, iU;
-    DevBuf<float> cfmax;
-    DevBuf<int32_t> imax, blk_cnt, blk_x, blk_y, sp_x, sp_y, sp_round, round_start, counters, status;
-    DevBuf<float> sp_amp, blk_amp;
-    DevBuf<unsigned long long> colkey;
-    DevBuf<__nv_bfloat16> B0T, Up16;   // BF16 path: transposed projection, templates
-    DevBuf<float> B0T_hi, B0T_lo, Up_hi, Up_lo;  // FP32 path (3xTF32): tf32 hi/lo splits
-    DevBuf<__nv_bfloat16> Uw16;                  // templates with the whitening folded in (BF16 path)
-    DevBuf<float> Uw_hi, Uw_lo;                  // ... (FP32 path)
-    DevBuf<float> U, R;                          // U [T,K,C]; R [K,K,2nt-1] basis lag correlations
-    DevBuf<float2> hpH, hpTw;                    // highpass spectrum and twiddles (FFT form)
-    DevBuf<float> cf2, pre_cf, Pc_hi, Pc_lo;     // BF16 re-check: runner-up Cf, saved maxima, gathered projection
-    DevBuf<int32_t> rc_tiles, pre_im, rc_count;  // ... listed tiles, saved argmax, [tiles, flips, near columns]
-    int32_t* rc_host = nullptr;                  // pinned copy of rc_count (read by lss_get_stats)
-    cudaEvent_t rc_ev = nullptr;                 // recorded after that copy
-    bool rc_pending = false;
-    int64_t last_scored = 0;                     // samples of the last BF16 scoring
-    int CKpad = 0;
-    int sm_count = 0;
-    DevBuf<unsigned int> bar;
-    DevBuf<int64_t> rec_time, rec_count;
-    DevBuf<int32_t> rec_tmpl, rec_slot;
-    DevBuf<float> rec_amp, rec_pc;
-
-    int fail(int code, const std::string& m) {
-        err = m;
-        return code;
-    }
-    int cuda_fail(cudaError_t e, const char* where) {
-        err = std::string(where) + ": " + cudaGetErrorString(e);
-        return LSS_ERR_CUDA;
-    }
-    ~lss_handle() {
-        int dev = 0;
-        if (cudaGetDevice(&dev) == cudaSuccess && dev != cfg.device) cudaSetDevice(cfg.device);
-        for (auto& e : ev)
-            if (e) cudaEventDestroy(e);
-        raw.release(); chan_map.release(); sums.release(); taps.release(); Mw.release(); Wrot.release(); Mdrift.release();
-        X1.release(); Xh.release(); X.release(); B.release();
-        nm.release(); ctcP.release(); wave.release(); wpca.release(); Ucc.release(); Xres.release();
-        tF.release(); iCC.release(); iU.release(); cfmax.release(); imax.release(); blk_cnt.release();
-        blk_x.release(); blk_y.release(); sp_x.release(); sp_y.release(); sp_round.release();
-        round_start.release(); counters.release(); status.release(); sp_amp.release(); blk_amp.release(); colkey.release();
-        bar.release(); rec_time.release(); rec_count.release(); rec_tmpl.release(); rec_slot.release(); rec_amp.release();
-        rec_pc.release(); B0T.release(); Up16.release();
-        B0T_hi.release(); B0T_lo.release(); Up_hi.release(); Up_lo.release();
-        Uw16.release(); Uw_hi.release(); Uw_lo.release(); U.release(); R.release(); hpH.release(); hpTw.release();
-        cf2.release(); pre_cf.release(); Pc_hi.release(); Pc_lo.release(); rc_tiles.release(); pre_im.release();
-        rc_count.release();
-        if (rc_ev) cudaEventDestroy(rc_ev);
-        if (rc_host) cudaFreeHost(rc_host);
-    }
-};
-
-#define CK(call)                                                   \
-    do {                                                           \
-        cudaError_t e_ = (call);                                   \
-        if (e_ != cudaSuccess) return h->cuda_fail(e_, #call);     \
-    } while (0)
 
 // Circular-correlation taps of the highpass for a batch of N samples: the
 // impulse response is zero-padded or centre-cropped to N exactly as
@@ -222,6 +127,8 @@ static int set_mixing(lss_handle* h, const float* M) {
         CK(launch_build_uw(h->U.p, h->Mw.p, h->T, h->K, C, h->CKpad, h->Uw16.p, nullptr, nullptr, 0));
         h->stats.launches += 1;
     }
+    // callers may sort on streams that do not wait for the legacy default stream
+    CK(cudaStreamSynchronize(0));
     return LSS_OK;
 }
 
@@ -345,13 +252,15 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
         if (h->hpL < 0) return LSS_ERR_ARG;
     }
 
-    h->mp_grid = mp_max_grid(cfg->device);
+    // one CTA per >= 128 columns (short streaming batches leave SMs to other probes)
+    h->mp_grid = std::min<int>(mp_max_grid(cfg->device), (int)std::max<int64_t>(1, (h->N + 127) / 128));
     cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, cfg->device);
     h->CKpad = (C * K + 63) / 64 * 64;
     const int64_t cap = cfg->max_spikes;
 #define ALLOC(buf, cnt)                                                                    \
     do {                                                                                   \
         cudaError_t e_ = h->buf.alloc(cnt);                                                \
+        h->dev_bytes += std::max<size_t>(h->buf.n, 1) * sizeof(*h->buf.p);                 \
         if (e_ != cudaSuccess) {                                                           \
             g_create_err = std::string("cudaMalloc " #buf ": ") + cudaGetErrorString(e_);  \
             return LSS_ERR_CUDA;                                                           \
@@ -579,6 +488,7 @@ int lss_get_stats(const lss_handle* h, lss_stats* out) {
 
 int lss_set_drift(lss_handle* h, const float* M) {
     if (!h) return LSS_ERR_ARG;
+    if (h->streaming) return h->fail(LSS_ERR_STATE, "handle is owned by a serving loop");
     CK(cudaSetDevice(h->cfg.device));
     return set_mixing(h, M);
 }
@@ -616,6 +526,12 @@ static int run_filter(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t
         src = h->raw.p;
     }
     h->mark(1, s);
+    return run_ingest(h, src, map, Xout, s, pre_out);
+}
+
+int lss::run_ingest(lss_handle* h, const int16_t* src, const IngestMap& map, float* Xout, cudaStream_t s,
+                    const float** pre_out) {
+    const int64_t N = h->N;
     const float sign = h->cfg.invert_sign ? -1.f : 1.f;
     CK(launch_chan_sums(src, h->Cbin, h->chan_map.p, h->C, N, map, h->sums.p, s));
     CK(launch_car(src, h->Cbin, h->chan_map.p, h->C, N, map, sign, h->sums.p, h->cfg.do_car, h->X1.p, h->ld, s));
@@ -640,8 +556,8 @@ static int run_filter(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t
     return LSS_OK;
 }
 
-static int run_scores(lss_handle* h, const float* X, int64_t ldx, int64_t N, float* B, cudaStream_t s,
-                      bool* maxima_ready = nullptr, bool folded = false) {
+int lss::run_scores(lss_handle* h, const float* X, int64_t ldx, int64_t N, float* B, cudaStream_t s,
+                   bool* maxima_ready, bool folded) {
     if (h->cfg.precision == LSS_PREC_BF16_RECHECK) {
         CK(launch_pca_proj_t(X, ldx, h->C, N, h->wpca.p, h->K, h->nt, h->B0T.p, h->CKpad, s));
         h->mark(5, s);
@@ -667,10 +583,12 @@ static int run_scores(lss_handle* h, const float* X, int64_t ldx, int64_t N, flo
                                   h->imax.p, h->nt, h->status.p, h->sm_count, s, ex2));
         CK(launch_recheck_flips(h->cfmax.p, h->imax.p, h->rc_tiles.p, h->pre_cf.p, h->pre_im.p, h->rc_count.p, (int)N,
                                 th2, s));
-        CK(cudaMemcpyAsync(h->rc_host, h->rc_count.p, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-        CK(cudaEventRecord(h->rc_ev, s));
-        h->rc_pending = true;
-        h->last_scored = N;
+        if (!h->capturing) {
+            CK(cudaMemcpyAsync(h->rc_host, h->rc_count.p, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+            CK(cudaEventRecord(h->rc_ev, s));
+            h->rc_pending = true;
+            h->last_scored = N;
+        }
         h->stats.launches += 6;
         h->mark(6, s);
         if (maxima_ready) *maxima_ready = true;
@@ -687,9 +605,7 @@ static int run_scores(lss_handle* h, const float* X, int64_t ldx, int64_t N, flo
     return LSS_OK;
 }
 
-// Runs the rounds on h->B (already holding the score field); returns spikes.
-static int run_mp(lss_handle* h, int64_t N, int32_t* n_out, int32_t* rounds_out, cudaStream_t s,
-                  bool maxima_ready = false) {
+int lss::enqueue_mp(lss_handle* h, int64_t N, cudaStream_t s, bool maxima_ready) {
     if (N <= 2 * h->nt) return h->fail(LSS_ERR_ARG, "batch shorter than 2*nt + 1 samples");
     MPArgs a{};
     a.B = h->B.p;
@@ -726,6 +642,14 @@ static int run_mp(lss_handle* h, int64_t N, int32_t* n_out, int32_t* rounds_out,
     CK(cudaMemsetAsync(h->colkey.p, 0, 2 * h->ld * sizeof(unsigned long long), s));
     CK(launch_mp(a, G, s));
     h->stats.launches += 1;
+    return LSS_OK;
+}
+
+// Runs the rounds on h->B (already holding the score field); returns spikes.
+static int run_mp(lss_handle* h, int64_t N, int32_t* n_out, int32_t* rounds_out, cudaStream_t s,
+                  bool maxima_ready = false) {
+    int rc = enqueue_mp(h, N, s, maxima_ready);
+    if (rc) return rc;
     int32_t hc[4], st = 0;
     CK(cudaMemcpyAsync(hc, h->counters.p, sizeof(hc), cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(&st, h->status.p, sizeof(st), cudaMemcpyDeviceToHost, s));
@@ -756,6 +680,7 @@ extern "C" {
 int lss_filter(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ibatch, int64_t n_batches,
                int32_t raw_on_device, float* X_dev, void* stream) {
     if (!h || !X_dev) return LSS_ERR_ARG;
+    if (h->streaming) return h->fail(LSS_ERR_STATE, "handle is owned by a serving loop");
     CK(cudaSetDevice(h->cfg.device));
     cudaStream_t s = (cudaStream_t)stream;
     // the GEMM writes rows of stride ld; the caller's buffer has stride N
@@ -769,6 +694,7 @@ int lss_filter(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ibatch
 
 int lss_scores(lss_handle* h, const float* X_dev, int64_t N, float* B_dev, void* stream) {
     if (!h || !X_dev || !B_dev) return LSS_ERR_ARG;
+    if (h->streaming) return h->fail(LSS_ERR_STATE, "handle is owned by a serving loop");
     if (N <= 0 || N > h->N) return h->fail(LSS_ERR_ARG, "N out of range");
     CK(cudaSetDevice(h->cfg.device));
     cudaStream_t s = (cudaStream_t)stream;
@@ -814,6 +740,7 @@ static int match_common(lss_handle* h, int64_t N, const float* Xsrc, int64_t* st
 int lss_match(lss_handle* h, const float* X_dev, int64_t N, int64_t* st_dev, float* amps_dev, float* xres_dev,
               int64_t capacity, int64_t* n_spikes, void* stream) {
     if (!h || !X_dev) return LSS_ERR_ARG;
+    if (h->streaming) return h->fail(LSS_ERR_STATE, "handle is owned by a serving loop");
     if (N <= 0 || N > h->N) return h->fail(LSS_ERR_ARG, "N out of range (1..NT+2nt)");
     CK(cudaSetDevice(h->cfg.device));
     cudaStream_t s = (cudaStream_t)stream;
@@ -829,6 +756,7 @@ int lss_match(lss_handle* h, const float* X_dev, int64_t N, int64_t* st_dev, flo
 int lss_match_scores(lss_handle* h, const float* B_dev, int64_t N, int64_t* st_dev, float* amps_dev,
                      int64_t capacity, int64_t* n_spikes, void* stream) {
     if (!h || !B_dev) return LSS_ERR_ARG;
+    if (h->streaming) return h->fail(LSS_ERR_STATE, "handle is owned by a serving loop");
     if (N <= 0 || N > h->N) return h->fail(LSS_ERR_ARG, "N out of range (1..NT+2nt)");
     CK(cudaSetDevice(h->cfg.device));
     cudaStream_t s = (cudaStream_t)stream;
@@ -841,6 +769,7 @@ int lss_match_scores(lss_handle* h, const float* B_dev, int64_t N, int64_t* st_d
 int lss_sort_batch(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ibatch, int64_t n_batches,
                    int32_t raw_on_device, lss_records* out, void* stream) {
     if (!h || !out) return LSS_ERR_ARG;
+    if (h->streaming) return h->fail(LSS_ERR_STATE, "handle is owned by a serving loop");
     if (!out->time || !out->template_id || !out->amplitude) return h->fail(LSS_ERR_ARG, "null record arrays");
     CK(cudaSetDevice(h->cfg.device));
     cudaStream_t s = (cudaStream_t)stream;
@@ -863,7 +792,7 @@ int lss_sort_batch(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ib
     if (want_pc && n > 0) {
         CK(launch_pc_features_folded(Xh, h->ld, h->C, h->nt, h->K, h->nC, h->T, h->wpca.p, h->Mw.p, h->U.p, h->R.p,
                                      h->iCC.p, h->iU.p, h->Ucc.p, h->sp_x.p, h->sp_y.p, h->sp_amp.p,
-                                     h->round_start.p, rounds, n, h->tF.p, h->status.p,
+                                     h->round_start.p, rounds, n, nullptr, h->tF.p, h->status.p,
                                      bf16 ? nullptr : h->B0T_hi.p, bf16 ? nullptr : h->B0T_lo.p, h->CKpad, s));
         h->stats.launches += 1;
     }
@@ -874,8 +803,13 @@ int lss_sort_batch(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ib
     float* d_amp = out->on_device ? out->amplitude : h->rec_amp.p;
     float* d_pc = want_pc ? (out->on_device ? out->pc : h->rec_pc.p) : nullptr;
     const int64_t dcap = out->on_device ? cap : std::min<int64_t>(cap, h->cfg.max_spikes);
-    CK(launch_records(h->sp_x.p, h->sp_y.p, h->sp_amp.p, want_pc ? h->tF.p : nullptr, h->rec_slot.p, n, feat,
-                      ibatch, h->nt, h->NT, h->cfg.nt0min, d_time, d_tmpl, d_amp, d_pc, dcap, h->rec_count.p, s));
+    RecordClock rclk;
+    rclk.ibatch = ibatch;
+    rclk.NT = h->NT;
+    rclk.nt = h->nt;
+    rclk.nt0min = h->cfg.nt0min;
+    CK(launch_records(h->sp_x.p, h->sp_y.p, h->sp_amp.p, want_pc ? h->tF.p : nullptr, h->rec_slot.p, n, feat, rclk,
+                      d_time, d_tmpl, d_amp, d_pc, dcap, h->rec_count.p, s));
     h->stats.launches += (n > 0) ? 2 : 1;
     int64_t count = 0;
     int32_t st = 0;

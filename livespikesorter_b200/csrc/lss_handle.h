@@ -1,0 +1,135 @@
+// Internal: the sorter handle behind the C ABI (include/lss.h) and the
+// stage functions shared by the batch entry points (lss_api.cpp) and the
+// streaming loop (serve.cpp). Every device buffer is allocated once by
+// lss_create; the stages only enqueue work on the caller's stream.
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <string>
+
+#include "lss.h"
+#include "lss_kernels.cuh"
+
+namespace lss {
+
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaError_t alloc(size_t count) {
+        n = count;
+        return cudaMalloc(reinterpret_cast<void**>(&p), std::max<size_t>(count, 1) * sizeof(T));
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+    }
+};
+
+inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+}  // namespace lss
+
+using lss::DevBuf;
+
+struct lss_handle {
+    lss_config cfg{};
+    std::string err;
+    int C = 0, Cbin = 0, T = 0, K = 0, nt = 0, nC = 0, NT = 0, N = 0;
+    int64_t ld = 0;
+    int hpL = -1;  // FIR half length; -1 = no highpass
+    int mp_grid = 0;
+    size_t dev_bytes = 0;                        // device memory allocated by lss_create
+    std::vector<float> h_hp;
+    lss_stats stats{};
+    bool prof = false;
+    bool capturing = false;                      // inside a graph capture: no host-side copies or timing events
+    bool streaming = false;                      // owned by a serving loop: the batch entry points are refused
+    cudaEvent_t ev[11] = {};
+    lss_stage_times times{};
+
+    void mark(int i, cudaStream_t s) {
+        if (prof) cudaEventRecord(ev[i], s);
+    }
+
+    DevBuf<int16_t> raw;
+    DevBuf<int32_t> chan_map;
+    DevBuf<long long> sums;
+    DevBuf<float> taps, Mw, Wrot, Mdrift, X1, Xh, X, B, nm, ctcP, wave, wpca, Ucc, Xres, tF;
+    DevBuf<int64_t> iCC, iU;
+    DevBuf<float> cfmax;
+    DevBuf<int32_t> imax, blk_cnt, blk_x, blk_y, sp_x, sp_y, sp_round, round_start, counters, status;
+    DevBuf<float> sp_amp, blk_amp;
+    DevBuf<unsigned long long> colkey;
+    DevBuf<__nv_bfloat16> B0T, Up16;   // BF16 path: transposed projection, templates
+    DevBuf<float> B0T_hi, B0T_lo, Up_hi, Up_lo;  // FP32 path (3xTF32): tf32 hi/lo splits
+    DevBuf<__nv_bfloat16> Uw16;                  // templates with the whitening folded in (BF16 path)
+    DevBuf<float> Uw_hi, Uw_lo;                  // ... (FP32 path)
+    DevBuf<float> U, R;                          // U [T,K,C]; R [K,K,2nt-1] basis lag correlations
+    DevBuf<float2> hpH, hpTw;                    // highpass spectrum and twiddles (FFT form)
+    DevBuf<float> cf2, pre_cf, Pc_hi, Pc_lo;     // BF16 re-check: runner-up Cf, saved maxima, gathered projection
+    DevBuf<int32_t> rc_tiles, pre_im, rc_count;  // ... listed tiles, saved argmax, [tiles, flips, near columns]
+    int32_t* rc_host = nullptr;                  // pinned copy of rc_count (read by lss_get_stats)
+    cudaEvent_t rc_ev = nullptr;                 // recorded after that copy
+    bool rc_pending = false;
+    int64_t last_scored = 0;                     // samples of the last BF16 scoring
+    int CKpad = 0;
+    int sm_count = 0;
+    DevBuf<unsigned int> bar;
+    DevBuf<int64_t> rec_time, rec_count;
+    DevBuf<int32_t> rec_tmpl, rec_slot;
+    DevBuf<float> rec_amp, rec_pc;
+
+    int fail(int code, const std::string& m) {
+        err = m;
+        return code;
+    }
+    int cuda_fail(cudaError_t e, const char* where) {
+        err = std::string(where) + ": " + cudaGetErrorString(e);
+        return LSS_ERR_CUDA;
+    }
+    ~lss_handle() {
+        int dev = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess && dev != cfg.device) cudaSetDevice(cfg.device);
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+        raw.release(); chan_map.release(); sums.release(); taps.release(); Mw.release(); Wrot.release(); Mdrift.release();
+        X1.release(); Xh.release(); X.release(); B.release();
+        nm.release(); ctcP.release(); wave.release(); wpca.release(); Ucc.release(); Xres.release();
+        tF.release(); iCC.release(); iU.release(); cfmax.release(); imax.release(); blk_cnt.release();
+        blk_x.release(); blk_y.release(); sp_x.release(); sp_y.release(); sp_round.release();
+        round_start.release(); counters.release(); status.release(); sp_amp.release(); blk_amp.release(); colkey.release();
+        bar.release(); rec_time.release(); rec_count.release(); rec_tmpl.release(); rec_slot.release(); rec_amp.release();
+        rec_pc.release(); B0T.release(); Up16.release();
+        B0T_hi.release(); B0T_lo.release(); Up_hi.release(); Up_lo.release();
+        Uw16.release(); Uw_hi.release(); Uw_lo.release(); U.release(); R.release(); hpH.release(); hpTw.release();
+        cf2.release(); pre_cf.release(); Pc_hi.release(); Pc_lo.release(); rc_tiles.release(); pre_im.release();
+        rc_count.release();
+        if (rc_ev) cudaEventDestroy(rc_ev);
+        if (rc_host) cudaFreeHost(rc_host);
+    }
+};
+
+#define CK(call)                                                   \
+    do {                                                           \
+        cudaError_t e_ = (call);                                   \
+        if (e_ != cudaSuccess) return h->cuda_fail(e_, #call);     \
+    } while (0)
+
+namespace lss {
+
+// Ingest (channel sums, CAR, highpass; optional whitening into Xout) of the
+// batch whose raw rows `src` (device) are read through `map`.
+int run_ingest(lss_handle* h, const int16_t* src, const IngestMap& map, float* Xout, cudaStream_t s,
+               const float** pre_out);
+// Projection and score GEMM of X [C, ldx] into B; *maxima_ready when the
+// column maxima were fused into the GEMM.
+int run_scores(lss_handle* h, const float* X, int64_t ldx, int64_t N, float* B, cudaStream_t s,
+               bool* maxima_ready = nullptr, bool folded = false);
+// Matching-pursuit rounds on h->B, enqueued only (counts stay on the device).
+int enqueue_mp(lss_handle* h, int64_t N, cudaStream_t s, bool maxima_ready);
+
+}  // namespace lss

@@ -11,10 +11,17 @@ namespace lss {
 // (kilosort/io.py:584-637): row = clamp(s - lead, 0, nsamp-1); columns at or
 // past lead + nsamp are zero when zero_tail (batch 0) and replicate the last
 // row otherwise (last batch).
+// Batch column s reads raw row src_row(s): Kilosort's padded batch
+// (io.py:584-637) with `lead` replicated leading rows and the tail replicated
+// or zero. With base_dev set the rows come from a ring of ring_rows rows
+// instead: column s is stream row *base_dev + s (rows before the stream start
+// replicate row 0), stored at ring index row % ring_rows.
 struct IngestMap {
-    int64_t lead;
-    int64_t nsamp;
-    int32_t zero_tail;
+    int64_t lead = 0;
+    int64_t nsamp = 0;
+    int32_t zero_tail = 0;
+    const int64_t* base_dev = nullptr;
+    int64_t ring_rows = 0;
 };
 
 // ---- ingest (ingest.cu) ----
@@ -129,10 +136,17 @@ cudaError_t launch_xres(const float* X, int64_t ldx, int32_t C, int32_t N, int32
                         const int32_t* round_start, const int32_t* counters, int32_t rounds,
                         float* Xres, int32_t* status, cudaStream_t s);
 // slot: scratch [n] for the output position of each spike
+struct RecordClock {
+    int64_t ibatch = 0;                    // batch index (host value) ...
+    const int64_t* ibatch_dev = nullptr;   // ... or read from the device
+    const int32_t* counters = nullptr;     // spike count read from the device (counters[0])
+    int64_t shift = 0;                     // extra sample offset of the batch window
+    int32_t NT = 0, nt = 0, nt0min = 0;
+    int32_t slots = 0;                     // > 0: outputs are rings of `slots` batches
+};
 cudaError_t launch_records(const int32_t* sp_x, const int32_t* sp_y, const float* sp_amp, const float* tF,
-                           int32_t* slot, int32_t n, int32_t feat_len, int64_t ibatch, int32_t nt,
-                           int32_t NT, int32_t nt0min, int64_t* out_time, int32_t* out_tmpl,
-                           float* out_amp, float* out_pc, int64_t capacity, int64_t* out_count,
+                           int32_t* slot, int32_t n, int32_t feat_len, const RecordClock& rc, int64_t* out_time,
+                           int32_t* out_tmpl, float* out_amp, float* out_pc, int64_t capacity, int64_t* out_count,
                            cudaStream_t s);
 // PC features from the highpassed batch (or, when Phi is given, the projection rows
 // P = Phi + Plo [N, ldp] of the score GEMM) and the folded whitening (no residual array)
@@ -140,8 +154,9 @@ cudaError_t launch_pc_features_folded(const float* Xh, int64_t ldx, int32_t C, i
                                       int32_t T, const float* wpca, const float* Mw, const float* U, const float* R,
                                       const int64_t* iCC, const int64_t* iU, const float* Ucc, const int32_t* sp_x,
                                       const int32_t* sp_y, const float* sp_amp, const int32_t* round_start,
-                                      int32_t rounds, int32_t n, float* tF, int32_t* status, const float* Phi,
-                                      const float* Plo, int64_t ldp, cudaStream_t s);
+                                      int32_t rounds, int32_t n, const int32_t* counters, float* tF,
+                                      int32_t* status, const float* Phi, const float* Plo, int64_t ldp,
+                                      cudaStream_t s);
 cudaError_t launch_st_out(const int32_t* sp_x, const int32_t* sp_y, const float* sp_amp, int32_t n,
                           int64_t* st, float* amps, cudaStream_t s);
 

@@ -470,8 +470,19 @@ cudaError_t launch_mp(MPArgs a, int grid, cudaStream_t s) {
         if (e != cudaSuccess) return e;
     }
     cudaMemsetAsync(a.bar, 0, 2 * sizeof(unsigned int), s);
-    void* args[] = {&a};
-    return cudaLaunchCooperativeKernel((void*)k_mp, dim3(grid), dim3(MP_THREADS), args, smem, s);
+    // cooperative (all CTAs co-resident for the grid barrier); the launch-attribute
+    // form is also valid inside stream capture
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(grid);
+    lc.blockDim = dim3(MP_THREADS);
+    lc.dynamicSmemBytes = smem;
+    lc.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    lc.attrs = attr;
+    lc.numAttrs = 1;
+    return cudaLaunchKernelEx(&lc, k_mp, a);
 }
 
 // ---------------------------------------------------------------------------

@@ -1,0 +1,538 @@
+// Streaming serving loop (lss_server_* in include/lss.h).
+//
+// The reference runs one OnlineSpikesV2 object per probe on its own host
+// thread (main.cpp:77-85); each loop iteration of runSpikeSorting
+// (OnlineSpikesV2.cu:632-820) fetches the latest window, copies it to the
+// device synchronously, sorts it and copies the spikes back. Here a server
+// owns one device and admits several probe streams; each probe's batch is a
+// CUDA graph (captured once per probe, i.e. per batch length and template
+// set) that reads its window straight from a device ring of raw rows and
+// writes its records into pinned host memory, so a batch costs one H2D copy
+// of the new block, one graph launch and one host callback, and batches of
+// different probes overlap on the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "lss.h"
+#include "lss_handle.h"
+#include "lss_kernels.cuh"
+
+namespace lss {
+
+// Per-batch summary the graph's last kernel writes to pinned host memory.
+struct StreamMail {
+    int64_t batch;
+    int32_t spikes, rounds, status, pad;
+};
+
+// state[0] = batch index (starts at -1), state[1] = first stream row of the
+// batch window.
+__global__ void k_stream_begin(int64_t* state, int64_t NT, int64_t lead) {
+    const int64_t b = state[0] + 1;
+    state[0] = b;
+    state[1] = b * NT - lead;
+}
+
+__global__ void k_stream_end(const int64_t* state, const int32_t* counters, const int32_t* status, StreamMail* mail,
+                             int32_t slots) {
+    const int64_t b = state[0];
+    StreamMail m;
+    m.batch = b;
+    m.spikes = counters[0];
+    m.rounds = counters[1];
+    m.status = *status;
+    m.pad = 0;
+    mail[b % slots] = m;
+}
+
+static int64_t now_ns() {
+    return std::chrono::duration_cast<std::chrono::nanoseconds>(
+               std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
+
+}  // namespace lss
+
+using namespace lss;
+
+namespace {
+
+struct Slot {
+    std::atomic<int> done{0};
+    int64_t batch = -1;
+    int64_t arrival_ns = 0;
+    int64_t emit_ns = 0;
+    struct Probe* owner = nullptr;
+};
+
+struct Result {
+    int64_t batch = -1;
+    int32_t status = 0;
+    int64_t count = 0;
+    std::vector<int64_t> time;
+    std::vector<int32_t> tmpl;
+    std::vector<float> amp;
+    std::vector<float> pc;
+};
+
+template <typename T>
+struct HostBuf {
+    T* p = nullptr;
+    T* d = nullptr;  // device alias of mapped memory
+    cudaError_t alloc(size_t n, bool mapped) {
+        cudaError_t e = cudaHostAlloc(reinterpret_cast<void**>(&p), std::max<size_t>(n, 1) * sizeof(T),
+                                      mapped ? cudaHostAllocMapped : cudaHostAllocDefault);
+        if (e != cudaSuccess) return e;
+        std::memset(p, 0, std::max<size_t>(n, 1) * sizeof(T));
+        if (mapped) return cudaHostGetDevicePointer(reinterpret_cast<void**>(&d), p, 0);
+        return cudaSuccess;
+    }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = d = nullptr;
+    }
+};
+
+struct Probe {
+    lss_handle* h = nullptr;
+    cudaStream_t s = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int64_t NT = 0, nt = 0, Cbin = 0, R = 0, D = 0, cap = 0, feat = 0;
+    DevBuf<int16_t> ring;
+    DevBuf<int64_t> state;
+    HostBuf<int16_t> staging;                  // D blocks of NT rows
+    HostBuf<int64_t> o_time, o_count;
+    HostBuf<int32_t> o_tmpl;
+    HostBuf<float> o_amp, o_pc;
+    HostBuf<StreamMail> mail;
+    std::unique_ptr<Slot[]> slots;
+    int64_t fill = 0;                          // rows in the block being assembled
+    int64_t next = 0;                          // next batch to launch
+    int64_t harvest = 0;                       // next batch to harvest
+    std::deque<Result> ready;
+    std::vector<double> lat_ms;
+    size_t bytes = 0;
+    std::mutex m;
+    std::condition_variable cv;
+    std::string err;
+
+    int fail(int code, const std::string& msg) {
+        err = msg;
+        lss::set_thread_error(msg.c_str());
+        return code;
+    }
+    ~Probe() {
+        if (s) cudaStreamSynchronize(s);
+        if (exec) cudaGraphExecDestroy(exec);
+        if (s) cudaStreamDestroy(s);
+        ring.release();
+        state.release();
+        staging.release();
+        o_time.release();
+        o_count.release();
+        o_tmpl.release();
+        o_amp.release();
+        o_pc.release();
+        mail.release();
+        if (h) lss_destroy(h);
+    }
+};
+
+void CUDART_CB on_batch_done(void* arg) {
+    Slot* sl = static_cast<Slot*>(arg);
+    sl->emit_ns = lss::now_ns();
+    Probe* p = sl->owner;
+    {
+        std::lock_guard<std::mutex> lk(p->m);
+        sl->done.store(1);
+    }
+    p->cv.notify_all();
+}
+
+#define PCK(call)                                                                   \
+    do {                                                                            \
+        cudaError_t e_ = (call);                                                    \
+        if (e_ != cudaSuccess) return p->fail(LSS_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+// The batch's device work, enqueued on p->s (captured into the probe's graph).
+int enqueue_stream_batch(Probe* p) {
+    lss_handle* h = p->h;
+    cudaStream_t s = p->s;
+    k_stream_begin<<<1, 1, 0, s>>>(p->state.p, p->NT, 2 * p->nt);
+    PCK(cudaGetLastError());
+    IngestMap map;
+    map.base_dev = p->state.p + 1;
+    map.ring_rows = p->R;
+    const float* Xh = nullptr;
+    int rc = run_ingest(h, p->ring.p, map, nullptr, s, &Xh);
+    if (rc) return p->fail(rc, h->err);
+    PCK(cudaMemsetAsync(h->status.p, 0, sizeof(int32_t), s));
+    bool ready = false;
+    rc = run_scores(h, Xh, h->ld, h->N, h->B.p, s, &ready, /*folded=*/true);
+    if (rc) return p->fail(rc, h->err);
+    rc = enqueue_mp(h, h->N, s, ready);
+    if (rc) return p->fail(rc, h->err);
+    const bool bf16 = h->cfg.precision == LSS_PREC_BF16_RECHECK;
+    if (p->feat > 0) {
+        const int grid = (int)std::min<int64_t>(p->cap, 2 * (int64_t)h->sm_count);
+        PCK(launch_pc_features_folded(Xh, h->ld, h->C, h->nt, h->K, h->nC, h->T, h->wpca.p, h->Mw.p, h->U.p,
+                                      h->R.p, h->iCC.p, h->iU.p, h->Ucc.p, h->sp_x.p, h->sp_y.p, h->sp_amp.p,
+                                      h->round_start.p, 0, grid, h->counters.p, h->tF.p, h->status.p,
+                                      bf16 ? nullptr : h->B0T_hi.p, bf16 ? nullptr : h->B0T_lo.p, h->CKpad, s));
+    }
+    RecordClock rclk;
+    rclk.ibatch_dev = p->state.p;
+    rclk.counters = h->counters.p;
+    rclk.shift = -p->nt;
+    rclk.NT = (int32_t)p->NT;
+    rclk.nt = (int32_t)p->nt;
+    rclk.nt0min = h->cfg.nt0min;
+    rclk.slots = (int32_t)p->D;
+    PCK(launch_records(h->sp_x.p, h->sp_y.p, h->sp_amp.p, p->feat > 0 ? h->tF.p : nullptr, h->rec_slot.p,
+                       (int32_t)std::min<int64_t>(p->cap, h->cfg.max_spikes), (int32_t)p->feat, rclk, p->o_time.d,
+                       p->o_tmpl.d, p->o_amp.d, p->feat > 0 ? p->o_pc.d : nullptr, p->cap, p->o_count.d, s));
+    k_stream_end<<<1, 1, 0, s>>>(p->state.p, h->counters.p, h->status.p, p->mail.d, (int32_t)p->D);
+    PCK(cudaGetLastError());
+    return LSS_OK;
+}
+
+int capture(Probe* p) {
+    lss_handle* h = p->h;
+    const bool prof = h->prof;
+    h->prof = false;
+    h->capturing = true;
+    cudaGraph_t g = nullptr;
+    PCK(cudaStreamBeginCapture(p->s, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_stream_batch(p);
+    const cudaError_t e = cudaStreamEndCapture(p->s, &g);
+    h->capturing = false;
+    h->prof = prof;
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return p->fail(LSS_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    const cudaError_t ei = cudaGraphInstantiate(&p->exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) return p->fail(LSS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+    return LSS_OK;
+}
+
+// Moves the oldest in-flight batch's results into p->ready (waits for it when
+// `wait`). Caller holds p->m through `lk`. Returns LSS_OK (possibly nothing
+// moved when !wait), or an error.
+int harvest_one(Probe* p, std::unique_lock<std::mutex>& lk, bool wait) {
+    if (p->harvest >= p->next) return LSS_OK;
+    Slot& sl = p->slots[p->harvest % p->D];
+    if (!sl.done.load()) {
+        if (!wait) return LSS_OK;
+        // the device work is bounded (every wait in the kernels gives up), so
+        // this wait ends; 60 s covers a cold first launch
+        if (!p->cv.wait_for(lk, std::chrono::seconds(60), [&] { return sl.done.load() != 0; }))
+            return p->fail(LSS_ERR_TIMEOUT, "stream batch did not finish within 60 s");
+    }
+    const int64_t k = p->harvest % p->D;
+    const StreamMail mail = p->mail.p[k];
+    Result r;
+    r.batch = sl.batch;
+    r.status = mail.status;
+    if (mail.batch != sl.batch) r.status |= 1 << 30;  // mailbox out of step: report as a state error
+    r.count = p->o_count.p[k];
+    const int64_t n = std::min<int64_t>(r.count, p->cap);
+    r.time.assign(p->o_time.p + k * p->cap, p->o_time.p + k * p->cap + n);
+    r.tmpl.assign(p->o_tmpl.p + k * p->cap, p->o_tmpl.p + k * p->cap + n);
+    r.amp.assign(p->o_amp.p + k * p->cap, p->o_amp.p + k * p->cap + n);
+    if (p->feat > 0)
+        r.pc.assign(p->o_pc.p + (k * p->cap) * p->feat, p->o_pc.p + (k * p->cap + n) * p->feat);
+    p->lat_ms.push_back((double)(sl.emit_ns - sl.arrival_ns) * 1e-6);
+    sl.done.store(0);
+    p->harvest += 1;
+    p->ready.push_back(std::move(r));
+    return LSS_OK;
+}
+
+int launch_block(Probe* p, int64_t arrival_ns) {
+    const int64_t b = p->next;
+    const int64_t k = b % p->D;
+    PCK(cudaMemcpyAsync(p->ring.p + ((b * p->NT) % p->R) * p->Cbin, p->staging.p + k * p->NT * p->Cbin,
+                        (size_t)(p->NT * p->Cbin) * sizeof(int16_t), cudaMemcpyHostToDevice, p->s));
+    Slot& sl = p->slots[k];
+    sl.batch = b;
+    sl.arrival_ns = arrival_ns > 0 ? arrival_ns : lss::now_ns();
+    sl.done.store(0);
+    PCK(cudaGraphLaunch(p->exec, p->s));
+    PCK(cudaLaunchHostFunc(p->s, on_batch_done, &sl));
+    p->next = b + 1;
+    return LSS_OK;
+}
+
+}  // namespace
+
+struct lss_server {
+    int device = 0;
+    int64_t budget = 0, used = 0;
+    std::vector<std::unique_ptr<Probe>> probes;
+    std::mutex m;
+};
+
+extern "C" {
+
+int lss_server_create(int32_t device, int64_t memory_budget_bytes, int32_t max_probes, lss_server** out) {
+    if (!out || max_probes <= 0 || memory_budget_bytes <= 0) {
+        lss::set_thread_error("lss_server_create: bad argument");
+        return LSS_ERR_ARG;
+    }
+    auto* s = new lss_server;
+    s->device = device;
+    s->budget = memory_budget_bytes;
+    s->probes.resize(max_probes);
+    *out = s;
+    return LSS_OK;
+}
+
+void lss_server_destroy(lss_server* s) {
+    if (!s) return;
+    cudaSetDevice(s->device);
+    s->probes.clear();
+    delete s;
+}
+
+int lss_server_admit(lss_server* s, const lss_config* cfg, const lss_tensors* t, const float* drift_M, int32_t depth,
+                     int64_t capacity, int32_t* probe) {
+    if (!s || !cfg || !t || !probe || depth < 1 || depth > 64 || capacity <= 0) {
+        lss::set_thread_error("lss_server_admit: bad argument");
+        return LSS_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lk(s->m);
+    int slot = -1;
+    for (size_t i = 0; i < s->probes.size(); ++i)
+        if (!s->probes[i]) { slot = (int)i; break; }
+    if (slot < 0) {
+        lss::set_thread_error("no probe slot free");
+        return LSS_ERR_BUSY;
+    }
+    if (cfg->device != s->device) {
+        lss::set_thread_error("probe config names another device than the server's");
+        return LSS_ERR_ARG;
+    }
+    cudaSetDevice(s->device);
+    auto p = std::make_unique<Probe>();
+    int rc = lss_create(cfg, t, &p->h);
+    if (rc) return rc;
+    lss_handle* h = p->h;
+    p->NT = h->NT;
+    p->nt = h->nt;
+    p->Cbin = h->Cbin;
+    p->D = depth;
+    p->cap = capacity;
+    p->feat = (h->nC > 0 && h->iCC.p) ? (int64_t)h->nC * h->K : 0;
+    // ring: the oldest in-flight window plus the blocks written behind it
+    const int64_t win = p->NT + 2 * p->nt;
+    p->R = ((win + p->NT - 1) / p->NT + depth) * p->NT;
+    const size_t ring_bytes = (size_t)p->R * p->Cbin * sizeof(int16_t);
+    p->bytes = h->dev_bytes + ring_bytes + 2 * sizeof(int64_t);
+    if (s->used + (int64_t)p->bytes > s->budget) {
+        lss::set_thread_error("device memory budget exhausted");
+        return LSS_ERR_BUSY;  // p's destructor frees the handle
+    }
+    auto cfail = [&](cudaError_t e, const char* what) {
+        lss::set_thread_error((std::string(what) + ": " + cudaGetErrorString(e)).c_str());
+        return LSS_ERR_CUDA;
+    };
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&p->s, cudaStreamNonBlocking)) != cudaSuccess) return cfail(e, "stream");
+    if ((e = p->ring.alloc((size_t)p->R * p->Cbin)) != cudaSuccess) return cfail(e, "ring");
+    if ((e = p->state.alloc(2)) != cudaSuccess) return cfail(e, "state");
+    const int64_t init[2] = {-1, 0};
+    if ((e = cudaMemcpy(p->state.p, init, sizeof(init), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return cfail(e, "state");
+    if ((e = cudaMemset(p->ring.p, 0, ring_bytes)) != cudaSuccess) return cfail(e, "ring");
+    if ((e = p->staging.alloc((size_t)depth * p->NT * p->Cbin, false)) != cudaSuccess) return cfail(e, "staging");
+    if ((e = p->o_time.alloc((size_t)depth * capacity, true)) != cudaSuccess) return cfail(e, "records");
+    if ((e = p->o_tmpl.alloc((size_t)depth * capacity, true)) != cudaSuccess) return cfail(e, "records");
+    if ((e = p->o_amp.alloc((size_t)depth * capacity, true)) != cudaSuccess) return cfail(e, "records");
+    if ((e = p->o_pc.alloc((size_t)depth * capacity * std::max<int64_t>(p->feat, 1), true)) != cudaSuccess)
+        return cfail(e, "records");
+    if ((e = p->o_count.alloc((size_t)depth, true)) != cudaSuccess) return cfail(e, "records");
+    if ((e = p->mail.alloc((size_t)depth, true)) != cudaSuccess) return cfail(e, "mailbox");
+    p->slots.reset(new Slot[depth]);
+    for (int i = 0; i < depth; ++i) p->slots[i].owner = p.get();
+    if (drift_M) {
+        rc = lss_set_drift(h, drift_M);
+        if (rc) {
+            lss::set_thread_error(h->err.c_str());
+            return rc;
+        }
+    }
+    h->streaming = true;
+    rc = capture(p.get());
+    if (rc) {
+        lss::set_thread_error(p->err.c_str());
+        return rc;
+    }
+    s->used += (int64_t)p->bytes;
+    s->probes[slot] = std::move(p);
+    *probe = slot;
+    return LSS_OK;
+}
+
+static Probe* get_probe(lss_server* s, int32_t probe) {
+    if (!s || probe < 0 || probe >= (int32_t)s->probes.size()) return nullptr;
+    return s->probes[probe].get();
+}
+
+int lss_server_push(lss_server* s, int32_t probe, const int16_t* rows, int64_t n_rows, int64_t arrival_ns) {
+    Probe* p = get_probe(s, probe);
+    if (!p || (!rows && n_rows > 0) || n_rows < 0) {
+        lss::set_thread_error("lss_server_push: bad probe or rows");
+        return LSS_ERR_ARG;
+    }
+    cudaSetDevice(s->device);
+    std::unique_lock<std::mutex> lk(p->m);
+    while (n_rows > 0) {
+        if (p->fill == 0 && p->next - p->harvest >= p->D) {
+            // the staging block and result slot of batch next - D are reused:
+            // that batch must have finished and been moved out
+            int rc = harvest_one(p, lk, true);
+            if (rc) return rc;
+        }
+        const int64_t take = std::min(n_rows, p->NT - p->fill);
+        std::memcpy(p->staging.p + ((p->next % p->D) * p->NT + p->fill) * p->Cbin, rows,
+                    (size_t)(take * p->Cbin) * sizeof(int16_t));
+        p->fill += take;
+        rows += take * p->Cbin;
+        n_rows -= take;
+        if (p->fill == p->NT) {
+            int rc = launch_block(p, arrival_ns);
+            if (rc) return rc;
+            p->fill = 0;
+        }
+    }
+    return LSS_OK;
+}
+
+int lss_server_poll(lss_server* s, int32_t probe, lss_records* out, int64_t* batch, int32_t wait) {
+    Probe* p = get_probe(s, probe);
+    if (!p || !out || !batch) {
+        lss::set_thread_error("lss_server_poll: bad argument");
+        return LSS_ERR_ARG;
+    }
+    if (out->on_device) {
+        lss::set_thread_error("lss_server_poll: records are returned in host memory");
+        return LSS_ERR_ARG;
+    }
+    std::unique_lock<std::mutex> lk(p->m);
+    *batch = -1;
+    out->count = 0;
+    if (p->ready.empty()) {
+        int rc = harvest_one(p, lk, wait != 0);
+        if (rc) return rc;
+    }
+    if (p->ready.empty()) return LSS_OK;
+    Result r = std::move(p->ready.front());
+    p->ready.pop_front();
+    *batch = r.batch;
+    out->count = r.count;
+    if (r.status & STATUS_TIMEOUT) {
+        lss::set_thread_error("a bounded device-side wait gave up in this batch");
+        return LSS_ERR_TIMEOUT;
+    }
+    if (r.status & (STATUS_CAPACITY | STATUS_LIST)) {
+        lss::set_thread_error("spike list capacity exceeded in this batch");
+        return LSS_ERR_CAPACITY;
+    }
+    if (r.status & (1 << 30)) {
+        lss::set_thread_error("stream mailbox out of step");
+        return LSS_ERR_STATE;
+    }
+    if (r.count > p->cap || r.count > out->capacity) {
+        lss::set_thread_error("record capacity smaller than the batch's spike count");
+        return LSS_ERR_CAPACITY;
+    }
+    if (!out->time || !out->template_id || !out->amplitude) {
+        lss::set_thread_error("null record arrays");
+        return LSS_ERR_ARG;
+    }
+    std::copy(r.time.begin(), r.time.end(), out->time);
+    std::copy(r.tmpl.begin(), r.tmpl.end(), out->template_id);
+    std::copy(r.amp.begin(), r.amp.end(), out->amplitude);
+    if (out->pc && p->feat > 0) std::copy(r.pc.begin(), r.pc.end(), out->pc);
+    return LSS_OK;
+}
+
+int lss_server_release(lss_server* s, int32_t probe) {
+    if (!get_probe(s, probe)) {
+        lss::set_thread_error("lss_server_release: bad probe");
+        return LSS_ERR_ARG;
+    }
+    cudaSetDevice(s->device);
+    std::lock_guard<std::mutex> lk(s->m);
+    s->used -= (int64_t)s->probes[probe]->bytes;
+    s->probes[probe].reset();  // the destructor waits for the probe's stream
+    return LSS_OK;
+}
+
+int lss_server_set_drift(lss_server* s, int32_t probe, const float* drift_M) {
+    Probe* p = get_probe(s, probe);
+    if (!p || !drift_M) {
+        lss::set_thread_error("lss_server_set_drift: bad argument");
+        return LSS_ERR_ARG;
+    }
+    cudaSetDevice(s->device);
+    std::unique_lock<std::mutex> lk(p->m);
+    while (p->harvest < p->next) {
+        int rc = harvest_one(p, lk, true);
+        if (rc) return rc;
+    }
+    p->h->streaming = false;
+    int rc = lss_set_drift(p->h, drift_M);
+    p->h->streaming = true;
+    if (rc) lss::set_thread_error(p->h->err.c_str());
+    return rc;
+}
+
+int lss_server_latency(lss_server* s, int32_t probe, double* p50_ms, double* p99_ms, int64_t* batches) {
+    Probe* p = get_probe(s, probe);
+    if (!p || !p50_ms || !p99_ms || !batches) {
+        lss::set_thread_error("lss_server_latency: bad argument");
+        return LSS_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lk(p->m);
+    std::vector<double> v = p->lat_ms;
+    *batches = (int64_t)v.size();
+    if (v.empty()) {
+        *p50_ms = *p99_ms = 0.0;
+        return LSS_OK;
+    }
+    std::sort(v.begin(), v.end());
+    auto pct = [&](double q) {
+        const double pos = q * (double)(v.size() - 1);
+        const size_t i = (size_t)pos;
+        const double f = pos - (double)i;
+        return i + 1 < v.size() ? v[i] * (1.0 - f) + v[i + 1] * f : v[i];
+    };
+    *p50_ms = pct(0.50);
+    *p99_ms = pct(0.99);
+    return LSS_OK;
+}
+
+int lss_server_memory(lss_server* s, int64_t* used, int64_t* budget) {
+    if (!s || !used || !budget) return LSS_ERR_ARG;
+    std::lock_guard<std::mutex> lk(s->m);
+    *used = s->used;
+    *budget = s->budget;
+    return LSS_OK;
+}
+
+}  // extern "C"

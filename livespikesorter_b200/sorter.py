@@ -36,41 +36,53 @@ def _stream(device) -> int | None:
     return torch.cuda.current_stream(device).cuda_stream
 
 
+def build_config(*, U, wPCA, ctc, Wrot, hp_filter=None, drift=None, iCC=None, iU=None, Ucc=None, chan_map=None,
+                 nm=None, NT: int = 60000, nt0min: int = 20, Th: float = 8.0, n_chan_bin: int | None = None,
+                 max_rounds: int = 100, max_spikes: int = 100000, do_CAR: bool = True, invert_sign: bool = False,
+                 precision: str = 'fp32', device: int = 0):
+    """``(lss_config, lss_tensors, keep)`` for ``lss_create``; ``keep`` holds the
+    host tensors the pointers refer to and must outlive the call."""
+    U = _f32(U)
+    T, K, C = U.shape
+    wPCA = _f32(wPCA)
+    nt = wPCA.shape[1]
+    k = dict(U=U, wPCA=wPCA, ctc=_f32(ctc), Wrot=_f32(Wrot),
+             hp=None if hp_filter is None else _f32(hp_filter),
+             drift=None if drift is None else _f32(drift),
+             iCC=None if iCC is None else _i64(iCC), iU=None if iU is None else _i64(iU),
+             Ucc=None if Ucc is None else _f32(Ucc),
+             cmap=None if chan_map is None else torch.as_tensor(np.asarray(chan_map), dtype=torch.int32).contiguous(),
+             nm=None if nm is None else _f32(nm))
+    nC = 0 if k['iCC'] is None else k['iCC'].shape[0]
+    cfg = LssConfig(n_chan=C, n_chan_bin=n_chan_bin or C, n_templates=T, n_pcs=K, nt=nt, n_nearest=nC,
+                    batch_size=NT, nt0min=nt0min, th_learned=float(Th), max_rounds=max_rounds,
+                    max_spikes=max_spikes, do_car=int(do_CAR), invert_sign=int(invert_sign),
+                    precision={'fp32': 0, 'bf16': 1}[precision], device=device,
+                    hp_len=0 if k['hp'] is None else k['hp'].numel())
+    tens = LssTensors(wall3=_ptr(k['U']), wpca=_ptr(k['wPCA']), ctc=_ptr(k['ctc']), whitening=_ptr(k['Wrot']),
+                      drift=_ptr(k['drift']), hp_filter=_ptr(k['hp']), iCC=_ptr(k['iCC']), iU=_ptr(k['iU']),
+                      Ucc=_ptr(k['Ucc']), chan_map=_ptr(k['cmap']), nm=_ptr(k['nm']))
+    return cfg, tens, k
+
+
+def setup_kwargs(setup) -> dict:
+    """Constructor arguments of a ``synth.SortSetup``."""
+    return dict(U=setup.U, wPCA=setup.wPCA, ctc=setup.ctc, Wrot=setup.Wrot, hp_filter=setup.hp_filter,
+                iCC=setup.iCC, iU=setup.iU, Ucc=setup.Ucc, NT=setup.NT, nt0min=setup.nt0min, Th=setup.Th)
+
+
 class Sorter:
     """One sorter handle: templates, ctc, whitening, filters and all device
     workspaces live on ``device`` for the handle's lifetime."""
 
-    def __init__(self, *, U, wPCA, ctc, Wrot, hp_filter=None, drift=None, iCC=None, iU=None, Ucc=None,
-                 chan_map=None, nm=None, NT: int = 60000, nt0min: int = 20, Th: float = 8.0,
-                 n_chan_bin: int | None = None, max_rounds: int = 100, max_spikes: int = 100000,
-                 do_CAR: bool = True, invert_sign: bool = False, precision: str = 'fp32', device: int = 0):
+    def __init__(self, *, device: int = 0, **kw):
         self._lib = _lib.load()
-        U = _f32(U)
-        T, K, C = U.shape
-        wPCA = _f32(wPCA)
-        nt = wPCA.shape[1]
-        self._keep = dict(U=U, wPCA=wPCA, ctc=_f32(ctc), Wrot=_f32(Wrot),
-                          hp=None if hp_filter is None else _f32(hp_filter),
-                          drift=None if drift is None else _f32(drift),
-                          iCC=None if iCC is None else _i64(iCC), iU=None if iU is None else _i64(iU),
-                          Ucc=None if Ucc is None else _f32(Ucc),
-                          cmap=None if chan_map is None else torch.as_tensor(np.asarray(chan_map), dtype=torch.int32).contiguous(),
-                          nm=None if nm is None else _f32(nm))
-        k = self._keep
-        nC = 0 if k['iCC'] is None else k['iCC'].shape[0]
-        cfg = LssConfig(n_chan=C, n_chan_bin=n_chan_bin or C, n_templates=T, n_pcs=K, nt=nt, n_nearest=nC,
-                        batch_size=NT, nt0min=nt0min, th_learned=float(Th), max_rounds=max_rounds,
-                        max_spikes=max_spikes, do_car=int(do_CAR), invert_sign=int(invert_sign),
-                        precision={'fp32': 0, 'bf16': 1}[precision], device=device,
-                        hp_len=0 if k['hp'] is None else k['hp'].numel())
-        tens = LssTensors(wall3=_ptr(k['U']), wpca=_ptr(k['wPCA']), ctc=_ptr(k['ctc']), whitening=_ptr(k['Wrot']),
-                          drift=_ptr(k['drift']), hp_filter=_ptr(k['hp']), iCC=_ptr(k['iCC']), iU=_ptr(k['iU']),
-                          Ucc=_ptr(k['Ucc']), chan_map=_ptr(k['cmap']), nm=_ptr(k['nm']))
+        cfg, tens, keep = build_config(device=device, **kw)
         h = __import__('ctypes').c_void_p()
         check(self._lib.lss_create(cfg, tens, h))
+        del keep
         self._h = h
         self._init_dims(device)
-        del self._keep
 
     @classmethod
     def from_dir(cls, path: str, **overrides) -> 'Sorter':
@@ -94,8 +106,7 @@ class Sorter:
     @classmethod
     def from_setup(cls, setup, **kw) -> 'Sorter':
         """Build from a ``synth.SortSetup``."""
-        return cls(U=setup.U, wPCA=setup.wPCA, ctc=setup.ctc, Wrot=setup.Wrot, hp_filter=setup.hp_filter,
-                   iCC=setup.iCC, iU=setup.iU, Ucc=setup.Ucc, NT=setup.NT, nt0min=setup.nt0min, Th=setup.Th, **kw)
+        return cls(**(setup_kwargs(setup) | kw))
 
     def _init_dims(self, device):
         cfg = LssConfig()
