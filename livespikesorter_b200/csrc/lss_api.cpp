@@ -252,8 +252,9 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
         if (h->hpL < 0) return LSS_ERR_ARG;
     }
 
-    // one CTA per >= 128 columns (short streaming batches leave SMs to other probes)
-    h->mp_grid = std::min<int>(mp_max_grid(cfg->device), (int)std::max<int64_t>(1, (h->N + 127) / 128));
+    // one CTA per >= 32 columns (a serving loop lowers it further so that
+    // its probes' rounds kernels fit on the device together)
+    h->mp_grid = std::min<int>(mp_max_grid(cfg->device), (int)std::max<int64_t>(1, (h->N + 31) / 32));
     cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, cfg->device);
     h->CKpad = (C * K + 63) / 64 * 64;
     const int64_t cap = cfg->max_spikes;
@@ -596,9 +597,11 @@ int lss::run_scores(lss_handle* h, const float* X, int64_t ldx, int64_t N, float
     }
     CK(launch_pca_proj_t_tf32(X, ldx, h->C, N, h->wpca.p, h->K, h->nt, h->B0T_hi.p, h->B0T_lo.p, h->CKpad, s));
     h->mark(5, s);
+    TcExtra ex;
+    ex.keys = h->colkey.p;  // free until the rounds start (they clear it)
     CK(launch_score_tc_tf32x3(h->B0T_hi.p, h->B0T_lo.p, h->CKpad, (int)N, folded ? h->Uw_hi.p : h->Up_hi.p,
                               folded ? h->Uw_lo.p : h->Up_lo.p, h->T, h->CKpad, h->nm.p, B, h->ld, h->cfmax.p,
-                              h->imax.p, h->nt, h->status.p, h->sm_count, s));
+                              h->imax.p, h->nt, h->status.p, h->sm_count, s, ex));
     h->stats.launches += 2;
     h->mark(6, s);
     if (maxima_ready) *maxima_ready = true;

@@ -54,8 +54,9 @@ struct TcPlan {
     int nacc;      // accumulator buffers in tensor memory
     size_t smem;
     int kblock;    // K elements per pipeline stage
+    int pass_w;    // templates per pass
 };
-TcPlan tc_plan(int T, bool tf32);
+TcPlan tc_plan(int T, bool tf32, int pass_w = 512);
 // Optional epilogue behaviour of the score GEMM.
 struct TcExtra {
     // GEMM row r scores sample rowmap[r / map_rows] * map_rows + r % map_rows
@@ -65,6 +66,7 @@ struct TcExtra {
     const int32_t* count_dev = nullptr;
     int ncols = 0;                    // batch samples when rowmap is set
     float* cf2 = nullptr;             // runner-up Cf per sample
+    unsigned long long* keys = nullptr;  // [N] scratch: lets short batches split templates over CTAs
 };
 // B[t, s] (row stride ldb) = sum_kk B0T[s, kk] * Up[t, kk] with B0T [N, ldk] and Up [Tpad, CKpad]
 // bf16, CKpad a multiple of 64; also writes the column maxima cfmax/imax of Cf.

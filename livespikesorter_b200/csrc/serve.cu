@@ -226,6 +226,17 @@ int capture(Probe* p) {
     const cudaError_t ei = cudaGraphInstantiate(&p->exec, g, 0);
     cudaGraphDestroy(g);
     if (ei != cudaSuccess) return p->fail(LSS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+    // one launch on the zeroed ring (no spikes) so that the stream's first
+    // batch does not pay for the graph's upload and first-launch set-up; the
+    // stream state is reset afterwards
+    PCK(cudaGraphUpload(p->exec, p->s));
+    PCK(cudaGraphLaunch(p->exec, p->s));
+    const int64_t init[2] = {-1, 0};
+    PCK(cudaMemcpyAsync(p->state.p, init, sizeof(init), cudaMemcpyHostToDevice, p->s));
+    PCK(cudaStreamSynchronize(p->s));
+    const StreamMail m0 = p->mail.p[0];
+    if (m0.status != 0 || m0.spikes != 0)
+        return p->fail(LSS_ERR_STATE, "warm-up launch of the stream graph did not come back clean");
     return LSS_OK;
 }
 
@@ -375,6 +386,9 @@ int lss_server_admit(lss_server* s, const lss_config* cfg, const lss_tensors* t,
             return rc;
         }
     }
+    // every admitted probe's rounds kernel (a cooperative grid, one CTA per
+    // SM) must fit beside the others': at most SMs / max_probes CTAs each
+    h->mp_grid = std::max(1, std::min(h->mp_grid, h->sm_count / (int)s->probes.size()));
     h->streaming = true;
     rc = capture(p.get());
     if (rc) {

@@ -32,6 +32,7 @@ namespace tc {
 
 constexpr int BM = 128;               // samples per tile
 constexpr int MAX_NP = 512;           // templates per pass (TMEM columns)
+constexpr int SPLIT_W = 128;          // templates per work item in split mode
 constexpr int THREADS = 192;
 
 // Element kinds of the score GEMM.
@@ -66,6 +67,9 @@ struct Args {
     const int32_t* count_dev; // rows = min(N, count_dev[0] * map_rows) (null: N)
     int ncols;                // samples in the batch (edge columns are the first/last nt)
     float* cf2;               // runner-up Cf of each column (null: not tracked)
+    int pass_w;               // templates per pass (<= MAX_NP)
+    unsigned long long* keys; // split mode: one work item per (sample tile, pass); column maxima are
+                              // combined as atomicMax of (Cf bits << 32 | ~t) (null: a CTA owns whole rows)
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -275,7 +279,10 @@ __global__ void __launch_bounds__(THREADS, 1)
 
     const int rows = a.count_dev ? min(a.N, a.count_dev[0] * a.map_rows) : a.N;
     const int ntiles = (rows + BM - 1) / BM;
-    const int npass = (a.Tpad + MAX_NP - 1) / MAX_NP;
+    const int PW = a.pass_w;
+    const int npass = (a.Tpad + PW - 1) / PW;
+    const bool split = a.keys != nullptr;
+    const int items = split ? ntiles * npass : ntiles;
 
     if (warp == 0) {
         if (lane == 0) {
@@ -285,9 +292,11 @@ __global__ void __launch_bounds__(THREADS, 1)
             uint32_t last_ph[8];
             bool pending[8] = {false, false, false, false, false, false, false, false};
             bool ok = true;
-            for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-                for (int p = 0; p < npass && ok; ++p) {
-                    const int np = min(MAX_NP, a.Tpad - p * MAX_NP);
+            for (int it = blockIdx.x; it < items && ok; it += gridDim.x) {
+                const int tile = split ? it / npass : it;
+                const int pb = split ? it % npass : 0, pe = split ? pb + 1 : npass;
+                for (int p = pb; p < pe && ok; ++p) {
+                    const int np = min(PW, a.Tpad - p * PW);
                     const int nbox = (np + a.box_rows - 1) / a.box_rows;
                     const uint32_t bytes = KD::PARTS * (KD::A_TILE + (uint32_t)nbox * a.box_rows * KD::ROW);
                     for (int kb = 0; kb < a.KB; ++kb) {
@@ -299,7 +308,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                         tma_load_2d(sa, &tmA, kx, tile * BM, full_bar(stage));
                         if (TF32) tma_load_2d(sa + KD::A_TILE, &tmAlo, kx, tile * BM, full_bar(stage));
                         for (int bx = 0; bx < nbox; ++bx) {
-                            const int row = p * MAX_NP + bx * a.box_rows;
+                            const int row = p * PW + bx * a.box_rows;
                             tma_load_2d(sb + bx * a.box_rows * KD::ROW, &tmB, kx, row, full_bar(stage));
                             if (TF32) tma_load_2d(sb + b_part + bx * a.box_rows * KD::ROW, &tmBlo, kx, row, full_bar(stage));
                         }
@@ -323,9 +332,10 @@ __global__ void __launch_bounds__(THREADS, 1)
             uint32_t acc_ph[2] = {0, 0};
             int acc = 0;
             bool ok = true;
-            for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-                for (int p = 0; p < npass && ok; ++p) {
-                    const int np = min(MAX_NP, a.Tpad - p * MAX_NP);
+            for (int it = blockIdx.x; it < items && ok; it += gridDim.x) {
+                const int pb = split ? it % npass : 0, pe = split ? pb + 1 : npass;
+                for (int p = pb; p < pe && ok; ++p) {
+                    const int np = min(PW, a.Tpad - p * PW);
                     if (!mbar_wait(acce_bar(acc), acc_ph[acc] ^ 1u, abort_flag, a.status)) { ok = false; break; }
                     fence_after();
                     const uint32_t dcol = tmem + (uint32_t)(acc * 256);
@@ -380,22 +390,24 @@ __global__ void __launch_bounds__(THREADS, 1)
         uint32_t acc_ph[2] = {0, 0};
         int acc = 0;
         bool ok = true;
-        for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        for (int it = blockIdx.x; it < items && ok; it += gridDim.x) {
+            const int tile = split ? it / npass : it;
+            const int pb = split ? it % npass : 0, pe = split ? pb + 1 : npass;
             const int gr = tile * BM + row;
             const int n = (a.rowmap && gr < rows) ? a.rowmap[gr / a.map_rows] * a.map_rows + gr % a.map_rows : gr;
             const bool valid = gr < rows && n < a.ncols;
             const bool edge = (n < a.nt) || (n >= a.ncols - a.nt);
             const bool second = a.cf2 != nullptr;
             ColMax m;
-            for (int p = 0; p < npass; ++p) {
-                const int np = min(MAX_NP, a.Tpad - p * MAX_NP);
+            for (int p = pb; p < pe; ++p) {
+                const int np = min(PW, a.Tpad - p * PW);
                 if (!mbar_wait(accf_bar(acc), acc_ph[acc], abort_flag, a.status)) { ok = false; break; }
                 fence_after();
                 const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * 256);
                 for (int c = 0; c < np; c += 16) {
                     uint32_t r[16];
                     tmem_ld16(tbase + (uint32_t)c, r);
-                    const int t0 = p * MAX_NP + c;
+                    const int t0 = p * PW + c;
                     if (valid) {
 #pragma unroll
                         for (int j = 0; j < 16; ++j) {
@@ -418,9 +430,15 @@ __global__ void __launch_bounds__(THREADS, 1)
                 acc = (acc + 1) % a.nacc;
             }
             if (ok && valid) {
-                a.cfmax[n] = edge ? 0.f : m.best;
-                a.imax[n] = edge ? 0 : m.bi;
-                if (second) a.cf2[n] = edge ? 0.f : m.second;
+                if (split) {
+                    const float cf = edge ? 0.f : fmaxf(m.best, 0.f);
+                    const uint32_t t = edge ? 0u : (uint32_t)m.bi;
+                    atomicMax(a.keys + n, ((unsigned long long)__float_as_uint(cf) << 32) | (unsigned long long)(~t));
+                } else {
+                    a.cfmax[n] = edge ? 0.f : m.best;
+                    a.imax[n] = edge ? 0 : m.bi;
+                    if (second) a.cf2[n] = edge ? 0.f : m.second;
+                }
             }
         }
     }
@@ -430,6 +448,17 @@ __global__ void __launch_bounds__(THREADS, 1)
         fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(MAX_NP) : "memory");
     }
+}
+
+// Split mode: column maxima from the combined keys (the keys are left for the
+// next user to clear).
+__global__ void k_keys_to_maxima(const unsigned long long* __restrict__ keys, int N, float* __restrict__ cfmax,
+                                 int32_t* __restrict__ imax) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const unsigned long long k = keys[n];
+    cfmax[n] = __uint_as_float((uint32_t)(k >> 32));
+    imax[n] = (int32_t)(~(uint32_t)k);
 }
 
 }  // namespace tc
@@ -471,14 +500,15 @@ static bool make_map(CUtensorMap* m, const void* base, int64_t rows, int64_t col
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-TcPlan tc_plan(int T, bool tf32) {
+TcPlan tc_plan(int T, bool tf32, int pass_w) {
     TcPlan p{};
     p.Tpad = (T + 15) / 16 * 16;
-    const int np0 = std::min(tc::MAX_NP, p.Tpad);
+    p.pass_w = std::min(pass_w, tc::MAX_NP);
+    const int np0 = std::min(p.pass_w, p.Tpad);
     p.box_rows = (np0 <= 256) ? np0 : ((np0 + 1) / 2 + 7) / 8 * 8;
     int b_rows = 0;  // largest pass rounded up to whole boxes
-    for (int off = 0; off < p.Tpad; off += tc::MAX_NP) {
-        const int np = std::min(tc::MAX_NP, p.Tpad - off);
+    for (int off = 0; off < p.Tpad; off += p.pass_w) {
+        const int np = std::min(p.pass_w, p.Tpad - off);
         b_rows = std::max(b_rows, (np + p.box_rows - 1) / p.box_rows * p.box_rows);
     }
     p.b_rows = b_rows;
@@ -497,7 +527,12 @@ template <bool TF32>
 static cudaError_t launch_tc(const void* A, const void* Alo, int64_t ldk, int N, const void* Bm, const void* Blo, int T,
                              int CKpad, const float* nm, float* Bout, int64_t ldb, float* cfmax, int32_t* imax, int nt,
                              int32_t* status, int grid, cudaStream_t s, const TcExtra& ex) {
-    const TcPlan p = tc_plan(T, TF32);
+    // Few sample tiles (short streaming batches): one work item per (tile,
+    // pass of SPLIT_W templates) so that more SMs share the templates; the
+    // column maxima are then combined through 64-bit keys.
+    const int ntiles = (N + tc::BM - 1) / tc::BM;
+    const bool split = ex.keys && !ex.cf2 && !ex.rowmap && 2 * ntiles < grid && T > tc::SPLIT_W;
+    const TcPlan p = tc_plan(T, TF32, split ? tc::SPLIT_W : tc::MAX_NP);
     if (p.stages < 2 || CKpad % p.kblock) return cudaErrorInvalidValue;
     CUtensorMap ma, malo, mb, mblo;
     if (!make_map(&ma, A, N, CKpad, ldk, tc::BM, TF32) || !make_map(&mb, Bm, p.Tpad, CKpad, CKpad, p.box_rows, TF32))
@@ -531,10 +566,17 @@ static cudaError_t launch_tc(const void* A, const void* Alo, int64_t ldk, int N,
     a.count_dev = ex.count_dev;
     a.ncols = ex.rowmap ? ex.ncols : N;
     a.cf2 = ex.cf2;
+    a.pass_w = p.pass_w;
+    a.keys = split ? ex.keys : nullptr;
     cudaError_t e = cudaFuncSetAttribute(tc::k_score_tc<TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
     if (e != cudaSuccess) return e;
-    const int ntiles = (N + tc::BM - 1) / tc::BM;
-    tc::k_score_tc<TF32><<<std::min(grid, ntiles), tc::THREADS, p.smem, s>>>(ma, malo, mb, mblo, a);
+    const int items = split ? ntiles * ((p.Tpad + p.pass_w - 1) / p.pass_w) : ntiles;
+    if (split) {
+        e = cudaMemsetAsync(ex.keys, 0, (size_t)N * sizeof(unsigned long long), s);
+        if (e != cudaSuccess) return e;
+    }
+    tc::k_score_tc<TF32><<<std::min(grid, items), tc::THREADS, p.smem, s>>>(ma, malo, mb, mblo, a);
+    if (split) tc::k_keys_to_maxima<<<(N + 255) / 256, 256, 0, s>>>(ex.keys, N, cfmax, imax);
     return cudaGetLastError();
 }
 

@@ -175,11 +175,15 @@ def run_streams(server, streams: list[Stream], *, realtime: bool = True, jitter_
                 still.append(st)
                 continue
             nb = st.n_blocks if st.n_blocks is not None else st.raw.shape[0] // st.block
-            start_ns = clock() if realtime else t0
             sched = arrival_schedule(nb, st.block, jitter_frac, rng) if realtime else np.zeros(nb)
             st.admitted_s = (clock() - t0) * 1e-9
-            active[pid] = [st, sched, 0, start_ns]
+            active[pid] = [st, sched, 0, None]
         waiting = still
+        # a stream's clock starts once the admissions of this pass are done
+        # (an admission builds the probe's handle and graph)
+        for a in active.values():
+            if a[3] is None:
+                a[3] = clock() if realtime else t0
         # pushes of blocks that have arrived
         progressed = False
         next_due = None
