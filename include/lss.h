@@ -205,6 +205,30 @@ int  lss_set_profiling(lss_handle* h, int32_t on);
 int  lss_get_stage_times(const lss_handle* h, lss_stage_times* out);
 
 /* ------------------------------------------------------------------------
+ * Reconstruction and its adjoint, for refining U and the temporal basis by
+ * gradient on residual energy with the spike assignments held fixed. No
+ * counterpart in the reference (Kilosort's reconstruction is the residual
+ * update of template_matching.py:195-198; its templates are learned offline).
+ *   R[c, s] = sum_i amp_i sum_k U[y_i, k, c] wPCA[k, s - x_i + nt/2]
+ * dtype 0 = float32, 1 = float64 (every floating-point array in that type).
+ * U [T, K, C], wPCA [K, nt], R / dR [C, N] row-major, device memory.
+ * lss_recon_forward needs the spikes sorted by x (x_sorted and y, amp in the
+ * same order). lss_recon_backward takes the spikes in any order plus
+ * order_by_template (spike indices grouped by template) and
+ * template_start [T + 1] (template t's spikes are
+ * order_by_template[template_start[t] .. template_start[t+1])); it writes
+ * dU [T, K, C], dwPCA [K, nt] and, when damp is not null, dL/damp [n]; work
+ * holds T * K * nt elements. Both are deterministic.
+ * ---------------------------------------------------------------------- */
+int  lss_recon_forward(int32_t dtype, const void* U, const void* wPCA, int32_t T, int32_t K, int32_t C, int32_t nt,
+                       const int32_t* x_sorted, const int32_t* y, const void* amp, int64_t n, void* R, int64_t N,
+                       void* stream);
+int  lss_recon_backward(int32_t dtype, const void* U, const void* wPCA, int32_t T, int32_t K, int32_t C, int32_t nt,
+                        const int32_t* x, const void* amp, const int32_t* order_by_template,
+                        const int32_t* template_start, const void* dR, int64_t N, void* dU, void* dwPCA,
+                        void* damp, void* work, void* stream);
+
+/* ------------------------------------------------------------------------
  * Streaming serving loop. No counterpart in the reference as an API: there
  * each probe runs its own OnlineSpikesV2 object on its own thread
  * (main.cpp:77-85), whose runSpikeSorting loop (OnlineSpikesV2.cu:632-820)

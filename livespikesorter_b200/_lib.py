@@ -19,7 +19,7 @@ EXPORTS = ('lss_create', 'lss_create_from_dir', 'lss_destroy', 'lss_last_error',
            'lss_sort_batch', 'lss_get_stats', 'lss_set_profiling', 'lss_get_stage_times',
            'lss_mp_rounds_noalloc', 'lss_server_create', 'lss_server_destroy', 'lss_server_admit',
            'lss_server_push', 'lss_server_poll', 'lss_server_release', 'lss_server_set_drift',
-           'lss_server_latency', 'lss_server_memory')
+           'lss_server_latency', 'lss_server_memory', 'lss_recon_forward', 'lss_recon_backward')
 
 
 class LssConfig(ct.Structure):
@@ -104,6 +104,8 @@ def load() -> ct.CDLL:
         'lss_server_latency': ([P, I32, ct.POINTER(ct.c_double), ct.POINTER(ct.c_double), ct.POINTER(I64)],
                                ct.c_int),
         'lss_server_memory': ([P, ct.POINTER(I64), ct.POINTER(I64)], ct.c_int),
+        'lss_recon_forward': ([I32, P, P, I32, I32, I32, I32, P, P, P, I64, P, I64, P], ct.c_int),
+        'lss_recon_backward': ([I32, P, P, I32, I32, I32, I32, P, P, P, P, P, I64, P, P, P, P, P], ct.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

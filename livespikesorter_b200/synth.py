@@ -188,10 +188,7 @@ def make_setup_and_units(probe: Probe, T: int, seed: int, nt: int = 61, nt0min: 
 
     # whitened templates at the median amplitude, projected on the basis
     fp = _footprints(probe.xc, probe.yc, cx, cy)                     # [T, C]
-    amp_bits = 80.0 / UV_PER_BIT
-    tmpl = amp_bits * fp[:, :, None] * wf[:, None, :]                # [T, C, nt]
-    tw = np.einsum('ij,tjm->tim', Wrot.double().numpy(), tmpl)      # whitened
-    U = torch.from_numpy(np.einsum('tcm,km->tkc', tw, wPCA.double().numpy())).float().contiguous()
+    U = _project_templates(fp, wf, Wrot, wPCA)
 
     ctc = st.prepare_matching(wPCA, U)
     iCC, iU, Ucc = st.prepare_extract(probe.xc, probe.yc, U, nC)
@@ -200,6 +197,26 @@ def make_setup_and_units(probe: Probe, T: int, seed: int, nt: int = 61, nt0min: 
                       hp, iKxx, iCC.contiguous(), iU.contiguous(), Ucc.contiguous())
     units = dict(cx=cx, cy=cy, waves=waves, rates=rates, fp=fp)
     return setup, units
+
+
+def _project_templates(fp: np.ndarray, wf: np.ndarray, Wrot: torch.Tensor, wPCA: torch.Tensor) -> torch.Tensor:
+    """U [T, K, C]: footprints x filtered waveforms at the median amplitude,
+    whitened and projected on the temporal basis."""
+    amp_bits = 80.0 / UV_PER_BIT
+    tmpl = amp_bits * fp[:, :, None] * wf[:, None, :]                # [T, C, nt]
+    tw = np.einsum('ij,tjm->tim', Wrot.double().numpy(), tmpl)      # whitened
+    return torch.from_numpy(np.einsum('tcm,km->tkc', tw, wPCA.double().numpy())).float().contiguous()
+
+
+def true_templates(setup: SortSetup, units: dict, fp_shift_um: float = 0.0,
+                   fp_scale: np.ndarray | None = None) -> torch.Tensor:
+    """Templates of the units as rendered with shifted / scaled footprints
+    (the ground truth template refinement should recover)."""
+    probe = setup.probe
+    wf = _hp_apply(units['waves'], setup.hp_filter.double().numpy())
+    scale = np.ones(len(units['cx'])) if fp_scale is None else fp_scale
+    fp = _footprints(probe.xc, probe.yc, units['cx'], units['cy'] + fp_shift_um) * scale[:, None]
+    return _project_templates(fp, wf, setup.Wrot, setup.wPCA)
 
 
 def _fft_hp(hp: torch.Tensor, n: int) -> torch.Tensor:
@@ -282,7 +299,9 @@ def config(index: int, duration_s: float | None = None, seed: int = 0,
             return setup, render(setup, units, duration_s or 60.0, seed + 100, drift_um_per_min=5.0)
         rng = np.random.default_rng(seed + 5)
         sc = rng.uniform(0.9, 1.1, setup.T)
-        return setup, render(setup, units, duration_s or 32.0, seed + 100, fp_shift_um=10.0, fp_scale=sc)
+        rec = render(setup, units, duration_s or 32.0, seed + 100, fp_shift_um=10.0, fp_scale=sc)
+        rec.meta['U_true'] = true_templates(setup, units, 10.0, sc)
+        return setup, rec
     if index == 2:
         probe = probe_staggered(C or 384)
         setup, units = make_setup_and_units(probe, T or 800, seed, dup_frac=0.1)
