@@ -86,8 +86,34 @@ typedef struct lss_records {
     float*   pc;           /* [capacity, nC, K] or NULL                            */
     int64_t  capacity;
     int64_t  count;
-    int32_t  on_device;    /* 1: the four arrays are device pointers               */
+    int32_t  on_device;    /* 1: the arrays are device pointers                    */
+    /* filled only when post-processing is on (lss_set_postprocess); may be NULL */
+    float*   x_pos;        /* [capacity] spike position (compute_spike_positions)  */
+    float*   y_pos;        /* [capacity]                                           */
+    int32_t* cluster;      /* [capacity] nearest cluster centroid (or template)    */
 } lss_records;
+
+/* Post-processing of every batch's spikes (off by default):
+ *  - position from the PC-feature energy on the nC nearest channels
+ *    (kilosort/postprocessing.py:33-46; OnlineSpikesV2.cu:189-244), needs xc/yc;
+ *  - cluster = nearest of n_clusters centroids [n_clusters, 2] (x, y), first
+ *    index on ties (OnlineSpikesV2::closestCluster, OnlineSpikesV2.cu:1028-1043,
+ *    with the reference's cluster_centroids.npy); n_clusters = 0: cluster = template;
+ *  - removal of spikes closer than dt_samples to the last kept spike of their
+ *    cluster (kilosort/postprocessing.py:10-31; OnlineSpikesV2::saveSpikes,
+ *    OnlineSpikesV2.cu:1131-1164), carried from batch to batch (reset by a
+ *    first batch, ibatch = 0, or lss_reset_postprocess); dt_samples = 0: off;
+ *  - records in time order (ties in matching order).
+ * Pass NULL to switch it off. */
+typedef struct lss_post_config {
+    const float* xc;            /* [n_chan] channel x (um), or NULL */
+    const float* yc;            /* [n_chan] channel y (um), or NULL */
+    const float* centroids_xy;  /* [n_clusters, 2] or NULL           */
+    int32_t n_clusters;
+    int32_t dt_samples;         /* Kilosort's duplicate_spike_bins (7 at 30 kHz) */
+} lss_post_config;
+int  lss_set_postprocess(lss_handle* h, const lss_post_config* post);
+int  lss_reset_postprocess(lss_handle* h);
 
 /* Construction. Replaces OnlineSpikesV2::OnlineSpikesV2 / initializeSorter /
  * initializeStaticMemory (OnlineSpikesV2.cu:247-280, 321-352, 470-608): all
@@ -258,11 +284,11 @@ typedef struct lss_server lss_server;
 int  lss_server_create(int32_t device, int64_t memory_budget_bytes, int32_t max_probes, lss_server** out);
 void lss_server_destroy(lss_server* s);
 /* Admits a probe: creates its handle from (cfg, t), applies the drift matrix
- * M [C, C] when given, allocates its ring (`depth` batches in flight) and
+ * M [C, C] and the post-processing when given, allocates its ring (`depth` batches in flight) and
  * result ring (`capacity` records per batch) and captures its graph.
  * LSS_ERR_BUSY when no slot is free or the handle would exceed the budget. */
 int  lss_server_admit(lss_server* s, const lss_config* cfg, const lss_tensors* t, const float* drift_M,
-                      int32_t depth, int64_t capacity, int32_t* probe);
+                      const lss_post_config* post, int32_t depth, int64_t capacity, int32_t* probe);
 /* Appends n_rows raw int16 rows [n_rows, n_chan_bin] (host) to the probe's
  * stream; every completed NT-row block launches its batch. arrival_ns: host
  * CLOCK_MONOTONIC time the rows arrived (<= 0: now). Blocks only when `depth`

@@ -19,7 +19,8 @@ EXPORTS = ('lss_create', 'lss_create_from_dir', 'lss_destroy', 'lss_last_error',
            'lss_sort_batch', 'lss_get_stats', 'lss_set_profiling', 'lss_get_stage_times',
            'lss_mp_rounds_noalloc', 'lss_server_create', 'lss_server_destroy', 'lss_server_admit',
            'lss_server_push', 'lss_server_poll', 'lss_server_release', 'lss_server_set_drift',
-           'lss_server_latency', 'lss_server_memory', 'lss_recon_forward', 'lss_recon_backward')
+           'lss_server_latency', 'lss_server_memory', 'lss_recon_forward', 'lss_recon_backward',
+           'lss_set_postprocess', 'lss_reset_postprocess')
 
 
 class LssConfig(ct.Structure):
@@ -41,7 +42,13 @@ class LssTensors(ct.Structure):
 class LssRecords(ct.Structure):
     _fields_ = [('time', ct.c_void_p), ('template_id', ct.c_void_p), ('amplitude', ct.c_void_p),
                 ('pc', ct.c_void_p), ('capacity', ct.c_int64), ('count', ct.c_int64),
-                ('on_device', ct.c_int32)]
+                ('on_device', ct.c_int32), ('x_pos', ct.c_void_p), ('y_pos', ct.c_void_p),
+                ('cluster', ct.c_void_p)]
+
+
+class LssPostConfig(ct.Structure):
+    _fields_ = [('xc', ct.c_void_p), ('yc', ct.c_void_p), ('centroids_xy', ct.c_void_p),
+                ('n_clusters', ct.c_int32), ('dt_samples', ct.c_int32)]
 
 
 class LssStats(ct.Structure):
@@ -95,8 +102,10 @@ def load() -> ct.CDLL:
                                    ct.POINTER(I32), ct.POINTER(I32), P], ct.c_int),
         'lss_server_create': ([I32, I64, I32, ct.POINTER(P)], ct.c_int),
         'lss_server_destroy': ([P], None),
-        'lss_server_admit': ([P, ct.POINTER(LssConfig), ct.POINTER(LssTensors), P, I32, I64, ct.POINTER(I32)],
-                             ct.c_int),
+        'lss_server_admit': ([P, ct.POINTER(LssConfig), ct.POINTER(LssTensors), P, ct.POINTER(LssPostConfig), I32,
+                              I64, ct.POINTER(I32)], ct.c_int),
+        'lss_set_postprocess': ([P, ct.POINTER(LssPostConfig)], ct.c_int),
+        'lss_reset_postprocess': ([P], ct.c_int),
         'lss_server_push': ([P, I32, P, I64, I64], ct.c_int),
         'lss_server_poll': ([P, I32, ct.POINTER(LssRecords), ct.POINTER(I64), I32], ct.c_int),
         'lss_server_release': ([P, I32], ct.c_int),

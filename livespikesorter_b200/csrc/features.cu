@@ -186,7 +186,7 @@ cudaError_t launch_records(const int32_t* sp_x, const int32_t* sp_y, const float
                            int32_t* out_tmpl, float* out_amp, float* out_pc, int64_t capacity, int64_t* out_count,
                            cudaStream_t s) {
     // n: the spike count, or (rc.counters != null) an upper bound that sizes the write grid
-    k_records_scan<<<1, 1024, 0, s>>>(sp_x, n, rc, slot, out_count);
+    if (!rc.presorted) k_records_scan<<<1, 1024, 0, s>>>(sp_x, n, rc, slot, out_count);
     const int64_t total = (int64_t)n * (3 + (tF ? feat_len : 0));
     if (total > 0) {
         const int64_t blocks = std::min<int64_t>((total + 255) / 256, rc.counters ? 1184 : INT32_MAX);

@@ -678,7 +678,118 @@ static int run_xres(lss_handle* h, const float* X, int64_t ldx, int64_t N, int r
     return LSS_OK;
 }
 
+int lss::enqueue_records(lss_handle* h, const RecordClock& rc_in, int32_t n_bound, bool with_pc, bool tf_ready,
+                         int64_t* time, int32_t* tmpl, float* amp, float* pc, float* x, float* y, int32_t* clu,
+                         int64_t cap, int64_t* count, cudaStream_t s) {
+    RecordClock rc = rc_in;
+    const int feat = h->nC * h->K;
+    if (h->post) {
+        PostArgs a = h->pa;
+        a.tF = tf_ready ? h->tF.p : nullptr;
+        CK(launch_post(a, rc, n_bound, h->rec_slot.p, count, s));
+        rc.presorted = 1;
+        h->stats.launches += 5;
+    }
+    CK(launch_records(h->sp_x.p, h->sp_y.p, h->sp_amp.p, with_pc ? h->tF.p : nullptr, h->rec_slot.p, n_bound, feat,
+                      rc, time, tmpl, amp, pc, cap, count, s));
+    h->stats.launches += (n_bound > 0) ? 2 : 1;
+    if (h->post && (x || y || clu)) {
+        CK(launch_post_write(h->pa, rc, h->rec_slot.p, n_bound, x, y, clu, cap, s));
+        h->stats.launches += 1;
+    }
+    return LSS_OK;
+}
+
 extern "C" {
+
+int lss_reset_postprocess(lss_handle* h) {
+    if (!h) return LSS_ERR_ARG;
+    if (!h->post) return LSS_OK;
+    CK(cudaSetDevice(h->cfg.device));
+    std::vector<int64_t> init(h->plast.n, -(int64_t(1) << 62));
+    CK(cudaMemcpy(h->plast.p, init.data(), init.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
+    return LSS_OK;
+}
+
+int lss_set_postprocess(lss_handle* h, const lss_post_config* pc) {
+    if (!h) return LSS_ERR_ARG;
+    if (h->streaming) return h->fail(LSS_ERR_STATE, "handle is owned by a serving loop");
+    CK(cudaSetDevice(h->cfg.device));
+    if (!pc) {
+        h->post = false;
+        return LSS_OK;
+    }
+    if (pc->n_clusters < 0 || pc->dt_samples < 0 || (pc->n_clusters > 0 && !pc->centroids_xy))
+        return h->fail(LSS_ERR_ARG, "bad post-processing config");
+    if ((pc->xc == nullptr) != (pc->yc == nullptr)) return h->fail(LSS_ERR_ARG, "give both xc and yc or neither");
+    if (pc->xc && (h->nC <= 0 || !h->iCC.p)) return h->fail(LSS_ERR_STATE, "positions need iCC / iU / Ucc");
+    if (pc->n_clusters > 0 && !pc->xc) return h->fail(LSS_ERR_ARG, "clusters need channel positions");
+    if (h->nC > 16) return h->fail(LSS_ERR_ARG, "positions support at most 16 nearest channels");
+    if (h->N >= (1 << 20) || h->cfg.max_spikes >= (1 << 20))
+        return h->fail(LSS_ERR_ARG, "post-processing keys need batches and spike lists below 2^20");
+    const int64_t nmax = h->cfg.max_spikes;
+    const size_t sort_bytes = post_sort_bytes((int32_t)nmax);
+    auto al = [&](auto& buf, size_t n) -> cudaError_t {
+        if (buf.p) h->dev_bytes -= std::max<size_t>(buf.n, 1) * sizeof(*buf.p);
+        buf.release();
+        cudaError_t e = buf.alloc(n);
+        if (e == cudaSuccess) h->dev_bytes += std::max<size_t>(n, 1) * sizeof(*buf.p);
+        return e;
+    };
+    const int nclu = pc->n_clusters > 0 ? pc->n_clusters : h->T;
+    CK(al(h->pk, 4 * (size_t)nmax));
+    CK(al(h->psort, sort_bytes));
+    CK(al(h->pkeep, (size_t)nmax));
+    CK(al(h->plast, (size_t)nclu));
+    CK(al(h->pxy, 2 * (size_t)nmax));
+    CK(al(h->pclu, (size_t)nmax));
+    CK(al(h->rec_x, (size_t)nmax));
+    CK(al(h->rec_y, (size_t)nmax));
+    CK(al(h->rec_clu, (size_t)nmax));
+    CK(al(h->pcen, 2 * (size_t)std::max(pc->n_clusters, 1)));
+    CK(al(h->pchan, 2 * (size_t)h->C));
+    PostArgs a;
+    a.sp_x = h->sp_x.p;
+    a.sp_y = h->sp_y.p;
+    a.nC = h->nC;
+    a.K = h->K;
+    a.C = h->C;
+    a.iCC = h->iCC.p;
+    a.iU = h->iU.p;
+    if (pc->xc) {
+        CK(cudaMemcpy(h->pchan.p, pc->xc, h->C * sizeof(float), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h->pchan.p + h->C, pc->yc, h->C * sizeof(float), cudaMemcpyHostToDevice));
+        a.xc = h->pchan.p;
+        a.yc = h->pchan.p + h->C;
+    }
+    if (pc->n_clusters > 0) {
+        std::vector<float> cx(pc->n_clusters), cy(pc->n_clusters);
+        for (int i = 0; i < pc->n_clusters; ++i) {
+            cx[i] = pc->centroids_xy[2 * i];
+            cy[i] = pc->centroids_xy[2 * i + 1];
+        }
+        CK(cudaMemcpy(h->pcen.p, cx.data(), cx.size() * sizeof(float), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h->pcen.p + pc->n_clusters, cy.data(), cy.size() * sizeof(float), cudaMemcpyHostToDevice));
+        a.cen_x = h->pcen.p;
+        a.cen_y = h->pcen.p + pc->n_clusters;
+        a.n_clu = pc->n_clusters;
+    }
+    a.dt = pc->dt_samples;
+    a.key_c = h->pk.p;
+    a.key_c_sorted = h->pk.p + nmax;
+    a.key_t = h->pk.p + 2 * nmax;
+    a.key_t_sorted = h->pk.p + 3 * nmax;
+    a.sort_tmp = h->psort.p;
+    a.sort_bytes = sort_bytes;
+    a.keep = h->pkeep.p;
+    a.last_time = h->plast.p;
+    a.px = h->pxy.p;
+    a.py = h->pxy.p + nmax;
+    a.clu = h->pclu.p;
+    h->pa = a;
+    h->post = true;
+    return lss_reset_postprocess(h);
+}
 
 int lss_filter(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ibatch, int64_t n_batches,
                int32_t raw_on_device, float* X_dev, void* stream) {
@@ -790,9 +901,10 @@ int lss_sort_batch(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ib
     if (rc) return rc;
     const int feat = h->nC * h->K;
     const bool want_pc = out->pc != nullptr && feat > 0;
+    const bool need_tf = want_pc || (h->post && h->pa.xc != nullptr && feat > 0);
     const bool bf16 = h->cfg.precision == LSS_PREC_BF16_RECHECK;
     h->mark(8, s);
-    if (want_pc && n > 0) {
+    if (need_tf && n > 0) {
         CK(launch_pc_features_folded(Xh, h->ld, h->C, h->nt, h->K, h->nC, h->T, h->wpca.p, h->Mw.p, h->U.p, h->R.p,
                                      h->iCC.p, h->iU.p, h->Ucc.p, h->sp_x.p, h->sp_y.p, h->sp_amp.p,
                                      h->round_start.p, rounds, n, nullptr, h->tF.p, h->status.p,
@@ -811,9 +923,17 @@ int lss_sort_batch(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ib
     rclk.NT = h->NT;
     rclk.nt = h->nt;
     rclk.nt0min = h->cfg.nt0min;
-    CK(launch_records(h->sp_x.p, h->sp_y.p, h->sp_amp.p, want_pc ? h->tF.p : nullptr, h->rec_slot.p, n, feat, rclk,
-                      d_time, d_tmpl, d_amp, d_pc, dcap, h->rec_count.p, s));
-    h->stats.launches += (n > 0) ? 2 : 1;
+    if (h->post && ibatch == 0) {
+        int rc0 = lss_reset_postprocess(h);
+        if (rc0) return rc0;
+    }
+    const bool want_post = h->post && (out->x_pos || out->y_pos || out->cluster);
+    float* d_x = want_post && out->x_pos ? (out->on_device ? out->x_pos : h->rec_x.p) : nullptr;
+    float* d_y = want_post && out->y_pos ? (out->on_device ? out->y_pos : h->rec_y.p) : nullptr;
+    int32_t* d_clu = want_post && out->cluster ? (out->on_device ? out->cluster : h->rec_clu.p) : nullptr;
+    rc = enqueue_records(h, rclk, n, want_pc, need_tf, d_time, d_tmpl, d_amp, d_pc, d_x, d_y, d_clu, dcap,
+                         h->rec_count.p, s);
+    if (rc) return rc;
     int64_t count = 0;
     int32_t st = 0;
     CK(cudaMemcpyAsync(&count, h->rec_count.p, sizeof(count), cudaMemcpyDeviceToHost, s));
@@ -828,6 +948,9 @@ int lss_sort_batch(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ib
         CK(cudaMemcpyAsync(out->amplitude, d_amp, count * sizeof(float), cudaMemcpyDeviceToHost, s));
         if (want_pc)
             CK(cudaMemcpyAsync(out->pc, d_pc, count * feat * sizeof(float), cudaMemcpyDeviceToHost, s));
+        if (d_x) CK(cudaMemcpyAsync(out->x_pos, d_x, count * sizeof(float), cudaMemcpyDeviceToHost, s));
+        if (d_y) CK(cudaMemcpyAsync(out->y_pos, d_y, count * sizeof(float), cudaMemcpyDeviceToHost, s));
+        if (d_clu) CK(cudaMemcpyAsync(out->cluster, d_clu, count * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     }
     h->mark(10, s);
     CK(cudaStreamSynchronize(s));

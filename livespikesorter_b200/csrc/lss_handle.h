@@ -81,6 +81,16 @@ struct lss_handle {
     DevBuf<unsigned int> bar;
     DevBuf<int64_t> rec_time, rec_count;
     DevBuf<int32_t> rec_tmpl, rec_slot;
+    // post-processing (positions, clusters, duplicates, time order)
+    bool post = false;
+    lss::PostArgs pa;
+    DevBuf<unsigned long long> pk;               // 4 key arrays of max_spikes
+    DevBuf<unsigned char> psort, pkeep;
+    DevBuf<int64_t> plast;
+    DevBuf<float> pxy, pcen, pchan;              // per-spike x|y, centroids x|y, channel x|y
+    DevBuf<int32_t> pclu;
+    DevBuf<float> rec_x, rec_y;                  // host-records staging of x, y, cluster
+    DevBuf<int32_t> rec_clu;
     DevBuf<float> rec_amp, rec_pc;
 
     int fail(int code, const std::string& m) {
@@ -108,6 +118,8 @@ struct lss_handle {
         Uw16.release(); Uw_hi.release(); Uw_lo.release(); U.release(); R.release(); hpH.release(); hpTw.release();
         cf2.release(); pre_cf.release(); Pc_hi.release(); Pc_lo.release(); rc_tiles.release(); pre_im.release();
         rc_count.release();
+        pk.release(); psort.release(); pkeep.release(); plast.release(); pxy.release(); pcen.release();
+        pchan.release(); pclu.release(); rec_x.release(); rec_y.release(); rec_clu.release();
         if (rc_ev) cudaEventDestroy(rc_ev);
         if (rc_host) cudaFreeHost(rc_host);
     }
@@ -131,5 +143,11 @@ int run_scores(lss_handle* h, const float* X, int64_t ldx, int64_t N, float* B, 
                bool* maxima_ready = nullptr, bool folded = false);
 // Matching-pursuit rounds on h->B, enqueued only (counts stay on the device).
 int enqueue_mp(lss_handle* h, int64_t N, cudaStream_t s, bool maxima_ready);
+// Record slots / count for the batch's spikes (post-processing when on, else
+// the matching order with the first-batch drop), then the records themselves.
+// n_bound: the spike count, or an upper bound when rc reads it from the device.
+int enqueue_records(lss_handle* h, const RecordClock& rc, int32_t n_bound, bool with_pc, bool tf_ready,
+                    int64_t* time, int32_t* tmpl, float* amp, float* pc, float* x, float* y, int32_t* clu,
+                    int64_t cap, int64_t* count, cudaStream_t s);
 
 }  // namespace lss

@@ -139,6 +139,7 @@ cudaError_t launch_xres(const float* X, int64_t ldx, int32_t C, int32_t N, int32
                         float* Xres, int32_t* status, cudaStream_t s);
 // slot: scratch [n] for the output position of each spike
 struct RecordClock {
+    int32_t presorted = 0;                 // output slots already computed (post-processing)
     int64_t ibatch = 0;                    // batch index (host value) ...
     const int64_t* ibatch_dev = nullptr;   // ... or read from the device
     const int32_t* counters = nullptr;     // spike count read from the device (counters[0])
@@ -146,6 +147,38 @@ struct RecordClock {
     int32_t NT = 0, nt = 0, nt0min = 0;
     int32_t slots = 0;                     // > 0: outputs are rings of `slots` batches
 };
+// ---- post-processing (post.cu): positions, clusters, duplicates, time order ----
+struct PostArgs {
+    const int32_t* sp_x = nullptr;
+    const int32_t* sp_y = nullptr;
+    const float* tF = nullptr;             // [n, nC, K] PC features (null: no positions)
+    int nC = 0, K = 0, C = 0;
+    const int64_t* iCC = nullptr;
+    const int64_t* iU = nullptr;
+    const float* xc = nullptr;             // channel coordinates (null: no positions)
+    const float* yc = nullptr;
+    const float* cen_x = nullptr;          // cluster centroids (n_clu = 0: cluster = template)
+    const float* cen_y = nullptr;
+    int n_clu = 0;
+    int dt = 0;                            // duplicate window in samples (0: off)
+    unsigned long long* key_c = nullptr;   // [n_max] scratch keys and their sorted copies
+    unsigned long long* key_c_sorted = nullptr;
+    unsigned long long* key_t = nullptr;
+    unsigned long long* key_t_sorted = nullptr;
+    void* sort_tmp = nullptr;
+    size_t sort_bytes = 0;
+    uint8_t* keep = nullptr;               // [n_max]
+    int64_t* last_time = nullptr;          // [clusters] last kept time, carried across batches
+    float* px = nullptr;                   // [n_max] per-spike position and cluster
+    float* py = nullptr;
+    int32_t* clu = nullptr;
+};
+size_t post_sort_bytes(int32_t n_max);
+cudaError_t launch_post(const PostArgs& a, const RecordClock& rc, int32_t n_max, int32_t* slot, int64_t* out_count,
+                        cudaStream_t s);
+cudaError_t launch_post_write(const PostArgs& a, const RecordClock& rc, const int32_t* slot, int32_t n_max,
+                              float* out_x, float* out_y, int32_t* out_clu, int64_t capacity, cudaStream_t s);
+
 cudaError_t launch_records(const int32_t* sp_x, const int32_t* sp_y, const float* sp_amp, const float* tF,
                            int32_t* slot, int32_t n, int32_t feat_len, const RecordClock& rc, int64_t* out_time,
                            int32_t* out_tmpl, float* out_amp, float* out_pc, int64_t capacity, int64_t* out_count,

@@ -83,6 +83,8 @@ struct Result {
     std::vector<int32_t> tmpl;
     std::vector<float> amp;
     std::vector<float> pc;
+    std::vector<float> x, y;
+    std::vector<int32_t> clu;
 };
 
 template <typename T>
@@ -113,7 +115,8 @@ struct Probe {
     HostBuf<int16_t> staging;                  // D blocks of NT rows
     HostBuf<int64_t> o_time, o_count;
     HostBuf<int32_t> o_tmpl;
-    HostBuf<float> o_amp, o_pc;
+    HostBuf<float> o_amp, o_pc, o_x, o_y;
+    HostBuf<int32_t> o_clu;
     HostBuf<StreamMail> mail;
     std::unique_ptr<Slot[]> slots;
     int64_t fill = 0;                          // rows in the block being assembled
@@ -143,6 +146,9 @@ struct Probe {
         o_tmpl.release();
         o_amp.release();
         o_pc.release();
+        o_x.release();
+        o_y.release();
+        o_clu.release();
         mail.release();
         if (h) lss_destroy(h);
     }
@@ -199,9 +205,10 @@ int enqueue_stream_batch(Probe* p) {
     rclk.nt = (int32_t)p->nt;
     rclk.nt0min = h->cfg.nt0min;
     rclk.slots = (int32_t)p->D;
-    PCK(launch_records(h->sp_x.p, h->sp_y.p, h->sp_amp.p, p->feat > 0 ? h->tF.p : nullptr, h->rec_slot.p,
-                       (int32_t)std::min<int64_t>(p->cap, h->cfg.max_spikes), (int32_t)p->feat, rclk, p->o_time.d,
-                       p->o_tmpl.d, p->o_amp.d, p->feat > 0 ? p->o_pc.d : nullptr, p->cap, p->o_count.d, s));
+    rc = enqueue_records(h, rclk, (int32_t)std::min<int64_t>(p->cap, h->cfg.max_spikes), p->feat > 0, p->feat > 0,
+                         p->o_time.d, p->o_tmpl.d, p->o_amp.d, p->feat > 0 ? p->o_pc.d : nullptr, p->o_x.d, p->o_y.d,
+                         p->o_clu.d, p->cap, p->o_count.d, s);
+    if (rc) return p->fail(rc, h->err);
     k_stream_end<<<1, 1, 0, s>>>(p->state.p, h->counters.p, h->status.p, p->mail.d, (int32_t)p->D);
     PCK(cudaGetLastError());
     return LSS_OK;
@@ -266,6 +273,11 @@ int harvest_one(Probe* p, std::unique_lock<std::mutex>& lk, bool wait) {
     r.amp.assign(p->o_amp.p + k * p->cap, p->o_amp.p + k * p->cap + n);
     if (p->feat > 0)
         r.pc.assign(p->o_pc.p + (k * p->cap) * p->feat, p->o_pc.p + (k * p->cap + n) * p->feat);
+    if (p->o_x.p) {
+        r.x.assign(p->o_x.p + k * p->cap, p->o_x.p + k * p->cap + n);
+        r.y.assign(p->o_y.p + k * p->cap, p->o_y.p + k * p->cap + n);
+        r.clu.assign(p->o_clu.p + k * p->cap, p->o_clu.p + k * p->cap + n);
+    }
     p->lat_ms.push_back((double)(sl.emit_ns - sl.arrival_ns) * 1e-6);
     sl.done.store(0);
     p->harvest += 1;
@@ -319,8 +331,8 @@ void lss_server_destroy(lss_server* s) {
     delete s;
 }
 
-int lss_server_admit(lss_server* s, const lss_config* cfg, const lss_tensors* t, const float* drift_M, int32_t depth,
-                     int64_t capacity, int32_t* probe) {
+int lss_server_admit(lss_server* s, const lss_config* cfg, const lss_tensors* t, const float* drift_M,
+                     const lss_post_config* post, int32_t depth, int64_t capacity, int32_t* probe) {
     if (!s || !cfg || !t || !probe || depth < 1 || depth > 64 || capacity <= 0) {
         lss::set_thread_error("lss_server_admit: bad argument");
         return LSS_ERR_ARG;
@@ -384,6 +396,21 @@ int lss_server_admit(lss_server* s, const lss_config* cfg, const lss_tensors* t,
         if (rc) {
             lss::set_thread_error(h->err.c_str());
             return rc;
+        }
+    }
+    if (post) {
+        rc = lss_set_postprocess(h, post);
+        if (rc) {
+            lss::set_thread_error(h->err.c_str());
+            return rc;
+        }
+        if ((e = p->o_x.alloc((size_t)depth * capacity, true)) != cudaSuccess) return cfail(e, "records");
+        if ((e = p->o_y.alloc((size_t)depth * capacity, true)) != cudaSuccess) return cfail(e, "records");
+        if ((e = p->o_clu.alloc((size_t)depth * capacity, true)) != cudaSuccess) return cfail(e, "records");
+        p->bytes = h->dev_bytes + ring_bytes + 2 * sizeof(int64_t);
+        if (s->used + (int64_t)p->bytes > s->budget) {
+            lss::set_thread_error("device memory budget exhausted");
+            return LSS_ERR_BUSY;
         }
     }
     // every admitted probe's rounds kernel (a cooperative grid, one CTA per
@@ -482,6 +509,9 @@ int lss_server_poll(lss_server* s, int32_t probe, lss_records* out, int64_t* bat
     std::copy(r.tmpl.begin(), r.tmpl.end(), out->template_id);
     std::copy(r.amp.begin(), r.amp.end(), out->amplitude);
     if (out->pc && p->feat > 0) std::copy(r.pc.begin(), r.pc.end(), out->pc);
+    if (out->x_pos && !r.x.empty()) std::copy(r.x.begin(), r.x.end(), out->x_pos);
+    if (out->y_pos && !r.y.empty()) std::copy(r.y.begin(), r.y.end(), out->y_pos);
+    if (out->cluster && !r.clu.empty()) std::copy(r.clu.begin(), r.clu.end(), out->cluster);
     return LSS_OK;
 }
 

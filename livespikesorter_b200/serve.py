@@ -28,7 +28,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import LSS_ERR_BUSY, LssRecords, check
-from .sorter import _f32, _ptr, build_config
+from .sorter import _f32, _ptr, build_config, post_config
 
 FS = 30000
 
@@ -55,14 +55,18 @@ class ProbeServer:
         except Exception:
             pass
 
-    def admit(self, *, depth: int = 4, capacity: int = 8192, drift=None, **sorter_kwargs) -> int | None:
-        """Admits a probe (``Sorter`` constructor arguments, NT = block size).
-        Returns its id, or None when memory or slots are not free now."""
+    def admit(self, *, depth: int = 4, capacity: int = 8192, drift=None, post: dict | None = None,
+              **sorter_kwargs) -> int | None:
+        """Admits a probe (``Sorter`` constructor arguments, NT = block size;
+        ``post``: ``sorter.post_config`` arguments for positions, clusters and
+        duplicate removal). Returns its id, or None when memory or slots are
+        not free now."""
         cfg, tens, keep = build_config(device=self.device, **sorter_kwargs)
         M = None if drift is None else _f32(drift)
+        pcfg, pkeep = post_config(**post) if post is not None else (None, None)
         pid = ctypes.c_int32(-1)
-        rc = self._lib.lss_server_admit(self._s, cfg, tens, _ptr(M), depth, capacity, ctypes.byref(pid))
-        del keep
+        rc = self._lib.lss_server_admit(self._s, cfg, tens, _ptr(M), pcfg, depth, capacity, ctypes.byref(pid))
+        del keep, pkeep
         if rc == LSS_ERR_BUSY:
             return None
         check(rc)
@@ -70,7 +74,8 @@ class ProbeServer:
         self._out[pid.value] = dict(
             time=np.empty(capacity, np.int64), tmpl=np.empty(capacity, np.int32),
             amp=np.empty(capacity, np.float32), pc=np.empty((capacity, max(nC, 1), K), np.float32),
-            nC=nC, K=K, cap=capacity, Cbin=cfg.n_chan_bin)
+            x=np.empty(capacity, np.float32), y=np.empty(capacity, np.float32), clu=np.empty(capacity, np.int32),
+            nC=nC, K=K, cap=capacity, Cbin=cfg.n_chan_bin, post=post is not None)
         return pid.value
 
     def push(self, probe: int, rows: np.ndarray, arrival_ns: int = 0):
@@ -86,15 +91,20 @@ class ProbeServer:
         o = self._out[probe]
         rec = LssRecords(time=o['time'].ctypes.data, template_id=o['tmpl'].ctypes.data,
                          amplitude=o['amp'].ctypes.data, pc=o['pc'].ctypes.data if o['nC'] > 0 else None,
-                         capacity=o['cap'], count=0, on_device=0)
+                         capacity=o['cap'], count=0, on_device=0,
+                         x_pos=o['x'].ctypes.data if o['post'] else None,
+                         y_pos=o['y'].ctypes.data if o['post'] else None,
+                         cluster=o['clu'].ctypes.data if o['post'] else None)
         b = ctypes.c_int64(-1)
         check(self._lib.lss_server_poll(self._s, probe, rec, ctypes.byref(b), int(wait)))
         if b.value < 0:
             return None
         n = rec.count
-        return b.value, dict(time=o['time'][:n].copy(), template=o['tmpl'][:n].copy(),
-                             amplitude=o['amp'][:n].copy(),
-                             pc=o['pc'][:n].copy() if o['nC'] > 0 else None)
+        out = dict(time=o['time'][:n].copy(), template=o['tmpl'][:n].copy(), amplitude=o['amp'][:n].copy(),
+                   pc=o['pc'][:n].copy() if o['nC'] > 0 else None)
+        if o['post']:
+            out.update(x=o['x'][:n].copy(), y=o['y'][:n].copy(), cluster=o['clu'][:n].copy())
+        return b.value, out
 
     def release(self, probe: int):
         check(self._lib.lss_server_release(self._s, probe))
@@ -127,6 +137,7 @@ class Stream:
     drift: object = None
     depth: int = 4
     capacity: int = 8192
+    post: dict | None = None        # sorter.post_config arguments
     # filled by run_streams
     results: dict = field(default_factory=dict)
     latency: dict = field(default_factory=dict)
@@ -168,7 +179,8 @@ def run_streams(server, streams: list[Stream], *, realtime: bool = True, jitter_
             if (now - t0) * 1e-9 < st.start_s or refused_at.get(id(st)) == releases:
                 still.append(st)
                 continue
-            pid = server.admit(depth=st.depth, capacity=st.capacity, drift=st.drift, **st.sorter_kwargs)
+            pid = server.admit(depth=st.depth, capacity=st.capacity, drift=st.drift, post=st.post,
+                               **st.sorter_kwargs)
             if pid is None:
                 st.waited = True
                 refused_at[id(st)] = releases

@@ -13,7 +13,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import LssConfig, LssRecords, LssStageTimes, LssStats, LssTensors, STAGES, check
+from ._lib import LssConfig, LssPostConfig, LssRecords, LssStageTimes, LssStats, LssTensors, STAGES, check
 
 
 def _f32(x) -> torch.Tensor:
@@ -63,6 +63,20 @@ def build_config(*, U, wPCA, ctc, Wrot, hp_filter=None, drift=None, iCC=None, iU
                       drift=_ptr(k['drift']), hp_filter=_ptr(k['hp']), iCC=_ptr(k['iCC']), iU=_ptr(k['iU']),
                       Ucc=_ptr(k['Ucc']), chan_map=_ptr(k['cmap']), nm=_ptr(k['nm']))
     return cfg, tens, k
+
+
+def post_config(xc=None, yc=None, centroids=None, dt: int = 7):
+    """``(lss_post_config, keep)`` for positions (channel coordinates xc, yc),
+    nearest-centroid clusters (``centroids`` [n, 2]) and duplicate removal
+    within ``dt`` samples; ``keep`` holds the arrays the pointers refer to."""
+    k = dict(xc=None if xc is None else np.ascontiguousarray(xc, np.float32),
+             yc=None if yc is None else np.ascontiguousarray(yc, np.float32),
+             cen=None if centroids is None else np.ascontiguousarray(centroids, np.float32).reshape(-1, 2))
+    cfg = LssPostConfig(xc=None if k['xc'] is None else k['xc'].ctypes.data,
+                        yc=None if k['yc'] is None else k['yc'].ctypes.data,
+                        centroids_xy=None if k['cen'] is None else k['cen'].ctypes.data,
+                        n_clusters=0 if k['cen'] is None else k['cen'].shape[0], dt_samples=int(dt))
+    return cfg, k
 
 
 def setup_kwargs(setup) -> dict:
@@ -199,18 +213,43 @@ class Sorter:
         amp = torch.empty(cap, dtype=torch.float32, device=dev, pin_memory=pin)
         pc = torch.empty((cap, self.nC, self.K), dtype=torch.float32, device=dev, pin_memory=pin) \
             if (with_pc and self.nC > 0) else None
+        post = getattr(self, '_post', False)
+        xs = torch.empty(cap, dtype=torch.float32, device=dev, pin_memory=pin) if post else None
+        ys = torch.empty(cap, dtype=torch.float32, device=dev, pin_memory=pin) if post else None
+        clu = torch.empty(cap, dtype=torch.int32, device=dev, pin_memory=pin) if post else None
         rec = LssRecords(time=time.data_ptr(), template_id=tmpl.data_ptr(), amplitude=amp.data_ptr(),
-                         pc=_ptr(pc), capacity=cap, count=0, on_device=int(on_device))
+                         pc=_ptr(pc), capacity=cap, count=0, on_device=int(on_device), x_pos=_ptr(xs),
+                         y_pos=_ptr(ys), cluster=_ptr(clu))
         self._check(self._lib.lss_sort_batch(self._h, raw_t.data_ptr(), raw_t.shape[0], ibatch, n_batches,
                                              raw_dev, rec, _stream(self.device)))
         n = rec.count
-        return dict(time=time[:n], template=tmpl[:n], amplitude=amp[:n], pc=None if pc is None else pc[:n])
+        out = dict(time=time[:n], template=tmpl[:n], amplitude=amp[:n], pc=None if pc is None else pc[:n])
+        if post:
+            out.update(x=xs[:n], y=ys[:n], cluster=clu[:n])
+        return out
 
     def stats(self) -> dict:
         s = LssStats()
         self._check(self._lib.lss_get_stats(self._h, s))
         return dict(rounds=s.rounds, spikes=s.spikes, recheck_columns=s.recheck_columns,
                     recheck_flips=s.recheck_flips, recheck_rescored=s.recheck_rescored, launches=s.launches)
+
+    def set_postprocess(self, xc=None, yc=None, centroids=None, dt: int = 7, enable: bool = True):
+        """Positions, nearest-centroid clusters, duplicate removal within dt
+        samples and time order for the records of later batches
+        (``lss_set_postprocess``); ``enable=False`` switches it off."""
+        if not enable:
+            self._check(self._lib.lss_set_postprocess(self._h, None))
+            self._post = False
+            return
+        cfg, keep = post_config(xc, yc, centroids, dt)
+        self._check(self._lib.lss_set_postprocess(self._h, cfg))
+        del keep
+        self._post = True
+
+    def reset_postprocess(self):
+        """Forget the last kept time per cluster (a new stream)."""
+        self._check(self._lib.lss_reset_postprocess(self._h))
 
     def set_profiling(self, on: bool = True):
         self._check(self._lib.lss_set_profiling(self._h, int(on)))

@@ -15,6 +15,12 @@ LiveSpikeSorter's sorter mirrors, as vendored in the reference under
 * ``prepare_extract``    <- ``template_matching.py:20-26``
 * ``run_matching``       <- ``template_matching.py:128-202``
 * ``extract_batch``      <- ``template_matching.py:46-73`` (xfeat and time conversion)
+* ``spike_positions``    <- ``postprocessing.py:33-46``  (compute_spike_positions)
+* ``remove_duplicates``  <- ``postprocessing.py:10-31``
+* ``closest_cluster``    <- LiveSpikeSorter ``OnlineSpikesV2.cu:1028-1043`` (closestCluster)
+* ``postprocess``        <- the order of ``io.py:233-246`` (positions, then
+                            duplicates per cluster on time-sorted spikes) with
+                            ``saveSpikes``' cluster relabelling (``OnlineSpikesV2.cu:1131-1164``)
 
 It is the checker, never the thing measured or shipped: only ``tests/``,
 ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` import it.
@@ -300,3 +306,59 @@ def margin_report(B: torch.Tensor, nm: torch.Tensor, Th: float, nt: int) -> dict
     top2 = torch.topk(Cf, 2, dim=0).values
     best, second = top2[0], top2[1]
     return {'best': best, 'runner_up_gap': best - second, 'threshold_gap': best - Th ** 2}
+
+
+def spike_positions(st: np.ndarray, tF: torch.Tensor, iCC: torch.Tensor, iU: torch.Tensor, xc, yc):
+    """x, y of each spike from its PC-feature energy on the nearest channels
+    (postprocessing.py:33-46)."""
+    tmass = (tF ** 2).sum(-1)
+    tmass = tmass / tmass.sum(1, keepdim=True)
+    xc = torch.as_tensor(np.asarray(xc)).to(tmass.dtype)
+    yc = torch.as_tensor(np.asarray(yc)).to(tmass.dtype)
+    chs = iCC[:, iU[torch.as_tensor(st[:, 1]).long()]]
+    xs = (xc[chs.T] * tmass).sum(1).numpy()
+    ys = (yc[chs.T] * tmass).sum(1).numpy()
+    return xs, ys
+
+
+def remove_duplicates(spike_times: np.ndarray, spike_clusters: np.ndarray, dt: int, t0=None):
+    """Same-cluster spikes within dt samples of the last kept one are dropped
+    (postprocessing.py:10-31). ``t0`` optionally carries the last kept time
+    per cluster in (and is updated): the reference processes the whole
+    recording at once, a stream carries it from batch to batch."""
+    keep = np.zeros(spike_times.size, bool)
+    last = {} if t0 is None else t0
+    for i in range(spike_times.size):
+        t, c = int(spike_times[i]), int(spike_clusters[i])
+        prev = last.get(c, t - dt)
+        if t >= prev + dt:
+            last[c] = t
+            keep[i] = True
+    return spike_times[keep], spike_clusters[keep], keep
+
+
+def closest_cluster(xs: np.ndarray, ys: np.ndarray, centroids: np.ndarray) -> np.ndarray:
+    """Nearest centroid (float32 distances, first index on ties), as
+    OnlineSpikesV2::closestCluster (OnlineSpikesV2.cu:1028-1043)."""
+    out = np.empty(len(xs), np.int64)
+    cx = centroids[:, 0].astype(np.float32)
+    cy = centroids[:, 1].astype(np.float32)
+    for i in range(len(xs)):
+        dx = np.float32(xs[i]) - cx
+        dy = np.float32(ys[i]) - cy
+        d = np.sqrt(dx * dx + dy * dy, dtype=np.float32)
+        out[i] = int(np.argmin(d))
+    return out
+
+
+def postprocess(times: np.ndarray, templates: np.ndarray, tF: torch.Tensor, iCC, iU, xc, yc,
+                centroids: np.ndarray | None, dt: int, t0=None):
+    """One batch's records in matching order -> (order, x, y, cluster) of the
+    kept spikes in time order (ties in matching order)."""
+    st = np.stack([times, templates], 1)
+    xs, ys = spike_positions(st, tF, iCC, iU, xc, yc)
+    clu = closest_cluster(xs, ys, centroids) if centroids is not None and len(centroids) else templates.copy()
+    order = np.argsort(times, kind='stable')
+    _, _, keep = remove_duplicates(times[order], clu[order], dt, t0)
+    o = order[keep]
+    return o, xs[o], ys[o], clu[o]

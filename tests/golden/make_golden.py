@@ -103,6 +103,37 @@ def ks4_extract_case(name: str, C: int, T: int, NT: int, n_batches: int, seed: i
     print(name, 'batches', bfile.n_batches, 'spikes', len(st_all))
 
 
+def post_case():
+    """Reference postprocessing (postprocessing.py:10-46) on the c32_t12
+    extract output: spike positions, and duplicate removal per template and
+    per nearest-centroid cluster."""
+    import_reference()
+    from kilosort.postprocessing import compute_spike_positions, remove_duplicates
+    sys.path.insert(0, str(HERE.parents[1] / 'oracle'))
+    import ks4_oracle as ko
+    g = np.load(HERE / 'ks4_extract_c32_t12.npz')
+    st = g['extract_st']
+    sti = np.stack([st[:, 0], st[:, 1]], 1).astype(np.int64)
+    tF = torch.from_numpy(g['extract_tF'])
+    ops = dict(xc=g['xc'], yc=g['yc'], iCC=torch.from_numpy(g['iCC']), iU=torch.from_numpy(g['iU']))
+    xs, ys = compute_spike_positions(sti, tF, ops)
+    # dt: Kilosort's default (7 samples at 30 kHz) removes nothing in this
+    # sparse case, so a wide window (600 samples) exercises the removal
+    dt = 600
+    t = sti[:, 0].astype(np.int64)
+    _, _, keep_t = remove_duplicates(t, sti[:, 1].astype(np.int32), np.int32(dt))
+    # centroids: four well separated points over the probe; clusters by the
+    # reference's nearest-centroid rule (restated: its code is C++)
+    rng = np.random.default_rng(3)
+    cen = np.stack([rng.uniform(g['xc'].min(), g['xc'].max(), 4), np.linspace(g['yc'].min(), g['yc'].max(), 4)], 1)
+    cen = cen.astype(np.float32)
+    clu = ko.closest_cluster(xs, ys, cen)
+    _, _, keep_c = remove_duplicates(t, clu.astype(np.int32), np.int32(dt))
+    np.savez_compressed(HERE / 'post_c32_t12.npz', xs=xs, ys=ys, dt=dt, keep_t=keep_t, centroids=cen, clu=clu,
+                        keep_c=keep_c)
+    print('post', len(t), 'kept (templates)', int(keep_t.sum()), 'kept (centroids)', int(keep_c.sum()))
+
+
 if __name__ == '__main__':
     torch.set_num_threads(8)
     known_answer()
@@ -111,3 +142,4 @@ if __name__ == '__main__':
     ks4_extract_case('c32_t12', C=32, T=12, NT=4000, n_batches=3, seed=11, drift=False, tail=1500)
     # two batches with drift correction and the padded-highpass branch (N > 30122)
     ks4_extract_case('c16_t8_drift', C=16, T=8, NT=31000, n_batches=2, seed=12, drift=True, tail=7000)
+    post_case()

@@ -126,3 +126,46 @@ def test_fp64_oracle_agrees_with_fp32_on_clear_margins():
                                    dtype=torch.float64)
     assert torch.equal(st32, st64)
     np.testing.assert_allclose(a32.numpy(), a64.numpy(), rtol=1e-5)
+
+
+def test_postprocess_oracle_reproduces_reference_fixture():
+    """Positions and duplicate removal restated in the oracle equal the
+    reference's compute_spike_positions / remove_duplicates output
+    (tests/golden/post_c32_t12.npz, made by make_golden.post_case)."""
+    g = np.load(GOLDEN / 'ks4_extract_c32_t12.npz')
+    p = np.load(GOLDEN / 'post_c32_t12.npz')
+    st = np.stack([g['extract_st'][:, 0], g['extract_st'][:, 1]], 1).astype(np.int64)
+    xs, ys = ko.spike_positions(st, torch.from_numpy(g['extract_tF']), torch.from_numpy(g['iCC']),
+                                torch.from_numpy(g['iU']), g['xc'], g['yc'])
+    assert np.array_equal(xs, p['xs']) and np.array_equal(ys, p['ys'])
+    dt = int(p['dt'])
+    _, _, keep = ko.remove_duplicates(st[:, 0], st[:, 1], dt)
+    assert np.array_equal(keep, p['keep_t'])
+    clu = ko.closest_cluster(xs, ys, p['centroids'])
+    assert np.array_equal(clu, p['clu'])
+    _, _, keep = ko.remove_duplicates(st[:, 0], clu, dt)
+    assert np.array_equal(keep, p['keep_c'])
+    # carrying the last kept time across a split gives the same answer
+    t0 = {}
+    k1 = ko.remove_duplicates(st[:30, 0], clu[:30], dt, t0)[2]
+    k2 = ko.remove_duplicates(st[30:, 0], clu[30:], dt, t0)[2]
+    assert np.array_equal(np.concatenate([k1, k2]), p['keep_c'])
+
+
+def test_postprocess_oracle_matches_live_reference(reference_ks):
+    from kilosort.postprocessing import compute_spike_positions, remove_duplicates
+    g = np.random.default_rng(5)
+    n, nC, K, C, T = 400, 6, 4, 24, 9
+    tF = torch.from_numpy(g.standard_normal((n, nC, K)).astype(np.float32))
+    st = np.stack([np.sort(g.integers(0, 30000, n)), g.integers(0, T, n)], 1).astype(np.int64)
+    iCC = torch.from_numpy(g.integers(0, C, (nC, C)))
+    iU = torch.from_numpy(g.integers(0, C, T))
+    xc, yc = g.uniform(0, 50, C).astype(np.float32), g.uniform(0, 700, C).astype(np.float32)
+    ops = dict(xc=xc, yc=yc, iCC=iCC, iU=iU)
+    xs, ys = compute_spike_positions(st, tF, ops)
+    xo, yo = ko.spike_positions(st, tF, iCC, iU, xc, yc)
+    assert np.array_equal(xs, xo) and np.array_equal(ys, yo)
+    for dt in (7, 90):
+        a = remove_duplicates(st[:, 0], st[:, 1].astype(np.int32), np.int32(dt))
+        b = ko.remove_duplicates(st[:, 0], st[:, 1], dt)
+        assert np.array_equal(a[2], b[2])
