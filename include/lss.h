@@ -231,6 +231,22 @@ int  lss_set_profiling(lss_handle* h, int32_t on);
 int  lss_get_stage_times(const lss_handle* h, lss_stage_times* out);
 
 /* ------------------------------------------------------------------------
+ * Output formats of the reference's consumers (host records, host code).
+ * lss_format_spike_lines: spikeOutput.txt lines "time,template,amplitude,y\n"
+ * (OnlineSpikesV2::writeSpikesToFile, OnlineSpikesV2.cu:1117-1124) with time
+ * + recording_offset, the template id or (use_cluster) the cluster, floats as
+ * %g; y = y_pos or 0. lss_serialize_payload: the decoder's
+ * OnlineSpikesPayload (onlineSpikesPayload.h:8-48) in cereal's binary
+ * archive layout, `long` fields long_bytes (4 for the reference's Windows
+ * build, 8 for LP64) wide. Both write at most cap bytes into buf (NULL: size
+ * only) and return the full length, or -1 on bad arguments. */
+int64_t lss_format_spike_lines(const lss_records* rec, int64_t recording_offset, int32_t use_cluster, char* buf,
+                               int64_t cap);
+int64_t lss_serialize_payload(const lss_records* rec, int64_t recording_offset, int64_t stream_sample_ct,
+                              double vrms, float p2p, int64_t process_time, int32_t long_bytes, int32_t use_cluster,
+                              uint8_t* buf, int64_t cap);
+
+/* ------------------------------------------------------------------------
  * Reconstruction and its adjoint, for refining U and the temporal basis by
  * gradient on residual energy with the spike assignments held fixed. No
  * counterpart in the reference (Kilosort's reconstruction is the residual
