@@ -231,6 +231,21 @@ int  lss_set_profiling(lss_handle* h, int32_t on);
 int  lss_get_stage_times(const lss_handle* h, lss_stage_times* out);
 
 /* ------------------------------------------------------------------------
+ * One-time set-up on the GPU in FP64 (hot swap without Python).
+ * lss_set_templates: new U [T, K, C] (same shapes) and optionally a new
+ * wPCA [K, nt]; rebuilds nm, ctc (prepare_matching,
+ * template_matching.py:110-121, in FP64 rounded to FP32), iU and Ucc
+ * (template_matching.py:20-26, with the handle's iCC), the score GEMM's
+ * operands, template waveforms and the basis correlations.
+ * lss_set_drift_model: channel positions [C] and the interpolation width
+ * (datashift.py:213-219: iKxx = (Kxx + 0.01 I)^-1, FP64 on the host, once);
+ * lss_set_drift_shift: M = Kyx iKxx for a vertical shift in um
+ * (preprocessing.py:44-69, one block) on the GPU, then as lss_set_drift. */
+int  lss_set_templates(lss_handle* h, const float* U, const float* wPCA);
+int  lss_set_drift_model(lss_handle* h, const float* xc, const float* yc, float sig_interp);
+int  lss_set_drift_shift(lss_handle* h, double dshift);
+
+/* ------------------------------------------------------------------------
  * Output formats of the reference's consumers (host records, host code).
  * lss_format_spike_lines: spikeOutput.txt lines "time,template,amplitude,y\n"
  * (OnlineSpikesV2::writeSpikesToFile, OnlineSpikesV2.cu:1117-1124) with time

@@ -20,7 +20,8 @@ EXPORTS = ('lss_create', 'lss_create_from_dir', 'lss_destroy', 'lss_last_error',
            'lss_mp_rounds_noalloc', 'lss_server_create', 'lss_server_destroy', 'lss_server_admit',
            'lss_server_push', 'lss_server_poll', 'lss_server_release', 'lss_server_set_drift',
            'lss_server_latency', 'lss_server_memory', 'lss_recon_forward', 'lss_recon_backward',
-           'lss_set_postprocess', 'lss_reset_postprocess', 'lss_format_spike_lines', 'lss_serialize_payload')
+           'lss_set_postprocess', 'lss_reset_postprocess', 'lss_format_spike_lines', 'lss_serialize_payload',
+           'lss_set_templates', 'lss_set_drift_model', 'lss_set_drift_shift')
 
 
 class LssConfig(ct.Structure):
@@ -106,6 +107,9 @@ def load() -> ct.CDLL:
                               I64, ct.POINTER(I32)], ct.c_int),
         'lss_set_postprocess': ([P, ct.POINTER(LssPostConfig)], ct.c_int),
         'lss_reset_postprocess': ([P], ct.c_int),
+        'lss_set_templates': ([P, P, P], ct.c_int),
+        'lss_set_drift_model': ([P, P, P, ct.c_float], ct.c_int),
+        'lss_set_drift_shift': ([P, ct.c_double], ct.c_int),
         'lss_format_spike_lines': ([ct.POINTER(LssRecords), I64, I32, P, I64], I64),
         'lss_serialize_payload': ([ct.POINTER(LssRecords), I64, I64, ct.c_double, ct.c_float, I64, I32, I32, P,
                                    I64], I64),

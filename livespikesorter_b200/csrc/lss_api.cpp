@@ -110,15 +110,8 @@ static void fft_double(std::vector<std::complex<double>>& a) {
     }
 }
 
-static int set_mixing(lss_handle* h, const float* M) {
+int lss::rebuild_uw(lss_handle* h) {
     const int C = h->C;
-    if (!M) {
-        CK(cudaMemcpy(h->Mw.p, h->Wrot.p, (size_t)C * C * sizeof(float), cudaMemcpyDeviceToDevice));
-    } else {
-        CK(cudaMemcpy(h->Mdrift.p, M, (size_t)C * C * sizeof(float), cudaMemcpyHostToDevice));
-        CK(launch_sgemm(h->Mdrift.p, C, h->Wrot.p, C, h->Mw.p, C, C, C, C, 0));
-        h->stats.launches += 1;
-    }
     // templates with the whitening folded in, for lss_sort_batch
     const bool bf16 = h->cfg.precision == LSS_PREC_BF16_RECHECK;
     CK(launch_build_uw(h->U.p, h->Mw.p, h->T, h->K, C, h->CKpad, nullptr, h->Uw_hi.p, h->Uw_lo.p, 0));
@@ -130,6 +123,23 @@ static int set_mixing(lss_handle* h, const float* M) {
     // callers may sort on streams that do not wait for the legacy default stream
     CK(cudaStreamSynchronize(0));
     return LSS_OK;
+}
+
+int lss::mix_device_drift(lss_handle* h) {
+    const int C = h->C;
+    CK(launch_sgemm(h->Mdrift.p, C, h->Wrot.p, C, h->Mw.p, C, C, C, C, 0));
+    h->stats.launches += 1;
+    return rebuild_uw(h);
+}
+
+static int set_mixing(lss_handle* h, const float* M) {
+    const int C = h->C;
+    if (!M) {
+        CK(cudaMemcpy(h->Mw.p, h->Wrot.p, (size_t)C * C * sizeof(float), cudaMemcpyDeviceToDevice));
+        return rebuild_uw(h);
+    }
+    CK(cudaMemcpy(h->Mdrift.p, M, (size_t)C * C * sizeof(float), cudaMemcpyHostToDevice));
+    return mix_device_drift(h);
 }
 
 static int validate(const lss_config* c, std::string& err) {

@@ -91,6 +91,9 @@ struct lss_handle {
     DevBuf<int32_t> pclu;
     DevBuf<float> rec_x, rec_y;                  // host-records staging of x, y, cluster
     DevBuf<int32_t> rec_clu;
+    // drift model on the device: channel positions (x | y) and (Kxx + 0.01 I)^-1, FP64
+    DevBuf<double> dm_pos, dm_ik;
+    float dm_sig = 20.f;
     DevBuf<float> rec_amp, rec_pc;
 
     int fail(int code, const std::string& m) {
@@ -120,6 +123,7 @@ struct lss_handle {
         rc_count.release();
         pk.release(); psort.release(); pkeep.release(); plast.release(); pxy.release(); pcen.release();
         pchan.release(); pclu.release(); rec_x.release(); rec_y.release(); rec_clu.release();
+        dm_pos.release(); dm_ik.release();
         if (rc_ev) cudaEventDestroy(rc_ev);
         if (rc_host) cudaFreeHost(rc_host);
     }
@@ -141,6 +145,10 @@ int run_ingest(lss_handle* h, const int16_t* src, const IngestMap& map, float* X
 // column maxima were fused into the GEMM.
 int run_scores(lss_handle* h, const float* X, int64_t ldx, int64_t N, float* B, cudaStream_t s,
                bool* maxima_ready = nullptr, bool folded = false);
+// Whitening-folded template operands from U and Mw (after a template or drift change).
+int rebuild_uw(lss_handle* h);
+// Mw = Mdrift @ Wrot with Mdrift already on the device, then rebuild_uw.
+int mix_device_drift(lss_handle* h);
 // Matching-pursuit rounds on h->B, enqueued only (counts stay on the device).
 int enqueue_mp(lss_handle* h, int64_t N, cudaStream_t s, bool maxima_ready);
 // Record slots / count for the batch's spikes (post-processing when on, else

@@ -234,6 +234,25 @@ class Sorter:
         return dict(rounds=s.rounds, spikes=s.spikes, recheck_columns=s.recheck_columns,
                     recheck_flips=s.recheck_flips, recheck_rescored=s.recheck_rescored, launches=s.launches)
 
+    def set_templates(self, U, wPCA=None):
+        """Swap in new templates (same shapes) and optionally a new temporal
+        basis; ctc, nm, iU, Ucc and the GEMM operands are rebuilt on the GPU."""
+        Ut = _f32(U)
+        Wt = None if wPCA is None else _f32(wPCA)
+        if tuple(Ut.shape) != (self.T, self.K, self.C):
+            raise ValueError(f'U must be [{self.T}, {self.K}, {self.C}]')
+        self._check(self._lib.lss_set_templates(self._h, Ut.data_ptr(), _ptr(Wt)))
+
+    def set_drift_model(self, xc, yc, sig_interp: float = 20.0):
+        """Channel positions for drift matrices computed on the GPU."""
+        x = np.ascontiguousarray(xc, np.float32)
+        y = np.ascontiguousarray(yc, np.float32)
+        self._check(self._lib.lss_set_drift_model(self._h, x.ctypes.data, y.ctypes.data, float(sig_interp)))
+
+    def set_drift_shift(self, dshift: float):
+        """Drift correction for a vertical shift (um), matrix built on the GPU."""
+        self._check(self._lib.lss_set_drift_shift(self._h, float(dshift)))
+
     def set_postprocess(self, xc=None, yc=None, centroids=None, dt: int = 7, enable: bool = True):
         """Positions, nearest-centroid clusters, duplicate removal within dt
         samples and time order for the records of later batches
