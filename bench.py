@@ -95,6 +95,15 @@ class Clocks:
             self.proc = subprocess.Popen(['nvidia-smi', f'--id={self.index}', f'--query-gpu={q}',
                                           '--format=csv,noheader,nounits', '-lms', '100'],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
+            # the sampler's start-up (NVML initialisation) must not fall into
+            # the timed region: wait for its first sample
+            t0 = time.time()
+            while time.time() - t0 < 5.0 and self.proc.poll() is None:
+                self.f.flush()
+                if self.path.exists() and self.path.stat().st_size > 0:
+                    break
+                time.sleep(0.02)
+            time.sleep(0.2)
         except Exception:
             self.proc = None
         return self

@@ -27,9 +27,9 @@
 //      (Cf bits << 32 | ~t): larger score first, smaller template index on ties
 //      (torch.max's first-index rule). The key buffers alternate by round
 //      parity; each CTA clears its columns of the buffer the next round writes.
-// Work items of U are (spike, block of template rows); a CTA runs four of
-// them at once in independent 128-thread groups (named barriers), each thread
-// owning one column and streaming its rows eight at a time.
+// Work items of U are (spike, block of template rows, chunk of 32 owned
+// columns), each run by one warp without any barrier: a lane owns one column
+// and streams its rows eight at a time.
 // The grid barrier spins at most ~2 s before setting STATUS_TIMEOUT and
 // returning, so the kernel can never hang the device. Everything another CTA
 // writes during the kernel is read with ld.global.cg (L2), never through the
@@ -43,8 +43,6 @@
 namespace lss {
 
 constexpr int MP_THREADS = 512;
-constexpr int MP_GROUPS = 4;                       // independent item groups per CTA
-constexpr int MP_GT = MP_THREADS / MP_GROUPS;      // threads (columns) per group
 constexpr int MP_LIST = 31;                        // spikes that may cover one owned window
 constexpr int MP_MAX_GRID = 1024;
 constexpr unsigned MP_SPIN_LIMIT = 1u << 24;
@@ -112,9 +110,6 @@ __device__ __forceinline__ float ld_stream(const float* a, uint64_t pol) {
     return v;
 }
 
-__device__ __forceinline__ void group_sync(int g) {
-    asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(MP_GT) : "memory");
-}
 
 __device__ __forceinline__ float cf_of(float b, float nmv) {
     const float r = fmaxf(b, 0.f);
@@ -125,10 +120,6 @@ __device__ __forceinline__ unsigned long long pack_key(float cf, int t) {
     return ((unsigned long long)__float_as_uint(cf) << 32) | (unsigned long long)(0xFFFFFFFFu - (unsigned)t);
 }
 
-struct ListEnt {
-    int x, y, par;
-    float amp;
-};
 
 // Running maximum of Cf = fl(fl(r*r) / nm) (r = relu(b)) with the first index
 // on ties. The correctly rounded quotient is formed only for candidates:
@@ -181,8 +172,6 @@ __global__ void __launch_bounds__(MP_THREADS, 1) k_mp(MPArgs a) {
     extern __shared__ float smem[];
     __shared__ int s_pref[MP_MAX_GRID + 1];
     __shared__ int s_wcnt[MP_THREADS / 32];
-    __shared__ ListEnt s_list[MP_GROUPS][MP_LIST];
-    __shared__ int s_prevx[MP_GROUPS], s_nlist[MP_GROUPS];
     __shared__ int s_cnt, s_total;
 
     const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
@@ -320,20 +309,22 @@ __global__ void __launch_bounds__(MP_THREADS, 1) k_mp(MPArgs a) {
             for (int s = lo + tid; s < hi; s += MP_THREADS) kprev[s] = 0ull;  // next round's key buffer
         }
         {
-            // rows per item: enough items to fill every group, at least 8 rows
-            const int groups = G * MP_GROUPS;
-            int nrb = (2 * groups + total - 1) / total;
+            // Work items are (spike, block of template rows, chunk of 32 owned
+            // columns), each run by one warp on its own: lane L holds spike
+            // q - 1 + L of the round (lane 0 the previous spike), whose
+            // windows may cover the owned columns; no barrier inside the phase.
+            const int NW = MP_THREADS / 32;
+            const int wid = b * NW + warp, wtot = G * NW;
+            const int nch = (2 * nt + 1 + 31) / 32;
+            int nrb = (2 * wtot + total * nch - 1) / (total * nch);
             nrb = max(nrb, (T + 63) / 64);
             nrb = min(nrb, (T + 7) / 8);
             const int tb = ((T + nrb - 1) / nrb + 7) & ~7;  // whole 8-row batches
             nrb = (T + tb - 1) / tb;
-            const int items = total * nrb;
-            const int g = tid / MP_GT, lt = tid % MP_GT;
-            // warp 0 of the group gathers the spike list of an item: lane 0 the
-            // previous spike, lanes 1..31 spikes q, q+1, ...; the loads for the
-            // next item are issued before the current item's rows are streamed
+            const int per_spike = nrb * nch;
+            const int items = total * per_spike;
             auto fetch = [&](int it2, int& x, int& y, float& amp) {
-                const int j = it2 / nrb - 1 + lt;
+                const int j = it2 / per_spike - 1 + lane;
                 x = INT_MAX;
                 y = 0;
                 amp = 0.f;
@@ -351,91 +342,91 @@ __global__ void __launch_bounds__(MP_THREADS, 1) k_mp(MPArgs a) {
             };
             int fx = 0, fy = 0;
             float fa = 0.f;
-            if (lt < 32) fetch(b * MP_GROUPS + g, fx, fy, fa);
-            for (int it = b * MP_GROUPS + g; it < items; it += groups) {
-                const int q = it / nrb, rb = it % nrb;
-                if (lt < 32) {
-                    const int j = q - 1 + lt;
-                    const int x = fx, y = fy;
-                    const float amp = fa;
-                    const int xi = __shfl_sync(0xffffffffu, x, 1);
-                    const bool ok = lt >= 1 && j < total && x <= xi + 2 * nt;
-                    const unsigned bal = __ballot_sync(0xffffffffu, ok);
-                    if (ok) s_list[g][lt - 1] = ListEnt{x, y, (j & 1), amp};
-                    if (lt == 0) {
-                        s_prevx[g] = (q > 0) ? x : INT_MIN / 2;
-                        s_nlist[g] = __popc(bal);
-                        if (__popc(bal) == MP_LIST && q + MP_LIST < total) atomicOr(a.status, STATUS_LIST);
-                    }
-                    fetch(it + groups, fx, fy, fa);
-                }
-                group_sync(g);
-                const int nl = s_nlist[g];
-                const int xi = s_list[g][0].x;
-                const int lo_own = max(max(xi - nt, s_prevx[g] + nt + 1), 0);
+            fetch(wid, fx, fy, fa);
+            for (int it = wid; it < items; it += wtot) {
+                const int q = it / per_spike, rem = it % per_spike, rb = rem / nch, ch = rem % nch;
+                const int x = fx, y = fy;
+                const float amp = fa;
+                fetch(it + wtot, fx, fy, fa);  // the next item's list loads are in flight meanwhile
+                const int j = q - 1 + lane;
+                const int xi = __shfl_sync(0xffffffffu, x, 1);
+                const int xprev = __shfl_sync(0xffffffffu, x, 0);
+                const bool ok = lane >= 1 && j < total && x <= xi + 2 * nt;
+                const int nl = __popc(__ballot_sync(0xffffffffu, ok));
+                if (lane == 0 && ch == 0 && rb == 0 && nl == MP_LIST && q + MP_LIST < total)
+                    atomicOr(a.status, STATUS_LIST);
+                const int lo_own = max(max(xi - nt, (q > 0 ? xprev : INT_MIN / 2) + nt + 1), 0);
                 const int hi_own = min(xi + nt, N - 1);
-                const int t0 = rb * tb, t1 = min(T, t0 + tb);
-                for (int c0 = lo_own; c0 <= hi_own; c0 += MP_GT) {
-                    const int s = c0 + lt;
-                    if (s > hi_own) continue;
-                    int e0 = -1, e1 = -1;
-                    for (int e = 0; e < nl; ++e) {
-                        if (s_list[g][e].x > s + nt) break;
-                        if (s_list[g][e].par) e1 = e; else e0 = e;
+                if (lo_own + ch * 32 > hi_own) continue;  // warp-uniform: nothing owned in this chunk
+                const int s = lo_own + ch * 32 + lane;
+                const bool active = s <= hi_own;
+                // last even and last odd spike of the list whose window covers s
+                int e0 = -1, e1 = -1;
+                for (int e = 0; e < nl; ++e) {
+                    const int ex = __shfl_sync(0xffffffffu, x, e + 1);
+                    if (active && ex <= s + nt) {
+                        if ((q + e) & 1) e1 = e; else e0 = e;
                     }
-                    const float* c0p = nullptr;
-                    const float* c1p = nullptr;
-                    float a0 = 0.f, a1 = 0.f;
-                    if (e0 >= 0) {
-                        c0p = a.ctcP + (int64_t)s_list[g][e0].y * T * L2 + (s - s_list[g][e0].x + nt);
-                        a0 = s_list[g][e0].amp;
-                    }
-                    if (e1 >= 0) {
-                        c1p = a.ctcP + (int64_t)s_list[g][e1].y * T * L2 + (s - s_list[g][e1].x + nt);
-                        a1 = s_list[g][e1].amp;
-                    }
-                    const bool edge = (s < nt) || (s >= N - nt);
-                    ColMax m;
-                    const uint64_t pk = policy_keep(), ps = policy_stream();
-                    float* bp = a.B + (int64_t)t0 * a.ldb + s;
-                    const float* p0 = c0p ? c0p + (int64_t)t0 * L2 : nullptr;
-                    const float* p1 = c1p ? c1p + (int64_t)t0 * L2 : nullptr;
-                    const int64_t ldb = a.ldb;
-                    int t = t0;
-                    for (; t + 8 <= t1; t += 8) {
-                        float v[8], w0[8], w1[8];
-#pragma unroll
-                        for (int u = 0; u < 8; ++u) v[u] = ld_keep(bp + u * ldb, pk);
-                        if (p0) {
-#pragma unroll
-                            for (int u = 0; u < 8; ++u) w0[u] = ld_stream(p0 + u * L2, ps);
-                        }
-                        if (p1) {
-#pragma unroll
-                            for (int u = 0; u < 8; ++u) w1[u] = ld_stream(p1 + u * L2, ps);
-                        }
-#pragma unroll
-                        for (int u = 0; u < 8; ++u) {
-                            float x = v[u];
-                            if (p0) x = __fsub_rn(x, __fmul_rn(a0, w0[u]));
-                            if (p1) x = __fsub_rn(x, __fmul_rn(a1, w1[u]));
-                            st_keep(bp + u * ldb, x, pk);
-                            if (!edge) m.consider(x, s_nm[t + u], s_inv[t + u], t + u);
-                        }
-                        bp += 8 * ldb;
-                        if (p0) p0 += 8 * L2;
-                        if (p1) p1 += 8 * L2;
-                    }
-                    for (; t < t1; ++t, bp += ldb) {
-                        float x = ld_keep(bp, pk);
-                        if (p0) { x = __fsub_rn(x, __fmul_rn(a0, ld_stream(p0, ps))); p0 += L2; }
-                        if (p1) { x = __fsub_rn(x, __fmul_rn(a1, ld_stream(p1, ps))); p1 += L2; }
-                        st_keep(bp, x, pk);
-                        if (!edge) m.consider(x, s_nm[t], s_inv[t], t);
-                    }
-                    if (!edge && t1 > t0) atomicMax(knext + s, pack_key(m.best, m.bi));
                 }
-                group_sync(g);
+                const int x0 = __shfl_sync(0xffffffffu, x, max(e0, 0) + 1);
+                const int y0 = __shfl_sync(0xffffffffu, y, max(e0, 0) + 1);
+                const float a0s = __shfl_sync(0xffffffffu, amp, max(e0, 0) + 1);
+                const int x1 = __shfl_sync(0xffffffffu, x, max(e1, 0) + 1);
+                const int y1 = __shfl_sync(0xffffffffu, y, max(e1, 0) + 1);
+                const float a1s = __shfl_sync(0xffffffffu, amp, max(e1, 0) + 1);
+                if (!active) continue;
+                const float* c0p = nullptr;
+                const float* c1p = nullptr;
+                float a0 = 0.f, a1 = 0.f;
+                if (e0 >= 0) {
+                    c0p = a.ctcP + (int64_t)y0 * T * L2 + (s - x0 + nt);
+                    a0 = a0s;
+                }
+                if (e1 >= 0) {
+                    c1p = a.ctcP + (int64_t)y1 * T * L2 + (s - x1 + nt);
+                    a1 = a1s;
+                }
+                const int t0 = rb * tb, t1 = min(T, t0 + tb);
+                const bool edge = (s < nt) || (s >= N - nt);
+                ColMax m;
+                const uint64_t pk = policy_keep(), ps = policy_stream();
+                float* bp = a.B + (int64_t)t0 * a.ldb + s;
+                const float* p0 = c0p ? c0p + (int64_t)t0 * L2 : nullptr;
+                const float* p1 = c1p ? c1p + (int64_t)t0 * L2 : nullptr;
+                const int64_t ldb = a.ldb;
+                int t = t0;
+                for (; t + 8 <= t1; t += 8) {
+                    float v[8], w0[8], w1[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) v[u] = ld_keep(bp + u * ldb, pk);
+                    if (p0) {
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) w0[u] = ld_stream(p0 + u * L2, ps);
+                    }
+                    if (p1) {
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) w1[u] = ld_stream(p1 + u * L2, ps);
+                    }
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        float xv = v[u];
+                        if (p0) xv = __fsub_rn(xv, __fmul_rn(a0, w0[u]));
+                        if (p1) xv = __fsub_rn(xv, __fmul_rn(a1, w1[u]));
+                        st_keep(bp + u * ldb, xv, pk);
+                        if (!edge) m.consider(xv, s_nm[t + u], s_inv[t + u], t + u);
+                    }
+                    bp += 8 * ldb;
+                    if (p0) p0 += 8 * L2;
+                    if (p1) p1 += 8 * L2;
+                }
+                for (; t < t1; ++t, bp += ldb) {
+                    float xv = ld_keep(bp, pk);
+                    if (p0) { xv = __fsub_rn(xv, __fmul_rn(a0, ld_stream(p0, ps))); p0 += L2; }
+                    if (p1) { xv = __fsub_rn(xv, __fmul_rn(a1, ld_stream(p1, ps))); p1 += L2; }
+                    st_keep(bp, xv, pk);
+                    if (!edge) m.consider(xv, s_nm[t], s_inv[t], t);
+                }
+                if (!edge && t1 > t0) atomicMax(knext + s, pack_key(m.best, m.bi));
             }
         }
         base += total;
