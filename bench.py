@@ -93,7 +93,7 @@ class Clocks:
                  'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
             self.f = open(self.path, 'w')
             self.proc = subprocess.Popen(['nvidia-smi', f'--id={self.index}', f'--query-gpu={q}',
-                                          '--format=csv,noheader,nounits', '-lms', '100'],
+                                          '--format=csv,noheader,nounits', '-lms', '200'],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
             # the sampler's start-up (NVML initialisation) must not fall into
             # the timed region: wait for its first sample

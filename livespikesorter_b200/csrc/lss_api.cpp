@@ -120,8 +120,10 @@ int lss::rebuild_uw(lss_handle* h) {
         CK(launch_build_uw(h->U.p, h->Mw.p, h->T, h->K, C, h->CKpad, h->Uw16.p, nullptr, nullptr, 0));
         h->stats.launches += 1;
     }
-    // callers may sort on streams that do not wait for the legacy default stream
-    CK(cudaStreamSynchronize(0));
+    // callers may sort on streams that do not wait for the legacy default
+    // stream: the batch entry points wait for this event on their stream
+    if (!h->mix_ev) CK(cudaEventCreateWithFlags(&h->mix_ev, cudaEventDisableTiming));
+    CK(cudaEventRecord(h->mix_ev, 0));
     return LSS_OK;
 }
 
@@ -807,6 +809,7 @@ int lss_filter(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ibatch
     if (h->streaming) return h->fail(LSS_ERR_STATE, "handle is owned by a serving loop");
     CK(cudaSetDevice(h->cfg.device));
     cudaStream_t s = (cudaStream_t)stream;
+    CK(wait_mixing(h, s));
     // the GEMM writes rows of stride ld; the caller's buffer has stride N
     int rc = run_filter(h, raw, n_rows, ibatch, n_batches, raw_on_device, h->X.p, s);
     if (rc) return rc;
@@ -822,6 +825,7 @@ int lss_scores(lss_handle* h, const float* X_dev, int64_t N, float* B_dev, void*
     if (N <= 0 || N > h->N) return h->fail(LSS_ERR_ARG, "N out of range");
     CK(cudaSetDevice(h->cfg.device));
     cudaStream_t s = (cudaStream_t)stream;
+    CK(wait_mixing(h, s));
     CK(cudaMemcpy2DAsync(h->X.p, h->ld * sizeof(float), X_dev, N * sizeof(float), N * sizeof(float), h->C,
                          cudaMemcpyDeviceToDevice, s));
     CK(cudaMemsetAsync(h->status.p, 0, sizeof(int32_t), s));
@@ -868,6 +872,7 @@ int lss_match(lss_handle* h, const float* X_dev, int64_t N, int64_t* st_dev, flo
     if (N <= 0 || N > h->N) return h->fail(LSS_ERR_ARG, "N out of range (1..NT+2nt)");
     CK(cudaSetDevice(h->cfg.device));
     cudaStream_t s = (cudaStream_t)stream;
+    CK(wait_mixing(h, s));
     CK(cudaMemcpy2DAsync(h->X.p, h->ld * sizeof(float), X_dev, N * sizeof(float), N * sizeof(float), h->C,
                          cudaMemcpyDeviceToDevice, s));
     CK(cudaMemsetAsync(h->status.p, 0, sizeof(int32_t), s));
@@ -884,6 +889,7 @@ int lss_match_scores(lss_handle* h, const float* B_dev, int64_t N, int64_t* st_d
     if (N <= 0 || N > h->N) return h->fail(LSS_ERR_ARG, "N out of range (1..NT+2nt)");
     CK(cudaSetDevice(h->cfg.device));
     cudaStream_t s = (cudaStream_t)stream;
+    CK(wait_mixing(h, s));
     CK(cudaMemcpy2DAsync(h->B.p, h->ld * sizeof(float), B_dev, N * sizeof(float), N * sizeof(float), h->T,
                          cudaMemcpyDeviceToDevice, s));
     CK(cudaMemsetAsync(h->status.p, 0, sizeof(int32_t), s));
@@ -897,6 +903,7 @@ int lss_sort_batch(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ib
     if (!out->time || !out->template_id || !out->amplitude) return h->fail(LSS_ERR_ARG, "null record arrays");
     CK(cudaSetDevice(h->cfg.device));
     cudaStream_t s = (cudaStream_t)stream;
+    CK(wait_mixing(h, s));
     // the whitening / drift matrix is folded into the templates (set_mixing), so
     // the scores come from the highpassed batch directly
     const float* Xh = nullptr;
@@ -906,18 +913,22 @@ int lss_sort_batch(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ib
     bool ready = false;
     rc = run_scores(h, Xh, h->ld, h->N, h->B.p, s, &ready, /*folded=*/true);
     if (rc) return rc;
-    int32_t n = 0, rounds = 0;
-    rc = run_mp(h, h->N, &n, &rounds, s, ready);
+    // rounds, features and records all read the spike count on the device:
+    // the batch has one host synchronisation, at its end
+    rc = enqueue_mp(h, h->N, s, ready);
     if (rc) return rc;
+    h->mark(7, s);
     const int feat = h->nC * h->K;
     const bool want_pc = out->pc != nullptr && feat > 0;
     const bool need_tf = want_pc || (h->post && h->pa.xc != nullptr && feat > 0);
     const bool bf16 = h->cfg.precision == LSS_PREC_BF16_RECHECK;
+    const int32_t n_bound = h->cfg.max_spikes;
     h->mark(8, s);
-    if (need_tf && n > 0) {
+    if (need_tf) {
+        const int grid = std::min(n_bound, 4 * h->sm_count);
         CK(launch_pc_features_folded(Xh, h->ld, h->C, h->nt, h->K, h->nC, h->T, h->wpca.p, h->Mw.p, h->U.p, h->R.p,
                                      h->iCC.p, h->iU.p, h->Ucc.p, h->sp_x.p, h->sp_y.p, h->sp_amp.p,
-                                     h->round_start.p, rounds, n, nullptr, h->tF.p, h->status.p,
+                                     h->round_start.p, 0, grid, h->counters.p, h->tF.p, h->status.p,
                                      bf16 ? nullptr : h->B0T_hi.p, bf16 ? nullptr : h->B0T_lo.p, h->CKpad, s));
         h->stats.launches += 1;
     }
@@ -930,6 +941,7 @@ int lss_sort_batch(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ib
     const int64_t dcap = out->on_device ? cap : std::min<int64_t>(cap, h->cfg.max_spikes);
     RecordClock rclk;
     rclk.ibatch = ibatch;
+    rclk.counters = h->counters.p;
     rclk.NT = h->NT;
     rclk.nt = h->nt;
     rclk.nt0min = h->cfg.nt0min;
@@ -941,15 +953,21 @@ int lss_sort_batch(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ib
     float* d_x = want_post && out->x_pos ? (out->on_device ? out->x_pos : h->rec_x.p) : nullptr;
     float* d_y = want_post && out->y_pos ? (out->on_device ? out->y_pos : h->rec_y.p) : nullptr;
     int32_t* d_clu = want_post && out->cluster ? (out->on_device ? out->cluster : h->rec_clu.p) : nullptr;
-    rc = enqueue_records(h, rclk, n, want_pc, need_tf, d_time, d_tmpl, d_amp, d_pc, d_x, d_y, d_clu, dcap,
+    rc = enqueue_records(h, rclk, n_bound, want_pc, need_tf, d_time, d_tmpl, d_amp, d_pc, d_x, d_y, d_clu, dcap,
                          h->rec_count.p, s);
     if (rc) return rc;
     int64_t count = 0;
-    int32_t st = 0;
+    int32_t st = 0, hc[4];
     CK(cudaMemcpyAsync(&count, h->rec_count.p, sizeof(count), cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(&st, h->status.p, sizeof(st), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(hc, h->counters.p, sizeof(hc), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    if (st & STATUS_LIST) return h->fail(LSS_ERR_CAPACITY, "residual tile touched by more than 1024 spikes");
+    if (st & STATUS_TIMEOUT) return h->fail(LSS_ERR_TIMEOUT, "a bounded device-side wait timed out");
+    if (st & STATUS_CAPACITY) return h->fail(LSS_ERR_CAPACITY, "more than max_spikes spikes in one batch");
+    if (st & STATUS_LIST)
+        return h->fail(LSS_ERR_CAPACITY, "more than 32 peaks inside one 2*nt window, or a feature list overflow");
+    h->stats.spikes = hc[0];
+    h->stats.rounds = hc[1];
     out->count = count;
     if (count > cap) return h->fail(LSS_ERR_CAPACITY, "record capacity smaller than the spike count");
     if (!out->on_device && count > 0) {

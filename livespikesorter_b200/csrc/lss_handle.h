@@ -74,6 +74,7 @@ struct lss_handle {
     DevBuf<int32_t> rc_tiles, pre_im, rc_count;  // ... listed tiles, saved argmax, [tiles, flips, near columns]
     int32_t* rc_host = nullptr;                  // pinned copy of rc_count (read by lss_get_stats)
     cudaEvent_t rc_ev = nullptr;                 // recorded after that copy
+    cudaEvent_t mix_ev = nullptr;                // recorded after the whitening-folded templates are rebuilt
     bool rc_pending = false;
     int64_t last_scored = 0;                     // samples of the last BF16 scoring
     int CKpad = 0;
@@ -125,6 +126,7 @@ struct lss_handle {
         pchan.release(); pclu.release(); rec_x.release(); rec_y.release(); rec_clu.release();
         dm_pos.release(); dm_ik.release();
         if (rc_ev) cudaEventDestroy(rc_ev);
+        if (mix_ev) cudaEventDestroy(mix_ev);
         if (rc_host) cudaFreeHost(rc_host);
     }
 };
@@ -147,6 +149,10 @@ int run_scores(lss_handle* h, const float* X, int64_t ldx, int64_t N, float* B, 
                bool* maxima_ready = nullptr, bool folded = false);
 // Whitening-folded template operands from U and Mw (after a template or drift change).
 int rebuild_uw(lss_handle* h);
+// Orders stream s after the last template / drift rebuild (no host wait).
+inline cudaError_t wait_mixing(lss_handle* h, cudaStream_t s) {
+    return h->mix_ev ? cudaStreamWaitEvent(s, h->mix_ev, 0) : cudaSuccess;
+}
 // Mw = Mdrift @ Wrot with Mdrift already on the device, then rebuild_uw.
 int mix_device_drift(lss_handle* h);
 // Matching-pursuit rounds on h->B, enqueued only (counts stay on the device).

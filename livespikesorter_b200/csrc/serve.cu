@@ -398,6 +398,7 @@ int lss_server_admit(lss_server* s, const lss_config* cfg, const lss_tensors* t,
             return rc;
         }
     }
+    if (h->mix_ev && (e = cudaEventSynchronize(h->mix_ev)) != cudaSuccess) return cfail(e, "template rebuild");
     if (post) {
         rc = lss_set_postprocess(h, post);
         if (rc) {
@@ -541,6 +542,7 @@ int lss_server_set_drift(lss_server* s, int32_t probe, const float* drift_M) {
     }
     p->h->streaming = false;
     int rc = lss_set_drift(p->h, drift_M);
+    if (!rc && p->h->mix_ev && cudaEventSynchronize(p->h->mix_ev) != cudaSuccess) rc = LSS_ERR_CUDA;
     p->h->streaming = true;
     if (rc) lss::set_thread_error(p->h->err.c_str());
     return rc;
