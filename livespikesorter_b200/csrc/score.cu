@@ -30,7 +30,7 @@ __device__ __forceinline__ float tf32_rna(float x) {
 // Thread = (channel, 8-sample group) with the channel fastest across a warp,
 // so the K values a thread writes per sample land next to its neighbours'
 // and a warp writes 32*K contiguous outputs per sample row.
-template <int KPC, int PC, bool TF32>
+template <int KPC, int PC, bool TF32, int NTP>
 __global__ void __launch_bounds__(256) k_pca_proj_t(const float* __restrict__ X, int64_t ldx, int32_t C, int64_t N,
                                                     const float* __restrict__ wpca, int32_t nt, void* __restrict__ out0,
                                                     float* __restrict__ out_lo, int64_t ldk,
@@ -40,7 +40,7 @@ __global__ void __launch_bounds__(256) k_pca_proj_t(const float* __restrict__ X,
     if (tiles && (int)blockIdx.x >= *ntiles) return;
     const int64_t s0 = tiles ? (int64_t)tiles[blockIdx.x] * PT_S : (int64_t)blockIdx.x * PT_S;
     const int64_t o0 = (int64_t)blockIdx.x * PT_S;
-    const int ntp = (nt + 7) & ~7;
+    const int ntp = NTP ? NTP : (nt + 7) & ~7;     // taps padded to 8 (zero weights)
     const int xw = PT_S + ntp + 9;                 // staged samples per channel row (odd: no bank conflicts)
     float* ws = sm;                                // [KPC][ntp]
     float* xs = ws + KPC * ntp;                    // [PC][xw]
@@ -48,14 +48,15 @@ __global__ void __launch_bounds__(256) k_pca_proj_t(const float* __restrict__ X,
     const int c0 = blockIdx.y * PC;
     const int nc = min(PC, C - c0);
     const int half = nt / 2;
-    for (int e = threadIdx.x; e < KPC * ntp; e += blockDim.x) {
-        const int k = e / ntp, m = e % ntp;
-        ws[e] = (m < nt) ? wpca[k * nt + m] : 0.f;
-    }
-    for (int e = threadIdx.x; e < PC * xw; e += blockDim.x) {
-        const int c = e / xw, p = e % xw;
-        const int64_t g = s0 - half + p;
-        xs[e] = (c < nc && g >= 0 && g < N) ? X[(int64_t)(c0 + c) * ldx + g] : 0.f;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    for (int k = warp; k < KPC; k += nwarps)
+        for (int m = lane; m < ntp; m += 32) ws[k * ntp + m] = (m < nt) ? wpca[k * nt + m] : 0.f;
+    for (int c = warp; c < PC; c += nwarps) {
+        const float* xrow = X + (int64_t)(c0 + c) * ldx;
+        for (int p = lane; p < xw; p += 32) {
+            const int64_t g = s0 - half + p;
+            xs[c * xw + p] = (c < nc && g >= 0 && g < N) ? xrow[g] : 0.f;
+        }
     }
     __syncthreads();
     for (int task = threadIdx.x; task < PC * (PT_S / 8); task += blockDim.x) {
@@ -70,17 +71,20 @@ __global__ void __launch_bounds__(256) k_pca_proj_t(const float* __restrict__ X,
         float w[16];
 #pragma unroll
         for (int r = 0; r < 8; ++r) w[r] = xr[r];
+        // every accumulator sums its taps in ascending order (one fmaf each)
+#pragma unroll(NTP ? NTP / 8 : 1)
         for (int mb = 0; mb < ntp; mb += 8) {
 #pragma unroll
             for (int r = 0; r < 8; ++r) w[8 + r] = xr[mb + 8 + r];
 #pragma unroll
-            for (int u = 0; u < 8; ++u) {
+            for (int k = 0; k < KPC; ++k) {
+                const float4 wa = *reinterpret_cast<const float4*>(ws + k * ntp + mb);
+                const float4 wb = *reinterpret_cast<const float4*>(ws + k * ntp + mb + 4);
+                const float tk[8] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
 #pragma unroll
-                for (int k = 0; k < KPC; ++k) {
-                    const float t = ws[k * ntp + mb + u];
+                for (int u = 0; u < 8; ++u)
 #pragma unroll
-                    for (int r = 0; r < 8; ++r) acc[k][r] = fmaf(t, w[r + u], acc[k][r]);
-                }
+                    for (int r = 0; r < 8; ++r) acc[k][r] = fmaf(tk[u], w[r + u], acc[k][r]);
             }
 #pragma unroll
             for (int r = 0; r < 8; ++r) w[r] = w[8 + r];
@@ -92,42 +96,41 @@ __global__ void __launch_bounds__(256) k_pca_proj_t(const float* __restrict__ X,
     }
     __syncthreads();
     // rows of nc*KPC outputs, written as 16-byte vectors (ldk and c0*KPC are
-    // multiples of 4, so every vector is aligned)
+    // multiples of 4, so every vector is aligned); one warp per sample row
     const int seg = nc * KPC;
     const int nv4 = seg / 4;
-    for (int e = threadIdx.x; e < PT_S * nv4; e += blockDim.x) {
-        const int r = e / nv4, q = e % nv4;
+    for (int r = warp; r < PT_S; r += nwarps) {
         const int64_t s = s0 + r;
         if (s >= N) continue;
-        const float4 v = *reinterpret_cast<const float4*>(stage + r * (PC * KPC) + 4 * q);
-        const int64_t o = (o0 + r) * ldk + (int64_t)c0 * KPC + 4 * q;
-        if (TF32) {
-            const float4 hi = make_float4(tf32_rna(v.x), tf32_rna(v.y), tf32_rna(v.z), tf32_rna(v.w));
-            const float4 lo = make_float4(__fsub_rn(v.x, hi.x), __fsub_rn(v.y, hi.y), __fsub_rn(v.z, hi.z),
-                                          __fsub_rn(v.w, hi.w));
-            *reinterpret_cast<float4*>(static_cast<float*>(out0) + o) = hi;
-            *reinterpret_cast<float4*>(out_lo + o) = lo;
-        } else {
-            __nv_bfloat16* d = static_cast<__nv_bfloat16*>(out0) + o;
-            d[0] = __float2bfloat16_rn(v.x);
-            d[1] = __float2bfloat16_rn(v.y);
-            d[2] = __float2bfloat16_rn(v.z);
-            d[3] = __float2bfloat16_rn(v.w);
+        const int64_t orow = (o0 + r) * ldk + (int64_t)c0 * KPC;
+        const float* srow = stage + r * (PC * KPC);
+        for (int q = lane; q < nv4; q += 32) {
+            const float4 v = *reinterpret_cast<const float4*>(srow + 4 * q);
+            const int64_t o = orow + 4 * q;
+            if (TF32) {
+                const float4 hi = make_float4(tf32_rna(v.x), tf32_rna(v.y), tf32_rna(v.z), tf32_rna(v.w));
+                const float4 lo = make_float4(__fsub_rn(v.x, hi.x), __fsub_rn(v.y, hi.y), __fsub_rn(v.z, hi.z),
+                                              __fsub_rn(v.w, hi.w));
+                *reinterpret_cast<float4*>(static_cast<float*>(out0) + o) = hi;
+                *reinterpret_cast<float4*>(out_lo + o) = lo;
+            } else {
+                __nv_bfloat16* d = static_cast<__nv_bfloat16*>(out0) + o;
+                d[0] = __float2bfloat16_rn(v.x);
+                d[1] = __float2bfloat16_rn(v.y);
+                d[2] = __float2bfloat16_rn(v.z);
+                d[3] = __float2bfloat16_rn(v.w);
+            }
         }
-    }
-    // tail (seg not a multiple of 4)
-    for (int e = threadIdx.x; e < PT_S * (seg - 4 * nv4); e += blockDim.x) {
-        const int r = e / (seg - 4 * nv4), j = 4 * nv4 + e % (seg - 4 * nv4);
-        const int64_t s = s0 + r;
-        if (s >= N) continue;
-        const float v = stage[r * (PC * KPC) + j];
-        const int64_t o = (o0 + r) * ldk + (int64_t)c0 * KPC + j;
-        if (TF32) {
-            const float hi = tf32_rna(v);
-            static_cast<float*>(out0)[o] = hi;
-            out_lo[o] = __fsub_rn(v, hi);
-        } else {
-            static_cast<__nv_bfloat16*>(out0)[o] = __float2bfloat16_rn(v);
+        // tail (seg not a multiple of 4)
+        for (int j = 4 * nv4 + lane; j < seg; j += 32) {
+            const float v = srow[j];
+            if (TF32) {
+                const float hi = tf32_rna(v);
+                static_cast<float*>(out0)[orow + j] = hi;
+                out_lo[orow + j] = __fsub_rn(v, hi);
+            } else {
+                static_cast<__nv_bfloat16*>(out0)[orow + j] = __float2bfloat16_rn(v);
+            }
         }
     }
 }
@@ -139,10 +142,16 @@ static cudaError_t launch_pjt(const float* X, int64_t ldx, int32_t C, int64_t N,
     constexpr int PC = 32;
     const int ntp = (nt + 7) & ~7;
     const size_t smem = sizeof(float) * ((size_t)KPC * ntp + (size_t)PC * (PT_S + ntp + 9) + 4 + (size_t)PT_S * PC * KPC);
-    if (smem > 48 * 1024)
-        cudaFuncSetAttribute(k_pca_proj_t<KPC, PC, TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     dim3 grid((unsigned)((N + PT_S - 1) / PT_S), (unsigned)((C + PC - 1) / PC));
-    k_pca_proj_t<KPC, PC, TF32><<<grid, 256, smem, s>>>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles);
+    if (ntp == 64) {  // nt = 57..64 (Kilosort's 61): taps fully unrolled
+        auto kern = k_pca_proj_t<KPC, PC, TF32, 64>;
+        if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kern<<<grid, 256, smem, s>>>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles);
+    } else {
+        auto kern = k_pca_proj_t<KPC, PC, TF32, 0>;
+        if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kern<<<grid, 256, smem, s>>>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles);
+    }
     return cudaGetLastError();
 }
 
