@@ -277,18 +277,26 @@ __device__ __forceinline__ void pc_features_one(
             while (e < b && sp_x[e] < x + nt) ++e;
             cnt = e - lo;
         }
-        s_cnt[threadIdx.x] = cnt;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int o = s_n;
-            for (int q = 0; q < (int)blockDim.x; ++q) {
-                const int c = s_cnt[q];
-                s_cnt[q] = o;
-                o += c;
+        // exclusive prefix of the counts over the block (warp scans, then the
+        // warp totals), offset by the entries listed so far
+        {
+            const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+            int inc = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int u = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o) inc += u;
             }
-            s_n = o;
+            __shared__ int s_wtot[8];
+            if (lane == 31) s_wtot[wp] = inc;
+            __syncthreads();
+            int before = s_n;
+            for (int w2 = 0; w2 < wp; ++w2) before += s_wtot[w2];
+            s_cnt[threadIdx.x] = before + inc - cnt;
+            __syncthreads();
+            if (threadIdx.x == blockDim.x - 1) s_n = before + inc;
+            __syncthreads();
         }
-        __syncthreads();
         for (int q = 0; q < cnt; ++q) {
             const int slot = s_cnt[threadIdx.x] + q;
             if (slot < FT_LIST) {
