@@ -248,67 +248,106 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
                        __fadd_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
 }
 
-// Forward FFT of src (HF points) into src, using dst as the ping-pong buffer
-// (HF = 4^6: an even number of radix-4 stages ends back in src).
-__device__ __forceinline__ void fft4096(float2* src, float2* dst, const float2* __restrict__ tw) {
-    float2* a = src;
-    float2* b = dst;
-    for (int L = 1; L < HF; L *= 4) {
-        const int step = HF / (4 * L);
-        for (int j = threadIdx.x; j < HF / 4; j += blockDim.x) {
-            const int k = j % L, m = j / L;
-            const float2 w1 = __ldg(tw + k * step);
-            const float2 w2 = __ldg(tw + ((2 * k * step) & (HF - 1)));
-            const float2 w3 = __ldg(tw + ((3 * k * step) & (HF - 1)));
-            const float2 a0 = a[j];
-            const float2 a1 = cmul(a[j + HF / 4], w1);
-            const float2 a2 = cmul(a[j + HF / 2], w2);
-            const float2 a3 = cmul(a[j + 3 * HF / 4], w3);
-            const float2 s02 = make_float2(a0.x + a2.x, a0.y + a2.y), d02 = make_float2(a0.x - a2.x, a0.y - a2.y);
-            const float2 s13 = make_float2(a1.x + a3.x, a1.y + a3.y), d13 = make_float2(a1.x - a3.x, a1.y - a3.y);
-            const int base = m * 4 * L + k;
-            b[base] = make_float2(s02.x + s13.x, s02.y + s13.y);
-            b[base + L] = make_float2(d02.x + d13.y, d02.y - d13.x);       // d02 - i*d13
-            b[base + 2 * L] = make_float2(s02.x - s13.x, s02.y - s13.y);
-            b[base + 3 * L] = make_float2(d02.x - d13.y, d02.y + d13.x);   // d02 + i*d13
-        }
-        __syncthreads();
-        float2* t = a;
-        a = b;
-        b = t;
-    }
+// Shared-memory index with one pad slot per 16 points (radix-16 passes write
+// with stride 16: the pad spreads those writes over the banks).
+__device__ __forceinline__ int pad16(int i) { return i + (i >> 4); }
+constexpr int HFP = HF + HF / 16;
+
+__device__ __forceinline__ void dft4(float2& x0, float2& x1, float2& x2, float2& x3) {
+    const float2 s02 = make_float2(x0.x + x2.x, x0.y + x2.y), d02 = make_float2(x0.x - x2.x, x0.y - x2.y);
+    const float2 s13 = make_float2(x1.x + x3.x, x1.y + x3.y), d13 = make_float2(x1.x - x3.x, x1.y - x3.y);
+    x0 = make_float2(s02.x + s13.x, s02.y + s13.y);
+    x1 = make_float2(d02.x + d13.y, d02.y - d13.x);  // d02 - i*d13
+    x2 = make_float2(s02.x - s13.x, s02.y - s13.y);
+    x3 = make_float2(d02.x - d13.y, d02.y + d13.x);  // d02 + i*d13
 }
 
-__global__ void __launch_bounds__(512) k_highpass_fft(const float* __restrict__ X1, int64_t ldx, int32_t C, int64_t N,
+// In-register 16-point forward DFT, natural order in and out (n = 4 n1 + n2,
+// k = k1 + 4 k2: four 4-point DFTs, twiddles exp(-2 pi i n2 k1 / 16), four
+// more 4-point DFTs).
+__device__ __forceinline__ void dft16(float2 v[16]) {
+    const float c1 = 0.92387953251128674f, s1 = 0.38268343236508977f, r2 = 0.70710678118654752f;
+    const float2 W[10] = {{1.f, 0.f}, {c1, -s1}, {r2, -r2}, {s1, -c1}, {0.f, -1.f},
+                          {-s1, -c1}, {-r2, -r2}, {-c1, -s1}, {-1.f, 0.f}, {-c1, s1}};
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) dft4(v[n2], v[4 + n2], v[8 + n2], v[12 + n2]);
+    // v[4 k1 + n2] now holds y[n2][k1]
+#pragma unroll
+    for (int n2 = 1; n2 < 4; ++n2)
+#pragma unroll
+        for (int k1 = 1; k1 < 4; ++k1) v[4 * k1 + n2] = cmul(v[4 * k1 + n2], W[n2 * k1]);
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) dft4(v[4 * k1], v[4 * k1 + 1], v[4 * k1 + 2], v[4 * k1 + 3]);
+    // v[4 k1 + k2] holds X[k1 + 4 k2]: transpose to natural order
+    float2 t[16];
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1)
+#pragma unroll
+        for (int k2 = 0; k2 < 4; ++k2) t[k1 + 4 * k2] = v[4 * k1 + k2];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = t[i];
+}
+
+// One radix-16 Stockham pass (L = 1, 16, 256 known at compile time).
+template <int L>
+__device__ __forceinline__ void fft16_pass(const float2* a, float2* b, const float2* __restrict__ tw) {
+    constexpr int step = HF / (16 * L);
+    constexpr int lg = (L == 1) ? 0 : (L == 16) ? 4 : 8;
+    for (int j = threadIdx.x; j < HF / 16; j += blockDim.x) {
+        const int k = j & (L - 1), m = j >> lg;
+        float2 v[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) v[i] = a[pad16(j + (HF / 16) * i)];
+        if (L > 1) {
+#pragma unroll
+            for (int i = 1; i < 16; ++i) v[i] = cmul(v[i], __ldg(tw + ((i * k * step) & (HF - 1))));
+        }
+        dft16(v);
+        const int base = m * 16 * L + k;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) b[pad16(base + L * i)] = v[i];
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(256) k_highpass_fft(const float* __restrict__ X1, int64_t ldx, int32_t C, int64_t N,
                                                       int32_t L, const float2* __restrict__ H,
                                                       const float2* __restrict__ tw, float* __restrict__ Xh) {
     extern __shared__ float2 fbuf[];
     float2* A = fbuf;
-    float2* Bb = fbuf + HF;
+    float2* Bb = fbuf + HFP;
     const int c1 = 2 * blockIdx.y, c2 = c1 + 1;
     const bool two = c2 < C;
     const int64_t start = (int64_t)blockIdx.x * (HF - 2 * L);
     const float* x1 = X1 + (int64_t)c1 * ldx;
     const float* x2 = X1 + (int64_t)(two ? c2 : c1) * ldx;
     for (int n = threadIdx.x; n < HF; n += blockDim.x) {
-        int64_t g = (start - L + n) % N;
-        if (g < 0) g += N;
-        A[n] = make_float2(x1[g], two ? x2[g] : 0.f);
+        int64_t g = start - L + n;  // circular index (the modulo only near the ends)
+        if (g < 0 || g >= N) {
+            g %= N;
+            if (g < 0) g += N;
+        }
+        A[pad16(n)] = make_float2(x1[g], two ? x2[g] : 0.f);
     }
     __syncthreads();
-    fft4096(A, Bb, tw);
+    // passes: A -> Bb -> A -> Bb
+    fft16_pass<1>(A, Bb, tw);
+    fft16_pass<16>(Bb, A, tw);
+    fft16_pass<256>(A, Bb, tw);
     // conj(Z * H): the second forward transform then gives conj(F * y)
     for (int n = threadIdx.x; n < HF; n += blockDim.x) {
-        const float2 z = cmul(A[n], __ldg(H + n));
-        A[n] = make_float2(z.x, -z.y);
+        const float2 z = cmul(Bb[pad16(n)], __ldg(H + n));
+        Bb[pad16(n)] = make_float2(z.x, -z.y);
     }
     __syncthreads();
-    fft4096(A, Bb, tw);
+    fft16_pass<1>(Bb, A, tw);
+    fft16_pass<16>(A, Bb, tw);
+    fft16_pass<256>(Bb, A, tw);
     const float inv = 1.f / (float)HF;
     for (int n = L + threadIdx.x; n < HF - L; n += blockDim.x) {
         const int64_t i = start + (n - L);
         if (i >= N) break;
-        const float2 r = A[n];
+        const float2 r = A[pad16(n)];
         Xh[(int64_t)c1 * ldx + i] = r.x * inv;
         if (two) Xh[(int64_t)c2 * ldx + i] = -r.y * inv;
     }
@@ -317,10 +356,10 @@ __global__ void __launch_bounds__(512) k_highpass_fft(const float* __restrict__ 
 cudaError_t launch_highpass_fft(const float* X1, int64_t ldx, int32_t C, int64_t N, int32_t L, const float2* H,
                                 const float2* tw, float* Xh, cudaStream_t s) {
     if (L > 1024) return cudaErrorInvalidValue;
-    const size_t smem = 2 * HF * sizeof(float2);
+    const size_t smem = 2 * HFP * sizeof(float2);
     cudaFuncSetAttribute(k_highpass_fft, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     dim3 grid((unsigned)((N + (HF - 2 * L) - 1) / (HF - 2 * L)), (unsigned)((C + 1) / 2));
-    k_highpass_fft<<<grid, 512, smem, s>>>(X1, ldx, C, N, L, H, tw, Xh);
+    k_highpass_fft<<<grid, 256, smem, s>>>(X1, ldx, C, N, L, H, tw, Xh);
     return cudaGetLastError();
 }
 
