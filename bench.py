@@ -21,6 +21,7 @@ value = total recording-seconds of all ranks / max over ranks of device time.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import subprocess
@@ -168,6 +169,8 @@ def run_b200(args):
     def timed(K, W, host):
         for i in range(W):
             step(i, host)
+        gc.collect()
+        gc.disable()  # no collector pauses inside the timed region
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
@@ -182,6 +185,7 @@ def run_b200(args):
             spikes.append(len(r['time']))
             rounds.append(s.stats()['rounds'])
         torch.cuda.synchronize()
+        gc.enable()
         per = np.array([ev[i].elapsed_time(ev[i + 1]) for i in range(K)])
         tot = float(ev[0].elapsed_time(ev[K]))
         if dist:
@@ -232,6 +236,7 @@ def run_b200(args):
         'latency_ms_p50': float(np.percentile(per, 50)), 'latency_ms_p99': float(np.percentile(per, 99)),
         'roofline': roof, 'gpu_launches': int(launches), 'clocks': clocks,
         'stage_ms': mean_st, 'spikes_per_batch': float(np.mean(spikes)), 'rounds_per_batch': float(np.mean(rounds)),
+        'step_ms': [round(float(v), 3) for v in per],
     }
     if args.precision == 'bf16':
         out['bf16'] = bf16_report(s, setup, local, rows_d, drifts, ids, nb)
