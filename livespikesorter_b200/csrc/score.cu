@@ -196,7 +196,7 @@ cudaError_t launch_pca_proj_tiles_tf32(const float* X, int64_t ldx, int32_t C, i
 // CTA: 128 output channels c' x UW_ROWS rows (t, k); U rows staged in shared
 // memory, each Mw element loaded once per UW_ROWS FMAs; every output still
 // sums over c in order.
-constexpr int UW_ROWS = 16;
+constexpr int UW_ROWS = 4;
 __global__ void __launch_bounds__(128) k_build_uw(const float* __restrict__ U, const float* __restrict__ Mw,
                                                   int32_t T, int32_t K, int32_t C, int64_t ldk,
                                                   __nv_bfloat16* __restrict__ out16, float* __restrict__ hi,
