@@ -81,8 +81,9 @@ def workload_desc(T, precision):
 class Clocks:
     """nvidia-smi sampling during the timed region."""
 
-    def __init__(self, index):
+    def __init__(self, index, period_ms=200):
         self.index = index
+        self.period_ms = period_ms
         self.proc = None
         self.path = ROOT / 'gpurun_out' / f'clocks_{os.getpid()}.csv'
 
@@ -94,7 +95,7 @@ class Clocks:
                  'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
             self.f = open(self.path, 'w')
             self.proc = subprocess.Popen(['nvidia-smi', f'--id={self.index}', f'--query-gpu={q}',
-                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                          '--format=csv,noheader,nounits', '-lms', str(self.period_ms)],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
             # the sampler's start-up (NVML initialisation) must not fall into
             # the timed region: wait for its first sample
@@ -383,11 +384,14 @@ def run_serving(args):
 
     srv = ProbeServer(device=local, memory_budget=40 << 30, max_probes=8)
     run_streams(srv, streams(n_blocks=max(3, args.warmup)), realtime=False)            # warm-up
-    with Clocks(local) as clk:
+    # a clock sample takes the driver for a moment: sample every second here
+    with Clocks(local, period_ms=1000) as clk:
         rt = run_streams(srv, streams(), realtime=True, jitter_frac=0.2, seed=5 + rank)
     clocks = clk.summary()
     cap = run_streams(srv, streams(), realtime=False)
-    lat = {st.name: st.latency for st in rt['streams']}
+    lat = {st.name: {k: v for k, v in st.latency.items() if k != 'samples_ms'} for st in rt['streams']}
+    worst = {st.name: sorted(((round(v, 2), i) for i, v in enumerate(st.latency.get('samples_ms', []))))[-3:]
+             for st in rt['streams']}
     spikes = {st.name: int(sum(len(r['time']) for r in st.results.values())) for st in rt['streams']}
     out = {
         'metric': 'p99 arrival-to-emit latency, 4 concurrent 384ch probes, 10-100 ms blocks',
@@ -397,7 +401,7 @@ def run_serving(args):
         'config': {'workload': 'serving: 4 probes x 384 ch, T = 200/400/600/800, blocks 3000/1500/600/300 samples, '
                                f'{args.duration:g} s each, real-time arrival with 20% seeded jitter',
                    'parallelism': 'one GPU, probes overlap on separate streams'},
-        'latency_ms': lat, 'spikes': spikes,
+        'latency_ms': lat, 'worst_latencies_ms': worst, 'spikes': spikes,
         'realtime_rec_s_per_s': rt['rec_s_per_s'],
         'capacity_rec_s_per_s': cap['rec_s_per_s'], 'capacity_wall_s': cap['wall_s'],
         'clocks': clocks,

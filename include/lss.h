@@ -335,6 +335,9 @@ int  lss_server_release(lss_server* s, int32_t probe);
 int  lss_server_set_drift(lss_server* s, int32_t probe, const float* drift_M);
 /* Arrival-to-emit latency percentiles (ms) over the probe's polled batches. */
 int  lss_server_latency(lss_server* s, int32_t probe, double* p50_ms, double* p99_ms, int64_t* batches);
+/* Every polled batch's arrival-to-emit latency (ms), in batch order: up to
+ * capacity values into out_ms, *n = how many there are. */
+int  lss_server_latencies(lss_server* s, int32_t probe, double* out_ms, int64_t capacity, int64_t* n);
 /* Device memory held by admitted probes and the budget, in bytes. */
 int  lss_server_memory(lss_server* s, int64_t* used, int64_t* budget);
 

@@ -573,6 +573,18 @@ int lss_server_latency(lss_server* s, int32_t probe, double* p50_ms, double* p99
     return LSS_OK;
 }
 
+int lss_server_latencies(lss_server* s, int32_t probe, double* out_ms, int64_t capacity, int64_t* n) {
+    Probe* p = get_probe(s, probe);
+    if (!p || !n || (capacity > 0 && !out_ms)) {
+        lss::set_thread_error("lss_server_latencies: bad argument");
+        return LSS_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lk(p->m);
+    *n = (int64_t)p->lat_ms.size();
+    for (int64_t i = 0; i < std::min<int64_t>(capacity, *n); ++i) out_ms[i] = p->lat_ms[i];
+    return LSS_OK;
+}
+
 int lss_server_memory(lss_server* s, int64_t* used, int64_t* budget) {
     if (!s || !used || !budget) return LSS_ERR_ARG;
     std::lock_guard<std::mutex> lk(s->m);

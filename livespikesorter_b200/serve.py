@@ -21,6 +21,7 @@ The reference has no such loop as an API: each probe runs its own
 from __future__ import annotations
 
 import ctypes
+import gc
 import time
 from dataclasses import dataclass, field
 
@@ -114,10 +115,16 @@ class ProbeServer:
         Mt = _f32(M)
         check(self._lib.lss_server_set_drift(self._s, probe, Mt.data_ptr()))
 
-    def latency(self, probe: int) -> dict:
+    def latency(self, probe: int, samples: bool = False) -> dict:
         p50, p99, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_int64()
         check(self._lib.lss_server_latency(self._s, probe, ctypes.byref(p50), ctypes.byref(p99), ctypes.byref(n)))
-        return dict(p50_ms=p50.value, p99_ms=p99.value, batches=n.value)
+        out = dict(p50_ms=p50.value, p99_ms=p99.value, batches=n.value)
+        if samples:
+            buf = np.zeros(max(n.value, 1), np.float64)
+            m = ctypes.c_int64()
+            check(self._lib.lss_server_latencies(self._s, probe, buf.ctypes.data, len(buf), ctypes.byref(m)))
+            out['samples_ms'] = buf[:m.value].tolist()
+        return out
 
     def memory(self) -> tuple[int, int]:
         u, b = ctypes.c_int64(), ctypes.c_int64()
@@ -164,6 +171,17 @@ def run_streams(server, streams: list[Stream], *, realtime: bool = True, jitter_
     Streams whose admission is refused wait and retry after each release.
     """
     rng = np.random.default_rng(seed)
+    gc_was = gc.isenabled()
+    gc.collect()
+    gc.disable()  # a collector pause would show up as arrival-to-emit latency
+    try:
+        return _run_streams(server, streams, realtime, jitter_frac, rng, clock, sleep)
+    finally:
+        if gc_was:
+            gc.enable()
+
+
+def _run_streams(server, streams, realtime, jitter_frac, rng, clock, sleep):
     t0 = clock()
     waiting = sorted(streams, key=lambda s: s.start_s)
     active = {}        # probe id -> [stream, schedule, next block index, stream start ns]
@@ -224,7 +242,7 @@ def run_streams(server, streams: list[Stream], *, realtime: bool = True, jitter_
                 samples += st.block
                 progressed = True
             if k == len(sched) and len(st.results) == len(sched):
-                st.latency = server.latency(pid)
+                st.latency = server.latency(pid, samples=True)
                 server.release(pid)
                 releases += 1
                 del active[pid]
@@ -233,10 +251,10 @@ def run_streams(server, streams: list[Stream], *, realtime: bool = True, jitter_
         if not progressed:
             if realtime and next_due is not None:
                 gap = (next_due - clock()) * 1e-9
-                if gap > 2e-4:
-                    sleep(min(gap - 1e-4, 1e-3))
+                if gap > 3e-4:
+                    sleep(min(gap - 2e-4, 5e-4))
             else:
-                sleep(5e-5)
+                sleep(2e-5)
     wall = (clock() - t0) * 1e-9
     return dict(wall_s=wall, rec_s=samples / FS, rec_s_per_s=samples / FS / wall if wall > 0 else 0.0,
                 streams=done)
