@@ -395,17 +395,28 @@ __global__ void __launch_bounds__(MP_THREADS, 1) k_mp(MPArgs a) {
                 const float* p1 = c1p ? c1p + (int64_t)t0 * L2 : nullptr;
                 const int64_t ldb = a.ldb;
                 int t = t0;
-                for (; t + 8 <= t1; t += 8) {
-                    float v[8], w0[8], w1[8];
+                // software pipelined: the next eight rows' loads are issued
+                // before the current eight are updated (the rows of a column
+                // belong to this lane alone)
+                float v[8], w0[8], w1[8];
+                if (t + 8 <= t1) {
 #pragma unroll
                     for (int u = 0; u < 8; ++u) v[u] = ld_keep(bp + u * ldb, pk);
-                    if (p0) {
 #pragma unroll
-                        for (int u = 0; u < 8; ++u) w0[u] = ld_stream(p0 + u * L2, ps);
-                    }
-                    if (p1) {
+                    for (int u = 0; u < 8; ++u) w0[u] = p0 ? ld_stream(p0 + u * L2, ps) : 0.f;
 #pragma unroll
-                        for (int u = 0; u < 8; ++u) w1[u] = ld_stream(p1 + u * L2, ps);
+                    for (int u = 0; u < 8; ++u) w1[u] = p1 ? ld_stream(p1 + u * L2, ps) : 0.f;
+                }
+                for (; t + 8 <= t1; t += 8) {
+                    float nv[8], nw0[8], nw1[8];
+                    const bool more = t + 16 <= t1;
+                    if (more) {
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) nv[u] = ld_keep(bp + (8 + u) * ldb, pk);
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) nw0[u] = p0 ? ld_stream(p0 + (8 + u) * L2, ps) : 0.f;
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) nw1[u] = p1 ? ld_stream(p1 + (8 + u) * L2, ps) : 0.f;
                     }
 #pragma unroll
                     for (int u = 0; u < 8; ++u) {
@@ -418,6 +429,14 @@ __global__ void __launch_bounds__(MP_THREADS, 1) k_mp(MPArgs a) {
                     bp += 8 * ldb;
                     if (p0) p0 += 8 * L2;
                     if (p1) p1 += 8 * L2;
+                    if (more) {
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) {
+                            v[u] = nv[u];
+                            w0[u] = nw0[u];
+                            w1[u] = nw1[u];
+                        }
+                    }
                 }
                 for (; t < t1; ++t, bp += ldb) {
                     float xv = ld_keep(bp, pk);
