@@ -403,6 +403,134 @@ __device__ __forceinline__ void pc_features_one(
     }
 }
 
+// Warp per spike (projection-row path, nC = NCC and K = KPC known at compile
+// time): lane l sums channels l, l + 32, ... of every (j, k) feature, the 32
+// partial sums are combined by a butterfly, then each lane owns one or two
+// features for the neighbour corrections (list order) and the amp * Ucc term.
+constexpr int FW_LIST = 256;  // neighbours per spike (all rounds, within +-nt)
+template <int KPC, int NCC>
+__global__ void __launch_bounds__(256, 2) k_pc_features_warp(
+    int32_t C, int32_t nt, int32_t T, const float* __restrict__ Mw, const float* __restrict__ U,
+    const float* __restrict__ R, const int64_t* __restrict__ iCC, const int64_t* __restrict__ iU,
+    const float* __restrict__ Ucc, const int32_t* __restrict__ sp_x, const int32_t* __restrict__ sp_y,
+    const float* __restrict__ sp_amp, const int32_t* __restrict__ round_start, int32_t rounds, int32_t n,
+    const int32_t* __restrict__ counters, float* __restrict__ tF, int32_t* status, const float* __restrict__ Phi,
+    const float* __restrict__ Plo, int64_t ldp) {
+    constexpr int F = NCC * KPC;
+    __shared__ int s_lx[8][FW_LIST], s_ly[8][FW_LIST];
+    __shared__ float s_la[8][FW_LIST];
+    if (counters) {
+        n = counters[0];
+        rounds = counters[1];
+    }
+    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+    const int nd = 2 * nt - 1;
+    for (int i = blockIdx.x * 8 + wl; i < n; i += gridDim.x * 8) {
+        const int x = sp_x[i], y = sp_y[i];
+        const int64_t u = iU[y];
+        int chl = 0;  // lane j < NCC holds channel j's index
+        if (lane < NCC) chl = (int)iCC[(int64_t)lane * C + u];
+        int ch[NCC];
+#pragma unroll
+        for (int j = 0; j < NCC; ++j) ch[j] = __shfl_sync(0xffffffffu, chl, j);
+        // ---- sum over channels: acc[j][k] = sum_c Mw[ch_j, c] * P[x, c*K + k]
+        float acc[NCC][KPC];
+#pragma unroll
+        for (int j = 0; j < NCC; ++j)
+#pragma unroll
+            for (int k = 0; k < KPC; ++k) acc[j][k] = 0.f;
+        const int64_t o = (int64_t)x * ldp;
+        for (int c = lane; c < C; c += 32) {
+            float pv[KPC];
+#pragma unroll
+            for (int k = 0; k < KPC; ++k) pv[k] = __fadd_rn(Phi[o + c * KPC + k], Plo[o + c * KPC + k]);
+#pragma unroll
+            for (int j = 0; j < NCC; ++j) {
+                const float mv = __ldg(Mw + (int64_t)ch[j] * C + c);
+#pragma unroll
+                for (int k = 0; k < KPC; ++k) acc[j][k] = fmaf(mv, pv[k], acc[j][k]);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < NCC; ++j)
+#pragma unroll
+            for (int k = 0; k < KPC; ++k) {
+                float v = acc[j][k];
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+                acc[j][k] = v;  // every lane holds the total
+            }
+        // ---- neighbours (any round, round order) whose window overlaps x's
+        int nl = 0;
+        for (int rb = 0; rb < rounds; rb += 32) {
+            const int r = rb + lane;
+            int lo = 0, cnt = 0;
+            if (r < rounds) {
+                const int b = round_start[r + 1];
+                int hi2 = b;
+                lo = round_start[r];
+                while (lo < hi2) {
+                    const int m = (lo + hi2) >> 1;
+                    if (sp_x[m] <= x - nt) lo = m + 1; else hi2 = m;
+                }
+                int e = lo;
+                while (e < b && sp_x[e] < x + nt) ++e;
+                cnt = e - lo;
+            }
+            int inc = cnt;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const int v2 = __shfl_up_sync(0xffffffffu, inc, off);
+                if (lane >= off) inc += v2;
+            }
+            const int base = nl + inc - cnt;
+            for (int q = 0; q < cnt; ++q) {
+                const int slot = base + q;
+                if (slot < FW_LIST) {
+                    s_lx[wl][slot] = sp_x[lo + q];
+                    s_ly[wl][slot] = sp_y[lo + q];
+                    s_la[wl][slot] = sp_amp[lo + q];
+                }
+            }
+            nl += __shfl_sync(0xffffffffu, inc, 31);
+        }
+        __syncwarp();
+        if (nl > FW_LIST) {
+            if (lane == 0) atomicOr(status, STATUS_LIST);
+            nl = FW_LIST;
+        }
+        // ---- each lane finishes features f = lane and lane + 32
+#pragma unroll
+        for (int h2 = 0; h2 < 2; ++h2) {
+            const int f = lane + 32 * h2;
+            if (f >= F) break;
+            const int j = f / KPC, k = f % KPC;
+            float v = 0.f;
+#pragma unroll
+            for (int jj = 0; jj < NCC; ++jj)
+#pragma unroll
+                for (int kk = 0; kk < KPC; ++kk)
+                    if (jj * KPC + kk == f) v = acc[jj][kk];
+            int chj = 0;
+#pragma unroll
+            for (int jj = 0; jj < NCC; ++jj)
+                if (jj == j) chj = ch[jj];
+            for (int q = 0; q < nl; ++q) {
+                const int d = x - s_lx[wl][q];
+                const float* rk = R + ((int64_t)k * KPC) * nd + (d + nt - 1);
+                const float* uy = U + (int64_t)s_ly[wl][q] * KPC * C + chj;
+                float sub = 0.f;
+#pragma unroll
+                for (int kk = 0; kk < KPC; ++kk) sub = fmaf(__ldg(uy + (int64_t)kk * C), __ldg(rk + (int64_t)kk * nd), sub);
+                v = __fsub_rn(v, __fmul_rn(s_la[wl][q], sub));
+            }
+            v = __fadd_rn(v, __fmul_rn(sp_amp[i], Ucc[((int64_t)j * T + y) * KPC + k]));
+            tF[(int64_t)i * F + f] = v;
+        }
+        __syncwarp();
+    }
+}
+
 // CTA per spike, grid-stride over the spikes; with counters != null the spike
 // and round counts are read from the matching pursuit's device counters
 // (graph-captured batches, whose launch does not know them).
@@ -433,6 +561,13 @@ cudaError_t launch_pc_features_folded(const float* Xh, int64_t ldx, int32_t C, i
                                       int32_t* status, const float* Phi, const float* Plo, int64_t ldp,
                                       cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
+    if (Phi && K == 6 && nC == 10) {
+        // warp per spike; n: the spike count or (counters) the grid bound in spikes
+        const int grid = (n + 7) / 8;
+        k_pc_features_warp<6, 10><<<grid, 256, 0, s>>>(C, nt, T, Mw, U, R, iCC, iU, Ucc, sp_x, sp_y, sp_amp,
+                                                       round_start, rounds, n, counters, tF, status, Phi, Plo, ldp);
+        return cudaGetLastError();
+    }
     if (nC * K > 256) return cudaErrorInvalidValue;  // one (j, k) per thread
     const size_t front = std::max<size_t>((size_t)K * nt + (size_t)FT_CH * (nt + 1) + (size_t)FT_CH * K +
                                               (size_t)nC * FT_CH,

@@ -925,7 +925,7 @@ int lss_sort_batch(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ib
     const int32_t n_bound = h->cfg.max_spikes;
     h->mark(8, s);
     if (need_tf) {
-        const int grid = std::min(n_bound, 8 * h->sm_count);
+        const int grid = std::min(n_bound, 16 * h->sm_count);
         CK(launch_pc_features_folded(Xh, h->ld, h->C, h->nt, h->K, h->nC, h->T, h->wpca.p, h->Mw.p, h->U.p, h->R.p,
                                      h->iCC.p, h->iU.p, h->Ucc.p, h->sp_x.p, h->sp_y.p, h->sp_amp.p,
                                      h->round_start.p, 0, grid, h->counters.p, h->tF.p, h->status.p,
