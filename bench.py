@@ -167,39 +167,70 @@ def run_b200(args):
         s.set_drift(drifts[j])
         return s.sort_batch(rows_h[j] if host else rows_d[j], ids[j], nb, on_device=not host)
 
+    def step_async(i):
+        j = i % len(ids)
+        s.set_drift(drifts[j])
+        return s.sort_batch_async(rows_d[j], ids[j], nb)
+
+    def profiled(K):
+        """Per-stage device times, spikes and rounds of K synchronous batches
+        (untimed: the stage events serialise the host and the device)."""
+        s.set_profiling(True)
+        stages, spikes, rounds = [], [], []
+        for i in range(K):
+            r = step(i, False)
+            stages.append(s.stage_times())
+            spikes.append(len(r['time']))
+            rounds.append(s.stats()['rounds'])
+        s.set_profiling(False)
+        return stages, spikes, rounds
+
     def timed(K, W, host):
+        """Device-resident steps are submitted back to back (lss_sort_batch_async,
+        one host wait at the end); host-buffer steps go through lss_sort_batch
+        with its host copies and wait."""
         for i in range(W):
-            step(i, host)
+            if host:
+                step(i, host)
+            else:
+                step_async(i)
+        if not host:
+            s.sync()
         gc.collect()
         gc.disable()  # no collector pauses inside the timed region
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(K + 1)]
-        stages, spikes, rounds = [], [], []
         launches0 = s.stats()['launches']
+        keep = []
         ev[0].record(stream)
         for i in range(K):
-            r = step(i, host)
+            if host:
+                step(i, host)
+            else:
+                keep.append(step_async(i))
             ev[i + 1].record(stream)
-            stages.append(s.stage_times())
-            spikes.append(len(r['time']))
-            rounds.append(s.stats()['rounds'])
+        if not host:
+            s.sync()
         torch.cuda.synchronize()
         gc.enable()
+        del keep
         per = np.array([ev[i].elapsed_time(ev[i + 1]) for i in range(K)])
         tot = float(ev[0].elapsed_time(ev[K]))
         if dist:
             t = torch.tensor([tot], device=f'cuda:{local}')
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             tot = float(t.item())
-        return tot, per, stages, spikes, rounds, s.stats()['launches'] - launches0
+        return tot, per, s.stats()['launches'] - launches0
 
     K, W = args.steps, max(3, args.warmup)
+    s.set_profiling(False)
     with Clocks(local) as clk:
-        tot, per, stages, spikes, rounds, launches = timed(K, W, host=False)
+        tot, per, launches = timed(K, W, host=False)
     clocks = clk.summary()
-    tot_h, per_h, stages_h, _, _, _ = timed(K, W, host=True)
+    tot_h, per_h, _ = timed(K, W, host=True)
+    stages, spikes, rounds = profiled(min(K, 2 * len(ids)))
     rec_s = setup.NT / FS
     value = world * K * rec_s / (tot / 1e3)
     e2e = world * K * rec_s / (tot_h / 1e3)

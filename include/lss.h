@@ -197,6 +197,17 @@ int  lss_scores(lss_handle* h, const float* X_dev, int64_t N, float* B_dev, void
 int  lss_sort_batch(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ibatch,
                     int64_t n_batches, int32_t raw_on_device, lss_records* out, void* stream);
 
+/* lss_sort_batch without any host wait, for pipelined submission: the
+ * records must be device arrays, the record count is written to count_dev
+ * (device or mapped memory) when the batch's work finishes, and errors are
+ * collected until lss_sync (which waits for the stream and returns the first
+ * error seen). Batches on one stream run in order; drift changes between
+ * them (lss_set_drift) wait for the batch before. */
+int  lss_sort_batch_async(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ibatch,
+                          int64_t n_batches, int32_t raw_on_device, lss_records* out, int64_t* count_dev,
+                          void* stream);
+int  lss_sync(lss_handle* h, void* stream);
+
 /* Statistics of the last lss_match / lss_sort_batch: rounds run and spikes;
  * for the BF16 path, of the last scoring: columns whose decisions lay within
  * the re-check margin, decisions (best template or threshold side) the FP32

@@ -21,7 +21,8 @@ EXPORTS = ('lss_create', 'lss_create_from_dir', 'lss_destroy', 'lss_last_error',
            'lss_server_push', 'lss_server_poll', 'lss_server_release', 'lss_server_set_drift',
            'lss_server_latency', 'lss_server_memory', 'lss_recon_forward', 'lss_recon_backward',
            'lss_set_postprocess', 'lss_reset_postprocess', 'lss_format_spike_lines', 'lss_serialize_payload',
-           'lss_set_templates', 'lss_set_drift_model', 'lss_set_drift_shift', 'lss_server_latencies')
+           'lss_set_templates', 'lss_set_drift_model', 'lss_set_drift_shift', 'lss_server_latencies',
+           'lss_sort_batch_async', 'lss_sync')
 
 
 class LssConfig(ct.Structure):
@@ -96,6 +97,8 @@ def load() -> ct.CDLL:
         'lss_match_scores': ([P, P, I64, P, P, I64, ct.POINTER(I64), P], ct.c_int),
         'lss_scores': ([P, P, I64, P, P], ct.c_int),
         'lss_sort_batch': ([P, P, I64, I64, I64, I32, ct.POINTER(LssRecords), P], ct.c_int),
+        'lss_sort_batch_async': ([P, P, I64, I64, I64, I32, ct.POINTER(LssRecords), P, P], ct.c_int),
+        'lss_sync': ([P, P], ct.c_int),
         'lss_get_stats': ([P, ct.POINTER(LssStats)], ct.c_int),
         'lss_set_profiling': ([P, I32], ct.c_int),
         'lss_get_stage_times': ([P, ct.POINTER(LssStageTimes)], ct.c_int),

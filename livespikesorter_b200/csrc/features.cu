@@ -581,4 +581,14 @@ cudaError_t launch_pc_features_folded(const float* Xh, int64_t ldx, int32_t C, i
     return cudaGetLastError();
 }
 
+// acc |= *st (errors of asynchronous batches, collected until lss_sync)
+__global__ void k_status_or(const int32_t* st, int32_t* acc) {
+    if (*st) atomicOr(acc, *st);
+}
+
+cudaError_t launch_status_or(const int32_t* st, int32_t* acc, cudaStream_t s) {
+    k_status_or<<<1, 1, 0, s>>>(st, acc);
+    return cudaGetLastError();
+}
+
 }  // namespace lss

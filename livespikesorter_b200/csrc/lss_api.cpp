@@ -134,13 +134,26 @@ int lss::mix_device_drift(lss_handle* h) {
     return rebuild_uw(h);
 }
 
+// Drift / whitening change, all on the legacy default stream without a host
+// wait: it first waits for the last batch enqueued on any stream (batch_ev),
+// the matrix goes through a pinned staging buffer, and the batch entry points
+// wait for mix_ev.
 static int set_mixing(lss_handle* h, const float* M) {
     const int C = h->C;
+    if (h->batch_ev) CK(cudaStreamWaitEvent(0, h->batch_ev, 0));
     if (!M) {
-        CK(cudaMemcpy(h->Mw.p, h->Wrot.p, (size_t)C * C * sizeof(float), cudaMemcpyDeviceToDevice));
+        CK(cudaMemcpyAsync(h->Mw.p, h->Wrot.p, (size_t)C * C * sizeof(float), cudaMemcpyDeviceToDevice, 0));
         return rebuild_uw(h);
     }
-    CK(cudaMemcpy(h->Mdrift.p, M, (size_t)C * C * sizeof(float), cudaMemcpyHostToDevice));
+    if (!h->m_pin) {
+        CK(cudaHostAlloc(reinterpret_cast<void**>(&h->m_pin), (size_t)C * C * sizeof(float), cudaHostAllocDefault));
+        CK(cudaEventCreateWithFlags(&h->m_pin_ev, cudaEventDisableTiming));
+    } else {
+        CK(cudaEventSynchronize(h->m_pin_ev));  // the previous upload has left the staging buffer
+    }
+    std::memcpy(h->m_pin, M, (size_t)C * C * sizeof(float));
+    CK(cudaMemcpyAsync(h->Mdrift.p, h->m_pin, (size_t)C * C * sizeof(float), cudaMemcpyHostToDevice, 0));
+    CK(cudaEventRecord(h->m_pin_ev, 0));
     return mix_device_drift(h);
 }
 
@@ -464,6 +477,10 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
         CK(cudaMemcpy(h->iU.p, t->iU, (size_t)T * sizeof(int64_t), cudaMemcpyHostToDevice));
     }
     CK(cudaMemset(h->colkey.p, 0, 2 * ld * sizeof(unsigned long long)));
+    CK(h->status_acc.alloc(1));
+    h->dev_bytes += 256;
+    CK(cudaMemset(h->status_acc.p, 0, sizeof(int32_t)));
+    CK(cudaEventCreateWithFlags(&h->batch_ev, cudaEventDisableTiming));
     CK(cudaMemcpy(h->Wrot.p, t->whitening, (size_t)C * C * sizeof(float), cudaMemcpyHostToDevice));
     rc = set_mixing(h, t->drift);
     if (rc) { g_create_err = h->err; return rc; }
@@ -896,8 +913,39 @@ int lss_match_scores(lss_handle* h, const float* B_dev, int64_t N, int64_t* st_d
     return match_common(h, N, nullptr, st_dev, amps_dev, nullptr, capacity, n_spikes, s);
 }
 
+static int sort_batch_impl(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ibatch, int64_t n_batches,
+                           int32_t raw_on_device, lss_records* out, void* stream, int64_t* count_dev);
+
 int lss_sort_batch(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ibatch, int64_t n_batches,
                    int32_t raw_on_device, lss_records* out, void* stream) {
+    return sort_batch_impl(h, raw, n_rows, ibatch, n_batches, raw_on_device, out, stream, nullptr);
+}
+
+int lss_sort_batch_async(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ibatch, int64_t n_batches,
+                         int32_t raw_on_device, lss_records* out, int64_t* count_dev, void* stream) {
+    if (!h || !out || !count_dev) return LSS_ERR_ARG;
+    if (!out->on_device) return h->fail(LSS_ERR_ARG, "asynchronous batches write device records");
+    return sort_batch_impl(h, raw, n_rows, ibatch, n_batches, raw_on_device, out, stream, count_dev);
+}
+
+int lss_sync(lss_handle* h, void* stream) {
+    if (!h) return LSS_ERR_ARG;
+    CK(cudaSetDevice(h->cfg.device));
+    CK(cudaStreamSynchronize((cudaStream_t)stream));
+    int32_t st = 0;
+    CK(cudaMemcpy(&st, h->status_acc.p, sizeof(st), cudaMemcpyDeviceToHost));
+    CK(cudaMemset(h->status_acc.p, 0, sizeof(st)));
+    if (st & STATUS_TIMEOUT) return h->fail(LSS_ERR_TIMEOUT, "a bounded device-side wait timed out");
+    if (st & STATUS_CAPACITY) return h->fail(LSS_ERR_CAPACITY, "more than max_spikes spikes in one batch");
+    if (st & STATUS_LIST)
+        return h->fail(LSS_ERR_CAPACITY, "more than 32 peaks inside one 2*nt window, or a feature list overflow");
+    return LSS_OK;
+}
+
+}  // extern "C"
+
+static int sort_batch_impl(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ibatch, int64_t n_batches,
+                           int32_t raw_on_device, lss_records* out, void* stream, int64_t* count_dev) {
     if (!h || !out) return LSS_ERR_ARG;
     if (h->streaming) return h->fail(LSS_ERR_STATE, "handle is owned by a serving loop");
     if (!out->time || !out->template_id || !out->amplitude) return h->fail(LSS_ERR_ARG, "null record arrays");
@@ -954,8 +1002,17 @@ int lss_sort_batch(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ib
     float* d_y = want_post && out->y_pos ? (out->on_device ? out->y_pos : h->rec_y.p) : nullptr;
     int32_t* d_clu = want_post && out->cluster ? (out->on_device ? out->cluster : h->rec_clu.p) : nullptr;
     rc = enqueue_records(h, rclk, n_bound, want_pc, need_tf, d_time, d_tmpl, d_amp, d_pc, d_x, d_y, d_clu, dcap,
-                         h->rec_count.p, s);
+                         count_dev ? count_dev : h->rec_count.p, s);
     if (rc) return rc;
+    if (count_dev) {
+        // asynchronous: errors accumulate for lss_sync; no host wait
+        CK(launch_status_or(h->status.p, h->status_acc.p, s));
+        h->stats.launches += 1;
+        h->mark(10, s);
+        CK(cudaEventRecord(h->batch_ev, s));
+        return LSS_OK;
+    }
+    CK(cudaEventRecord(h->batch_ev, s));
     int64_t count = 0;
     int32_t st = 0, hc[4];
     CK(cudaMemcpyAsync(&count, h->rec_count.p, sizeof(count), cudaMemcpyDeviceToHost, s));
@@ -989,6 +1046,8 @@ int lss_sort_batch(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ib
     }
     return LSS_OK;
 }
+
+extern "C" {
 
 int lss_set_profiling(lss_handle* h, int32_t on) {
     if (!h) return LSS_ERR_ARG;

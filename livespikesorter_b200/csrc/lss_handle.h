@@ -75,6 +75,10 @@ struct lss_handle {
     int32_t* rc_host = nullptr;                  // pinned copy of rc_count (read by lss_get_stats)
     cudaEvent_t rc_ev = nullptr;                 // recorded after that copy
     cudaEvent_t mix_ev = nullptr;                // recorded after the whitening-folded templates are rebuilt
+    cudaEvent_t batch_ev = nullptr;              // recorded after each batch's work (template rebuilds wait for it)
+    float* m_pin = nullptr;                      // pinned staging of drift matrices
+    cudaEvent_t m_pin_ev = nullptr;              // recorded after m_pin's last upload
+    DevBuf<int32_t> status_acc;                  // errors of asynchronous batches since the last lss_sync
     bool rc_pending = false;
     int64_t last_scored = 0;                     // samples of the last BF16 scoring
     int CKpad = 0;
@@ -127,6 +131,10 @@ struct lss_handle {
         dm_pos.release(); dm_ik.release();
         if (rc_ev) cudaEventDestroy(rc_ev);
         if (mix_ev) cudaEventDestroy(mix_ev);
+        if (batch_ev) cudaEventDestroy(batch_ev);
+        if (m_pin_ev) cudaEventDestroy(m_pin_ev);
+        if (m_pin) cudaFreeHost(m_pin);
+        status_acc.release();
         if (rc_host) cudaFreeHost(rc_host);
     }
 };

@@ -131,6 +131,7 @@ enum : int32_t { STATUS_TIMEOUT = 1, STATUS_CAPACITY = 2, STATUS_LIST = 4 };
 cudaError_t launch_mp(MPArgs a, int grid, cudaStream_t s);
 int mp_max_grid(int device);
 void set_thread_error(const char* msg);
+cudaError_t launch_status_or(const int32_t* st, int32_t* acc, cudaStream_t s);
 
 // ---- residual and PC features (features.cu); n = spikes of the batch ----
 cudaError_t launch_xres(const float* X, int64_t ldx, int32_t C, int32_t N, int32_t nt, const float* wave,

@@ -228,6 +228,27 @@ class Sorter:
             out.update(x=xs[:n], y=ys[:n], cluster=clu[:n])
         return out
 
+    def sort_batch_async(self, raw, ibatch: int, n_batches: int, capacity: int | None = None) -> dict:
+        """``sort_batch`` with device records and no host wait: returns the
+        record tensors and a device ``count``; call ``sync()`` before reading
+        them (it raises the first error the batches met)."""
+        raw_t, raw_dev = self._raw(raw)
+        cap = capacity or self.cfg.max_spikes
+        dev = self.device
+        time = torch.empty(cap, dtype=torch.int64, device=dev)
+        tmpl = torch.empty(cap, dtype=torch.int32, device=dev)
+        amp = torch.empty(cap, dtype=torch.float32, device=dev)
+        pc = torch.empty((cap, self.nC, self.K), dtype=torch.float32, device=dev) if self.nC > 0 else None
+        count = torch.zeros(1, dtype=torch.int64, device=dev)
+        rec = LssRecords(time=time.data_ptr(), template_id=tmpl.data_ptr(), amplitude=amp.data_ptr(),
+                         pc=_ptr(pc), capacity=cap, count=0, on_device=1, x_pos=None, y_pos=None, cluster=None)
+        self._check(self._lib.lss_sort_batch_async(self._h, raw_t.data_ptr(), raw_t.shape[0], ibatch, n_batches,
+                                                   raw_dev, rec, count.data_ptr(), _stream(self.device)))
+        return dict(time=time, template=tmpl, amplitude=amp, pc=pc, count=count)
+
+    def sync(self):
+        self._check(self._lib.lss_sync(self._h, _stream(self.device)))
+
     def stats(self) -> dict:
         s = LssStats()
         self._check(self._lib.lss_get_stats(self._h, s))
