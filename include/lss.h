@@ -318,8 +318,9 @@ int  lss_recon_backward(int32_t dtype, const void* U, const void* wPCA, int32_t 
  * samples in Kilosort's convention (trough-aligned: + nt0min - nt/2);
  * negative times are dropped. Results land in pinned host memory written by
  * the device; arrival-to-emit latency is measured from the arrival time given
- * to lss_server_push for the block's last row to the host callback that runs
- * when the batch's work has finished.
+ * to lss_server_push for the block's last row to the moment the server sees
+ * the batch's completion event (in lss_server_poll, or in a push that waits
+ * for the batch's slot).
  * ---------------------------------------------------------------------- */
 typedef struct lss_server lss_server;
 
@@ -339,8 +340,11 @@ int  lss_server_push(lss_server* s, int32_t probe, const int16_t* rows, int64_t 
 /* Oldest finished batch's records into `out` (host arrays); *batch = its
  * index, or -1 when none is finished (wait = 0) or none is in flight. */
 int  lss_server_poll(lss_server* s, int32_t probe, lss_records* out, int64_t* batch, int32_t wait);
-/* Waits for the probe's batches, frees its memory and slot. Finished batches
- * not yet polled are dropped. */
+/* Waits for the probe's batches and frees its slot; finished batches not yet
+ * polled are dropped. Its device and pinned memory are freed by a later
+ * admission that needs the room (released + admitted + the largest probe so
+ * far over the budget) or by lss_server_destroy: a free waits for the whole
+ * device, which the other probes' batches would see as latency. */
 int  lss_server_release(lss_server* s, int32_t probe);
 /* Replaces the probe's drift matrix after its in-flight batches finish. */
 int  lss_server_set_drift(lss_server* s, int32_t probe, const float* drift_M);
@@ -349,7 +353,16 @@ int  lss_server_latency(lss_server* s, int32_t probe, double* p50_ms, double* p9
 /* Every polled batch's arrival-to-emit latency (ms), in batch order: up to
  * capacity values into out_ms, *n = how many there are. */
 int  lss_server_latencies(lss_server* s, int32_t probe, double* out_ms, int64_t capacity, int64_t* n);
-/* Device memory held by admitted probes and the budget, in bytes. */
+/* The same latencies split in four (ms, 4 per batch, batch order, up to
+ * capacity batches; *n = how many batches there are): arrival -> graph launch
+ * (host), launch -> the batch's first kernel starts (queued behind the
+ * stream's or the device's other work), first kernel start -> last kernel
+ * end (device), last kernel end -> completion seen. The parts sum to the
+ * latency; the device times are mapped to the host clock by an offset taken
+ * at admission (error a few us). */
+int  lss_server_latency_parts(lss_server* s, int32_t probe, double* out_ms, int64_t capacity, int64_t* n);
+/* Device memory held by admitted probes (released ones not counted) and the
+ * budget, in bytes. */
 int  lss_server_memory(lss_server* s, int64_t* used, int64_t* budget);
 
 #ifdef __cplusplus

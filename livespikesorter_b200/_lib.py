@@ -22,6 +22,7 @@ EXPORTS = ('lss_create', 'lss_create_from_dir', 'lss_destroy', 'lss_last_error',
            'lss_server_latency', 'lss_server_memory', 'lss_recon_forward', 'lss_recon_backward',
            'lss_set_postprocess', 'lss_reset_postprocess', 'lss_format_spike_lines', 'lss_serialize_payload',
            'lss_set_templates', 'lss_set_drift_model', 'lss_set_drift_shift', 'lss_server_latencies',
+           'lss_server_latency_parts',
            'lss_sort_batch_async', 'lss_sync')
 
 
@@ -124,6 +125,7 @@ def load() -> ct.CDLL:
                                ct.c_int),
         'lss_server_memory': ([P, ct.POINTER(I64), ct.POINTER(I64)], ct.c_int),
         'lss_server_latencies': ([P, I32, P, I64, ct.POINTER(I64)], ct.c_int),
+        'lss_server_latency_parts': ([P, I32, P, I64, ct.POINTER(I64)], ct.c_int),
         'lss_recon_forward': ([I32, P, P, I32, I32, I32, I32, P, P, P, I64, P, I64, P], ct.c_int),
         'lss_recon_backward': ([I32, P, P, I32, I32, I32, I32, P, P, P, P, P, I64, P, P, P, P, P], ct.c_int),
     }

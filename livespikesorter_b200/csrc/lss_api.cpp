@@ -484,7 +484,9 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
     CK(cudaMemcpy(h->Wrot.p, t->whitening, (size_t)C * C * sizeof(float), cudaMemcpyHostToDevice));
     rc = set_mixing(h, t->drift);
     if (rc) { g_create_err = h->err; return rc; }
-    CK(cudaDeviceSynchronize());
+    // the set-up work is on the legacy stream; waiting for it alone leaves
+    // other handles' non-blocking streams (a serving loop's probes) running
+    CK(cudaStreamSynchronize(0));
     *out = hp.release();
     return LSS_OK;
 }

@@ -8,18 +8,18 @@
 // CUDA graph (captured once per probe, i.e. per batch length and template
 // set) that reads its window straight from a device ring of raw rows and
 // writes its records into pinned host memory, so a batch costs one H2D copy
-// of the new block, one graph launch and one host callback, and batches of
+// of the new block, one graph launch and one event, and batches of
 // different probes overlap on the device.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <atomic>
 #include <chrono>
-#include <condition_variable>
 #include <cstring>
 #include <deque>
 #include <memory>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -33,14 +33,24 @@ namespace lss {
 struct StreamMail {
     int64_t batch;
     int32_t spikes, rounds, status, pad;
+    int64_t t_begin, t_end;  // device global timer (ns) at the graph's first and last kernel
 };
 
+__device__ __forceinline__ int64_t global_timer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return (int64_t)t;
+}
+
+__global__ void k_global_timer(int64_t* out) { *out = global_timer_ns(); }
+
 // state[0] = batch index (starts at -1), state[1] = first stream row of the
-// batch window.
+// batch window, state[2] = device time at which the batch's work began.
 __global__ void k_stream_begin(int64_t* state, int64_t NT, int64_t lead) {
     const int64_t b = state[0] + 1;
     state[0] = b;
     state[1] = b * NT - lead;
+    state[2] = global_timer_ns();
 }
 
 __global__ void k_stream_end(const int64_t* state, const int32_t* counters, const int32_t* status, StreamMail* mail,
@@ -52,6 +62,8 @@ __global__ void k_stream_end(const int64_t* state, const int32_t* counters, cons
     m.rounds = counters[1];
     m.status = *status;
     m.pad = 0;
+    m.t_begin = state[2];
+    m.t_end = global_timer_ns();
     mail[b % slots] = m;
 }
 
@@ -67,12 +79,16 @@ using namespace lss;
 
 namespace {
 
+// One in-flight batch. Its completion is an event recorded behind the
+// batch's graph and queried by the thread that polls: a host callback in the
+// stream would hold the stream's next batch back until the driver's callback
+// thread had run it, and that thread was seen to run tens of ms late.
 struct Slot {
-    std::atomic<int> done{0};
+    cudaEvent_t ev = nullptr;
     int64_t batch = -1;
     int64_t arrival_ns = 0;
+    int64_t launch_ns = 0;
     int64_t emit_ns = 0;
-    struct Probe* owner = nullptr;
 };
 
 struct Result {
@@ -124,9 +140,10 @@ struct Probe {
     int64_t harvest = 0;                       // next batch to harvest
     std::deque<Result> ready;
     std::vector<double> lat_ms;
+    std::vector<double> parts_ms;              // 4 per batch, lss_server_latency_parts
+    int64_t gpu_offset_ns = 0;                 // host steady clock - device global timer
     size_t bytes = 0;
     std::mutex m;
-    std::condition_variable cv;
     std::string err;
 
     int fail(int code, const std::string& msg) {
@@ -136,6 +153,8 @@ struct Probe {
     }
     ~Probe() {
         if (s) cudaStreamSynchronize(s);
+        for (int64_t i = 0; slots && i < D; ++i)
+            if (slots[i].ev) cudaEventDestroy(slots[i].ev);
         if (exec) cudaGraphExecDestroy(exec);
         if (s) cudaStreamDestroy(s);
         ring.release();
@@ -153,17 +172,6 @@ struct Probe {
         if (h) lss_destroy(h);
     }
 };
-
-void CUDART_CB on_batch_done(void* arg) {
-    Slot* sl = static_cast<Slot*>(arg);
-    sl->emit_ns = lss::now_ns();
-    Probe* p = sl->owner;
-    {
-        std::lock_guard<std::mutex> lk(p->m);
-        sl->done.store(1);
-    }
-    p->cv.notify_all();
-}
 
 #define PCK(call)                                                                   \
     do {                                                                            \
@@ -247,19 +255,45 @@ int capture(Probe* p) {
     return LSS_OK;
 }
 
+// Offset from the device's global timer to the host's steady clock, taken
+// as the midpoint of the shortest of a few launch-and-wait round trips of a
+// kernel that reads the timer (error: half that round trip, a few us).
+int calibrate_clock(Probe* p) {
+    int64_t best_rt = INT64_MAX;
+    for (int i = 0; i < 5; ++i) {
+        const int64_t t0 = lss::now_ns();
+        k_global_timer<<<1, 1, 0, p->s>>>(p->state.p + 2);
+        PCK(cudaGetLastError());
+        int64_t g = 0;
+        PCK(cudaMemcpyAsync(&g, p->state.p + 2, sizeof(g), cudaMemcpyDeviceToHost, p->s));
+        PCK(cudaStreamSynchronize(p->s));
+        const int64_t t1 = lss::now_ns();
+        if (t1 - t0 < best_rt) {
+            best_rt = t1 - t0;
+            p->gpu_offset_ns = t0 + (t1 - t0) / 2 - g;
+        }
+    }
+    return LSS_OK;
+}
+
 // Moves the oldest in-flight batch's results into p->ready (waits for it when
 // `wait`). Caller holds p->m through `lk`. Returns LSS_OK (possibly nothing
 // moved when !wait), or an error.
 int harvest_one(Probe* p, std::unique_lock<std::mutex>& lk, bool wait) {
     if (p->harvest >= p->next) return LSS_OK;
     Slot& sl = p->slots[p->harvest % p->D];
-    if (!sl.done.load()) {
+    // the device work is bounded (every wait in the kernels gives up), so
+    // this wait ends; 60 s covers a cold first launch
+    const auto t0 = std::chrono::steady_clock::now();
+    cudaError_t q;
+    while ((q = cudaEventQuery(sl.ev)) == cudaErrorNotReady) {
         if (!wait) return LSS_OK;
-        // the device work is bounded (every wait in the kernels gives up), so
-        // this wait ends; 60 s covers a cold first launch
-        if (!p->cv.wait_for(lk, std::chrono::seconds(60), [&] { return sl.done.load() != 0; }))
+        if (std::chrono::steady_clock::now() - t0 > std::chrono::seconds(60))
             return p->fail(LSS_ERR_TIMEOUT, "stream batch did not finish within 60 s");
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
     }
+    if (q != cudaSuccess) return p->fail(LSS_ERR_CUDA, std::string("stream batch: ") + cudaGetErrorString(q));
+    sl.emit_ns = lss::now_ns();
     const int64_t k = p->harvest % p->D;
     const StreamMail mail = p->mail.p[k];
     Result r;
@@ -279,7 +313,10 @@ int harvest_one(Probe* p, std::unique_lock<std::mutex>& lk, bool wait) {
         r.clu.assign(p->o_clu.p + k * p->cap, p->o_clu.p + k * p->cap + n);
     }
     p->lat_ms.push_back((double)(sl.emit_ns - sl.arrival_ns) * 1e-6);
-    sl.done.store(0);
+    const int64_t beg = mail.t_begin + p->gpu_offset_ns, end = mail.t_end + p->gpu_offset_ns;
+    const double parts[4] = {(double)(sl.launch_ns - sl.arrival_ns) * 1e-6, (double)(beg - sl.launch_ns) * 1e-6,
+                             (double)(end - beg) * 1e-6, (double)(sl.emit_ns - end) * 1e-6};
+    p->parts_ms.insert(p->parts_ms.end(), parts, parts + 4);
     p->harvest += 1;
     p->ready.push_back(std::move(r));
     return LSS_OK;
@@ -292,10 +329,10 @@ int launch_block(Probe* p, int64_t arrival_ns) {
                         (size_t)(p->NT * p->Cbin) * sizeof(int16_t), cudaMemcpyHostToDevice, p->s));
     Slot& sl = p->slots[k];
     sl.batch = b;
-    sl.arrival_ns = arrival_ns > 0 ? arrival_ns : lss::now_ns();
-    sl.done.store(0);
+    sl.launch_ns = lss::now_ns();
+    sl.arrival_ns = arrival_ns > 0 ? arrival_ns : sl.launch_ns;
     PCK(cudaGraphLaunch(p->exec, p->s));
-    PCK(cudaLaunchHostFunc(p->s, on_batch_done, &sl));
+    PCK(cudaEventRecord(sl.ev, p->s));
     p->next = b + 1;
     return LSS_OK;
 }
@@ -306,8 +343,22 @@ struct lss_server {
     int device = 0;
     int64_t budget = 0, used = 0;
     std::vector<std::unique_ptr<Probe>> probes;
+    // Released probes, kept whole until an admission needs their room or the
+    // server is destroyed: freeing device and pinned memory waits for the
+    // whole device and holds the driver up, which would show as latency on
+    // every other probe's batches.
+    std::vector<std::unique_ptr<Probe>> retired;
+    int64_t retired_bytes = 0;
+    int64_t largest = 0;  // bytes of the largest probe admitted so far
     std::mutex m;
 };
+
+namespace {
+void free_retired(lss_server* s) {
+    s->retired.clear();
+    s->retired_bytes = 0;
+}
+}  // namespace
 
 extern "C" {
 
@@ -328,6 +379,7 @@ void lss_server_destroy(lss_server* s) {
     if (!s) return;
     cudaSetDevice(s->device);
     s->probes.clear();
+    free_retired(s);
     delete s;
 }
 
@@ -350,6 +402,7 @@ int lss_server_admit(lss_server* s, const lss_config* cfg, const lss_tensors* t,
         return LSS_ERR_ARG;
     }
     cudaSetDevice(s->device);
+    if (!s->retired.empty() && s->used + s->retired_bytes + s->largest > s->budget) free_retired(s);
     auto p = std::make_unique<Probe>();
     int rc = lss_create(cfg, t, &p->h);
     if (rc) return rc;
@@ -364,7 +417,7 @@ int lss_server_admit(lss_server* s, const lss_config* cfg, const lss_tensors* t,
     const int64_t win = p->NT + 2 * p->nt;
     p->R = ((win + p->NT - 1) / p->NT + depth) * p->NT;
     const size_t ring_bytes = (size_t)p->R * p->Cbin * sizeof(int16_t);
-    p->bytes = h->dev_bytes + ring_bytes + 2 * sizeof(int64_t);
+    p->bytes = h->dev_bytes + ring_bytes + 3 * sizeof(int64_t);
     if (s->used + (int64_t)p->bytes > s->budget) {
         lss::set_thread_error("device memory budget exhausted");
         return LSS_ERR_BUSY;  // p's destructor frees the handle
@@ -376,7 +429,7 @@ int lss_server_admit(lss_server* s, const lss_config* cfg, const lss_tensors* t,
     cudaError_t e;
     if ((e = cudaStreamCreateWithFlags(&p->s, cudaStreamNonBlocking)) != cudaSuccess) return cfail(e, "stream");
     if ((e = p->ring.alloc((size_t)p->R * p->Cbin)) != cudaSuccess) return cfail(e, "ring");
-    if ((e = p->state.alloc(2)) != cudaSuccess) return cfail(e, "state");
+    if ((e = p->state.alloc(3)) != cudaSuccess) return cfail(e, "state");
     const int64_t init[2] = {-1, 0};
     if ((e = cudaMemcpy(p->state.p, init, sizeof(init), cudaMemcpyHostToDevice)) != cudaSuccess)
         return cfail(e, "state");
@@ -390,7 +443,9 @@ int lss_server_admit(lss_server* s, const lss_config* cfg, const lss_tensors* t,
     if ((e = p->o_count.alloc((size_t)depth, true)) != cudaSuccess) return cfail(e, "records");
     if ((e = p->mail.alloc((size_t)depth, true)) != cudaSuccess) return cfail(e, "mailbox");
     p->slots.reset(new Slot[depth]);
-    for (int i = 0; i < depth; ++i) p->slots[i].owner = p.get();
+    for (int i = 0; i < depth; ++i)
+        if ((e = cudaEventCreateWithFlags(&p->slots[i].ev, cudaEventDisableTiming)) != cudaSuccess)
+            return cfail(e, "event");
     if (drift_M) {
         rc = lss_set_drift(h, drift_M);
         if (rc) {
@@ -408,7 +463,7 @@ int lss_server_admit(lss_server* s, const lss_config* cfg, const lss_tensors* t,
         if ((e = p->o_x.alloc((size_t)depth * capacity, true)) != cudaSuccess) return cfail(e, "records");
         if ((e = p->o_y.alloc((size_t)depth * capacity, true)) != cudaSuccess) return cfail(e, "records");
         if ((e = p->o_clu.alloc((size_t)depth * capacity, true)) != cudaSuccess) return cfail(e, "records");
-        p->bytes = h->dev_bytes + ring_bytes + 2 * sizeof(int64_t);
+        p->bytes = h->dev_bytes + ring_bytes + 3 * sizeof(int64_t);
         if (s->used + (int64_t)p->bytes > s->budget) {
             lss::set_thread_error("device memory budget exhausted");
             return LSS_ERR_BUSY;
@@ -419,11 +474,14 @@ int lss_server_admit(lss_server* s, const lss_config* cfg, const lss_tensors* t,
     h->mp_grid = std::max(1, std::min(h->mp_grid, h->sm_count / (int)s->probes.size()));
     h->streaming = true;
     rc = capture(p.get());
+    if (!rc) rc = calibrate_clock(p.get());
     if (rc) {
         lss::set_thread_error(p->err.c_str());
         return rc;
     }
+    if (s->used + s->retired_bytes + (int64_t)p->bytes > s->budget) free_retired(s);
     s->used += (int64_t)p->bytes;
+    s->largest = std::max<int64_t>(s->largest, (int64_t)p->bytes);
     s->probes[slot] = std::move(p);
     *probe = slot;
     return LSS_OK;
@@ -523,8 +581,14 @@ int lss_server_release(lss_server* s, int32_t probe) {
     }
     cudaSetDevice(s->device);
     std::lock_guard<std::mutex> lk(s->m);
-    s->used -= (int64_t)s->probes[probe]->bytes;
-    s->probes[probe].reset();  // the destructor waits for the probe's stream
+    std::unique_ptr<Probe> p = std::move(s->probes[probe]);
+    s->used -= (int64_t)p->bytes;
+    if (p->s && cudaStreamSynchronize(p->s) != cudaSuccess) {
+        p.reset();  // a failed stream: free now
+        return LSS_OK;
+    }
+    s->retired_bytes += (int64_t)p->bytes;
+    s->retired.push_back(std::move(p));
     return LSS_OK;
 }
 
@@ -582,6 +646,19 @@ int lss_server_latencies(lss_server* s, int32_t probe, double* out_ms, int64_t c
     std::lock_guard<std::mutex> lk(p->m);
     *n = (int64_t)p->lat_ms.size();
     for (int64_t i = 0; i < std::min<int64_t>(capacity, *n); ++i) out_ms[i] = p->lat_ms[i];
+    return LSS_OK;
+}
+
+int lss_server_latency_parts(lss_server* s, int32_t probe, double* out_ms, int64_t capacity, int64_t* n) {
+    Probe* p = get_probe(s, probe);
+    if (!p || !n || (capacity > 0 && !out_ms)) {
+        lss::set_thread_error("lss_server_latency_parts: bad argument");
+        return LSS_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lk(p->m);
+    *n = (int64_t)p->parts_ms.size() / 4;
+    const int64_t m = std::min<int64_t>(capacity, *n) * 4;
+    for (int64_t i = 0; i < m; ++i) out_ms[i] = p->parts_ms[i];
     return LSS_OK;
 }
 

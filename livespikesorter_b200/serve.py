@@ -11,8 +11,8 @@ stream's blocks arrive at real-time instants (block / fs apart, plus seeded
 jitter), are pushed as they arrive and their results are polled as they
 finish; streams that are not admitted yet wait in a queue and join when a
 release frees room (continuous batching). Latency is measured per batch from
-the block's scheduled arrival instant to the host callback that runs when the
-batch's work has finished on the device.
+the block's scheduled arrival instant to the poll that sees the batch's
+completion event.
 
 The reference has no such loop as an API: each probe runs its own
 ``OnlineSpikesV2`` on a host thread (main.cpp:77-85) whose ``runSpikeSorting``
@@ -23,6 +23,7 @@ from __future__ import annotations
 import ctypes
 import gc
 import time
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -124,6 +125,10 @@ class ProbeServer:
             m = ctypes.c_int64()
             check(self._lib.lss_server_latencies(self._s, probe, buf.ctypes.data, len(buf), ctypes.byref(m)))
             out['samples_ms'] = buf[:m.value].tolist()
+            parts = np.zeros((max(n.value, 1), 4), np.float64)
+            check(self._lib.lss_server_latency_parts(self._s, probe, parts.ctypes.data, len(parts), ctypes.byref(m)))
+            # per batch: arrival -> launch, launch -> device start, device span, device end -> completion seen
+            out['parts_ms'] = parts[:m.value].tolist()
         return out
 
     def memory(self) -> tuple[int, int]:
@@ -150,6 +155,8 @@ class Stream:
     latency: dict = field(default_factory=dict)
     admitted_s: float | None = None
     waited: bool = False
+    push_late_ms: list = field(default_factory=list)  # realtime: push instant - arrival instant
+    started_ns: int | None = None                      # when its blocks began to flow
 
 
 def arrival_schedule(n_blocks: int, block: int, jitter_frac: float, rng: np.random.Generator) -> np.ndarray:
@@ -162,68 +169,112 @@ def arrival_schedule(n_blocks: int, block: int, jitter_frac: float, rng: np.rand
 
 
 def run_streams(server, streams: list[Stream], *, realtime: bool = True, jitter_frac: float = 0.2, seed: int = 0,
-                clock=time.perf_counter_ns, sleep=time.sleep) -> dict:
+                start_together: bool = False, clock=time.perf_counter_ns, sleep=time.sleep) -> dict:
     """Feeds every stream to ``server`` and collects its results.
 
     realtime: blocks are pushed at their arrival instants (latency is then
     arrival -> emit); otherwise every block is available at once and the loop
     measures the server's capacity (recording-seconds sorted per second).
     Streams whose admission is refused wait and retry after each release.
+    start_together: the streams that ask to join at 0 s start streaming once
+    all of them are admitted (a rig whose probes are set up before the
+    acquisition starts); otherwise each starts as soon as it is admitted,
+    while the others' admissions are still running.
+
+    Admissions and releases run on one worker thread, in submission order:
+    building a probe (allocations, graph capture) or tearing one down
+    (frees, which wait for the device) takes tens to hundreds of ms, and on
+    the serving thread that would hold back the pushes of every other stream.
     """
     rng = np.random.default_rng(seed)
     gc_was = gc.isenabled()
     gc.collect()
     gc.disable()  # a collector pause would show up as arrival-to-emit latency
+    admin = ThreadPoolExecutor(max_workers=1, thread_name_prefix='lss-admin')
     try:
-        return _run_streams(server, streams, realtime, jitter_frac, rng, clock, sleep)
+        return _run_streams(server, streams, realtime, jitter_frac, rng, clock, sleep, admin, start_together)
     finally:
+        admin.shutdown(wait=True)
         if gc_was:
             gc.enable()
 
 
-def _run_streams(server, streams, realtime, jitter_frac, rng, clock, sleep):
+def _start(parked, active, start_ns, now):
+    for pid, (st, sched) in parked.items():
+        active[pid] = [st, sched, 0, start_ns]
+        st.started_ns = now
+    parked.clear()
+
+
+def _run_streams(server, streams, realtime, jitter_frac, rng, clock, sleep, admin, start_together):
     t0 = clock()
-    waiting = sorted(streams, key=lambda s: s.start_s)
+    held = [st for st in streams if st.start_s <= 0] if start_together else []
+    parked = {}        # probe id -> stream, admitted and waiting for the others in `held`
+    order = {id(st): i for i, st in enumerate(sorted(streams, key=lambda s: s.start_s))}
+    waiting = sorted(streams, key=lambda s: order[id(s)])
     active = {}        # probe id -> [stream, schedule, next block index, stream start ns]
+    admitting = {}     # future -> (stream, releases completed when it was submitted)
+    releasing = []     # futures
     done = []
     samples = 0
     releases = 0       # a refused stream retries only after a release
     refused_at = {}
-    while waiting or active:
+    while waiting or active or admitting or releasing or parked:
+        progressed = False
+        # finished admissions and releases
+        for f in [f for f in releasing if f.done()]:
+            releasing.remove(f)
+            f.result()
+            releases += 1
+            progressed = True
+        for f in [f for f in admitting if f.done()]:
+            st, rel0 = admitting.pop(f)
+            pid = f.result()
+            progressed = True
+            is_held = any(h is st for h in held)
+            if pid is None:
+                st.waited = True
+                refused_at[id(st)] = rel0
+                waiting = sorted(waiting + [st], key=lambda s: order[id(s)])  # keeps its place
+                if is_held:  # not all of them fit: the admitted ones start now
+                    held = []
+                    _start(parked, active, clock() if realtime else t0, clock())
+                continue
+            nb = st.n_blocks if st.n_blocks is not None else st.raw.shape[0] // st.block
+            sched = arrival_schedule(nb, st.block, jitter_frac, rng) if realtime else np.zeros(nb)
+            st.admitted_s = (clock() - t0) * 1e-9
+            if is_held:
+                parked[pid] = (st, sched)
+                if len(parked) == len(held):
+                    held = []
+                    _start(parked, active, clock() if realtime else t0, clock())
+                continue
+            # a stream's clock starts once its probe is built
+            st.started_ns = clock()
+            active[pid] = [st, sched, 0, st.started_ns if realtime else t0]
+        # admission requests (in request order)
         now = clock()
-        # admissions (in request order; a refused stream keeps its place)
         still = []
         for st in waiting:
             if (now - t0) * 1e-9 < st.start_s or refused_at.get(id(st)) == releases:
                 still.append(st)
                 continue
-            pid = server.admit(depth=st.depth, capacity=st.capacity, drift=st.drift, post=st.post,
-                               **st.sorter_kwargs)
-            if pid is None:
-                st.waited = True
-                refused_at[id(st)] = releases
-                still.append(st)
-                continue
-            nb = st.n_blocks if st.n_blocks is not None else st.raw.shape[0] // st.block
-            sched = arrival_schedule(nb, st.block, jitter_frac, rng) if realtime else np.zeros(nb)
-            st.admitted_s = (clock() - t0) * 1e-9
-            active[pid] = [st, sched, 0, None]
+            f = admin.submit(server.admit, depth=st.depth, capacity=st.capacity, drift=st.drift, post=st.post,
+                             **st.sorter_kwargs)
+            admitting[f] = (st, releases)
         waiting = still
-        # a stream's clock starts once the admissions of this pass are done
-        # (an admission builds the probe's handle and graph)
-        for a in active.values():
-            if a[3] is None:
-                a[3] = clock() if realtime else t0
         # pushes of blocks that have arrived
-        progressed = False
         next_due = None
         for pid, a in active.items():
             st, sched, k, start_ns = a
             while k < len(sched):
                 due = start_ns + int(sched[k] * 1e9)
-                if realtime and clock() < due:
-                    next_due = due if next_due is None else min(next_due, due)
-                    break
+                if realtime:
+                    now = clock()
+                    if now < due:
+                        next_due = due if next_due is None else min(next_due, due)
+                        break
+                    st.push_late_ms.append((now - due) * 1e-6)
                 rows = st.raw[k * st.block:(k + 1) * st.block]
                 server.push(pid, rows, due if realtime else 0)
                 k += 1
@@ -243,18 +294,23 @@ def _run_streams(server, streams, realtime, jitter_frac, rng, clock, sleep):
                 progressed = True
             if k == len(sched) and len(st.results) == len(sched):
                 st.latency = server.latency(pid, samples=True)
-                server.release(pid)
-                releases += 1
                 del active[pid]
+                releasing.append(admin.submit(server.release, pid))
                 done.append(st)
                 progressed = True
         if not progressed:
             if realtime and next_due is not None:
                 gap = (next_due - clock()) * 1e-9
                 if gap > 3e-4:
-                    sleep(min(gap - 2e-4, 5e-4))
+                    # short naps: results are seen by polling, so the nap bounds their delay
+                    sleep(min(gap - 2e-4, 2e-4))
             else:
                 sleep(2e-5)
-    wall = (clock() - t0) * 1e-9
+    end = clock()
+    wall = (end - t0) * 1e-9
+    first = min((st.started_ns for st in done if st.started_ns is not None), default=end)
+    span = (end - first) * 1e-9
+    # rec_s_per_s counts the admissions' time too; rec_s_per_s_streaming starts
+    # at the first stream's start
     return dict(wall_s=wall, rec_s=samples / FS, rec_s_per_s=samples / FS / wall if wall > 0 else 0.0,
-                streams=done)
+                rec_s_per_s_streaming=samples / FS / span if span > 0 else 0.0, streams=done)

@@ -8,7 +8,8 @@
   and is admitted when another is released; every probe's records are the
   same alone and in the mix (bit-identical: the per-probe work is
   deterministic and the probes share no device memory).
-* A real-time run reports arrival-to-emit latency for every batch.
+* A real-time run reports arrival-to-emit latency for every batch, and its
+  split into host, queueing, device and callback time.
 """
 import numpy as np
 import pytest
@@ -109,6 +110,13 @@ def test_realtime_latency_is_reported():
     for st in out['streams']:
         assert st.latency['batches'] == st.n_blocks
         assert 0 < st.latency['p50_ms'] <= st.latency['p99_ms'] < 1000
+        # the four parts of each batch's latency add up to it
+        parts, lat = np.array(st.latency['parts_ms']), np.array(st.latency['samples_ms'])
+        assert parts.shape == (st.n_blocks, 4)
+        assert np.allclose(parts.sum(1), lat, rtol=0, atol=1e-6)
+        assert np.all(parts[:, 0] >= 0) and np.all(parts[:, 2] > 0)
+        # device times mapped to the host clock: the offset's error is a few us
+        assert np.all(parts[:, 1] > -0.05) and np.all(parts[:, 3] > -0.05)
     assert out['wall_s'] >= 0.35
 
 
