@@ -145,15 +145,19 @@ static int set_mixing(lss_handle* h, const float* M) {
         CK(cudaMemcpyAsync(h->Mw.p, h->Wrot.p, (size_t)C * C * sizeof(float), cudaMemcpyDeviceToDevice, 0));
         return rebuild_uw(h);
     }
+    const size_t cc = (size_t)C * C;
     if (!h->m_pin) {
-        CK(cudaHostAlloc(reinterpret_cast<void**>(&h->m_pin), (size_t)C * C * sizeof(float), cudaHostAllocDefault));
-        CK(cudaEventCreateWithFlags(&h->m_pin_ev, cudaEventDisableTiming));
-    } else {
-        CK(cudaEventSynchronize(h->m_pin_ev));  // the previous upload has left the staging buffer
+        CK(cudaHostAlloc(reinterpret_cast<void**>(&h->m_pin), lss_handle::M_PIN_SLOTS * cc * sizeof(float),
+                         cudaHostAllocDefault));
+        for (cudaEvent_t& e : h->m_pin_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
-    std::memcpy(h->m_pin, M, (size_t)C * C * sizeof(float));
-    CK(cudaMemcpyAsync(h->Mdrift.p, h->m_pin, (size_t)C * C * sizeof(float), cudaMemcpyHostToDevice, 0));
-    CK(cudaEventRecord(h->m_pin_ev, 0));
+    const int k = h->m_pin_next;
+    h->m_pin_next = (k + 1) % lss_handle::M_PIN_SLOTS;
+    CK(cudaEventSynchronize(h->m_pin_ev[k]));  // the slot's previous upload has left it
+    float* slot = h->m_pin + k * cc;
+    std::memcpy(slot, M, cc * sizeof(float));
+    CK(cudaMemcpyAsync(h->Mdrift.p, slot, cc * sizeof(float), cudaMemcpyHostToDevice, 0));
+    CK(cudaEventRecord(h->m_pin_ev[k], 0));
     return mix_device_drift(h);
 }
 

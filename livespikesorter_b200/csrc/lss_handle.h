@@ -76,8 +76,12 @@ struct lss_handle {
     cudaEvent_t rc_ev = nullptr;                 // recorded after that copy
     cudaEvent_t mix_ev = nullptr;                // recorded after the whitening-folded templates are rebuilt
     cudaEvent_t batch_ev = nullptr;              // recorded after each batch's work (template rebuilds wait for it)
-    float* m_pin = nullptr;                      // pinned staging of drift matrices
-    cudaEvent_t m_pin_ev = nullptr;              // recorded after m_pin's last upload
+    // pinned staging of drift matrices: a ring, so that a caller submitting
+    // batches ahead waits for the upload M_PIN_SLOTS matrices back, not the last
+    static constexpr int M_PIN_SLOTS = 16;
+    float* m_pin = nullptr;                      // [M_PIN_SLOTS][C][C]
+    cudaEvent_t m_pin_ev[M_PIN_SLOTS] = {};      // recorded after each slot's last upload
+    int m_pin_next = 0;
     DevBuf<int32_t> status_acc;                  // errors of asynchronous batches since the last lss_sync
     bool rc_pending = false;
     int64_t last_scored = 0;                     // samples of the last BF16 scoring
@@ -132,7 +136,8 @@ struct lss_handle {
         if (rc_ev) cudaEventDestroy(rc_ev);
         if (mix_ev) cudaEventDestroy(mix_ev);
         if (batch_ev) cudaEventDestroy(batch_ev);
-        if (m_pin_ev) cudaEventDestroy(m_pin_ev);
+        for (cudaEvent_t e : m_pin_ev)
+            if (e) cudaEventDestroy(e);
         if (m_pin) cudaFreeHost(m_pin);
         status_acc.release();
         if (rc_host) cudaFreeHost(rc_host);

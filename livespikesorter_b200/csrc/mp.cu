@@ -45,6 +45,14 @@ namespace lss {
 constexpr int MP_THREADS = 512;
 constexpr int MP_LIST = 31;                        // spikes that may cover one owned window
 constexpr int MP_MAX_GRID = 1024;
+// U-phase work items: at least MP_ITEMS_PER_WARP items per warp and at most
+// MP_ROWS_PER_ITEM template rows per item (whole 8-row batches)
+#ifndef MP_ITEMS_PER_WARP
+#define MP_ITEMS_PER_WARP 2
+#endif
+#ifndef MP_ROWS_PER_ITEM
+#define MP_ROWS_PER_ITEM 128
+#endif
 constexpr unsigned MP_SPIN_LIMIT = 1u << 24;
 
 __device__ __forceinline__ bool grid_sync(unsigned int* bar, int32_t* status) {
@@ -316,8 +324,8 @@ __global__ void __launch_bounds__(MP_THREADS, 1) k_mp(MPArgs a) {
             const int NW = MP_THREADS / 32;
             const int wid = b * NW + warp, wtot = G * NW;
             const int nch = (2 * nt + 1 + 31) / 32;
-            int nrb = (2 * wtot + total * nch - 1) / (total * nch);
-            nrb = max(nrb, (T + 63) / 64);
+            int nrb = (MP_ITEMS_PER_WARP * wtot + total * nch - 1) / (total * nch);
+            nrb = max(nrb, (T + MP_ROWS_PER_ITEM - 1) / MP_ROWS_PER_ITEM);
             nrb = min(nrb, (T + 7) / 8);
             const int tb = ((T + nrb - 1) / nrb + 7) & ~7;  // whole 8-row batches
             nrb = (T + tb - 1) / tb;
