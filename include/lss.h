@@ -198,11 +198,15 @@ int  lss_sort_batch(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t i
                     int64_t n_batches, int32_t raw_on_device, lss_records* out, void* stream);
 
 /* lss_sort_batch without any host wait, for pipelined submission: the
- * records must be device arrays, the record count is written to count_dev
- * (device or mapped memory) when the batch's work finishes, and errors are
- * collected until lss_sync (which waits for the stream and returns the first
- * error seen). Batches on one stream run in order; drift changes between
- * them (lss_set_drift) wait for the batch before. */
+ * records must be device-accessible (device arrays, or pinned host memory,
+ * which the kernels then write across the bus; out->on_device = 1), the
+ * record count is written to count_dev (device or pinned memory) when the
+ * batch's work finishes, and errors are collected until lss_sync (which waits
+ * for the stream and returns the first error seen). Batches on one stream run
+ * in order; drift changes between them (lss_set_drift) wait for the batch
+ * before. Host rows (raw_on_device = 0) are uploaded on the handle's own
+ * stream into one of two device buffers while the previous batch computes;
+ * pinned rows must stay unchanged until the batch has finished. */
 int  lss_sort_batch_async(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ibatch,
                           int64_t n_batches, int32_t raw_on_device, lss_records* out, int64_t* count_dev,
                           void* stream);

@@ -534,12 +534,15 @@ int lss_set_drift(lss_handle* h, const float* M) {
 // ---------------------------------------------------------------- stages
 // Ingest of one padded batch. Xout (may be null) receives the whitened,
 // drift-corrected batch; *pre_out the highpassed batch before whitening.
-static int run_filter(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ibatch, int64_t n_batches,
-                      int32_t raw_on_device, float* Xout, cudaStream_t s, const float** pre_out = nullptr) {
+// The rows of a batch that are read (Kilosort's batch layout): the first
+// batch is NT + nt rows with the nt leading ones replicated, the last may be
+// short, the others are NT + 2nt.
+static int batch_map(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ibatch, int64_t n_batches,
+                     IngestMap& map) {
     if (!raw || n_rows <= 0) return h->fail(LSS_ERR_ARG, "empty raw batch");
     if (ibatch < 0 || n_batches <= 0 || ibatch >= n_batches) return h->fail(LSS_ERR_ARG, "ibatch out of range");
     const int64_t N = h->N;
-    IngestMap map{};
+    map = IngestMap{};
     if (ibatch == 0) {
         map.lead = h->nt;
         map.nsamp = std::min<int64_t>(n_rows, h->NT + h->nt);
@@ -555,6 +558,14 @@ static int run_filter(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t
         map.nsamp = N;
         map.zero_tail = 0;
     }
+    return LSS_OK;
+}
+
+static int run_filter(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ibatch, int64_t n_batches,
+                      int32_t raw_on_device, float* Xout, cudaStream_t s, const float** pre_out = nullptr) {
+    IngestMap map;
+    int rc = batch_map(h, raw, n_rows, ibatch, n_batches, map);
+    if (rc) return rc;
     const int16_t* src = raw;
     h->mark(0, s);
     if (!raw_on_device) {
@@ -927,10 +938,27 @@ int lss_sort_batch(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ib
     return sort_batch_impl(h, raw, n_rows, ibatch, n_batches, raw_on_device, out, stream, nullptr);
 }
 
+// A pointer the kernels may dereference: device, managed, or pinned host
+// memory (pinned host memory is mapped under unified addressing).
+static bool device_accessible(const void* p) {
+    if (!p) return true;
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type != cudaMemoryTypeUnregistered;
+}
+
 int lss_sort_batch_async(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ibatch, int64_t n_batches,
                          int32_t raw_on_device, lss_records* out, int64_t* count_dev, void* stream) {
     if (!h || !out || !count_dev) return LSS_ERR_ARG;
     if (!out->on_device) return h->fail(LSS_ERR_ARG, "asynchronous batches write device records");
+    for (const void* p : {(const void*)out->time, (const void*)out->template_id, (const void*)out->amplitude,
+                          (const void*)out->pc, (const void*)out->x_pos, (const void*)out->y_pos,
+                          (const void*)out->cluster, (const void*)count_dev})
+        if (!device_accessible(p))
+            return h->fail(LSS_ERR_ARG, "asynchronous records and count must be device or pinned host memory");
     return sort_batch_impl(h, raw, n_rows, ibatch, n_batches, raw_on_device, out, stream, count_dev);
 }
 
@@ -958,11 +986,39 @@ static int sort_batch_impl(lss_handle* h, const int16_t* raw, int64_t n_rows, in
     CK(cudaSetDevice(h->cfg.device));
     cudaStream_t s = (cudaStream_t)stream;
     CK(wait_mixing(h, s));
+    // host rows of an asynchronous batch: upload on the handle's upload stream
+    // into the free one of two device buffers; the batch's stream waits for
+    // the upload, and the buffer is free again once the batch's ingest has
+    // read it, so the next batch's upload runs under this batch's work
+    int up_slot = -1;
+    if (count_dev && !raw_on_device) {
+        IngestMap map;
+        int rc0 = batch_map(h, raw, n_rows, ibatch, n_batches, map);
+        if (rc0) return rc0;
+        if (!h->up_s) {
+            CK(cudaStreamCreateWithFlags(&h->up_s, cudaStreamNonBlocking));
+            for (int i = 0; i < 2; ++i) {
+                CK(h->raw_up[i].alloc((size_t)h->N * h->Cbin));
+                CK(cudaEventCreateWithFlags(&h->up_done[i], cudaEventDisableTiming));
+                CK(cudaEventCreateWithFlags(&h->raw_free[i], cudaEventDisableTiming));
+            }
+        }
+        up_slot = h->raw_next;
+        h->raw_next ^= 1;
+        CK(cudaStreamWaitEvent(h->up_s, h->raw_free[up_slot], 0));
+        CK(cudaMemcpyAsync(h->raw_up[up_slot].p, raw, (size_t)map.nsamp * h->Cbin * sizeof(int16_t),
+                           cudaMemcpyHostToDevice, h->up_s));
+        CK(cudaEventRecord(h->up_done[up_slot], h->up_s));
+        CK(cudaStreamWaitEvent(s, h->up_done[up_slot], 0));
+        raw = h->raw_up[up_slot].p;
+        raw_on_device = 1;
+    }
     // the whitening / drift matrix is folded into the templates (set_mixing), so
     // the scores come from the highpassed batch directly
     const float* Xh = nullptr;
     int rc = run_filter(h, raw, n_rows, ibatch, n_batches, raw_on_device, nullptr, s, &Xh);
     if (rc) return rc;
+    if (up_slot >= 0) CK(cudaEventRecord(h->raw_free[up_slot], s));
     CK(cudaMemsetAsync(h->status.p, 0, sizeof(int32_t), s));
     bool ready = false;
     rc = run_scores(h, Xh, h->ld, h->N, h->B.p, s, &ready, /*folded=*/true);

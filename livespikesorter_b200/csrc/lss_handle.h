@@ -104,6 +104,13 @@ struct lss_handle {
     DevBuf<double> dm_pos, dm_ik;
     float dm_sig = 20.f;
     DevBuf<float> rec_amp, rec_pc;
+    // asynchronous batches from host memory: the rows are uploaded on their
+    // own stream into one of two device buffers, so that a batch's upload
+    // overlaps the work of the batch before it
+    DevBuf<int16_t> raw_up[2];
+    cudaStream_t up_s = nullptr;
+    cudaEvent_t up_done[2] = {}, raw_free[2] = {};
+    int raw_next = 0;
 
     int fail(int code, const std::string& m) {
         err = m;
@@ -118,6 +125,13 @@ struct lss_handle {
         if (cudaGetDevice(&dev) == cudaSuccess && dev != cfg.device) cudaSetDevice(cfg.device);
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
+        if (up_s) cudaStreamSynchronize(up_s);
+        for (int i = 0; i < 2; ++i) {
+            raw_up[i].release();
+            if (up_done[i]) cudaEventDestroy(up_done[i]);
+            if (raw_free[i]) cudaEventDestroy(raw_free[i]);
+        }
+        if (up_s) cudaStreamDestroy(up_s);
         raw.release(); chan_map.release(); sums.release(); taps.release(); Mw.release(); Wrot.release(); Mdrift.release();
         X1.release(); Xh.release(); X.release(); B.release();
         nm.release(); ctcP.release(); wave.release(); wpca.release(); Ucc.release(); Xres.release();

@@ -228,23 +228,32 @@ class Sorter:
             out.update(x=xs[:n], y=ys[:n], cluster=clu[:n])
         return out
 
-    def sort_batch_async(self, raw, ibatch: int, n_batches: int, capacity: int | None = None) -> dict:
-        """``sort_batch`` with device records and no host wait: returns the
-        record tensors and a device ``count``; call ``sync()`` before reading
-        them (it raises the first error the batches met)."""
-        raw_t, raw_dev = self._raw(raw)
+    def records(self, capacity: int | None = None, pinned: bool = False) -> dict:
+        """Record tensors for ``sort_batch_async``: device tensors, or pinned
+        host tensors that the batch's kernels write across the bus."""
         cap = capacity or self.cfg.max_spikes
-        dev = self.device
-        time = torch.empty(cap, dtype=torch.int64, device=dev)
-        tmpl = torch.empty(cap, dtype=torch.int32, device=dev)
-        amp = torch.empty(cap, dtype=torch.float32, device=dev)
-        pc = torch.empty((cap, self.nC, self.K), dtype=torch.float32, device=dev) if self.nC > 0 else None
-        count = torch.zeros(1, dtype=torch.int64, device=dev)
-        rec = LssRecords(time=time.data_ptr(), template_id=tmpl.data_ptr(), amplitude=amp.data_ptr(),
-                         pc=_ptr(pc), capacity=cap, count=0, on_device=1, x_pos=None, y_pos=None, cluster=None)
+        kw = dict(pin_memory=True) if pinned else dict(device=self.device)
+        return dict(time=torch.empty(cap, dtype=torch.int64, **kw), template=torch.empty(cap, dtype=torch.int32, **kw),
+                    amplitude=torch.empty(cap, dtype=torch.float32, **kw),
+                    pc=torch.empty((cap, self.nC, self.K), dtype=torch.float32, **kw) if self.nC > 0 else None,
+                    count=torch.zeros(1, dtype=torch.int64, **kw))
+
+    def sort_batch_async(self, raw, ibatch: int, n_batches: int, capacity: int | None = None,
+                         out: dict | None = None) -> dict:
+        """``sort_batch`` with no host wait: returns the record tensors and
+        ``count`` (new device tensors, or ``out`` from ``records()``); call
+        ``sync()`` before reading them (it raises the first error the batches
+        met). Host rows (pinned) upload under the previous batch's work and
+        must stay unchanged until then."""
+        raw_t, raw_dev = self._raw(raw)
+        o = out if out is not None else self.records(capacity)
+        cap = o['time'].shape[0]
+        rec = LssRecords(time=o['time'].data_ptr(), template_id=o['template'].data_ptr(),
+                         amplitude=o['amplitude'].data_ptr(), pc=_ptr(o['pc']), capacity=cap, count=0, on_device=1,
+                         x_pos=None, y_pos=None, cluster=None)
         self._check(self._lib.lss_sort_batch_async(self._h, raw_t.data_ptr(), raw_t.shape[0], ibatch, n_batches,
-                                                   raw_dev, rec, count.data_ptr(), _stream(self.device)))
-        return dict(time=time, template=tmpl, amplitude=amp, pc=pc, count=count)
+                                                   raw_dev, rec, o['count'].data_ptr(), _stream(self.device)))
+        return o
 
     def sync(self):
         self._check(self._lib.lss_sync(self._h, _stream(self.device)))
