@@ -236,7 +236,7 @@ cudaError_t launch_highpass(const float* X1, int64_t ldx, int32_t C, int64_t N, 
 // truncated impulse response has L <= 1024). One CTA filters two channels at
 // once as the real and imaginary parts of a 4096-point complex signal (the
 // filter is real, so both come out of one transform): the block x[start-L ..
-// start-L+4096) (indices mod N) is transformed by a radix-4 Stockham FFT in
+// start-L+4096) (indices mod N) is transformed by a radix-16 Stockham FFT in
 // shared memory, multiplied by H = conj(FFT(g)) where g holds the taps wrapped
 // around index 0 (a circular correlation), and transformed back; its outputs
 // L .. 4096-L-1 are exact (their taps never wrap inside the block).
