@@ -212,10 +212,7 @@ def run_b200(args):
         gc.enable()
         per = np.array([ev[i].elapsed_time(ev[i + 1]) for i in range(K)])
         tot = float(ev[0].elapsed_time(ev[K]))
-        if dist:
-            t = torch.tensor([tot], device=f'cuda:{local}')
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            tot = float(t.item())
+        tot = max_over_ranks(tot, dist, f'cuda:{local}')
         return tot, per, seen
 
     def step_host_async(i, out):
@@ -269,10 +266,7 @@ def run_b200(args):
         del keep
         per = np.array([ev[i].elapsed_time(ev[i + 1]) for i in range(K)])
         tot = float(ev[0].elapsed_time(ev[K]))
-        if dist:
-            t = torch.tensor([tot], device=f'cuda:{local}')
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            tot = float(t.item())
+        tot = max_over_ranks(tot, dist, f'cuda:{local}')
         return tot, per, s.stats()['launches'] - launches0
 
     K, W = args.steps, max(3, args.warmup)
@@ -342,6 +336,16 @@ def run_b200(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(out))
+
+
+def max_over_ranks(x: float, dist, device) -> float:
+    """The largest of every rank's x (x itself without a process group): a
+    multi-GPU step time is the slowest rank's."""
+    if not dist:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def profile_traffic(name):
