@@ -288,40 +288,43 @@ __device__ __forceinline__ void dft16(float2 v[16]) {
     for (int i = 0; i < 16; ++i) v[i] = t[i];
 }
 
-// One radix-16 Stockham pass (L = 1, 16, 256 known at compile time).
+// One radix-16 Stockham pass (L = 1, 16, 256 known at compile time), in
+// place: one butterfly per thread (blockDim.x == HF / 16), every thread reads
+// its 16 inputs before any thread writes. One buffer instead of two lets four
+// CTAs share an SM.
 template <int L>
-__device__ __forceinline__ void fft16_pass(const float2* a, float2* b, const float2* __restrict__ tw) {
+__device__ __forceinline__ void fft16_pass(float2* a, const float2* __restrict__ tw) {
     constexpr int step = HF / (16 * L);
     constexpr int lg = (L == 1) ? 0 : (L == 16) ? 4 : 8;
-    for (int j = threadIdx.x; j < HF / 16; j += blockDim.x) {
-        const int k = j & (L - 1), m = j >> lg;
-        float2 v[16];
+    const int j = threadIdx.x;
+    const int k = j & (L - 1), m = j >> lg;
+    float2 v[16];
 #pragma unroll
-        for (int i = 0; i < 16; ++i) v[i] = a[pad16(j + (HF / 16) * i)];
-        if (L > 1) {
+    for (int i = 0; i < 16; ++i) v[i] = a[pad16(j + (HF / 16) * i)];
+    if (L > 1) {
 #pragma unroll
-            for (int i = 1; i < 16; ++i) v[i] = cmul(v[i], __ldg(tw + ((i * k * step) & (HF - 1))));
-        }
-        dft16(v);
-        const int base = m * 16 * L + k;
-#pragma unroll
-        for (int i = 0; i < 16; ++i) b[pad16(base + L * i)] = v[i];
+        for (int i = 1; i < 16; ++i) v[i] = cmul(v[i], __ldg(tw + ((i * k * step) & (HF - 1))));
     }
+    dft16(v);
+    __syncthreads();
+    const int base = m * 16 * L + k;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) a[pad16(base + L * i)] = v[i];
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(256) k_highpass_fft(const float* __restrict__ X1, int64_t ldx, int32_t C, int64_t N,
-                                                      int32_t L, const float2* __restrict__ H,
-                                                      const float2* __restrict__ tw, float* __restrict__ Xh) {
-    extern __shared__ float2 fbuf[];
-    float2* A = fbuf;
-    float2* Bb = fbuf + HFP;
+constexpr int HF_THREADS = HF / 16;
+
+__global__ void __launch_bounds__(HF_THREADS, 4) k_highpass_fft(const float* __restrict__ X1, int64_t ldx, int32_t C,
+                                                               int64_t N, int32_t L, const float2* __restrict__ H,
+                                                               const float2* __restrict__ tw, float* __restrict__ Xh) {
+    extern __shared__ float2 A[];  // [HFP]: one padded 4096-point buffer, transformed in place
     const int c1 = 2 * blockIdx.y, c2 = c1 + 1;
     const bool two = c2 < C;
     const int64_t start = (int64_t)blockIdx.x * (HF - 2 * L);
     const float* x1 = X1 + (int64_t)c1 * ldx;
     const float* x2 = X1 + (int64_t)(two ? c2 : c1) * ldx;
-    for (int n = threadIdx.x; n < HF; n += blockDim.x) {
+    for (int n = threadIdx.x; n < HF; n += HF_THREADS) {
         int64_t g = start - L + n;  // circular index (the modulo only near the ends)
         if (g < 0 || g >= N) {
             g %= N;
@@ -330,21 +333,20 @@ __global__ void __launch_bounds__(256) k_highpass_fft(const float* __restrict__ 
         A[pad16(n)] = make_float2(x1[g], two ? x2[g] : 0.f);
     }
     __syncthreads();
-    // passes: A -> Bb -> A -> Bb
-    fft16_pass<1>(A, Bb, tw);
-    fft16_pass<16>(Bb, A, tw);
-    fft16_pass<256>(A, Bb, tw);
+    fft16_pass<1>(A, tw);
+    fft16_pass<16>(A, tw);
+    fft16_pass<256>(A, tw);
     // conj(Z * H): the second forward transform then gives conj(F * y)
-    for (int n = threadIdx.x; n < HF; n += blockDim.x) {
-        const float2 z = cmul(Bb[pad16(n)], __ldg(H + n));
-        Bb[pad16(n)] = make_float2(z.x, -z.y);
+    for (int n = threadIdx.x; n < HF; n += HF_THREADS) {
+        const float2 z = cmul(A[pad16(n)], __ldg(H + n));
+        A[pad16(n)] = make_float2(z.x, -z.y);
     }
     __syncthreads();
-    fft16_pass<1>(Bb, A, tw);
-    fft16_pass<16>(A, Bb, tw);
-    fft16_pass<256>(Bb, A, tw);
+    fft16_pass<1>(A, tw);
+    fft16_pass<16>(A, tw);
+    fft16_pass<256>(A, tw);
     const float inv = 1.f / (float)HF;
-    for (int n = L + threadIdx.x; n < HF - L; n += blockDim.x) {
+    for (int n = L + threadIdx.x; n < HF - L; n += HF_THREADS) {
         const int64_t i = start + (n - L);
         if (i >= N) break;
         const float2 r = A[pad16(n)];
@@ -356,10 +358,10 @@ __global__ void __launch_bounds__(256) k_highpass_fft(const float* __restrict__ 
 cudaError_t launch_highpass_fft(const float* X1, int64_t ldx, int32_t C, int64_t N, int32_t L, const float2* H,
                                 const float2* tw, float* Xh, cudaStream_t s) {
     if (L > 1024) return cudaErrorInvalidValue;
-    const size_t smem = 2 * HFP * sizeof(float2);
+    const size_t smem = HFP * sizeof(float2);
     cudaFuncSetAttribute(k_highpass_fft, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     dim3 grid((unsigned)((N + (HF - 2 * L) - 1) / (HF - 2 * L)), (unsigned)((C + 1) / 2));
-    k_highpass_fft<<<grid, 256, smem, s>>>(X1, ldx, C, N, L, H, tw, Xh);
+    k_highpass_fft<<<grid, HF_THREADS, smem, s>>>(X1, ldx, C, N, L, H, tw, Xh);
     return cudaGetLastError();
 }
 
