@@ -168,10 +168,10 @@ def run_b200(args):
         s.set_drift(drifts[j])
         return s.sort_batch(rows_h[j] if host else rows_d[j], ids[j], nb, on_device=not host)
 
-    def step_async(i):
+    def step_async(i, out):
         j = i % len(ids)
         s.set_drift(drifts[j])
-        return s.sort_batch_async(rows_d[j], ids[j], nb)
+        return s.sort_batch_async(rows_d[j], ids[j], nb, out=out)
 
     ring = [s.records(32768, pinned=True) for _ in range(E2E_RING)]
 
@@ -237,11 +237,14 @@ def run_b200(args):
         """Device-resident steps are submitted back to back (lss_sort_batch_async,
         one host wait at the end); host-buffer steps go through lss_sort_batch
         with its host copies and wait."""
+        # device record sets of every timed step, allocated before the timed
+        # region (the results stay valid until the final sync)
+        outs = [] if host else [s.records() for _ in range(max(K, W))]
         for i in range(W):
             if host:
                 step(i, host)
             else:
-                step_async(i)
+                step_async(i, outs[i])
         if not host:
             s.sync()
         gc.collect()
@@ -251,19 +254,18 @@ def run_b200(args):
         torch.cuda.synchronize()
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(K + 1)]
         launches0 = s.stats()['launches']
-        keep = []
         ev[0].record(stream)
         for i in range(K):
             if host:
                 step(i, host)
             else:
-                keep.append(step_async(i))
+                step_async(i, outs[i])
             ev[i + 1].record(stream)
         if not host:
             s.sync()
         torch.cuda.synchronize()
         gc.enable()
-        del keep
+        del outs
         per = np.array([ev[i].elapsed_time(ev[i + 1]) for i in range(K)])
         tot = float(ev[0].elapsed_time(ev[K]))
         tot = max_over_ranks(tot, dist, f'cuda:{local}')
