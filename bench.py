@@ -26,6 +26,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import threading
 import time
 from pathlib import Path
@@ -86,7 +87,7 @@ class Clocks:
         self.index = index
         self.period_ms = period_ms
         self.proc = None
-        self.path = ROOT / 'gpurun_out' / f'clocks_{os.getpid()}.csv'
+        self.path = Path(tempfile.gettempdir()) / f'lss_clocks_{os.getpid()}.csv'
 
     def __enter__(self):
         try:
