@@ -14,6 +14,8 @@
 // consumed from the other shared-memory buffer.
 #include "lss_kernels.cuh"
 
+#include <cuda_bf16.h>
+
 namespace lss {
 
 constexpr int GBM = 128, GBN = 128, GBK = 8;
@@ -92,10 +94,115 @@ __global__ void __launch_bounds__(256) k_sgemm(const float* __restrict__ A, int6
     }
 }
 
+// Small products (the C x C drift/whitening product, the folded templates)
+// give the 128x128 tiling a handful of CTAs; they run on 64x64 tiles instead
+// (BK = 16, 4x4 outputs per thread). Each output is the same FMA chain over
+// k in ascending order, so the two tilings give identical bits.
+constexpr int SBM = 64, SBN = 64, SBK = 16;
+
+struct StorePlain {
+    float* Cm;
+    int64_t ldc;
+    __device__ void operator()(int m, int n, float v) const { Cm[(int64_t)m * ldc + n] = v; }
+};
+
+// Folded-template layout of the score GEMM: row m = t*K + k, column n = c'
+// goes to [t, c'*K + k] of a row-stride-ldk array, as bf16 or as the tf32
+// split hi = rna(v), lo = v - hi.
+struct StoreFolded {
+    int K;
+    int64_t ldk;
+    __nv_bfloat16* out16;
+    float* hi;
+    float* lo;
+    __device__ void operator()(int m, int n, float v) const {
+        const int t = m / K, k = m - (m / K) * K;
+        const int64_t o = (int64_t)t * ldk + (int64_t)n * K + k;
+        if (out16) {
+            out16[o] = __float2bfloat16_rn(v);
+        } else {
+            uint32_t r;
+            asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
+            const float h = __uint_as_float(r);
+            hi[o] = h;
+            lo[o] = __fsub_rn(v, h);
+        }
+    }
+};
+
+template <class Store>
+__global__ void __launch_bounds__(256) k_sgemm64(const float* __restrict__ A, int64_t lda,
+                                                 const float* __restrict__ B, int64_t ldb, int M, int N, int K,
+                                                 Store store) {
+    __shared__ __align__(16) float As[SBK][SBM];
+    __shared__ __align__(16) float Bs[SBK][SBN];
+    const int tid = threadIdx.x;
+    const int m0 = blockIdx.y * SBM, n0 = blockIdx.x * SBN;
+    const int tx = tid & 15, ty = tid >> 4;
+    float acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
+    for (int k0 = 0; k0 < K; k0 += SBK) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int idx = tid + 256 * i;                 // 0 .. 1023
+            const int kk = idx & (SBK - 1), mm = idx >> 4;  // A slab: 64 rows x 16 k
+            const int gm = m0 + mm, gk = k0 + kk;
+            As[kk][mm] = (gm < M && gk < K) ? A[(int64_t)gm * lda + gk] : 0.f;
+            const int nn = idx & (SBN - 1), kb = idx >> 6;  // B slab: 16 k x 64 columns
+            const int gn = n0 + nn, gkb = k0 + kb;
+            Bs[kb][nn] = (gn < N && gkb < K) ? B[(int64_t)gkb * ldb + gn] : 0.f;
+        }
+        __syncthreads();
+        const int kn = min(SBK, K - k0);
+#pragma unroll
+        for (int kk = 0; kk < SBK; ++kk) {
+            if (kk < kn) {  // no terms past K: the chain is exactly k = 0 .. K-1
+                const float4 a = *reinterpret_cast<const float4*>(&As[kk][ty * 4]);
+                const float4 b = *reinterpret_cast<const float4*>(&Bs[kk][tx * 4]);
+                const float av[4] = {a.x, a.y, a.z, a.w};
+                const float bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int gm = m0 + ty * 4 + i;
+        if (gm >= M) continue;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int gn = n0 + tx * 4 + j;
+            if (gn < N) store(gm, gn, acc[i][j]);
+        }
+    }
+}
+
 cudaError_t launch_sgemm(const float* A, int64_t lda, const float* B, int64_t ldb, float* Cm, int64_t ldc,
                          int M, int N, int K, cudaStream_t s) {
+    // fewer 128x128 tiles than a B200 has SMs: 64x64 tiles
+    const int64_t big_ctas = (int64_t)((N + GBN - 1) / GBN) * ((M + GBM - 1) / GBM);
+    if (big_ctas < 148) {
+        dim3 grid((N + SBN - 1) / SBN, (M + SBM - 1) / SBM);
+        k_sgemm64<StorePlain><<<grid, 256, 0, s>>>(A, lda, B, ldb, M, N, K, StorePlain{Cm, ldc});
+        return cudaGetLastError();
+    }
     dim3 grid((N + GBN - 1) / GBN, (M + GBM - 1) / GBM);
     k_sgemm<<<grid, 256, 0, s>>>(A, lda, B, ldb, Cm, ldc, M, N, K);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sgemm_folded(const float* U, const float* Mw, int32_t T, int32_t K, int32_t C, int64_t ldk,
+                                __nv_bfloat16* out16, float* hi, float* lo, cudaStream_t s) {
+    // rows t*K + k of U [T, K, C] (row-major, stride C) times Mw [C, C]
+    dim3 grid((C + SBN - 1) / SBN, (T * K + SBM - 1) / SBM);
+    k_sgemm64<StoreFolded><<<grid, 256, 0, s>>>(U, C, Mw, C, T * K, C, C, StoreFolded{K, ldk, out16, hi, lo});
     return cudaGetLastError();
 }
 

@@ -39,6 +39,10 @@ cudaError_t launch_highpass_fft(const float* X1, int64_t ldx, int32_t C, int64_t
 // ---- dense FP32 GEMM (gemm_fp32.cu): C[M,N] = A[M,K] @ B[K,N], row-major ----
 cudaError_t launch_sgemm(const float* A, int64_t lda, const float* B, int64_t ldb, float* Cm, int64_t ldc,
                          int M, int N, int K, cudaStream_t s);
+// rows t*K + k of U [T, K, C] times Mw [C, C], stored as the score GEMM's
+// folded templates ([t, c'*K + k], bf16 or tf32 hi/lo)
+cudaError_t launch_sgemm_folded(const float* U, const float* Mw, int32_t T, int32_t K, int32_t C, int64_t ldk,
+                                __nv_bfloat16* out16, float* hi, float* lo, cudaStream_t s);
 
 // ---- temporal basis projection (score.cu) ----
 // transposed bf16 variant for the tensor-core GEMM: B0T[s, c*K + k], row stride ldk

@@ -192,54 +192,12 @@ cudaError_t launch_pca_proj_tiles_tf32(const float* X, int64_t ldx, int32_t C, i
 //   U_w[t, c'*K + k] = sum_c U[t, k, c] * Mw[c, c']       (Mw = M @ Wrot)
 // so that sum_kk U_w[t, kk] * P[s, kk] over the projection P of the
 // un-whitened batch equals the score of the whitened batch. Stored as bf16
-// (BF16 path) or as a tf32 hi/lo split (FP32 path), rows [Tpad, ldk].
-// CTA: 128 output channels c' x UW_ROWS rows (t, k); U rows staged in shared
-// memory, each Mw element loaded once per UW_ROWS FMAs; every output still
-// sums over c in order.
-constexpr int UW_ROWS = 4;
-__global__ void __launch_bounds__(128) k_build_uw(const float* __restrict__ U, const float* __restrict__ Mw,
-                                                  int32_t T, int32_t K, int32_t C, int64_t ldk,
-                                                  __nv_bfloat16* __restrict__ out16, float* __restrict__ hi,
-                                                  float* __restrict__ lo) {
-    extern __shared__ float us[];  // [UW_ROWS][C]
-    const int cp = blockIdx.x * blockDim.x + threadIdx.x;
-    const int tk0 = blockIdx.y * UW_ROWS;
-    const int nr = min(UW_ROWS, T * K - tk0);
-    for (int e = threadIdx.x; e < nr * C; e += blockDim.x) us[e] = U[(int64_t)tk0 * C + e];
-    __syncthreads();
-    if (cp >= C) return;
-    float acc[UW_ROWS];
-#pragma unroll
-    for (int r = 0; r < UW_ROWS; ++r) acc[r] = 0.f;
-    for (int c = 0; c < C; ++c) {
-        const float m = Mw[(int64_t)c * C + cp];
-#pragma unroll
-        for (int r = 0; r < UW_ROWS; ++r)
-            if (r < nr) acc[r] = fmaf(us[r * C + c], m, acc[r]);
-    }
-    for (int r = 0; r < nr; ++r) {
-        const int tk = tk0 + r, t = tk / K, k = tk % K;
-        const int64_t o = (int64_t)t * ldk + (int64_t)cp * K + k;
-        if (out16) {
-            out16[o] = __float2bfloat16_rn(acc[r]);
-        } else {
-            const float h = tf32_rna(acc[r]);
-            hi[o] = h;
-            lo[o] = __fsub_rn(acc[r], h);
-        }
-    }
-}
-
+// (BF16 path) or as a tf32 hi/lo split (FP32 path), rows [Tpad, ldk]. The
+// product is the 64x64-tile FP32 GEMM with a store into that layout; every
+// output sums over c in order.
 cudaError_t launch_build_uw(const float* U, const float* Mw, int32_t T, int32_t K, int32_t C, int64_t ldk,
                             __nv_bfloat16* out16, float* hi, float* lo, cudaStream_t s) {
-    const size_t smem = sizeof(float) * (size_t)UW_ROWS * C;
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(k_build_uw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-    }
-    dim3 grid((unsigned)((C + 127) / 128), (unsigned)((T * K + UW_ROWS - 1) / UW_ROWS));
-    k_build_uw<<<grid, 128, smem, s>>>(U, Mw, T, K, C, ldk, out16, hi, lo);
-    return cudaGetLastError();
+    return launch_sgemm_folded(U, Mw, T, K, C, ldk, out16, hi, lo, s);
 }
 
 
