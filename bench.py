@@ -326,14 +326,15 @@ def run_b200(args):
                      'latency_ms_p50': float(np.percentile(per_s, 50)),
                      'latency_ms_p99': float(np.percentile(per_s, 99))},
         'latency_ms_p50': float(np.percentile(per, 50)), 'latency_ms_p99': float(np.percentile(per, 99)),
-        'roofline': roof, 'gpu_launches': int(launches), 'clocks': clocks,
+        'roofline': roof, 'roofline_path': path_roofline(setup, float(np.mean(spikes)), T, value / world, hbm, tfl, src),
+        'gpu_launches': int(launches), 'clocks': clocks,
         'stage_ms': mean_st, 'spikes_per_batch': float(np.mean(spikes)), 'rounds_per_batch': float(np.mean(rounds)),
         'step_ms': [round(float(v), 3) for v in per],
     }
     if args.precision == 'bf16':
         out['bf16'] = bf16_report(s, setup, local, rows_d, drifts, ids, nb)
     if rank == 0 and not args.no_cpu_baseline:
-        out['cpu_baseline'] = cpu_baseline(setup, rec, budget_s=20.0)
+        out['cpu_baseline'] = cpu_baseline(setup, rec)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -349,6 +350,25 @@ def max_over_ranks(x: float, dist, device) -> float:
     t = torch.tensor([x], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def path_roofline(setup, spikes_per_batch, T, rec_s_per_s, hbm_gbs, tensor_tflops, src):
+    """The whole path against both bounds: algorithmic FLOPs and bytes per
+    recording-second (whitening/drift C^2, temporal basis C*K*nt, score GEMM
+    T*K*C per sample, plus 2*T*(2nt+1) FLOPs and 12*T*(2nt+1) bytes per
+    accepted spike; int16 in and the score field written and read once),
+    times the measured rate."""
+    C, K, nt = setup.C, setup.K, setup.nt
+    L2 = 2 * nt + 1
+    S = spikes_per_batch / (setup.NT / FS)  # accepted spikes per recording-second
+    flops = 2.0 * FS * (C * C + C * K * nt + T * K * C) + S * 2.0 * T * L2
+    nbytes = 2.0 * C * FS + 8.0 * T * FS + S * 12.0 * T * L2
+    f_t = flops * rec_s_per_s / 1e12 / tensor_tflops
+    f_h = nbytes * rec_s_per_s / 1e9 / hbm_gbs
+    return {'flops_per_rec_s': flops, 'bytes_per_rec_s': nbytes,
+            'tflops': flops * rec_s_per_s / 1e12, 'gbs': nbytes * rec_s_per_s / 1e9,
+            'frac_tensor': f_t, 'frac_hbm': f_h, 'bound': 'hbm' if f_h >= f_t else 'tensor',
+            'frac': max(f_t, f_h), 'peaks': f'{src}: HBM {hbm_gbs} GB/s, dense bf16 {tensor_tflops} TFLOP/s'}
 
 
 def profile_traffic(name):
@@ -404,23 +424,39 @@ def oracle_batch(setup, rec, ib, ns=None):
     return len(st)
 
 
-def cpu_baseline(setup, rec, budget_s=20.0):
+def cpu_model():
+    """The host CPU's model name (Linux /proc/cpuinfo), or the platform string."""
+    try:
+        for line in open('/proc/cpuinfo'):
+            if line.startswith('model name'):
+                return line.split(':', 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or platform.machine()
+
+
+def cpu_baseline(setup, rec, n_batches=5, budget_s=60.0):
+    """The oracle on the host cores: one warm-up batch, then n_batches full
+    batches (fewer if budget_s runs out, at least one); rate = batch length in
+    seconds / median seconds per batch."""
     cores = os.cpu_count() or 1
     torch.set_num_threads(cores)
-    oracle_batch(setup, rec, 1, ns=6000)  # warm-up
-    t0 = time.perf_counter()
-    n = 0
-    nb = 0
-    while True:
+    oracle_batch(setup, rec, 1)  # warm-up
+    times = []
+    t_start = time.perf_counter()
+    for nb in range(n_batches):
+        t = time.perf_counter()
         oracle_batch(setup, rec, 1 + nb % N_BATCH_POOL)
-        nb += 1
-        n = time.perf_counter() - t0
-        if n > budget_s or nb >= 3:
+        times.append(time.perf_counter() - t)
+        if time.perf_counter() - t_start > budget_s:
             break
-    rate = nb * setup.NT / FS / n
-    return {'value': rate, 'unit': 'rec-s/s', 'cores': cores, 'kind': 'port',
-            'sample': f'{nb} full batches (60000 samples each) of the same workload through the CPU oracle '
-                      f'(torch {torch.__version__}, {cores} threads): filter + run_matching + PC features'}
+    med = float(np.median(times))
+    return {'value': setup.NT / FS / med, 'unit': 'rec-s/s', 'cores': cores, 'kind': 'port',
+            'seconds_per_batch_median': med, 'cpu': cpu_model(),
+            'sample': f'median of {len(times)} full 60000-sample batches of the same workload (after one warm-up '
+                      f'batch) through the CPU oracle (torch {torch.__version__}, {cores} threads): filter + '
+                      f'run_matching + PC features'}
 
 
 def run_reference(args):
@@ -450,7 +486,7 @@ def run_reference(args):
         times.append(time.perf_counter() - t)
     tot = float(np.sum(times))
     value = args.steps * ns / FS / tot
-    cpu = {'value': value, 'unit': 'rec-s/s', 'cores': cores, 'kind': 'port',
+    cpu = {'value': value, 'unit': 'rec-s/s', 'cores': cores, 'kind': 'port', 'cpu': cpu_model(),
            'sample': f'each step: one {ns}-sample slice (+-61 context) of a 60000-sample batch through the '
                      f'oracle filter + run_matching + PC features, torch CPU, {cores} threads'}
     out = {'metric': METRIC, 'value': value, 'unit': 'rec-s/s', 'n_gpus': args.gpus, 'steps': args.steps,
