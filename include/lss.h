@@ -193,7 +193,9 @@ int  lss_scores(lss_handle* h, const float* X_dev, int64_t N, float* B_dev, void
 
 /* One batch end to end: ingest (a), scores (b), matching pursuit (c), PC
  * features (d), time conversion and first-batch negative-time drop
- * (template_matching.py:46-73). Records are in run_matching order. */
+ * (template_matching.py:46-73). Records are in run_matching order. Rows with
+ * raw_on_device = 1 and records with out->on_device = 1 must be device or
+ * pinned host memory (LSS_ERR_ARG otherwise). */
 int  lss_sort_batch(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ibatch,
                     int64_t n_batches, int32_t raw_on_device, lss_records* out, void* stream);
 

@@ -984,6 +984,16 @@ static int sort_batch_impl(lss_handle* h, const int16_t* raw, int64_t n_rows, in
     if (h->streaming) return h->fail(LSS_ERR_STATE, "handle is owned by a serving loop");
     if (!out->time || !out->template_id || !out->amplitude) return h->fail(LSS_ERR_ARG, "null record arrays");
     CK(cudaSetDevice(h->cfg.device));
+    // a pageable host pointer handed over as device memory would fault in the
+    // kernels: refuse it here
+    if (raw_on_device && !device_accessible(raw))
+        return h->fail(LSS_ERR_ARG, "raw_on_device rows must be device or pinned host memory");
+    if (out->on_device && !count_dev)
+        for (const void* p : {(const void*)out->time, (const void*)out->template_id, (const void*)out->amplitude,
+                              (const void*)out->pc, (const void*)out->x_pos, (const void*)out->y_pos,
+                              (const void*)out->cluster})
+            if (!device_accessible(p))
+                return h->fail(LSS_ERR_ARG, "on_device records must be device or pinned host memory");
     cudaStream_t s = (cudaStream_t)stream;
     CK(wait_mixing(h, s));
     // host rows of an asynchronous batch: upload on the handle's upload stream
