@@ -271,7 +271,8 @@ int  lss_set_drift_shift(lss_handle* h, double dshift);
  * OnlineSpikesPayload (onlineSpikesPayload.h:8-48) in cereal's binary
  * archive layout, `long` fields long_bytes (4 for the reference's Windows
  * build, 8 for LP64) wide. Both write at most cap bytes into buf (NULL: size
- * only) and return the full length, or -1 on bad arguments. */
+ * only) and return the full length, or -1 on bad arguments; a short buffer
+ * gets a prefix (whole lines and a terminating NUL for the spike lines). */
 int64_t lss_format_spike_lines(const lss_records* rec, int64_t recording_offset, int32_t use_cluster, char* buf,
                                int64_t cap);
 int64_t lss_serialize_payload(const lss_records* rec, int64_t recording_offset, int64_t stream_sample_ct,

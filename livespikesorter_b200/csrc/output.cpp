@@ -64,7 +64,9 @@ int64_t lss_format_spike_lines(const lss_records* rec, int64_t recording_offset,
         lss::set_thread_error("lss_format_spike_lines: no cluster array");
         return -1;
     }
-    int64_t len = 0;
+    // whole lines are copied while they fit with room for the terminator;
+    // the return value is always the full length
+    int64_t len = 0, written = 0;
     char line[128];
     for (int64_t i = 0; i < rec->count; ++i) {
         const int64_t id = use_cluster ? rec->cluster[i] : rec->template_id[i];
@@ -73,10 +75,13 @@ int64_t lss_format_spike_lines(const lss_records* rec, int64_t recording_offset,
                                     (long long)(recording_offset + rec->time[i]), (long long)id,
                                     (double)rec->amplitude[i], y);
         if (n < 0) return -1;
-        if (buf && len + n < cap) std::memcpy(buf + len, line, (size_t)n);
+        if (buf && written == len && len + n < cap) {
+            std::memcpy(buf + len, line, (size_t)n);
+            written += n;
+        }
         len += n;
     }
-    if (buf && len < cap) buf[len] = '\0';
+    if (buf && cap > 0) buf[written] = '\0';
     return len;
 }
 

@@ -43,3 +43,39 @@ def test_payload_layout_and_round_trip():
     assert len(b) == 80
     assert struct.unpack_from('<iiQi', b, 0) == (-3, 0, 1, 5)
     assert struct.unpack_from('<Qi', b, 20) == (1, 9)
+
+
+def test_short_buffers_and_bad_arguments():
+    import ctypes
+    from livespikesorter_b200 import _lib
+    from livespikesorter_b200.output import _records, spike_lines
+    lib = _lib.load()
+    r = _rec()
+    full = spike_lines(r)
+    rec, keep = _records(r)
+    # a buffer that holds the first line and a half: the first line, NUL-terminated, full length returned
+    first = full.splitlines(keepends=True)[0]
+    cap = len(first) + 5
+    buf = ctypes.create_string_buffer(b'\xff' * cap, cap)
+    assert lib.lss_format_spike_lines(rec, 0, 0, buf, cap) == len(full)
+    assert buf.value.decode() == first
+    assert lib.lss_format_spike_lines(rec, 0, 0, buf, 0) == len(full)  # nothing written
+    # payload into a short buffer: a prefix of the full payload, nothing past cap
+    n = lib.lss_serialize_payload(rec, 0, 0, 0.0, 0.0, 0, 4, 0, None, 0)
+    whole = (ctypes.c_uint8 * n)()
+    assert lib.lss_serialize_payload(rec, 0, 0, 0.0, 0.0, 0, 4, 0, whole, n) == n
+    part = (ctypes.c_uint8 * (n + 8))(*([0xAB] * (n + 8)))
+    assert lib.lss_serialize_payload(rec, 0, 0, 0.0, 0.0, 0, 4, 0, part, 30) == n
+    assert bytes(part)[30:] == b'\xab' * (n + 8 - 30)
+    k = max(i for i in range(31) if bytes(part)[:i] == bytes(whole)[:i])
+    assert bytes(part)[k:30] == b'\xab' * (30 - k)           # a field that did not fit is not started
+    # bad arguments: -1 and a message
+    assert lib.lss_serialize_payload(rec, 0, 0, 0.0, 0.0, 0, 3, 0, None, 0) == -1
+    assert b'long_bytes' in lib.lss_last_error(None)
+    dev = _lib.LssRecords(time=rec.time, template_id=rec.template_id, amplitude=rec.amplitude, pc=None,
+                          capacity=3, count=3, on_device=1)
+    assert lib.lss_format_spike_lines(dev, 0, 0, None, 0) == -1
+    nocl = _lib.LssRecords(time=rec.time, template_id=rec.template_id, amplitude=rec.amplitude, pc=None,
+                           capacity=3, count=3, on_device=0)
+    assert lib.lss_format_spike_lines(nocl, 0, 1, None, 0) == -1   # clusters asked for, none given
+    del keep
