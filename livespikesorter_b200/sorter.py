@@ -79,6 +79,33 @@ def post_config(xc=None, yc=None, centroids=None, dt: int = 7):
     return cfg, k
 
 
+def check_record_set(o: dict, nC: int, K: int) -> None:
+    """Raises ValueError unless ``o`` is a record set the kernels can write:
+    contiguous tensors of one capacity with the record dtypes (time int64,
+    template int32, amplitude f32, pc f32 [cap, nC, K] or None, count int64),
+    each on the GPU or in pinned host memory. A wrong dtype or a short array
+    would let the kernels write past its end."""
+    want = dict(time=torch.int64, template=torch.int32, amplitude=torch.float32, count=torch.int64)
+    for k, dt in want.items():
+        t = o.get(k)
+        if not isinstance(t, torch.Tensor) or t.dtype != dt or not t.is_contiguous():
+            raise ValueError(f'record set: {k} must be a contiguous {dt} tensor')
+    cap = o['time'].shape[0]
+    if o['time'].dim() != 1 or o['template'].shape != (cap,) or o['amplitude'].shape != (cap,):
+        raise ValueError('record set: time, template and amplitude must be 1-D of one capacity')
+    if o['count'].numel() < 1:
+        raise ValueError('record set: count needs one element')
+    pc = o.get('pc')
+    if pc is not None:
+        if (not isinstance(pc, torch.Tensor) or pc.dtype != torch.float32 or not pc.is_contiguous()
+                or tuple(pc.shape) != (cap, max(nC, 1), K)):
+            raise ValueError(f'record set: pc must be a contiguous float32 [{cap}, {max(nC, 1)}, {K}] tensor')
+    for k in ('time', 'template', 'amplitude', 'pc', 'count'):
+        t = o.get(k)
+        if t is not None and not (t.is_cuda or t.is_pinned()):
+            raise ValueError(f'record set: {k} must be on the GPU or in pinned host memory')
+
+
 def setup_kwargs(setup) -> dict:
     """Constructor arguments of a ``synth.SortSetup``."""
     return dict(U=setup.U, wPCA=setup.wPCA, ctc=setup.ctc, Wrot=setup.Wrot, hp_filter=setup.hp_filter,
@@ -247,6 +274,8 @@ class Sorter:
         must stay unchanged until then."""
         raw_t, raw_dev = self._raw(raw)
         o = out if out is not None else self.records(capacity)
+        if out is not None:
+            check_record_set(o, self.nC, self.K)
         cap = o['time'].shape[0]
         rec = LssRecords(time=o['time'].data_ptr(), template_id=o['template'].data_ptr(),
                          amplitude=o['amplitude'].data_ptr(), pc=_ptr(o['pc']), capacity=cap, count=0, on_device=1,
