@@ -73,3 +73,14 @@ def test_python_api_fails_loudly_without_library(monkeypatch, tmp_path):
     monkeypatch.setattr(_lib, 'LIB_PATH', tmp_path / 'missing.so')
     with pytest.raises(ImportError, match='no CPU fallback'):
         _lib.load()
+
+
+def test_plain_c_program_links_and_calls_the_abi(lib, tmp_path):
+    """include/lss.h is C99 and liblss_b200.so links into a C program."""
+    exe = tmp_path / 'c_caller'
+    libdir = ROOT / 'livespikesorter_b200'
+    subprocess.run(['gcc', '-std=c99', '-Wall', '-Wextra', '-Werror', '-pedantic', '-I', str(ROOT / 'include'),
+                    str(ROOT / 'tests' / 'c' / 'c_caller.c'), '-o', str(exe), '-L', str(libdir), '-llss_b200',
+                    f'-Wl,-rpath,{libdir}'], check=True, capture_output=True, text=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    assert out == '1100,3,12.5,0\n1250,0,0.25,0\ncreate=1 handle=null error=yes\n'
