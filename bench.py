@@ -2,11 +2,17 @@
 
 Workload (one step = one padded 60000-sample batch through the whole path:
 int16 ingest, highpass, whitening + drift, score GEMM, matching pursuit, PC
-features, records): 384-channel staggered probe, 400 templates, NT = 60000,
-linear drift of 5 um/min, FP32 path. Synthetic, seeded recording (no public
-dataset exists for this path). Metric: recording-seconds sorted per second.
+features, records): 384-channel staggered probe, 800 templates of which 10 %
+are near-duplicate pairs (footprint centres 10 um apart), NT = 60000, linear
+drift of 5 um/min, BF16 score GEMM with FP32 re-check of near decisions.
+Synthetic, seeded recording (no public dataset exists for this path). Metric:
+recording-seconds sorted per second. The same line carries the FP32 path's
+rate on the same batches, the BF16 path's spike agreement with it, the BF16
+score error against an FP64 score field, and the FP32 path on the
+400-template workload without near-duplicates.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+    python bench.py --templates 400 --precision fp32      # 400 templates, FP32 path
     python bench.py --workload serving [--duration S]
 
 The serving workload runs four independent 384-channel probes (200, 400,
@@ -49,8 +55,10 @@ def parse():
     p.add_argument('--steps', type=int, default=20)
     p.add_argument('--warmup', type=int, default=3)
     p.add_argument('--impl', default='b200', choices=['b200', 'reference'])
-    p.add_argument('--templates', type=int, default=400)
-    p.add_argument('--precision', default='fp32', choices=['fp32', 'bf16'])
+    p.add_argument('--templates', type=int, default=800,
+                   help='800: templates with 10%% near-duplicate pairs; other counts: no duplicates')
+    p.add_argument('--precision', default='bf16', choices=['fp32', 'bf16'])
+    p.add_argument('--no-extras', action='store_true', help='skip the FP32 / 400-template / FP64 extras')
     p.add_argument('--no-cpu-baseline', action='store_true')
     p.add_argument('--workload', default='batch', choices=['batch', 'serving', 'refine'])
     p.add_argument('--refine-steps', type=int, default=10)
@@ -59,8 +67,11 @@ def parse():
 
 
 def workload(T, rank):
+    """800 templates: 10 % near-duplicate pairs (the headline workload); any
+    other count: the same generator without duplicates. Both drift 5 um/min."""
     from livespikesorter_b200 import synth
-    setup, rec = synth.config(1, duration_s=(N_BATCH_POOL + 2) * 2.0, seed=17 + rank, T=T)
+    cfg = 2 if T == 800 else 1
+    setup, rec = synth.config(cfg, duration_s=(N_BATCH_POOL + 2) * 2.0, seed=17 + rank, T=T)
     return setup, rec
 
 
@@ -71,9 +82,11 @@ def batch_rows(rec, setup, ib):
 
 
 def workload_desc(T, precision):
-    return {'workload': f'384-ch staggered probe, {T} templates, NT=60000 int16 batches (+-61 context), '
+    dup = ' (10% near-duplicate pairs, centres 10 um apart)' if T == 800 else ''
+    path = 'BF16 score GEMM + FP32 re-check' if precision == 'bf16' else 'FP32 (3xTF32 tensor-core) score GEMM'
+    return {'workload': f'384-ch staggered probe, {T} templates{dup}, NT=60000 int16 batches (+-61 context), '
                         f'drift 5 um/min, highpass+whitening+drift, score GEMM, matching pursuit, PC features; '
-                        f'{precision.upper()} path',
+                        f'{path}',
             'channels': 384, 'templates': T, 'batch_samples': 60000, 'nt': 61, 'n_pcs': 6,
             'nearest_chans': 10, 'precision': precision,
             'l2': f'steps rotate over {N_BATCH_POOL} device-resident batches (276 MB int16) and each step '
@@ -331,8 +344,31 @@ def run_b200(args):
         'stage_ms': mean_st, 'spikes_per_batch': float(np.mean(spikes)), 'rounds_per_batch': float(np.mean(rounds)),
         'step_ms': [round(float(v), 3) for v in per],
     }
-    if args.precision == 'bf16':
-        out['bf16'] = bf16_report(s, setup, local, rows_d, drifts, ids, nb)
+    if not args.no_extras:
+        # the FP32 path on the same batches, and the BF16 path's agreement with it
+        s32 = s if args.precision == 'fp32' else Sorter.from_setup(setup, device=local)
+        if s32 is not s:
+            t32, st32 = device_resident_rate(s32, rows_d, drifts, ids, nb, K, W, stream, dist, local)
+            out['fp32_path'] = {'value': world * K * rec_s / (t32 / 1e3), 'unit': 'rec-s/s',
+                                'ms_per_step': t32 / K, 'stage_ms': st32,
+                                'api': 'lss_set_drift + lss_sort_batch_async, device-resident rows, same batches'}
+        if args.precision == 'bf16':
+            out['bf16'] = bf16_report(s, s32, rows_d, drifts, ids, nb)
+            out['bf16']['score_err_fp64'] = fp64_score_error(s, s32, setup, rows_d[0], drifts[0], ids[0], nb)
+        if T != 400:
+            # the 400-template workload without near-duplicates, FP32 path
+            setup4, rec4 = workload(400, rank)
+            s4 = Sorter.from_setup(setup4, device=local)
+            rows4 = [torch.from_numpy(batch_rows(rec4, setup4, ib)).cuda(local) for ib in ids]
+            dr4 = [setup4.drift_matrix(rec4.dshift[ib]) for ib in ids]
+            t4, st4 = device_resident_rate(s4, rows4, dr4, ids, rec4.n_batches, K, W, stream, dist, local)
+            out['t400_fp32'] = {'value': world * K * rec_s / (t4 / 1e3), 'unit': 'rec-s/s', 'ms_per_step': t4 / K,
+                                'stage_ms': st4, 'config': workload_desc(400, 'fp32')}
+            del s4, rows4
+        # the streaming loop: 4 probes, 3 s of real-time arrival each
+        sv = serving_report(local, rank, 3.0, 3)
+        out['serving'] = {k: sv[k] for k in ('metric', 'value', 'unit', 'latency_ms', 'realtime_rec_s_per_s',
+                                             'capacity_rec_s_per_s', 'clocks', 'config')}
     if rank == 0 and not args.no_cpu_baseline:
         out['cpu_baseline'] = cpu_baseline(setup, rec)
     if dist:
@@ -340,6 +376,70 @@ def run_b200(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(out))
+
+
+def device_resident_rate(s, rows_d, drifts, ids, nb, K, W, stream, dist, local):
+    """rec-s/s of K batches submitted back to back from device-resident rows
+    (lss_set_drift + lss_sort_batch_async, one host wait at the end), after W
+    warm-up batches; also the mean per-stage device times of two profiled
+    synchronous batches."""
+    outs = [s.records() for _ in range(max(K, W))]
+    for i in range(W):
+        j = i % len(ids)
+        s.set_drift(drifts[j])
+        s.sort_batch_async(rows_d[j], ids[j], nb, out=outs[i])
+    s.sync()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(K):
+        j = i % len(ids)
+        s.set_drift(drifts[j])
+        s.sort_batch_async(rows_d[j], ids[j], nb, out=outs[i])
+    e1.record(stream)
+    s.sync()
+    torch.cuda.synchronize()
+    tot = max_over_ranks(float(e0.elapsed_time(e1)), dist, f'cuda:{local}')
+    s.set_profiling(True)
+    st = []
+    for i in range(2):
+        s.set_drift(drifts[i % len(ids)])
+        s.sort_batch(rows_d[i % len(ids)], ids[i % len(ids)], nb, on_device=True)
+        st.append(s.stage_times())
+    s.set_profiling(False)
+    stages = {k: float(np.mean([x[k] for x in st])) for k in st[0]}
+    return tot, stages
+
+
+def fp64_score_error(s16, s32, setup, rows_d, drift, ib, nb):
+    """Max and RMS error of the BF16+re-check and the FP32 score fields against
+    an FP64 score field of the same filtered batch (torch float64 conv1d with
+    the temporal basis, then the template contraction: template_matching.py:
+    145-146), over all T x N scores."""
+    s32.set_drift(drift)
+    s16.set_drift(drift)
+    X = s32.filter(rows_d, ib, nb)
+    B16 = s16.scores(X).double()
+    B32 = s32.scores(X).double()
+    nt = setup.nt
+    W = setup.wPCA.double().to(X.device)
+    B0 = torch.nn.functional.conv1d(X.double().unsqueeze(1), W.unsqueeze(1), padding=nt // 2)
+    B64 = torch.einsum('ijk,kjl->il', setup.U.double().to(X.device), B0)
+    scale = float(B64.abs().max())
+    rms64 = float(B64.square().mean().sqrt())
+    out = {}
+    for name, B in (('bf16_recheck', B16), ('fp32', B32)):
+        d = B - B64
+        out[name] = {'max_abs': float(d.abs().max()), 'rms': float(d.square().mean().sqrt()),
+                     'max_rel_to_max_score': float(d.abs().max()) / scale,
+                     'rms_rel_to_rms_score': float(d.square().mean().sqrt()) / rms64}
+    out['fp64_max_abs_score'] = scale
+    out['fp64_rms_score'] = rms64
+    out['scores'] = int(B64.numel())
+    out['batch'] = int(ib)
+    return out
 
 
 def max_over_ranks(x: float, dist, device) -> float:
@@ -382,11 +482,9 @@ def profile_traffic(name):
     return None
 
 
-def bf16_report(s16, setup, local, rows_d, drifts, ids, nb):
+def bf16_report(s16, s32, rows_d, drifts, ids, nb):
     """Untimed: the BF16 path's re-check statistics and its spike agreement
     with the FP32 path over the batch pool ((time, template) pairs)."""
-    from livespikesorter_b200.sorter import Sorter
-    s32 = Sorter.from_setup(setup, device=local)
     near = rescored = flips = common = n32 = n16 = 0
     for j, ib in enumerate(ids):
         s16.set_drift(drifts[j])
@@ -492,7 +590,8 @@ def run_reference(args):
     out = {'metric': METRIC, 'value': value, 'unit': 'rec-s/s', 'n_gpus': args.gpus, 'steps': args.steps,
            'warmup': args.warmup, 'ms_per_step': tot / args.steps * 1e3, 'higher_is_better': True,
            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic', 'impl': 'reference',
-           'config': workload_desc(T, 'fp32') | {'parallelism': 'cpu'},
+           'config': workload_desc(T, 'fp32') | {'parallelism': 'cpu', 'samples_per_step': ns,
+                                                  'batch_samples_of_workload': setup.NT},
            'cpu_baseline': cpu, 'e2e': {'value': value, 'unit': 'rec-s/s', 'h2d_bytes_per_step': 0,
                                         'd2h_bytes_per_step': 0},
            'latency_ms_p50': float(np.percentile(times, 50) * 1e3),
@@ -502,14 +601,24 @@ def run_reference(args):
 
 def run_serving(args):
     """Four probes through the streaming loop: real-time latency, then capacity."""
-    from livespikesorter_b200 import synth
-    from livespikesorter_b200.serve import ProbeServer, Stream, run_streams
-    from livespikesorter_b200.sorter import setup_kwargs
     rank = int(os.environ.get('RANK', 0))
     local = int(os.environ.get('LOCAL_RANK', 0))
     torch.cuda.set_device(local)
+    out = serving_report(local, rank, args.duration, args.warmup)
+    if rank == 0:
+        print(json.dumps(out))
+
+
+def serving_report(local, rank, duration, warmup):
+    """Four 384-channel probes (200/400/600/800 templates, 3000/1500/600/300-
+    sample blocks) through the streaming loop: a real-time run with seeded
+    arrival jitter for latency, then a run with all blocks available at once
+    for capacity."""
+    from livespikesorter_b200 import synth
+    from livespikesorter_b200.serve import ProbeServer, Stream, run_streams
+    from livespikesorter_b200.sorter import setup_kwargs
     blocks = (3000, 1500, 600, 300)
-    probes = synth.streaming_probes(seed=23 + rank, duration_s=args.duration)
+    probes = synth.streaming_probes(seed=23 + rank, duration_s=duration)
 
     def streams(n_blocks=None):
         out = []
@@ -520,7 +629,7 @@ def run_serving(args):
         return out
 
     srv = ProbeServer(device=local, memory_budget=40 << 30, max_probes=8)
-    run_streams(srv, streams(n_blocks=max(3, args.warmup)), realtime=False)            # warm-up
+    run_streams(srv, streams(n_blocks=max(3, warmup)), realtime=False)            # warm-up
     # an NVML clock query stalls the submitting thread for tens of ms, which the
     # real-time run would count as latency: clocks are sampled during the
     # capacity run that follows, on the same streams and kernels
@@ -546,10 +655,10 @@ def run_serving(args):
     out = {
         'metric': 'p99 arrival-to-emit latency, 4 concurrent 384ch probes, 10-100 ms blocks',
         'value': max(v['p99_ms'] for v in lat.values()), 'unit': 'ms', 'higher_is_better': False,
-        'n_gpus': 1, 'steps': int(sum(v['batches'] for v in lat.values())), 'warmup': max(3, args.warmup),
+        'n_gpus': 1, 'steps': int(sum(v['batches'] for v in lat.values())), 'warmup': max(3, warmup),
         'dtype': 'f32', 'data': 'synthetic',
         'config': {'workload': 'serving: 4 probes x 384 ch, T = 200/400/600/800, blocks 3000/1500/600/300 samples, '
-                               f'{args.duration:g} s each, real-time arrival with 20% seeded jitter, '
+                               f'{duration:g} s each, real-time arrival with 20% seeded jitter, '
                                'streaming starts once the four probes are admitted',
                    'parallelism': 'one GPU, probes overlap on separate streams'},
         'latency_ms': lat, 'worst_latencies_ms': worst, 'push_late_max_ms': push_late, 'spikes': spikes,
@@ -558,17 +667,17 @@ def run_serving(args):
         'clocks': clocks,
     }
     srv.close()
-    if rank == 0:
-        print(json.dumps(out))
+    return out
 
 
 def run_refine(args):
     """Template refinement with fixed assignments: 384 ch, 400 templates, 16
     batches rendered from templates whose footprints are shifted 10 um and
     scaled +-10% from the sorter's. Sort every batch with the sorter's
-    templates, then take Adam steps on the residual energy of all 16 batches
-    through the hand-written adjoint; report steps/s and the template error
-    against the rendering templates before and after."""
+    templates, then take Gauss-Newton (Jacobi-preconditioned) steps on the
+    residual energy of all 16 batches through the hand-written adjoint; report
+    steps/s and the template error against the rendering templates before and
+    after."""
     from livespikesorter_b200 import synth
     from livespikesorter_b200.adjoint import refine
     from livespikesorter_b200.sorter import Sorter

@@ -175,8 +175,11 @@ int  lss_match_scores(lss_handle* h, const float* B_dev, int64_t N, int64_t* st_
  * for at most LSS_NOALLOC_MAX_SAMPLES columns; larger batches are rejected
  * with LSS_ERR_ARG. Needs no handle; runs on the calling thread's current
  * device. The first call on a device looks up the array's device address, so
- * make that first call before any stream capture. All calls share the array:
- * calls that overlap on the GPU race, so serialise them.
+ * make that first call before any stream capture; the address is kept for the
+ * life of the process, so do not call this again after cudaDeviceReset on that
+ * device. All calls share the array: calls that overlap on the GPU race, so
+ * serialise them. Every array must be memory of the current device or pinned
+ * host memory (LSS_ERR_ARG otherwise, before any launch).
  * B_dev f32 [T, ldb] is the score field and is updated in place;
  * nm_dev f32 [T]; ctc_permuted_dev f32 [T, T, 2nt+1] = ctc.permute(1,0,2)
  * (the reference's ctc_permuted.npy). Outputs: spike_x / spike_y / spike_amp
@@ -225,6 +228,11 @@ typedef struct lss_stats {
     int64_t recheck_flips;
     int64_t launches;      /* kernels this handle has launched since creation */
     int64_t recheck_rescored;
+    /* matching-pursuit update work items (spike segment x template-row block x
+     * 32 columns) of the last synchronous batch, and how many of them changed
+     * any score: the others were skipped as exact no-ops */
+    int64_t mp_items;
+    int64_t mp_items_updated;
 } lss_stats;
 int  lss_get_stats(const lss_handle* h, lss_stats* out);
 

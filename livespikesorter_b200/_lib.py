@@ -56,7 +56,8 @@ class LssPostConfig(ct.Structure):
 
 class LssStats(ct.Structure):
     _fields_ = [('rounds', ct.c_int32), ('spikes', ct.c_int64), ('recheck_columns', ct.c_int64),
-                ('recheck_flips', ct.c_int64), ('launches', ct.c_int64), ('recheck_rescored', ct.c_int64)]
+                ('recheck_flips', ct.c_int64), ('launches', ct.c_int64), ('recheck_rescored', ct.c_int64),
+                ('mp_items', ct.c_int64), ('mp_items_updated', ct.c_int64)]
 
 
 STAGES = ('h2d_ms', 'ingest_ms', 'highpass_ms', 'whiten_ms', 'project_ms', 'score_ms', 'mp_ms', 'xres_ms',

@@ -127,6 +127,38 @@ int lss::rebuild_uw(lss_handle* h) {
     return LSS_OK;
 }
 
+// Template rows of the block-skipping rounds, ordered along the probe: by the
+// centre of mass, over the channel index, of each template's energy
+// sum_k U[t, k, c]^2 (channels follow the probe's geometry in the channel map,
+// so templates adjacent in this order sit close together and their
+// cross-correlations with distant spikes vanish together). Any order gives the
+// same spikes; this one lets whole blocks be skipped. Then the |ctc| maxima per
+// (spike template, row) and (spike template, block).
+int lss::rebuild_mp_blocks(lss_handle* h) {
+    const int T = h->T, K = h->K, C = h->C, nb = h->mp_nb;
+    std::vector<float> u((size_t)T * K * C);
+    CK(cudaMemcpy(u.data(), h->U.p, u.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    std::vector<double> com(T, 0.0);
+    for (int t = 0; t < T; ++t) {
+        double w = 0.0, wc = 0.0;
+        for (int k = 0; k < K; ++k)
+            for (int c = 0; c < C; ++c) {
+                const double v = u[((size_t)t * K + k) * C + c];
+                w += v * v;
+                wc += v * v * c;
+            }
+        com[t] = w > 0.0 ? wc / w : 0.0;
+    }
+    std::vector<int32_t> perm((size_t)nb * MPB_ROWS, -1);
+    for (int t = 0; t < T; ++t) perm[t] = t;
+    std::stable_sort(perm.begin(), perm.begin() + T, [&](int32_t i, int32_t j) { return com[i] < com[j]; });
+    CK(cudaMemcpy(h->mp_perm.p, perm.data(), perm.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    CK(launch_ctc_block_max(h->ctcP.p, T, 2 * h->nt + 1, h->mp_perm.p, nb, h->mp_cmaxb.p, h->mp_cmaxr.p, 0));
+    CK(cudaDeviceSynchronize());
+    h->stats.launches += 2;
+    return LSS_OK;
+}
+
 int lss::mix_device_drift(lss_handle* h) {
     const int C = h->C;
     CK(launch_sgemm(h->Mdrift.p, C, h->Wrot.p, C, h->Mw.p, C, C, C, C, 0));
@@ -186,6 +218,22 @@ static int validate(const lss_config* c, std::string& err) {
     }
     if (c->batch_size > (1 << 26)) { err = "batch_size too large"; return LSS_ERR_ARG; }
     return LSS_OK;
+}
+
+// A pointer the kernels running on `device` may dereference: memory of that
+// device, managed memory, or pinned host memory (mapped under unified
+// addressing). Pageable host memory and another GPU's memory (no peer access
+// is enabled) are refused; a null pointer passes (optional arrays).
+bool lss::device_accessible(const void* p, int device) {
+    if (!p) return true;
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    if (a.type == cudaMemoryTypeUnregistered) return false;
+    if (a.type == cudaMemoryTypeDevice && a.device != device) return false;
+    return true;
 }
 
 extern "C" {
@@ -283,7 +331,7 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
 
     // one CTA per >= 32 columns (a serving loop lowers it further so that
     // its probes' rounds kernels fit on the device together)
-    h->mp_grid = std::min<int>(mp_max_grid(cfg->device), (int)std::max<int64_t>(1, (h->N + 31) / 32));
+    h->mp_grid = std::min<int>(mp_blocks_max_grid(cfg->device), (int)std::max<int64_t>(1, (h->N + 31) / 32));
     cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, cfg->device);
     h->CKpad = (C * K + 63) / 64 * 64;
     const int64_t cap = cfg->max_spikes;
@@ -368,6 +416,12 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
     ALLOC(cfmax, ld);
     ALLOC(imax, ld);
     ALLOC(colkey, 2 * ld);
+    h->mp_nb = (T + MPB_ROWS - 1) / MPB_ROWS;
+    ALLOC(mp_perm, (size_t)h->mp_nb * MPB_ROWS);
+    ALLOC(mp_cmaxb, (size_t)T * h->mp_nb);
+    ALLOC(mp_cmaxr, (size_t)T * T);
+    ALLOC(mp_bkey, (size_t)h->mp_nb * ld);
+    ALLOC(mp_bmin, (size_t)h->mp_nb * ld);
     ALLOC(blk_cnt, 4096);
     ALLOC(blk_x, ld);
     ALLOC(blk_y, ld);
@@ -487,6 +541,8 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
     CK(cudaEventCreateWithFlags(&h->batch_ev, cudaEventDisableTiming));
     CK(cudaMemcpy(h->Wrot.p, t->whitening, (size_t)C * C * sizeof(float), cudaMemcpyHostToDevice));
     rc = set_mixing(h, t->drift);
+    if (rc) { g_create_err = h->err; return rc; }
+    rc = rebuild_mp_blocks(h);
     if (rc) { g_create_err = h->err; return rc; }
     // the set-up work is on the legacy stream; waiting for it alone leaves
     // other handles' non-blocking streams (a serving loop's probes) running
@@ -683,13 +739,18 @@ int lss::enqueue_mp(lss_handle* h, int64_t N, cudaStream_t s, bool maxima_ready)
     a.counters = h->counters.p;
     a.status = h->status.p;
     a.bar = h->bar.p;
+    a.perm = h->mp_perm.p;
+    a.nb = h->mp_nb;
+    a.cmaxb = h->mp_cmaxb.p;
+    a.cmaxr = h->mp_cmaxr.p;
+    a.bkey = h->mp_bkey.p;
+    a.bmin = h->mp_bmin.p;
     const int G = h->mp_grid;
     a.cols_per_blk = (int)((N + G - 1) / G);
-    a.init_cols = maxima_ready ? 0 : 1;
+    a.init_cols = 1;  // the rounds take their block maxima from the field itself
     if (!maxima_ready) CK(cudaMemsetAsync(h->status.p, 0, sizeof(int32_t), s));
     CK(cudaMemsetAsync(h->counters.p, 0, 4 * sizeof(int32_t), s));
-    CK(cudaMemsetAsync(h->colkey.p, 0, 2 * h->ld * sizeof(unsigned long long), s));
-    CK(launch_mp(a, G, s));
+    CK(launch_mp_blocks(a, G, s));
     h->stats.launches += 1;
     return LSS_OK;
 }
@@ -705,13 +766,15 @@ static int run_mp(lss_handle* h, int64_t N, int32_t* n_out, int32_t* rounds_out,
     h->mark(7, s);
     CK(cudaStreamSynchronize(s));
     if (st & STATUS_TIMEOUT) return h->fail(LSS_ERR_TIMEOUT, "matching pursuit grid barrier timed out");
-    if (st & STATUS_LIST) return h->fail(LSS_ERR_CAPACITY, "more than 32 peaks inside one 2*nt window");
+    if (st & STATUS_LIST) return h->fail(LSS_ERR_CAPACITY, MSG_MP_LIST);
     if (st & STATUS_CAPACITY)
         return h->fail(LSS_ERR_CAPACITY, "more than max_spikes spikes in one batch");
     *n_out = hc[0];
     *rounds_out = hc[1];
     h->stats.rounds = hc[1];
     h->stats.spikes = hc[0];
+    h->stats.mp_items_updated = hc[2];
+    h->stats.mp_items = hc[3];
     return LSS_OK;
 }
 
@@ -938,18 +1001,6 @@ int lss_sort_batch(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ib
     return sort_batch_impl(h, raw, n_rows, ibatch, n_batches, raw_on_device, out, stream, nullptr);
 }
 
-// A pointer the kernels may dereference: device, managed, or pinned host
-// memory (pinned host memory is mapped under unified addressing).
-static bool device_accessible(const void* p) {
-    if (!p) return true;
-    cudaPointerAttributes a{};
-    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-    }
-    return a.type != cudaMemoryTypeUnregistered;
-}
-
 int lss_sort_batch_async(lss_handle* h, const int16_t* raw, int64_t n_rows, int64_t ibatch, int64_t n_batches,
                          int32_t raw_on_device, lss_records* out, int64_t* count_dev, void* stream) {
     if (!h || !out || !count_dev) return LSS_ERR_ARG;
@@ -957,8 +1008,9 @@ int lss_sort_batch_async(lss_handle* h, const int16_t* raw, int64_t n_rows, int6
     for (const void* p : {(const void*)out->time, (const void*)out->template_id, (const void*)out->amplitude,
                           (const void*)out->pc, (const void*)out->x_pos, (const void*)out->y_pos,
                           (const void*)out->cluster, (const void*)count_dev})
-        if (!device_accessible(p))
-            return h->fail(LSS_ERR_ARG, "asynchronous records and count must be device or pinned host memory");
+        if (!lss::device_accessible(p, h->cfg.device))
+            return h->fail(LSS_ERR_ARG,
+                           "asynchronous records and count must be memory of the handle's device or pinned host memory");
     return sort_batch_impl(h, raw, n_rows, ibatch, n_batches, raw_on_device, out, stream, count_dev);
 }
 
@@ -972,7 +1024,7 @@ int lss_sync(lss_handle* h, void* stream) {
     if (st & STATUS_TIMEOUT) return h->fail(LSS_ERR_TIMEOUT, "a bounded device-side wait timed out");
     if (st & STATUS_CAPACITY) return h->fail(LSS_ERR_CAPACITY, "more than max_spikes spikes in one batch");
     if (st & STATUS_LIST)
-        return h->fail(LSS_ERR_CAPACITY, "more than 32 peaks inside one 2*nt window, or a feature list overflow");
+        return h->fail(LSS_ERR_CAPACITY, std::string(MSG_MP_LIST) + ", or a PC-feature neighbour list overflow");
     return LSS_OK;
 }
 
@@ -986,14 +1038,15 @@ static int sort_batch_impl(lss_handle* h, const int16_t* raw, int64_t n_rows, in
     CK(cudaSetDevice(h->cfg.device));
     // a pageable host pointer handed over as device memory would fault in the
     // kernels: refuse it here
-    if (raw_on_device && !device_accessible(raw))
-        return h->fail(LSS_ERR_ARG, "raw_on_device rows must be device or pinned host memory");
+    if (raw_on_device && !lss::device_accessible(raw, h->cfg.device))
+        return h->fail(LSS_ERR_ARG, "raw_on_device rows must be memory of the handle's device or pinned host memory");
     if (out->on_device && !count_dev)
         for (const void* p : {(const void*)out->time, (const void*)out->template_id, (const void*)out->amplitude,
                               (const void*)out->pc, (const void*)out->x_pos, (const void*)out->y_pos,
                               (const void*)out->cluster})
-            if (!device_accessible(p))
-                return h->fail(LSS_ERR_ARG, "on_device records must be device or pinned host memory");
+            if (!lss::device_accessible(p, h->cfg.device))
+                return h->fail(LSS_ERR_ARG,
+                               "on_device records must be memory of the handle's device or pinned host memory");
     cudaStream_t s = (cudaStream_t)stream;
     CK(wait_mixing(h, s));
     // host rows of an asynchronous batch: upload on the handle's upload stream
@@ -1094,9 +1147,11 @@ static int sort_batch_impl(lss_handle* h, const int16_t* raw, int64_t n_rows, in
     if (st & STATUS_TIMEOUT) return h->fail(LSS_ERR_TIMEOUT, "a bounded device-side wait timed out");
     if (st & STATUS_CAPACITY) return h->fail(LSS_ERR_CAPACITY, "more than max_spikes spikes in one batch");
     if (st & STATUS_LIST)
-        return h->fail(LSS_ERR_CAPACITY, "more than 32 peaks inside one 2*nt window, or a feature list overflow");
+        return h->fail(LSS_ERR_CAPACITY, std::string(MSG_MP_LIST) + ", or a PC-feature neighbour list overflow");
     h->stats.spikes = hc[0];
     h->stats.rounds = hc[1];
+    h->stats.mp_items_updated = hc[2];
+    h->stats.mp_items = hc[3];
     out->count = count;
     if (count > cap) return h->fail(LSS_ERR_CAPACITY, "record capacity smaller than the spike count");
     if (!out->on_device && count > 0) {

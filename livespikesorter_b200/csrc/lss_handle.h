@@ -64,6 +64,12 @@ struct lss_handle {
     DevBuf<int32_t> imax, blk_cnt, blk_x, blk_y, sp_x, sp_y, sp_round, round_start, counters, status;
     DevBuf<float> sp_amp, blk_amp;
     DevBuf<unsigned long long> colkey;
+    // block-skipping rounds (mp_blocks.cu): template rows in blocks of
+    // MPB_ROWS ordered along the probe, |ctc| maxima, per-block column state
+    int mp_nb = 0;
+    DevBuf<int32_t> mp_perm;
+    DevBuf<float> mp_cmaxb, mp_cmaxr, mp_bmin;
+    DevBuf<unsigned long long> mp_bkey;
     DevBuf<__nv_bfloat16> B0T, Up16;   // BF16 path: transposed projection, templates
     DevBuf<float> B0T_hi, B0T_lo, Up_hi, Up_lo;  // FP32 path (3xTF32): tf32 hi/lo splits
     DevBuf<__nv_bfloat16> Uw16;                  // templates with the whitening folded in (BF16 path)
@@ -138,6 +144,7 @@ struct lss_handle {
         tF.release(); iCC.release(); iU.release(); cfmax.release(); imax.release(); blk_cnt.release();
         blk_x.release(); blk_y.release(); sp_x.release(); sp_y.release(); sp_round.release();
         round_start.release(); counters.release(); status.release(); sp_amp.release(); blk_amp.release(); colkey.release();
+        mp_perm.release(); mp_cmaxb.release(); mp_cmaxr.release(); mp_bmin.release(); mp_bkey.release();
         bar.release(); rec_time.release(); rec_count.release(); rec_tmpl.release(); rec_slot.release(); rec_amp.release();
         rec_pc.release(); B0T.release(); Up16.release();
         B0T_hi.release(); B0T_lo.release(); Up_hi.release(); Up_lo.release();
@@ -180,6 +187,9 @@ int rebuild_uw(lss_handle* h);
 inline cudaError_t wait_mixing(lss_handle* h, cudaStream_t s) {
     return h->mix_ev ? cudaStreamWaitEvent(s, h->mix_ev, 0) : cudaSuccess;
 }
+// Template order and |ctc| maxima of the block-skipping rounds (after the
+// templates or ctc change; synchronous).
+int rebuild_mp_blocks(lss_handle* h);
 // Mw = Mdrift @ Wrot with Mdrift already on the device, then rebuild_uw.
 int mix_device_drift(lss_handle* h);
 // Matching-pursuit rounds on h->B, enqueued only (counts stay on the device).

@@ -130,11 +130,34 @@ struct MPArgs {
     unsigned int* bar;        // [2] grid barrier count / generation, zero at launch
     int32_t cols_per_blk;     // W
     int32_t init_cols;        // 1: compute column maxima of B before round 0
+    // block-skipping rounds (mp_blocks.cu) only: template rows are grouped in
+    // blocks of MPB_ROWS (rows of templates close on the probe, by perm)
+    const int32_t* perm = nullptr;          // [nb * MPB_ROWS] template of each block row, -1 past T
+    int32_t nb = 0;                         // row blocks
+    const float* cmaxb = nullptr;           // [T(spike template), nb] max |ctc| over a block's rows and lags
+    const float* cmaxr = nullptr;           // [T(spike template), T(row)] max |ctc| over lags
+    unsigned long long* bkey = nullptr;     // [nb, ldk] per block and column: max (Cf bits << 32 | ~t)
+    float* bmin = nullptr;                  // [nb, ldk] per block and column: min |B|
 };
 enum : int32_t { STATUS_TIMEOUT = 1, STATUS_CAPACITY = 2, STATUS_LIST = 4 };
 cudaError_t launch_mp(MPArgs a, int grid, cudaStream_t s);
+// the same rounds, skipping (spike, row block) updates that provably leave
+// every score of the block unchanged; needs perm, nb, cmaxb, cmaxr, bkey, bmin
+constexpr int MPB_ROWS = 32;
+cudaError_t launch_mp_blocks(MPArgs a, int grid, cudaStream_t s);
+int mp_blocks_max_grid(int device);
+// per (spike template, block) and (spike template, row) maxima of |ctc| over lags
+cudaError_t launch_ctc_block_max(const float* ctcP, int32_t T, int32_t L2, const int32_t* perm, int32_t nb,
+                                 float* cmaxb, float* cmaxr, cudaStream_t s);
 int mp_max_grid(int device);
 void set_thread_error(const char* msg);
+// true when kernels on `device` may dereference p (that device's memory,
+// managed or pinned host memory) or p is null
+bool device_accessible(const void* p, int device);
+// the rounds' per-column spike lists hold MP_LIST spikes; more peaks than that
+// whose windows reach one column in one round overflow them (STATUS_LIST)
+constexpr int MP_LIST = 31;
+constexpr const char* MSG_MP_LIST = "more than 31 peaks within 2*nt samples of one another in one round";
 cudaError_t launch_status_or(const int32_t* st, int32_t* acc, cudaStream_t s);
 
 // ---- residual and PC features (features.cu); n = spikes of the batch ----

@@ -35,6 +35,7 @@
 // writes during the kernel is read with ld.global.cg (L2), never through the
 // non-coherent L1.
 #include "lss_kernels.cuh"
+#include "mp_common.cuh"
 
 #include <algorithm>
 #include <cfloat>
@@ -43,7 +44,7 @@
 namespace lss {
 
 constexpr int MP_THREADS = 512;
-constexpr int MP_LIST = 31;                        // spikes that may cover one owned window
+static_assert(MP_LIST == 31, "MSG_MP_LIST names the list length");
 constexpr int MP_MAX_GRID = 1024;
 // U-phase work items: at least MP_ITEMS_PER_WARP items per warp and at most
 // MP_ROWS_PER_ITEM template rows per item (whole 8-row batches)
@@ -53,129 +54,6 @@ constexpr int MP_MAX_GRID = 1024;
 #ifndef MP_ROWS_PER_ITEM
 #define MP_ROWS_PER_ITEM 128
 #endif
-constexpr unsigned MP_SPIN_LIMIT = 1u << 24;
-
-__device__ __forceinline__ bool grid_sync(unsigned int* bar, int32_t* status) {
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        volatile unsigned int* vgen = bar + 1;
-        const unsigned int gen = *vgen;
-        __threadfence();
-        const unsigned int arrived = atomicAdd(bar, 1u);
-        int ok = 1;
-        if (arrived == gridDim.x - 1) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            unsigned int spins = 0;
-            while (*vgen == gen) {
-                ++spins;
-                if ((spins & 255u) == 0u && (*(volatile int32_t*)status & STATUS_TIMEOUT)) {
-                    ok = 0;
-                    break;
-                }
-                if (spins > MP_SPIN_LIMIT) {
-                    atomicOr(status, STATUS_TIMEOUT);
-                    ok = 0;
-                    break;
-                }
-                if (spins > 64) __nanosleep(32);
-            }
-        }
-        __threadfence();
-        s_ok = ok;
-    }
-    __syncthreads();
-    return s_ok != 0;
-}
-
-// L2 residency: the score field is read-modify-written every round and fits
-// in L2 for a few hundred templates, while each spike's ctc slice is read once
-// per spike, so the field is kept (evict_last) and ctc streamed (evict_first).
-__device__ __forceinline__ uint64_t policy_keep() {
-    uint64_t p;
-    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
-    return p;
-}
-__device__ __forceinline__ uint64_t policy_stream() {
-    uint64_t p;
-    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
-    return p;
-}
-__device__ __forceinline__ float ld_keep(const float* a, uint64_t pol) {
-    float v;
-    asm volatile("ld.global.cg.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
-    return v;
-}
-__device__ __forceinline__ void st_keep(float* a, float v, uint64_t pol) {
-    asm volatile("st.global.cg.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(a), "f"(v), "l"(pol) : "memory");
-}
-__device__ __forceinline__ float ld_stream(const float* a, uint64_t pol) {
-    float v;
-    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
-    return v;
-}
-
-
-__device__ __forceinline__ float cf_of(float b, float nmv) {
-    const float r = fmaxf(b, 0.f);
-    return __fdiv_rn(__fmul_rn(r, r), nmv);
-}
-
-__device__ __forceinline__ unsigned long long pack_key(float cf, int t) {
-    return ((unsigned long long)__float_as_uint(cf) << 32) | (unsigned long long)(0xFFFFFFFFu - (unsigned)t);
-}
-
-
-// Running maximum of Cf = fl(fl(r*r) / nm) (r = relu(b)) with the first index
-// on ties. The correctly rounded quotient is formed only for candidates:
-// a = fl(fl(r*r) * fl(1/nm)) is within 3.01 ulp of it, so a < best*(1 - 8 ulp)
-// proves the exact value is below best (checked only while best is a normal
-// number, where the relative bounds hold).
-struct ColMax {
-    float best = -1.f;
-    float thr = -1.f;  // rounded-down best * (1 - 2^-21)
-    int bi = 0;
-    __device__ __forceinline__ void consider(float b, float nmv, float inv, int t) {
-        const float r = fmaxf(b, 0.f);
-        const float sq = __fmul_rn(r, r);
-        if (__fmul_rn(sq, inv) < thr) return;
-        const float cf = __fdiv_rn(sq, nmv);
-        if (cf > best) {
-            best = cf;
-            bi = t;
-            thr = (cf >= 1e-30f) ? __fmul_rd(cf, 0.99999952316f) : -1.f;
-        }
-    }
-};
-
-// Best Cf of column s over rows [t0, t1), loads issued eight rows at a time.
-__device__ __forceinline__ void column_best(const float* __restrict__ B, int64_t ldb, const float* s_nm,
-                                            const float* s_inv, int s, int t0, int t1, ColMax& m) {
-    const float* bp = B + (int64_t)t0 * ldb + s;
-    int t = t0;
-    for (; t + 8 <= t1; t += 8, bp += 8 * ldb) {
-        float v[8];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) v[u] = __ldcg(bp + u * ldb);
-#pragma unroll
-        for (int u = 0; u < 8; ++u) m.consider(v[u], s_nm[t + u], s_inv[t + u], t + u);
-    }
-    for (; t < t1; ++t, bp += ldb) m.consider(__ldcg(bp), s_nm[t], s_inv[t], t);
-}
-
-// Inclusive warp scan.
-__device__ __forceinline__ int warp_inc_scan(int v, int lane) {
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int u = __shfl_up_sync(0xffffffffu, v, o);
-        if (lane >= o) v += u;
-    }
-    return v;
-}
-
 __global__ void __launch_bounds__(MP_THREADS, 1) k_mp(MPArgs a) {
     extern __shared__ float smem[];
     __shared__ int s_pref[MP_MAX_GRID + 1];
@@ -544,7 +422,10 @@ static __device__ __align__(256) unsigned char g_mp_scratch[NA_BYTES];
 
 namespace {
 std::mutex g_na_mutex;
-unsigned char* g_na_base[256] = {};  // device address of g_mp_scratch, per device ordinal
+// device address of g_mp_scratch, per device ordinal, looked up on the first
+// call on that device; a cudaDeviceReset ends the context the address belongs
+// to, so a process that resets a device must not call this entry point again
+unsigned char* g_na_base[256] = {};
 }  // namespace
 
 extern "C" int lss_mp_rounds_noalloc(float* B_dev, int64_t ldb, int32_t n_templates, int32_t n_samples,
@@ -575,6 +456,15 @@ extern "C" int lss_mp_rounds_noalloc(float* B_dev, int64_t ldb, int32_t n_templa
         set_thread_error("lss_mp_rounds_noalloc: no current CUDA device");
         return LSS_ERR_CUDA;
     }
+    // every array the kernel dereferences must be memory of the current
+    // device (or pinned host memory): a pageable host array or another GPU's
+    // buffer would fault in the kernel, so it is refused before any launch
+    for (const void* p : {(const void*)B_dev, (const void*)nm_dev, (const void*)ctc_permuted_dev,
+                          (const void*)spike_x, (const void*)spike_y, (const void*)spike_amp})
+        if (!device_accessible(p, dev)) {
+            set_thread_error("lss_mp_rounds_noalloc: arrays must be memory of the current device or pinned host memory");
+            return LSS_ERR_ARG;
+        }
     unsigned char* base = nullptr;
     {
         // one-time set-up per device: the device address of the scratch array
@@ -642,8 +532,12 @@ extern "C" int lss_mp_rounds_noalloc(float* B_dev, int64_t ldb, int32_t n_templa
         set_thread_error("lss_mp_rounds_noalloc: grid barrier timed out");
         return LSS_ERR_TIMEOUT;
     }
-    if (st & (STATUS_CAPACITY | STATUS_LIST)) {
-        set_thread_error("lss_mp_rounds_noalloc: more spikes than capacity, or a 2*nt window with over 31 peaks");
+    if (st & STATUS_CAPACITY) {
+        set_thread_error("lss_mp_rounds_noalloc: more spikes than capacity");
+        return LSS_ERR_CAPACITY;
+    }
+    if (st & STATUS_LIST) {
+        set_thread_error(MSG_MP_LIST);
         return LSS_ERR_CAPACITY;
     }
     return LSS_OK;

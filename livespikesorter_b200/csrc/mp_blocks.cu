@@ -1,0 +1,443 @@
+// Greedy matching pursuit that skips template-row blocks whose update is an
+// exact no-op. Same rounds, same arithmetic and the same spikes, amplitudes
+// and final score field as k_mp (mp.cu) and Kilosort's round loop
+// (kilosort/template_matching.py:157-198, LiveSpikeSorter's
+// kilosortMatchingPursuit, OnlineSpikesV2.cu:873-971).
+//
+// Why most of the update can be skipped. A spike (x, y, a) changes score
+// B[t, s] to fl(B - fl(a * ctc[t, y, s - x + nt])). For |B| in [2^e, 2^(e+1))
+// the neighbouring floats are at least 2^(e-24) away, so any |d| < 2^(e-25)
+// leaves fl(B - d) == B bit for bit. Templates far apart on the probe have
+// cross-correlations many orders of magnitude below the scores they would
+// change (on a 384-channel probe about three quarters of all (row, spike)
+// updates are such no-ops), so:
+//   * template rows are grouped into blocks of MPB_ROWS templates that lie
+//     close together on the probe (perm: templates ordered by the centre of
+//     mass of their channel energy);
+//   * per block and column the kernel keeps bmin = min over the block's rows
+//     of |B| and bkey = max over the rows of (Cf bits << 32 | ~t), exact for
+//     the current field;
+//   * a (spike segment, block, 32-column chunk) work item whose terms all
+//     satisfy fl(|a| * cmaxb[y][block]) < 2^(e(bmin) - 25) is skipped: every
+//     score of the block is provably unchanged, and so are its bmin and bkey.
+//     In a processed block a single term is skipped per row by the same test
+//     with the row's own max |ctc| (cmaxr), as long as no earlier term of
+//     that row changed the score;
+//   * the peak phase takes each column's maximum over the block keys.
+// Everything that is computed is computed exactly as in k_mp: single-rounded
+// products and differences (__fmul_rn / __fsub_rn), Cf = fl(fl(r*r)/nm), the
+// largest Cf with the smallest template index on ties (torch.max), the two
+// interleaved passes per round (last even spike's term, then the last odd
+// spike's, per element).
+//
+// Round structure, work split and bounded grid barriers follow k_mp: the peak
+// phase owns W consecutive columns per CTA; the update phase prefix-sums the
+// per-CTA peak counts for the round's time order; update work items are
+// split into contiguous ranges per CTA and handed to warps through a shared
+// counter; every wait is bounded (STATUS_TIMEOUT).
+#include "lss_kernels.cuh"
+#include "mp_common.cuh"
+
+#include <algorithm>
+#include <climits>
+
+namespace lss {
+
+constexpr int MPB_THREADS = 512;
+constexpr int MPB_MAX_GRID = 1024;
+constexpr unsigned FULL = 0xffffffffu;
+
+// 2^(e - 25) for v in [2^e, 2^(e+1)) (v >= 0): any |d| below it leaves
+// fl(v' - d) == v' for every v' with |v'| >= v. Zero when v is zero,
+// subnormal, tiny, infinite or NaN (nothing is then skipped).
+__device__ __forceinline__ float quarter_ulp(float v) {
+    const unsigned e = (__float_as_uint(v) >> 23) & 0xFFu;
+    return (e > 25u && e < 255u) ? __uint_as_float((e - 25u) << 23) : 0.f;
+}
+
+// Running max of Cf over rows visited in any order: larger Cf first, smaller
+// template index on ties (torch.max's first index). The correctly rounded
+// quotient is formed only for candidates (see ColMax in mp_common.cuh).
+struct ColMaxAny {
+    float best = -1.f;
+    float thr = -1.f;
+    int bi = INT_MAX;
+    __device__ __forceinline__ void consider(float b, float nmv, float inv, int t) {
+        const float r = fmaxf(b, 0.f);
+        const float sq = __fmul_rn(r, r);
+        if (__fmul_rn(sq, inv) < thr) return;
+        const float cf = __fdiv_rn(sq, nmv);
+        if (cf > best || (cf == best && t < bi)) {
+            best = cf;
+            bi = t;
+            thr = (cf >= 1e-30f) ? __fmul_rd(cf, 0.99999952316f) : -1.f;
+        }
+    }
+};
+
+__global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
+    extern __shared__ float smem[];
+    __shared__ int s_pref[MPB_MAX_GRID + 1];
+    __shared__ int s_wcnt[MPB_THREADS / 32];
+    __shared__ int s_cnt, s_total, s_next;
+
+    const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int N = a.N, T = a.T, nt = a.nt, L2 = 2 * nt + 1, nb = a.nb;
+    const int W = a.cols_per_blk;
+    const int lo = min(N, b * W), hi = min(N, lo + W);
+    const int64_t ldk = a.ldk, ldb = a.ldb;
+
+    float* vals = smem;                                       // [W + 2nt]
+    int* ivals = reinterpret_cast<int*>(smem + W + 2 * nt);  // [W]
+    float* s_nm = smem + 2 * W + 2 * nt;                      // [T]
+    float* s_inv = s_nm + T;                                  // [T]
+    int* s_perm = reinterpret_cast<int*>(s_inv + T);          // [nb * MPB_ROWS]
+    for (int t = tid; t < T; t += MPB_THREADS) {
+        const float v = __ldg(a.nm + t);
+        s_nm[t] = v;
+        s_inv[t] = __frcp_rn(v);
+    }
+    for (int i = tid; i < nb * MPB_ROWS; i += MPB_THREADS) s_perm[i] = __ldg(a.perm + i);
+    __syncthreads();
+    const uint64_t pk = policy_keep(), ps = policy_stream();
+
+    // ---- block keys and minima of the owned columns for the initial field
+    {
+        const int ncol = hi - lo;
+        for (int w = tid; w < ncol * nb; w += MPB_THREADS) {
+            const int bb = w / ncol, s = lo + (w - bb * ncol);
+            const int r0 = bb * MPB_ROWS, nr = min(MPB_ROWS, T - r0);
+            ColMaxAny m;
+            float mn = INFINITY;
+            for (int r = 0; r < nr; r += 16) {
+                float v[16];
+#pragma unroll
+                for (int u = 0; u < 16; ++u)
+                    v[u] = (r + u < nr) ? ld_keep(a.B + (int64_t)s_perm[r0 + r + u] * ldb + s, pk) : 0.f;
+#pragma unroll
+                for (int u = 0; u < 16; ++u)
+                    if (r + u < nr) {
+                        const int t = s_perm[r0 + r + u];
+                        mn = fminf(mn, fabsf(v[u]));
+                        m.consider(v[u], s_nm[t], s_inv[t], t);
+                    }
+            }
+            a.bkey[bb * ldk + s] = pack_key(m.best, m.bi);
+            a.bmin[bb * ldk + s] = mn;
+        }
+    }
+    if (!grid_sync(a.bar, a.status)) return;
+
+    int base = 0;
+    int r = 0;
+    int n_items = 0, n_proc = 0;  // per warp, lane 0: update work items seen and processed
+    for (; r < a.max_rounds; ++r) {
+        // ---- P: column maxima from the block keys, pooled window, peaks
+        const int nv = (hi - lo) + 2 * nt;
+        for (int p = tid; p < nv; p += MPB_THREADS) {
+            const int s = lo - nt + p;
+            float v = -INFINITY;
+            if (s >= 0 && s < N) {
+                const bool own = (s >= lo && s < hi);
+                if (s < nt || s >= N - nt) {
+                    v = 0.f;  // Cf[:, :nt] = Cf[:, -nt:] = 0
+                    if (own) ivals[s - lo] = 0;
+                } else {
+                    unsigned long long k = 0ull;
+                    int bb = 0;
+                    for (; bb + 4 <= nb; bb += 4) {
+                        const unsigned long long k0 = __ldcg(a.bkey + (bb + 0) * ldk + s);
+                        const unsigned long long k1 = __ldcg(a.bkey + (bb + 1) * ldk + s);
+                        const unsigned long long k2 = __ldcg(a.bkey + (bb + 2) * ldk + s);
+                        const unsigned long long k3 = __ldcg(a.bkey + (bb + 3) * ldk + s);
+                        k = max(max(k, k0), max(max(k1, k2), k3));
+                    }
+                    for (; bb < nb; ++bb) k = max(k, __ldcg(a.bkey + bb * ldk + s));
+                    v = __uint_as_float((unsigned)(k >> 32));
+                    if (own) ivals[s - lo] = (int)(0xFFFFFFFFu - (unsigned)(k & 0xFFFFFFFFull));
+                }
+            }
+            vals[p] = v;
+        }
+        if (tid == 0) s_cnt = 0;
+        __syncthreads();
+        for (int c0 = lo; c0 < hi; c0 += MPB_THREADS) {
+            const int s = c0 + tid;
+            bool flag = false;
+            if (s < hi) {
+                const int p = s - lo + nt;
+                float cm = vals[p - nt];
+                for (int d = -nt + 1; d <= nt; ++d) cm = fmaxf(cm, vals[p + d]);
+                flag = (cm > a.th2) && (fabsf(__fsub_rn(cm, vals[p])) < 1e-9f);
+            }
+            const unsigned bal = __ballot_sync(FULL, flag);
+            if (lane == 0) s_wcnt[warp] = __popc(bal);
+            __syncthreads();
+            if (warp == 0) {
+                const int c = (lane < MPB_THREADS / 32) ? s_wcnt[lane] : 0;
+                const int inc = warp_inc_scan(c, lane);
+                if (lane < MPB_THREADS / 32) s_wcnt[lane] = inc - c;
+                if (lane == MPB_THREADS / 32 - 1) s_total = inc;
+            }
+            __syncthreads();
+            if (flag) {
+                const int k = s_cnt + s_wcnt[warp] + __popc(bal & ((1u << lane) - 1u));
+                const int y = ivals[s - lo];
+                a.blk_x[lo + k] = s;
+                a.blk_y[lo + k] = y;
+                a.blk_amp[lo + k] = __fdiv_rn(__ldcg(a.B + (int64_t)y * ldb + s), s_nm[y]);
+            }
+            __syncthreads();
+            if (tid == 0) s_cnt += s_total;
+        }
+        __syncthreads();
+        if (tid == 0) a.blk_cnt[b] = s_cnt;
+        if (!grid_sync(a.bar, a.status)) return;
+
+        // ---- U: global order of the round's spikes, records, block updates
+        {
+            int carry = 0;
+            for (int c0 = 0; c0 < G; c0 += MPB_THREADS) {
+                const int i = c0 + tid;
+                const int c = (i < G) ? __ldcg(a.blk_cnt + i) : 0;
+                const int inc = warp_inc_scan(c, lane);
+                if (lane == 31) s_wcnt[warp] = inc;
+                __syncthreads();
+                if (warp == 0) {
+                    const int wc = (lane < MPB_THREADS / 32) ? s_wcnt[lane] : 0;
+                    const int winc = warp_inc_scan(wc, lane);
+                    if (lane < MPB_THREADS / 32) s_wcnt[lane] = winc - wc;
+                    if (lane == MPB_THREADS / 32 - 1) s_total = winc;
+                }
+                __syncthreads();
+                if (i < G) s_pref[i] = carry + s_wcnt[warp] + inc - c;
+                carry += s_total;
+                __syncthreads();
+            }
+            if (tid == 0) s_pref[G] = carry;
+            __syncthreads();
+        }
+        const int total = s_pref[G];
+        if (total == 0) break;
+        if (base + total > a.capacity) {
+            if (tid == 0) atomicOr(a.status, STATUS_CAPACITY);
+            break;
+        }
+        const int nch = (L2 + 31) / 32;
+        const int per_spike = nb * nch;
+        const int items = total * per_spike;
+        const int per_cta = (items + G - 1) / G;
+        const int it_end = min(items, (b + 1) * per_cta);
+        {
+            const int cnt = s_pref[b + 1] - s_pref[b];
+            for (int k = tid; k < cnt; k += MPB_THREADS) {
+                const int i = base + s_pref[b] + k;
+                a.sp_x[i] = __ldcg(a.blk_x + lo + k);
+                a.sp_y[i] = __ldcg(a.blk_y + lo + k);
+                a.sp_amp[i] = __ldcg(a.blk_amp + lo + k);
+                if (a.sp_round) a.sp_round[i] = r;
+            }
+            if (b == 0 && tid == 0) a.round_start[r] = base;
+            if (tid == 0) s_next = b * per_cta;
+        }
+        __syncthreads();
+        {
+            // Work item (spike q, block bb, chunk ch): the columns of spike q's
+            // segment [max(x_q - nt, x_{q-1} + nt + 1), x_q + nt], 32 at a time,
+            // rows of block bb. Lane L holds spike q - 1 + L of the round.
+            int cur_q = -1, x = INT_MAX, y = 0;
+            float amp = 0.f;
+            for (;;) {
+                int it = 0;
+                if (lane == 0) it = atomicAdd(&s_next, 1);
+                it = __shfl_sync(FULL, it, 0);
+                if (it >= it_end) break;
+                const int q = it / per_spike, rem = it - q * per_spike, bb = rem / nch, ch = rem - bb * nch;
+                if (q != cur_q) {
+                    cur_q = q;
+                    const int j = q - 1 + lane;
+                    x = INT_MAX;
+                    y = 0;
+                    amp = 0.f;
+                    if (j >= 0 && j < total) {
+                        int lo2 = 0, hi2 = G;  // region c with s_pref[c] <= j < s_pref[c+1]
+                        while (hi2 - lo2 > 1) {
+                            const int m = (lo2 + hi2) >> 1;
+                            if (s_pref[m] <= j) lo2 = m; else hi2 = m;
+                        }
+                        const int idx = lo2 * W + (j - s_pref[lo2]);
+                        x = __ldcg(a.blk_x + idx);
+                        y = __ldcg(a.blk_y + idx);
+                        amp = __ldcg(a.blk_amp + idx);
+                    }
+                }
+                const int xi = __shfl_sync(FULL, x, 1);
+                const int xprev = __shfl_sync(FULL, x, 0);
+                const bool ok = lane >= 1 && (q - 1 + lane) < total && x <= xi + 2 * nt;
+                const int nl = __popc(__ballot_sync(FULL, ok));
+                if (lane == 0 && ch == 0 && bb == 0 && nl == MP_LIST && q + MP_LIST < total)
+                    atomicOr(a.status, STATUS_LIST);
+                const int lo_own = max(max(xi - nt, (q > 0 ? xprev : INT_MIN / 2) + nt + 1), 0);
+                const int hi_own = min(xi + nt, N - 1);
+                if (lo_own + ch * 32 > hi_own) continue;  // warp-uniform: nothing owned in this chunk
+                const int s = lo_own + ch * 32 + lane;
+                const bool active = s <= hi_own;
+                // last even and last odd spike of the list whose window covers s
+                int e0 = -1, e1 = -1;
+                for (int e = 0; e < nl; ++e) {
+                    const int ex = __shfl_sync(FULL, x, e + 1);
+                    if (active && ex <= s + nt) {
+                        if ((q + e) & 1) e1 = e; else e0 = e;
+                    }
+                }
+                const int x0 = __shfl_sync(FULL, x, max(e0, 0) + 1);
+                const int y0 = __shfl_sync(FULL, y, max(e0, 0) + 1);
+                const float a0 = __shfl_sync(FULL, amp, max(e0, 0) + 1);
+                const int x1 = __shfl_sync(FULL, x, max(e1, 0) + 1);
+                const int y1 = __shfl_sync(FULL, y, max(e1, 0) + 1);
+                const float a1 = __shfl_sync(FULL, amp, max(e1, 0) + 1);
+                // exact no-op test of the whole block for this column
+                float thr = 0.f;
+                bool noop = true;
+                if (active) {
+                    thr = quarter_ulp(__ldcg(a.bmin + bb * ldk + s));
+                    if (e0 >= 0 && !(__fmul_rn(fabsf(a0), __ldg(a.cmaxb + (int64_t)y0 * nb + bb)) < thr)) noop = false;
+                    if (e1 >= 0 && !(__fmul_rn(fabsf(a1), __ldg(a.cmaxb + (int64_t)y1 * nb + bb)) < thr)) noop = false;
+                }
+                ++n_items;
+                if (__all_sync(FULL, noop)) continue;
+                ++n_proc;
+                if (!active) continue;
+                const int r0 = bb * MPB_ROWS, nr = min(MPB_ROWS, T - r0);
+                const float* c0p = a.ctcP + (int64_t)y0 * T * L2 + (s - x0 + nt);
+                const float* c1p = a.ctcP + (int64_t)y1 * T * L2 + (s - x1 + nt);
+                const float* cr0 = a.cmaxr + (int64_t)y0 * T;
+                const float* cr1 = a.cmaxr + (int64_t)y1 * T;
+                const float fa0 = fabsf(a0), fa1 = fabsf(a1);
+                ColMaxAny m;
+                float mn = INFINITY;
+                for (int rr = 0; rr < nr; rr += 8) {
+                    int tt[8];
+                    float v[8], w0[8], w1[8];
+                    bool u0[8], u1[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) tt[u] = (rr + u < nr) ? s_perm[r0 + rr + u] : -1;
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) v[u] = tt[u] >= 0 ? ld_keep(a.B + (int64_t)tt[u] * ldb + s, pk) : 0.f;
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        // term 0 applies unless it is a no-op on the old score; term 1
+                        // may be skipped only when term 0 left the score unchanged
+                        u0[u] = tt[u] >= 0 && e0 >= 0 && !(__fmul_rn(fa0, __ldg(cr0 + tt[u])) < thr);
+                        u1[u] = tt[u] >= 0 && e1 >= 0 && (u0[u] || !(__fmul_rn(fa1, __ldg(cr1 + tt[u])) < thr));
+                    }
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) w0[u] = u0[u] ? ld_stream(c0p + (int64_t)tt[u] * L2, ps) : 0.f;
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) w1[u] = u1[u] ? ld_stream(c1p + (int64_t)tt[u] * L2, ps) : 0.f;
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        if (tt[u] < 0) continue;
+                        float xv = v[u];
+                        if (u0[u]) xv = __fsub_rn(xv, __fmul_rn(a0, w0[u]));
+                        if (u1[u]) xv = __fsub_rn(xv, __fmul_rn(a1, w1[u]));
+                        if (__float_as_uint(xv) != __float_as_uint(v[u])) st_keep(a.B + (int64_t)tt[u] * ldb + s, xv, pk);
+                        mn = fminf(mn, fabsf(xv));
+                        m.consider(xv, s_nm[tt[u]], s_inv[tt[u]], tt[u]);
+                    }
+                }
+                a.bkey[bb * ldk + s] = pack_key(m.best, m.bi);
+                a.bmin[bb * ldk + s] = mn;
+            }
+        }
+        base += total;
+        if (!grid_sync(a.bar, a.status)) return;
+    }
+    if (lane == 0 && n_items) {
+        atomicAdd(a.counters + 2, n_proc);
+        atomicAdd(a.counters + 3, n_items);
+    }
+    if (b == 0 && tid == 0) {
+        a.counters[0] = base;
+        a.counters[1] = r;
+        a.round_start[r] = base;
+    }
+}
+
+int mp_blocks_max_grid(int device) {
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    return std::min(sms, MPB_MAX_GRID);
+}
+
+static size_t mpb_smem_bytes(int cols_per_blk, int nt, int T, int nb) {
+    return sizeof(float) * ((size_t)cols_per_blk + 2 * nt) + sizeof(int) * (size_t)cols_per_blk +
+           sizeof(float) * 2 * (size_t)T + sizeof(int) * (size_t)nb * MPB_ROWS + 16;
+}
+
+cudaError_t launch_mp_blocks(MPArgs a, int grid, cudaStream_t s) {
+    if (grid > MPB_MAX_GRID || !a.perm || !a.cmaxb || !a.cmaxr || !a.bkey || !a.bmin ||
+        a.nb != (a.T + MPB_ROWS - 1) / MPB_ROWS)
+        return cudaErrorInvalidValue;
+    const size_t smem = mpb_smem_bytes(a.cols_per_blk, a.nt, a.T, a.nb);
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_mp_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    cudaError_t e = cudaMemsetAsync(a.bar, 0, 2 * sizeof(unsigned int), s);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(grid);
+    lc.blockDim = dim3(MPB_THREADS);
+    lc.dynamicSmemBytes = smem;
+    lc.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    lc.attrs = attr;
+    lc.numAttrs = 1;
+    return cudaLaunchKernelEx(&lc, k_mp_blocks, a);
+}
+
+// cmaxr[y, t] = max over lags of |ctcP[y, t, :]| (one warp per row); a NaN
+// lag makes the row's maximum infinite, so that nothing touching it is skipped
+__global__ void k_ctc_row_max(const float* __restrict__ ctcP, int64_t rows, int L2, float* __restrict__ cmaxr) {
+    const int64_t row = (int64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (row >= rows) return;
+    const float* p = ctcP + row * L2;
+    float m = 0.f;
+    for (int l = lane; l < L2; l += 32) {
+        const float v = __ldg(p + l);
+        m = (v != v) ? INFINITY : fmaxf(m, fabsf(v));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(FULL, m, o));
+    if (lane == 0) cmaxr[row] = m;
+}
+
+// cmaxb[y, b] = max over the rows of block b of cmaxr[y, row]
+__global__ void k_ctc_block_max(const float* __restrict__ cmaxr, int T, const int32_t* __restrict__ perm, int nb,
+                                float* __restrict__ cmaxb) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int64_t)T * nb) return;
+    const int y = (int)(i / nb), bb = (int)(i % nb);
+    float m = 0.f;
+    for (int r = 0; r < MPB_ROWS; ++r) {
+        const int t = perm[bb * MPB_ROWS + r];
+        if (t >= 0) m = fmaxf(m, cmaxr[(int64_t)y * T + t]);
+    }
+    cmaxb[i] = m;
+}
+
+cudaError_t launch_ctc_block_max(const float* ctcP, int32_t T, int32_t L2, const int32_t* perm, int32_t nb,
+                                 float* cmaxb, float* cmaxr, cudaStream_t s) {
+    const int64_t rows = (int64_t)T * T;
+    k_ctc_row_max<<<(unsigned)((rows + 7) / 8), 256, 0, s>>>(ctcP, rows, L2, cmaxr);
+    const int64_t nbk = (int64_t)T * nb;
+    k_ctc_block_max<<<(unsigned)((nbk + 255) / 256), 256, 0, s>>>(cmaxr, T, perm, nb, cmaxb);
+    return cudaGetLastError();
+}
+
+}  // namespace lss

@@ -42,7 +42,24 @@ __device__ __forceinline__ int64_t global_timer_ns() {
     return (int64_t)t;
 }
 
-__global__ void k_global_timer(int64_t* out) { *out = global_timer_ns(); }
+// Clock ping through mapped pinned memory: the kernel announces itself
+// (ping[0] = 5), waits for the host's go (ping[0] == 1), reads the global timer
+// at once, stores it in ping[1] and answers (ping[0] = 2). The wait gives up
+// after 1 s of device time (ping[0] = 3, no timestamp).
+__global__ void k_clock_ping(volatile int64_t* ping) {
+    ping[0] = 5;
+    __threadfence_system();
+    const int64_t t0 = global_timer_ns();
+    while (ping[0] != 1) {
+        if (global_timer_ns() - t0 > 1000000000ll) {
+            ping[0] = 3;
+            return;
+        }
+    }
+    ping[1] = global_timer_ns();
+    __threadfence_system();
+    ping[0] = 2;
+}
 
 // state[0] = batch index (starts at -1), state[1] = first stream row of the
 // batch window, state[2] = device time at which the batch's work began.
@@ -255,24 +272,44 @@ int capture(Probe* p) {
     return LSS_OK;
 }
 
-// Offset from the device's global timer to the host's steady clock, taken
-// as the midpoint of the shortest of a few launch-and-wait round trips of a
-// kernel that reads the timer (error: half that round trip, a few us).
+// Offset from the device's global timer to the host's steady clock. In each
+// of a few pings (k_clock_ping) the device reads its timer at a host moment
+// between t_go (the host wrote the go flag) and t_seen (the host saw the
+// answer), so offset = that moment - timestamp lies in [t_go - g, t_seen - g];
+// the ping with the narrowest bracket (a few us: two transfers over the bus)
+// gives the midpoint. With that bound, device timestamps map to host times
+// that keep the launch -> device start -> device end -> seen order.
 int calibrate_clock(Probe* p) {
-    int64_t best_rt = INT64_MAX;
-    for (int i = 0; i < 5; ++i) {
-        const int64_t t0 = lss::now_ns();
-        k_global_timer<<<1, 1, 0, p->s>>>(p->state.p + 2);
+    struct Ping {
+        HostBuf<int64_t> b;
+        ~Ping() { b.release(); }
+    } ping;
+    PCK(ping.b.alloc(2, true));
+    volatile int64_t* hp = ping.b.p;
+    int64_t best = INT64_MAX;
+    for (int i = 0; i < 16; ++i) {
+        hp[0] = 0;
+        hp[1] = 0;
+        k_clock_ping<<<1, 1, 0, p->s>>>(ping.b.d);
         PCK(cudaGetLastError());
-        int64_t g = 0;
-        PCK(cudaMemcpyAsync(&g, p->state.p + 2, sizeof(g), cudaMemcpyDeviceToHost, p->s));
+        const int64_t w0 = lss::now_ns();
+        bool started = false;
+        while (lss::now_ns() - w0 < 1000000000ll)
+            if (hp[0] == 5) { started = true; break; }
+        const int64_t t_go = lss::now_ns();
+        hp[0] = 1;
+        int64_t t_seen = 0;
+        while (started && lss::now_ns() - t_go < 1000000000ll)
+            if (hp[0] == 2) { t_seen = lss::now_ns(); break; }
         PCK(cudaStreamSynchronize(p->s));
-        const int64_t t1 = lss::now_ns();
-        if (t1 - t0 < best_rt) {
-            best_rt = t1 - t0;
-            p->gpu_offset_ns = t0 + (t1 - t0) / 2 - g;
+        if (!t_seen || hp[0] != 2) continue;  // the device gave up waiting: no sample
+        const int64_t g = hp[1];
+        if (t_seen - t_go < best) {
+            best = t_seen - t_go;
+            p->gpu_offset_ns = t_go + (t_seen - t_go) / 2 - g;
         }
     }
+    if (best == INT64_MAX) return p->fail(LSS_ERR_CUDA, "device clock calibration got no answer");
     return LSS_OK;
 }
 

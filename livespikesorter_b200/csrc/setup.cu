@@ -285,7 +285,10 @@ int lss_set_templates(lss_handle* h, const float* U, const float* wPCA) {
     for (int i = 0; i < T; ++i)
         if (!(nmv[i] > 0.f) || !std::isfinite(nmv[i]))
             return h->fail(LSS_ERR_ARG, "template " + std::to_string(i) + " has zero or non-finite energy");
-    // the whitening-folded operands follow the new templates
+    // the rounds' template order and |ctc| maxima, and the whitening-folded
+    // operands, follow the new templates
+    const int rc = rebuild_mp_blocks(h);
+    if (rc) return rc;
     return rebuild_uw(h);
 }
 

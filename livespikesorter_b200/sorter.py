@@ -79,12 +79,13 @@ def post_config(xc=None, yc=None, centroids=None, dt: int = 7):
     return cfg, k
 
 
-def check_record_set(o: dict, nC: int, K: int) -> None:
+def check_record_set(o: dict, nC: int, K: int, device=None) -> None:
     """Raises ValueError unless ``o`` is a record set the kernels can write:
     contiguous tensors of one capacity with the record dtypes (time int64,
     template int32, amplitude f32, pc f32 [cap, nC, K] or None, count int64),
-    each on the GPU or in pinned host memory. A wrong dtype or a short array
-    would let the kernels write past its end."""
+    each on the sorter's GPU (``device``, when given) or in pinned host memory.
+    A wrong dtype or a short array would let the kernels write past its end;
+    another GPU's tensor would be written without peer access."""
     want = dict(time=torch.int64, template=torch.int32, amplitude=torch.float32, count=torch.int64)
     for k, dt in want.items():
         t = o.get(k)
@@ -104,6 +105,8 @@ def check_record_set(o: dict, nC: int, K: int) -> None:
         t = o.get(k)
         if t is not None and not (t.is_cuda or t.is_pinned()):
             raise ValueError(f'record set: {k} must be on the GPU or in pinned host memory')
+        if t is not None and t.is_cuda and device is not None and t.device != torch.device(device):
+            raise ValueError(f'record set: {k} is on {t.device}, the sorter runs on {torch.device(device)}')
 
 
 def setup_kwargs(setup) -> dict:
@@ -275,7 +278,7 @@ class Sorter:
         raw_t, raw_dev = self._raw(raw)
         o = out if out is not None else self.records(capacity)
         if out is not None:
-            check_record_set(o, self.nC, self.K)
+            check_record_set(o, self.nC, self.K, self.device)
         cap = o['time'].shape[0]
         rec = LssRecords(time=o['time'].data_ptr(), template_id=o['template'].data_ptr(),
                          amplitude=o['amplitude'].data_ptr(), pc=_ptr(o['pc']), capacity=cap, count=0, on_device=1,
@@ -291,7 +294,8 @@ class Sorter:
         s = LssStats()
         self._check(self._lib.lss_get_stats(self._h, s))
         return dict(rounds=s.rounds, spikes=s.spikes, recheck_columns=s.recheck_columns,
-                    recheck_flips=s.recheck_flips, recheck_rescored=s.recheck_rescored, launches=s.launches)
+                    recheck_flips=s.recheck_flips, recheck_rescored=s.recheck_rescored, launches=s.launches,
+                    mp_items=s.mp_items, mp_items_updated=s.mp_items_updated)
 
     def set_templates(self, U, wPCA=None):
         """Swap in new templates (same shapes) and optionally a new temporal

@@ -8,7 +8,8 @@ ROOT = Path(__file__).resolve().parent.parent
 sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(ROOT / 'oracle'))
 
-REFERENCE = Path('/root/reference')
+# the reference tree (read only by the oracle pin tests); LSS_REFERENCE_ROOT overrides it
+REFERENCE = Path(os.environ.get('LSS_REFERENCE_ROOT', '/root/reference'))
 KS_SITE = REFERENCE / 'src/Python/run_online_spikes/Lib/site-packages'
 GOLDEN = Path(__file__).resolve().parent / 'golden'
 

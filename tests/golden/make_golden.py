@@ -1,6 +1,7 @@
 """Regenerate the golden fixtures in this directory from the reference itself.
 
-Run in a container that has the reference tree (``/root/reference``):
+Run where the reference tree is present (its root in ``LSS_REFERENCE_ROOT``,
+default ``/root/reference``):
 
     python tests/golden/make_golden.py
 
@@ -19,6 +20,7 @@ from __future__ import annotations
 
 import contextlib
 import io
+import os
 import sys
 import tempfile
 import types
@@ -27,7 +29,7 @@ from pathlib import Path
 import numpy as np
 import torch
 
-REF = Path('/root/reference')
+REF = Path(os.environ.get('LSS_REFERENCE_ROOT', '/root/reference'))
 KS_SITE = REF / 'src/Python/run_online_spikes/Lib/site-packages'
 HERE = Path(__file__).resolve().parent
 sys.path.insert(0, str(HERE.parent.parent))

@@ -1,0 +1,130 @@
+"""Parity with the oracle at the benchmark shapes (384 channels).
+
+* 400 templates, linear drift of 5 um/min corrected per batch through the
+  drift interpolation matrix: the first, a middle and the last batch of a
+  6-s recording;
+* 800 templates of which 10 % are near-duplicate pairs (footprint centres
+  10 um apart, the case that stresses runner-up decisions), drift on: the
+  same three batches.
+
+Each batch goes through lss_sort_batch (int16 rows in, records out) and
+through the oracle (filter + run_matching + PC features, FP32 torch on the
+CPU). Tolerances:
+* identical (time, template) sequence in run_matching order;
+* amplitudes within 1e-4 relative;
+* PC features within 1e-3 of their largest magnitude (FP32 projection sums in
+  another order than torch's conv1d / matmul).
+If the sequences differ, the failure message carries the margins of the first
+differing decision (its Cf minus Th^2, best minus runner-up template) and the
+FP64 oracle's choice there, so a flipped near-tie is told apart from an error.
+"""
+import numpy as np
+import pytest
+import torch
+
+import ks4_oracle as ko
+
+pytestmark = pytest.mark.gpu
+
+AMP_RTOL = 1e-4
+PC_TOL = 1e-3
+
+
+def _rows(raw, ib, nb, NT, nt):
+    """The rows padded_batch_to_torch reads for batch ib (kilosort/io.py:589-599)."""
+    if ib == 0:
+        return raw[0:NT + nt]
+    b0 = ib * NT - nt
+    return raw[b0:min(raw.shape[0], b0 + NT + 2 * nt)]
+
+
+def _oracle(setup, rec, ib, dtype=torch.float32):
+    NT, nt = setup.NT, setup.nt
+    X = ko.padded_batch(rec.raw, ib, NT, nt)
+    X = ko.filter_batch(X, hp_filter=setup.hp_filter, whiten_mat=setup.Wrot, drift_M=setup.drift_matrix(rec.dshift[ib]))
+    st, amps, Xres, rounds = ko.run_matching(X, setup.U, setup.ctc, setup.wPCA, setup.Th, nt, dtype=dtype,
+                                             return_rounds=True)
+    return X, st, amps, Xres, rounds
+
+
+def _report(setup, X, st_o, rounds_o, got, i):
+    """Margins of the first differing decision, and what the FP64 oracle picks."""
+    nt = setup.nt
+    U = setup.U
+    nm = (U.double() ** 2).sum(-1).sum(-1)
+    B = ko.score_field(X, U, setup.wPCA, nt, dtype=torch.float64)
+    m = ko.margin_report(B, nm, setup.Th, nt)
+    x = int(st_o[i, 0]) if i < len(st_o) else int(got[i, 0]) - setup.NT
+    st64, _, _ = ko.run_matching(X, U, setup.ctc, setup.wPCA, setup.Th, nt, dtype=torch.float64)
+    return (f'first difference at spike {i} (oracle round {int(rounds_o[i]) if i < len(rounds_o) else "-"}): '
+            f'oracle {st_o[i].tolist() if i < len(st_o) else None}, GPU {got[i].tolist() if i < len(got) else None}; '
+            f'round-1 margins at column {x}: Cf - Th^2 = {float(m["threshold_gap"][x]):.3e}, '
+            f'best - runner-up = {float(m["runner_up_gap"][x]):.3e}; FP64 oracle: {len(st64)} spikes, '
+            f'{"same" if len(st64) == len(st_o) and torch.equal(st64, st_o) else "different"} sequence as FP32')
+
+
+def _check_batches(T, dup, seed):
+    from livespikesorter_b200 import synth
+    from livespikesorter_b200.sorter import Sorter
+    cfg = 2 if dup else 1
+    setup, rec = synth.config(cfg, duration_s=6.0, seed=seed, T=T)
+    assert setup.C == 384 and setup.T == T
+    s = Sorter.from_setup(setup)
+    nb = rec.n_batches
+    NT, nt = setup.NT, setup.nt
+    total = 0
+    for ib in (0, nb // 2, nb - 1):
+        s.set_drift(setup.drift_matrix(rec.dshift[ib]))
+        r = s.sort_batch(np.ascontiguousarray(_rows(rec.raw, ib, nb, NT, nt)), ib, nb)
+        X, st, amps, Xres, rounds = _oracle(setup, rec, ib)
+        ref, ref_tf = ko.extract_batch(st, amps, Xres, setup.iCC, setup.iU, setup.Ucc, setup.wPCA, nt,
+                                       setup.nt0min, ib, NT)
+        got = np.stack([r['time'].numpy(), r['template'].numpy()], 1)
+        want = ref[:, :2].astype(np.int64)
+        if got.shape != want.shape or not np.array_equal(got, want):
+            n = min(len(got), len(want))
+            i = int(np.nonzero((got[:n] != want[:n]).any(1))[0][0]) if (got[:n] != want[:n]).any() else n
+            # records of batch 0 drop negative times: map back to matching order
+            off = 0 if ib != 0 else int(((st[:, 0] - nt - nt // 2 + setup.nt0min) < 0).sum())
+            pytest.fail(f'T={T} batch {ib}: {len(got)} GPU vs {len(want)} oracle spikes; '
+                        + _report(setup, X, st, rounds, torch.from_numpy(got), min(i + off, len(st) - 1)))
+        a = r['amplitude'].numpy().astype(np.float64)
+        b = ref[:, 2]
+        rel = np.abs(a - b) / np.maximum(np.abs(b), 1e-6)
+        assert rel.max() <= AMP_RTOL, (ib, rel.max())
+        tf = ref_tf.numpy()
+        assert np.abs(r['pc'].numpy() - tf).max() <= PC_TOL * np.abs(tf).max(), ib
+        total += len(got)
+    return total
+
+
+def test_fp32_spike_set_identical_at_384ch_400_templates_with_drift():
+    assert _check_batches(400, dup=False, seed=41) > 15000
+
+
+def test_fp32_spike_set_identical_at_384ch_800_templates_near_duplicates():
+    assert _check_batches(800, dup=True, seed=43) > 30000
+
+
+@pytest.mark.parametrize('T, dup', [(400, False), (800, True)])
+def test_rounds_bit_exact_on_given_scores_at_384ch(T, dup):
+    """The rounds alone on the oracle's own score field of a 384-channel batch:
+    spikes and amplitudes bit-identical to the oracle's run_matching, with most
+    template-row blocks skipped as exact no-ops."""
+    from livespikesorter_b200 import synth
+    from livespikesorter_b200.sorter import Sorter
+    setup, rec = synth.config(2 if dup else 1, duration_s=4.0, seed=47, T=T)
+    ib = 1
+    NT, nt = setup.NT, setup.nt
+    X = ko.padded_batch(rec.raw, ib, NT, nt)
+    X = ko.filter_batch(X, hp_filter=setup.hp_filter, whiten_mat=setup.Wrot, drift_M=setup.drift_matrix(rec.dshift[ib]))
+    B = ko.score_field(X, setup.U, setup.wPCA, nt)
+    nm = (setup.U ** 2).sum(-1).sum(-1)
+    st_o, amps_o, _ = ko.run_matching(X, setup.U, setup.ctc, setup.wPCA, setup.Th, nt, B=B, nm=nm)
+    s = Sorter.from_setup(setup, nm=nm)
+    st, amps = s.match_scores(B.cuda())
+    assert len(st_o) > 5000
+    assert torch.equal(st.cpu(), st_o)
+    assert torch.equal(amps.cpu(), amps_o)
+    stats = s.stats()
+    assert 0 < stats['mp_items_updated'] < 0.6 * stats['mp_items'], stats

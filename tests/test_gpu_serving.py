@@ -135,3 +135,51 @@ def test_server_rejects_bad_calls():
         check(srv2._lib.lss_server_push(srv2._s, 5, None, 1, 0))   # no such probe
     srv2.release(pid)
     assert srv2.admit(**kw) == 0             # the slot is free again
+
+
+def test_stream_batches_match_the_oracle_at_384ch():
+    """One 384-channel, 400-template probe streamed in 1500-sample blocks:
+    every stream batch against the oracle (filter + run_matching + PC
+    features) on the same window. Identical (time, template) sequence,
+    amplitudes within 1e-4 relative, PC features within 1e-3 of their
+    largest magnitude."""
+    import torch
+    import ks4_oracle as ko
+    from livespikesorter_b200 import synth
+    from livespikesorter_b200.serve import ProbeServer
+    from livespikesorter_b200.sorter import setup_kwargs
+    (setup, rec), = synth.streaming_probes(seed=13, duration_s=0.3, Ts=(400,))
+    NT, nt = 1500, setup.nt
+    kw = setup_kwargs(setup) | dict(NT=NT)
+    srv = ProbeServer(memory_budget=16 << 30)
+    pid = srv.admit(depth=3, capacity=16384, **kw)
+    nb = 5
+    for k in range(nb):
+        srv.push(pid, rec.raw[k * NT:(k + 1) * NT])
+    got = {}
+    for _ in range(nb):
+        b, r = srv.poll(pid, wait=True)
+        got[b] = r
+    srv.release(pid)
+    srv.close()
+    total = 0
+    for b in range(nb):
+        # the stream's window of batch b: rows [b*NT - 2nt, (b+1)*NT), row 0 replicated before the stream start
+        rows = (np.concatenate([np.repeat(rec.raw[:1], 2 * nt, 0), rec.raw[:NT]]) if b == 0
+                else rec.raw[b * NT - 2 * nt:(b + 1) * NT])
+        X = ko.filter_batch(torch.from_numpy(rows.T.astype(np.float32).copy()), hp_filter=setup.hp_filter,
+                            whiten_mat=setup.Wrot)
+        st, amps, Xres = ko.run_matching(X, setup.U, setup.ctc, setup.wPCA, setup.Th, nt)
+        _, tf = ko.extract_batch(st, amps, Xres, setup.iCC, setup.iU, setup.Ucc, setup.wPCA, nt, setup.nt0min, 1, NT)
+        # stream sample time of the window's column x
+        t = st[:, 0].numpy() - 2 * nt + b * NT - nt // 2 + setup.nt0min
+        keep = t >= 0
+        r = got[b]
+        assert np.array_equal(r['time'], t[keep]), b
+        assert np.array_equal(r['template'], st[:, 1].numpy()[keep]), b
+        a = amps[:, 0].numpy().astype(np.float64)[keep]
+        assert np.all(np.abs(r['amplitude'] - a) <= 1e-4 * np.maximum(np.abs(a), 1e-6)), b
+        ref_pc = tf.numpy()[keep]
+        assert np.abs(r['pc'] - ref_pc).max() <= 1e-3 * np.abs(ref_pc).max(), b
+        total += int(keep.sum())
+    assert total > 100

@@ -36,3 +36,13 @@ def test_pageable_host_record_sets_are_refused():
         check_record_set(_set(), 10, 6)
     with pytest.raises(ValueError, match='pinned'):
         check_record_set(_set(pc=None), 10, 6)
+
+
+@pytest.mark.gpu
+def test_record_sets_on_another_gpu_are_refused():
+    # a record set on cuda:0 handed to a sorter said to run on cuda:1: the
+    # kernels would write another GPU's memory without peer access
+    o = _set(**{k: v.cuda() for k, v in _set().items()})
+    check_record_set(o, 10, 6, 'cuda:0')
+    with pytest.raises(ValueError, match='sorter runs on cuda:1'):
+        check_record_set(o, 10, 6, 'cuda:1')

@@ -72,3 +72,22 @@ def test_no_alloc_rejects_oversized_batches():
                                    ctypes.byref(n), ctypes.byref(r), None)
     assert rc == LSS_ERR_ARG
     assert b'LSS_NOALLOC_MAX_SAMPLES' in lib.lss_last_error(None)
+
+
+def test_no_alloc_refuses_pageable_host_arrays():
+    """A pageable host array passed as the score field is refused with
+    LSS_ERR_ARG before anything is launched (it would fault in the kernel)."""
+    from livespikesorter_b200 import _lib
+    from livespikesorter_b200._lib import LSS_ERR_ARG
+    lib = _lib.load()
+    T, nt, N = 2, 61, 1000
+    host_B = np.zeros((T, N), np.float32)
+    dev = torch.zeros(T * T * (2 * nt + 1) + N, device='cuda')
+    outs = [torch.zeros(16, dtype=torch.int32, device='cuda') for _ in range(2)] + [torch.zeros(16, device='cuda')]
+    n, r = ctypes.c_int32(-7), ctypes.c_int32(-7)
+    rc = lib.lss_mp_rounds_noalloc(host_B.ctypes.data, N, T, N, nt, 8.0, dev.data_ptr(), dev.data_ptr(), 100, 16,
+                                   *(o.data_ptr() for o in outs), ctypes.byref(n), ctypes.byref(r), None)
+    torch.cuda.synchronize()
+    assert rc == LSS_ERR_ARG
+    assert b'current device' in lib.lss_last_error(None)
+    assert n.value == -7 and r.value == -7
