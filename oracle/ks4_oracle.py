@@ -7,12 +7,11 @@ LiveSpikeSorter's sorter mirrors, as vendored in the reference under
 * ``padded_batch``       <- ``io.py:584-637``        (BinaryRWFile.padded_batch_to_torch)
 * ``filter_batch``       <- ``io.py:757-790``        (BinaryFiltered.filter)
 * ``fft_highpass``       <- ``preprocessing.py:138-154``
-* ``get_highpass_filter``<- ``preprocessing.py:121-136``
-* ``whitening_*``        <- ``preprocessing.py:8-35``
-* ``get_drift_matrix``   <- ``preprocessing.py:44-69`` (nblocks == 1) and the
-                            ``iKxx`` precompute of ``datashift.py:215-219``
-* ``prepare_matching``   <- ``template_matching.py:110-121``
-* ``prepare_extract``    <- ``template_matching.py:20-26``
+* ``get_highpass_filter``, ``whitening_local``, ``get_drift_matrix`` / ``inv_kernel``,
+  ``prepare_matching``, ``prepare_extract`` <- ``preprocessing.py:8-35,44-69,121-136``,
+  ``datashift.py:215-219``, ``template_matching.py:20-26,110-121``: these one-time
+  setup steps are the product's own host code (``livespikesorter_b200/setup_tensors.py``),
+  re-exported here and pinned against the reference like the rest
 * ``run_matching``       <- ``template_matching.py:128-202``
 * ``extract_batch``      <- ``template_matching.py:46-73`` (xfeat and time conversion)
 * ``spike_positions``    <- ``postprocessing.py:33-46``  (compute_spike_positions)
@@ -43,6 +42,10 @@ import numpy as np
 import torch
 from torch.nn.functional import conv1d, max_pool1d
 from torch.fft import fft, ifft, fftshift
+
+from livespikesorter_b200 import setup_tensors as _setup
+from livespikesorter_b200.setup_tensors import (get_drift_matrix, get_highpass_filter,  # noqa: F401
+                                                inv_kernel, prepare_extract, whitening_local)
 
 
 # --------------------------------------------------------------------------
@@ -124,77 +127,16 @@ def filter_batch(X: torch.Tensor, chan_map=None, invert_sign=False, do_CAR=True,
 
 # --------------------------------------------------------------------------
 # one-time setup: preprocessing.py, datashift.py, template_matching.py
+#
+# The product's host-side setup (livespikesorter_b200/setup_tensors.py) holds
+# the one copy of these Kilosort steps; the oracle uses it, and
+# tests/test_oracle_pin.py pins it bit for bit against the reference itself.
 # --------------------------------------------------------------------------
-def get_highpass_filter(fs=30000, cutoff=300) -> torch.Tensor:
-    """preprocessing.py:121-136: filtfilt impulse response of a 3rd-order Butterworth."""
-    from scipy.signal import butter, filtfilt
-    NT = 30122
-    b, a = butter(3, cutoff, fs=fs, btype='high')
-    x = np.zeros(NT)
-    x[NT // 2] = 1
-    return torch.from_numpy(filtfilt(b, a, x).copy()).float()
-
-
-def whitening_from_covariance(CC: torch.Tensor) -> torch.Tensor:
-    """preprocessing.py:8-17 (ZCA)."""
-    E, D, V = torch.linalg.svd(CC)
-    eps = 1e-6
-    return (E / (D + eps) ** .5) @ E.T
-
-
-def whitening_local(CC: torch.Tensor, xc, yc, nrange=32) -> torch.Tensor:
-    """preprocessing.py:19-35."""
-    Nchan = CC.shape[0]
-    Wrot = torch.zeros((Nchan, Nchan), dtype=CC.dtype)
-    for j in range(Nchan):
-        ds = (xc[j] - xc) ** 2 + (yc[j] - yc) ** 2
-        ix = np.argsort(ds)[:nrange]
-        wrot = whitening_from_covariance(CC[np.ix_(ix, ix)])
-        Wrot[j, ix] = wrot[0]
-    return Wrot
-
-
-def kernel2D(x, y, sig=1):
-    """datashift.py:176-179 (numpy)."""
-    ds = ((x[:, np.newaxis] - y) ** 2).sum(-1)
-    return np.exp(-ds / (2 * sig ** 2))
-
-
-def inv_kernel(xc, yc, sig_interp=20) -> torch.Tensor:
-    """datashift.py:213-219: ``iKxx`` for the drift interpolation."""
-    xp = np.vstack((xc, yc)).T
-    Kxx = torch.from_numpy(kernel2D(xp, xp, sig_interp))
-    return torch.linalg.inv(Kxx + 0.01 * torch.eye(Kxx.shape[0], dtype=Kxx.dtype))
-
-
-def get_drift_matrix(xc, yc, dshift, iKxx: torch.Tensor, sig_interp=20) -> torch.Tensor:
-    """preprocessing.py:44-69 with nblocks == 1 (scalar shift)."""
-    xp = np.vstack((xc, yc)).T
-    yp = xp.copy()
-    yp[:, 1] -= dshift
-    xp = torch.from_numpy(xp)
-    yp = torch.from_numpy(yp)
-    ds = ((yp.unsqueeze(1) - xp) ** 2).sum(-1)
-    Kyx = torch.exp(-ds / (2 * sig_interp ** 2))
-    return Kyx @ iKxx.to(Kyx.dtype)
-
 
 def prepare_matching(wPCA: torch.Tensor, U: torch.Tensor, nt: int) -> torch.Tensor:
     """template_matching.py:110-121: ctc[i, j, l] template cross-correlations."""
-    W = wPCA.contiguous()
-    WtW = conv1d(W.reshape(-1, 1, nt), W.reshape(-1, 1, nt), padding=nt)
-    WtW = torch.flip(WtW, [2, ])
-    UtU = torch.einsum('ikl, jml -> ijkm', U, U)
-    return torch.einsum('ijkm, kml -> ijl', UtU, WtW)
-
-
-def prepare_extract(xc, yc, U: torch.Tensor, nC: int):
-    """template_matching.py:20-26: nearest-channel tables for PC features."""
-    ds = (xc - xc[:, np.newaxis]) ** 2 + (yc - yc[:, np.newaxis]) ** 2
-    iCC = torch.from_numpy(np.argsort(ds, 0)[:nC])
-    iU = torch.argmax((U ** 2).sum(1), -1)
-    Ucc = U[torch.arange(U.shape[0]), :, iCC[:, iU]]
-    return iCC, iU, Ucc
+    assert wPCA.shape[1] == nt
+    return _setup.prepare_matching(wPCA, U)
 
 
 # --------------------------------------------------------------------------

@@ -86,3 +86,40 @@ def test_bf16_recheck_agreement_on_synthetic_recording():
     assert len(a) > 1000
     assert st['recheck_columns'] > 0
     assert len(a & b) >= 0.99 * max(len(a), len(b)), (len(a), len(b), len(a & b), st)
+
+
+def test_bf16_recheck_at_800_templates_with_near_duplicates():
+    """384 channels, 800 templates of which 10 % are near-duplicate pairs
+    (centres 10 um apart: runner-up decisions sit close to the best), drift
+    on: the BF16 + FP32 re-check path keeps >= 0.99 spike agreement with the
+    FP32 path, and its score field stays within the bf16 rounding bound of the
+    FP32 path's (|dB| <= 2^-7 ||U_t|| ||P_s||, re-scored columns exact)."""
+    from livespikesorter_b200 import synth
+    from livespikesorter_b200.sorter import Sorter
+    setup, rec = synth.config(2, duration_s=4.0, seed=19, T=800)
+    s32 = Sorter.from_setup(setup)
+    s16 = Sorter.from_setup(setup, precision='bf16')
+    NT, nt = setup.NT, setup.nt
+    ib = 1
+    rows = np.ascontiguousarray(rec.raw[ib * NT - nt: ib * NT + NT + nt])
+    M = setup.drift_matrix(rec.dshift[ib])
+    s32.set_drift(M)
+    s16.set_drift(M)
+    r32 = s32.sort_batch(rows, ib, rec.n_batches)
+    r16 = s16.sort_batch(rows, ib, rec.n_batches)
+    st = s16.stats()
+    a = set(zip(r32['time'].tolist(), r32['template'].tolist()))
+    b = set(zip(r16['time'].tolist(), r16['template'].tolist()))
+    assert len(a) > 10000
+    assert st['recheck_columns'] > 0
+    assert len(a & b) >= 0.99 * max(len(a), len(b)), (len(a), len(b), len(a & b), st)
+    # score fields of one filtered batch
+    X = s32.filter(rows, ib, rec.n_batches)
+    B32 = s32.scores(X).double()
+    B16 = s16.scores(X).double()
+    U = setup.U.double().cuda()
+    P = torch.nn.functional.conv1d(X.double().unsqueeze(1), setup.wPCA.double().cuda().unsqueeze(1), padding=nt // 2)
+    bound = 2.0 ** -7 * U.reshape(U.shape[0], -1).norm(dim=1)[:, None] * P.permute(1, 0, 2).reshape(-1, P.shape[-1]).norm(dim=0)[None]
+    err = (B16 - B32).abs()
+    assert bool((err <= bound + 1e-6).all())
+    assert int(((B16 == B32).all(dim=0)).sum()) >= s16.stats()['recheck_rescored']
