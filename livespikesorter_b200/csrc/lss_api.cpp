@@ -118,7 +118,10 @@ int lss::rebuild_uw(lss_handle* h) {
     h->stats.launches += 1;
     if (bf16) {
         CK(launch_build_uw(h->U.p, h->Mw.p, h->T, h->K, C, h->CKpad, h->Uw16.p, nullptr, nullptr, 0));
-        h->stats.launches += 1;
+        // template norms of the BF16 error bound, for the folded and the plain operand
+        CK(launch_row_norms(h->Uw_hi.p, h->Uw_lo.p, h->T, h->CKpad, h->un_w.p, 0));
+        CK(launch_row_norms(h->Up_hi.p, h->Up_lo.p, h->T, h->CKpad, h->un_p.p, 0));
+        h->stats.launches += 3;
     }
     // callers may sort on streams that do not wait for the legacy default
     // stream: the batch entry points wait for this event on their stream
@@ -368,14 +371,19 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
         ALLOC(B0T, (size_t)h->N * h->CKpad);
         ALLOC(Up16, (size_t)plan.Tpad * h->CKpad);
         ALLOC(Uw16, (size_t)plan.Tpad * h->CKpad);
-        // FP32 re-check of near decisions: gathered projection rows, bookkeeping
-        const size_t rc_rows = (size_t)(h->N + RECHECK_TILE - 1) / RECHECK_TILE * RECHECK_TILE;
+        // FP32 re-check of open decisions: projection rows of the listed columns, bookkeeping
+        const size_t rc_rows = (size_t)(h->N + 127) / 128 * 128;
         ALLOC(Pc_hi, rc_rows * h->CKpad);
         ALLOC(Pc_lo, rc_rows * h->CKpad);
         ALLOC(cf2, ld);
-        ALLOC(pre_cf, rc_rows);
-        ALLOC(pre_im, rc_rows);
-        ALLOC(rc_tiles, rc_rows / RECHECK_TILE);
+        ALLOC(cf_lo, ld);
+        ALLOC(cf_hi, ld);
+        ALLOC(pn2, ld);
+        ALLOC(un_w, T);
+        ALLOC(un_p, T);
+        ALLOC(pre_cf, ld);
+        ALLOC(pre_im, ld);
+        ALLOC(rc_cols, ld);
         ALLOC(rc_count, 4);
         if (cudaMallocHost(&h->rc_host, 4 * sizeof(int32_t)) != cudaSuccess) {
             g_create_err = "pinned host allocation failed";
@@ -463,7 +471,7 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
             for (int e = 0; e < C * K; ++e) u16[(size_t)i * h->CKpad + e] = __float2bfloat16(up[(size_t)i * C * K + e]);
         CK(cudaMemcpy(h->Up16.p, u16.data(), u16.size() * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice));
         CK(cudaMemset(h->B0T.p, 0, (size_t)h->N * h->CKpad * sizeof(__nv_bfloat16)));
-        const size_t rc_bytes = (size_t)(h->N + RECHECK_TILE - 1) / RECHECK_TILE * RECHECK_TILE * h->CKpad * sizeof(float);
+        const size_t rc_bytes = (size_t)(h->N + 127) / 128 * 128 * h->CKpad * sizeof(float);
         CK(cudaMemset(h->Pc_hi.p, 0, rc_bytes));
         CK(cudaMemset(h->Pc_lo.p, 0, rc_bytes));
     }
@@ -573,7 +581,7 @@ int lss_get_stats(const lss_handle* h, lss_stats* out) {
         }
         out->recheck_columns = h->rc_host[2];
         out->recheck_flips = h->rc_host[1];
-        out->recheck_rescored = std::min<int64_t>((int64_t)h->rc_host[0] * RECHECK_TILE, h->last_scored);
+        out->recheck_rescored = h->rc_host[0];
     }
     return LSS_OK;
 }
@@ -662,29 +670,35 @@ int lss::run_ingest(lss_handle* h, const int16_t* src, const IngestMap& map, flo
 int lss::run_scores(lss_handle* h, const float* X, int64_t ldx, int64_t N, float* B, cudaStream_t s,
                    bool* maxima_ready, bool folded) {
     if (h->cfg.precision == LSS_PREC_BF16_RECHECK) {
-        CK(launch_pca_proj_t(X, ldx, h->C, N, h->wpca.p, h->K, h->nt, h->B0T.p, h->CKpad, s));
+        CK(launch_pca_proj_t(X, ldx, h->C, N, h->wpca.p, h->K, h->nt, h->B0T.p, h->CKpad, s, h->pn2.p));
         h->mark(5, s);
         TcExtra ex;
         ex.cf2 = h->cf2.p;
+        ex.un = folded ? h->un_w.p : h->un_p.p;
+        ex.pn2 = h->pn2.p;
+        ex.eps = BF16_SCORE_EPS;
+        ex.cf_lo = h->cf_lo.p;
+        ex.cf_hi = h->cf_hi.p;
         CK(launch_score_tc(h->B0T.p, h->CKpad, (int)N, folded ? h->Uw16.p : h->Up16.p, h->T, h->CKpad, h->nm.p, B,
                            h->ld, h->cfmax.p, h->imax.p, h->nt, h->status.p, h->sm_count, s, ex));
-        // FP32 re-check of the tiles holding columns whose decisions lie within
-        // the margin; the tile list and its length stay on the device
+        // FP32 re-check of the columns whose first-round decisions the BF16
+        // error bound leaves open; the column list and its length stay on the
+        // device
         const float th2 = h->cfg.th_learned * h->cfg.th_learned;
-        CK(launch_recheck_select(h->cfmax.p, h->cf2.p, h->imax.p, (int)N, h->nt, th2, h->rc_tiles.p, h->pre_cf.p,
-                                 h->pre_im.p, h->rc_count.p, s));
-        CK(launch_pca_proj_tiles_tf32(X, ldx, h->C, N, h->wpca.p, h->K, h->nt, h->rc_tiles.p, h->rc_count.p,
-                                      h->Pc_hi.p, h->Pc_lo.p, h->CKpad, s));
+        CK(launch_recheck_select(h->cf_lo.p, h->cf_hi.p, h->cf2.p, h->cfmax.p, h->imax.p, (int)N, h->nt, th2,
+                                 h->rc_cols.p, h->pre_cf.p, h->pre_im.p, h->rc_count.p, s));
+        CK(launch_pca_proj_cols_tf32(X, ldx, h->C, N, h->wpca.p, h->K, h->nt, h->rc_cols.p, h->rc_count.p, h->Pc_hi.p,
+                                     h->Pc_lo.p, h->CKpad, s));
         TcExtra ex2;
-        ex2.rowmap = h->rc_tiles.p;
-        ex2.map_rows = RECHECK_TILE;
+        ex2.rowmap = h->rc_cols.p;
+        ex2.map_rows = 1;
         ex2.count_dev = h->rc_count.p;
         ex2.ncols = (int)N;
-        const int max_rows = (int)((N + RECHECK_TILE - 1) / RECHECK_TILE * RECHECK_TILE);
+        const int max_rows = (int)((N + 127) / 128 * 128);
         CK(launch_score_tc_tf32x3(h->Pc_hi.p, h->Pc_lo.p, h->CKpad, max_rows, folded ? h->Uw_hi.p : h->Up_hi.p,
                                   folded ? h->Uw_lo.p : h->Up_lo.p, h->T, h->CKpad, h->nm.p, B, h->ld, h->cfmax.p,
                                   h->imax.p, h->nt, h->status.p, h->sm_count, s, ex2));
-        CK(launch_recheck_flips(h->cfmax.p, h->imax.p, h->rc_tiles.p, h->pre_cf.p, h->pre_im.p, h->rc_count.p, (int)N,
+        CK(launch_recheck_flips(h->cfmax.p, h->imax.p, h->rc_cols.p, h->pre_cf.p, h->pre_im.p, h->rc_count.p, (int)N,
                                 th2, s));
         if (!h->capturing) {
             CK(cudaMemcpyAsync(h->rc_host, h->rc_count.p, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost, s));

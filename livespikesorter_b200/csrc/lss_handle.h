@@ -76,8 +76,10 @@ struct lss_handle {
     DevBuf<float> Uw_hi, Uw_lo;                  // ... (FP32 path)
     DevBuf<float> U, R;                          // U [T,K,C]; R [K,K,2nt-1] basis lag correlations
     DevBuf<float2> hpH, hpTw;                    // highpass spectrum and twiddles (FFT form)
-    DevBuf<float> cf2, pre_cf, Pc_hi, Pc_lo;     // BF16 re-check: runner-up Cf, saved maxima, gathered projection
-    DevBuf<int32_t> rc_tiles, pre_im, rc_count;  // ... listed tiles, saved argmax, [tiles, flips, near columns]
+    // BF16 re-check: largest other upper bound of Cf, bounds of the best Cf, saved maxima,
+    // projection rows of the listed columns, ||P_s||^2, template norms (folded / plain)
+    DevBuf<float> cf2, cf_lo, cf_hi, pre_cf, Pc_hi, Pc_lo, pn2, un_w, un_p;
+    DevBuf<int32_t> rc_cols, pre_im, rc_count;   // ... listed columns, saved argmax, [columns, flips, columns]
     int32_t* rc_host = nullptr;                  // pinned copy of rc_count (read by lss_get_stats)
     cudaEvent_t rc_ev = nullptr;                 // recorded after that copy
     cudaEvent_t mix_ev = nullptr;                // recorded after the whitening-folded templates are rebuilt
@@ -149,7 +151,8 @@ struct lss_handle {
         rec_pc.release(); B0T.release(); Up16.release();
         B0T_hi.release(); B0T_lo.release(); Up_hi.release(); Up_lo.release();
         Uw16.release(); Uw_hi.release(); Uw_lo.release(); U.release(); R.release(); hpH.release(); hpTw.release();
-        cf2.release(); pre_cf.release(); Pc_hi.release(); Pc_lo.release(); rc_tiles.release(); pre_im.release();
+        cf2.release(); cf_lo.release(); cf_hi.release(); pre_cf.release(); Pc_hi.release(); Pc_lo.release();
+        pn2.release(); un_w.release(); un_p.release(); rc_cols.release(); pre_im.release();
         rc_count.release();
         pk.release(); psort.release(); pkeep.release(); plast.release(); pxy.release(); pcen.release();
         pchan.release(); pclu.release(); rec_x.release(); rec_y.release(); rec_clu.release();

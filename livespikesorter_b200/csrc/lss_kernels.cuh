@@ -46,8 +46,9 @@ cudaError_t launch_sgemm_folded(const float* U, const float* Mw, int32_t T, int3
 
 // ---- temporal basis projection (score.cu) ----
 // transposed bf16 variant for the tensor-core GEMM: B0T[s, c*K + k], row stride ldk
+// norm2 (optional, [N]): ||B0T[s, :]||^2 of the FP32 values before bf16 rounding
 cudaError_t launch_pca_proj_t(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
-                              int32_t nt, __nv_bfloat16* B0T, int64_t ldk, cudaStream_t s);
+                              int32_t nt, __nv_bfloat16* B0T, int64_t ldk, cudaStream_t s, float* norm2 = nullptr);
 
 // ---- tensor-core score GEMM (tc_gemm.cu) ----
 struct TcPlan {
@@ -71,6 +72,14 @@ struct TcExtra {
     int ncols = 0;                    // batch samples when rowmap is set
     float* cf2 = nullptr;             // runner-up Cf per sample
     unsigned long long* keys = nullptr;  // [N] scratch: lets short batches split templates over CTAs
+    // BF16 error bounds: un[t] = ||template row t||, pn2[s] = ||projection row s||^2; with them the
+    // epilogue writes cf_lo / cf_hi (bounds of the FP32 path's best Cf) and, in cf2, the largest
+    // upper bound of any other template, for |B - B_fp32| <= eps * un[t] * sqrt(pn2[s])
+    const float* un = nullptr;
+    const float* pn2 = nullptr;
+    float eps = 0.f;
+    float* cf_lo = nullptr;
+    float* cf_hi = nullptr;
 };
 // B[t, s] (row stride ldb) = sum_kk B0T[s, kk] * Up[t, kk] with B0T [N, ldk] and Up [Tpad, CKpad]
 // bf16, CKpad a multiple of 64; also writes the column maxima cfmax/imax of Cf.
@@ -90,17 +99,20 @@ cudaError_t launch_pca_proj_t_tf32(const float* X, int64_t ldx, int32_t C, int64
 cudaError_t launch_build_uw(const float* U, const float* Mw, int32_t T, int32_t K, int32_t C, int64_t ldk,
                             __nv_bfloat16* out16, float* hi, float* lo, cudaStream_t s);
 
-// FP32 re-check of the BF16 path (score.cu)
-constexpr int RECHECK_TILE = 64;  // samples per re-check tile (= projection CTA width)
-cudaError_t launch_recheck_select(const float* cfmax, const float* cf2, const int32_t* imax, int32_t N, int32_t nt,
-                                  float th2, int32_t* tiles, float* pre_cf, int32_t* pre_im, int32_t* count,
-                                  cudaStream_t s);
-// projection of the listed sample tiles into rows x*RECHECK_TILE.. (tf32 hi/lo), as launch_pca_proj_t_tf32
-cudaError_t launch_pca_proj_tiles_tf32(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
-                                       int32_t nt, const int32_t* tiles, const int32_t* ntiles, float* hi, float* lo,
-                                       int64_t ldk, cudaStream_t s);
-cudaError_t launch_recheck_flips(const float* cfmax, const int32_t* imax, const int32_t* tiles, const float* pre_cf,
+// FP32 re-check of the BF16 path (score.cu): columns whose first-round
+// decisions the BF16 error bound leaves open, their FP32 projection rows and
+// the count of decisions the re-check changed
+constexpr float BF16_SCORE_EPS = 0.0078125f;  // 2^-7: |B16 - B32| <= eps ||U_t|| ||P_s||
+cudaError_t launch_recheck_select(const float* cf_lo, const float* cf_hi, const float* ch, const float* cfmax,
+                                  const int32_t* imax, int32_t N, int32_t nt, float th2, int32_t* cols, float* pre_cf,
+                                  int32_t* pre_im, int32_t* count, cudaStream_t s);
+cudaError_t launch_pca_proj_cols_tf32(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
+                                      int32_t nt, const int32_t* cols, const int32_t* count, float* hi, float* lo,
+                                      int64_t ldk, cudaStream_t s);
+cudaError_t launch_recheck_flips(const float* cfmax, const int32_t* imax, const int32_t* cols, const float* pre_cf,
                                  const int32_t* pre_im, int32_t* count, int32_t N, float th2, cudaStream_t s);
+// un[t] = ||hi[t, :] + lo[t, :]|| over rows of length ld
+cudaError_t launch_row_norms(const float* hi, const float* lo, int32_t T, int64_t ld, float* un, cudaStream_t s);
 
 // ---- matching pursuit (mp.cu) ----
 struct MPArgs {

@@ -34,7 +34,8 @@ template <int KPC, int PC, bool TF32, int NTP>
 __global__ void __launch_bounds__(256) k_pca_proj_t(const float* __restrict__ X, int64_t ldx, int32_t C, int64_t N,
                                                     const float* __restrict__ wpca, int32_t nt, void* __restrict__ out0,
                                                     float* __restrict__ out_lo, int64_t ldk,
-                                                    const int32_t* __restrict__ tiles, const int32_t* __restrict__ ntiles) {
+                                                    const int32_t* __restrict__ tiles, const int32_t* __restrict__ ntiles,
+                                                    float* __restrict__ norm2) {
     extern __shared__ float sm[];
     // tiles != null: CTA x projects sample tile tiles[x] into output rows x*PT_S.. (the first *ntiles entries)
     if (tiles && (int)blockIdx.x >= *ntiles) return;
@@ -132,13 +133,21 @@ __global__ void __launch_bounds__(256) k_pca_proj_t(const float* __restrict__ X,
                 static_cast<__nv_bfloat16*>(out0)[orow + j] = __float2bfloat16_rn(v);
             }
         }
+        if (norm2) {
+            // this channel group's share of ||P[s, :]||^2 (the FP32 values, before rounding)
+            float q = 0.f;
+            for (int j = lane; j < seg; j += 32) q = fmaf(srow[j], srow[j], q);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) q += __shfl_xor_sync(0xffffffffu, q, o);
+            if (lane == 0) atomicAdd(norm2 + s, q);
+        }
     }
 }
 
 template <int KPC, bool TF32>
 static cudaError_t launch_pjt(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t nt,
                               void* out0, float* out_lo, int64_t ldk, const int32_t* tiles, const int32_t* ntiles,
-                              cudaStream_t s) {
+                              float* norm2, cudaStream_t s) {
     constexpr int PC = 32;
     const int ntp = (nt + 7) & ~7;
     const size_t smem = sizeof(float) * ((size_t)KPC * ntp + (size_t)PC * (PT_S + ntp + 9) + 4 + (size_t)PT_S * PC * KPC);
@@ -146,11 +155,11 @@ static cudaError_t launch_pjt(const float* X, int64_t ldx, int32_t C, int64_t N,
     if (ntp == 64) {  // nt = 57..64 (Kilosort's 61): taps fully unrolled
         auto kern = k_pca_proj_t<KPC, PC, TF32, 64>;
         if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        kern<<<grid, 256, smem, s>>>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles);
+        kern<<<grid, 256, smem, s>>>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles, norm2);
     } else {
         auto kern = k_pca_proj_t<KPC, PC, TF32, 0>;
         if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        kern<<<grid, 256, smem, s>>>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles);
+        kern<<<grid, 256, smem, s>>>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles, norm2);
     }
     return cudaGetLastError();
 }
@@ -158,35 +167,34 @@ static cudaError_t launch_pjt(const float* X, int64_t ldx, int32_t C, int64_t N,
 template <bool TF32>
 static cudaError_t pjt_dispatch(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
                                 int32_t nt, void* out0, float* out_lo, int64_t ldk, const int32_t* tiles,
-                                const int32_t* ntiles, cudaStream_t s) {
+                                const int32_t* ntiles, float* norm2, cudaStream_t s) {
+    if (norm2) {
+        const cudaError_t e = cudaMemsetAsync(norm2, 0, sizeof(float) * N, s);
+        if (e != cudaSuccess) return e;
+    }
     switch (K) {
-        case 1: return launch_pjt<1, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles, s);
-        case 2: return launch_pjt<2, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles, s);
-        case 3: return launch_pjt<3, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles, s);
-        case 4: return launch_pjt<4, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles, s);
-        case 5: return launch_pjt<5, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles, s);
-        case 6: return launch_pjt<6, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles, s);
-        case 7: return launch_pjt<7, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles, s);
-        case 8: return launch_pjt<8, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles, s);
+        case 1: return launch_pjt<1, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles, norm2, s);
+        case 2: return launch_pjt<2, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles, norm2, s);
+        case 3: return launch_pjt<3, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles, norm2, s);
+        case 4: return launch_pjt<4, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles, norm2, s);
+        case 5: return launch_pjt<5, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles, norm2, s);
+        case 6: return launch_pjt<6, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles, norm2, s);
+        case 7: return launch_pjt<7, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles, norm2, s);
+        case 8: return launch_pjt<8, TF32>(X, ldx, C, N, wpca, nt, out0, out_lo, ldk, tiles, ntiles, norm2, s);
         default: return cudaErrorInvalidValue;
     }
 }
 
 cudaError_t launch_pca_proj_t(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
-                              int32_t nt, __nv_bfloat16* B0T, int64_t ldk, cudaStream_t s) {
-    return pjt_dispatch<false>(X, ldx, C, N, wpca, K, nt, B0T, nullptr, ldk, nullptr, nullptr, s);
+                              int32_t nt, __nv_bfloat16* B0T, int64_t ldk, cudaStream_t s, float* norm2) {
+    return pjt_dispatch<false>(X, ldx, C, N, wpca, K, nt, B0T, nullptr, ldk, nullptr, nullptr, norm2, s);
 }
 
 cudaError_t launch_pca_proj_t_tf32(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
                                    int32_t nt, float* hi, float* lo, int64_t ldk, cudaStream_t s) {
-    return pjt_dispatch<true>(X, ldx, C, N, wpca, K, nt, hi, lo, ldk, nullptr, nullptr, s);
+    return pjt_dispatch<true>(X, ldx, C, N, wpca, K, nt, hi, lo, ldk, nullptr, nullptr, nullptr, s);
 }
 
-cudaError_t launch_pca_proj_tiles_tf32(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
-                                       int32_t nt, const int32_t* tiles, const int32_t* ntiles, float* hi, float* lo,
-                                       int64_t ldk, cudaStream_t s) {
-    return pjt_dispatch<true>(X, ldx, C, N, wpca, K, nt, hi, lo, ldk, tiles, ntiles, s);
-}
 
 // Templates with the whitening folded in, in the score GEMM's layout:
 //   U_w[t, c'*K + k] = sum_c U[t, k, c] * Mw[c, c']       (Mw = M @ Wrot)
@@ -202,114 +210,189 @@ cudaError_t launch_build_uw(const float* U, const float* Mw, int32_t T, int32_t 
 
 
 // ---------------------------------------------------------------------------
-// FP32 re-check of the BF16 path's near decisions (first round).
+// FP32 re-check of the BF16 path (first round), column by column.
 //
-// A column s needs its FP32 score when its BF16 maximum Cf could be above the
-// threshold (best >= Th^2 (1 - m)) and a decision taken on it lies within the
-// relative margin m = 1/16:
-//   * the threshold itself: |best - Th^2| <= m Th^2;
-//   * the runner-up template: second >= best (1 - m);
-//   * the peak test: best is within m of the window maximum and another column
-//     of the window is within m of best.
-// (BF16 rounding of both GEMM operands moves Cf by about 1% at the scores
-// spikes have, so m is several times the error.) Selection works on 64-sample
-// tiles (the projection's CTA width): a tile holding any such column is listed,
-// projected in FP32 by the FP32 path's own projection kernel, split into tf32
-// hi/lo and re-scored by the 3xTF32 GEMM through the tile list, which
-// overwrites the tile's scores and column maxima with the FP32 path's values.
-// Counts stay on the device: count[0] = listed tiles, count[1] = flips,
-// count[2] = near-decision columns.
+// Every BF16 score is within dB = 2^-7 ||U_t|| ||P_s|| of the FP32 path's
+// (bf16 rounding of both operands moves each product by at most 2^-8 of its
+// magnitude, sum |U||P| <= ||U|| ||P||, and both paths accumulate in FP32 with
+// errors far below that). From it the BF16 GEMM's epilogue gives each column
+// an interval [cf_lo, cf_hi] that holds the FP32 path's column maximum of Cf
+// for the same best template, and ch, the largest upper bound of Cf over the
+// other templates. The FP32 path's first-round decisions at a column can
+// differ from the BF16 path's only when
+//   * threshold:     cf_lo <= Th^2 < cf_hi;
+//   * best template: ch >= cf_lo (and cf_hi > Th^2);
+//   * peak test:     the interval of a column of the +-nt window overlaps the
+//                    column's own, and one of the two can exceed Th^2
+//                    (edge columns are exactly zero in both paths).
+// Those columns, and only those, are listed, projected with the FP32 path's
+// arithmetic and re-scored by its 3xTF32 GEMM through the list, which
+// overwrites their scores with the FP32 path's values; every other column's
+// first-round decisions are then provably the FP32 path's. count[0] = listed
+// columns, count[1] = decisions the re-check changed, count[2] = listed.
 // ---------------------------------------------------------------------------
-constexpr float RECHECK_MARGIN = 1.f / 16.f;
-constexpr int RS_TILE = 256;
-static_assert(RECHECK_TILE == PT_S, "re-check tiles are projection CTA tiles");
-static_assert(RS_TILE % RECHECK_TILE == 0, "selection CTAs cover whole re-check tiles");
+constexpr int RS_COLS = 256;
+constexpr int RS_MAX_NT = 256;
 
-__global__ void __launch_bounds__(RS_TILE) k_recheck_select(const float* __restrict__ cfmax, const float* __restrict__ cf2,
+__global__ void __launch_bounds__(RS_COLS) k_recheck_select(const float* __restrict__ cf_lo,
+                                                            const float* __restrict__ cf_hi,
+                                                            const float* __restrict__ ch,
+                                                            const float* __restrict__ cfmax,
                                                             const int32_t* __restrict__ imax, int32_t N, int32_t nt,
-                                                            float th2, int32_t* __restrict__ tiles,
+                                                            float th2, int32_t* __restrict__ cols,
                                                             float* __restrict__ pre_cf, int32_t* __restrict__ pre_im,
                                                             int32_t* __restrict__ count) {
-    constexpr int NTL = RS_TILE / RECHECK_TILE;
-    __shared__ float v[RS_TILE + 2 * 256];
-    __shared__ int flag[NTL], slot[NTL];
-    const int s0 = blockIdx.x * RS_TILE;
-    for (int p = threadIdx.x; p < RS_TILE + 2 * nt; p += blockDim.x) {
+    __shared__ float lo_s[RS_COLS + 2 * RS_MAX_NT], hi_s[RS_COLS + 2 * RS_MAX_NT];
+    const int s0 = blockIdx.x * RS_COLS;
+    for (int p = threadIdx.x; p < RS_COLS + 2 * nt; p += blockDim.x) {
         const int s = s0 - nt + p;
-        v[p] = (s >= 0 && s < N) ? cfmax[s] : -1.f;
+        const bool in = s >= nt && s < N - nt;  // edge and outside columns: exactly zero
+        lo_s[p] = in ? cf_lo[s] : 0.f;
+        hi_s[p] = in ? cf_hi[s] : 0.f;
     }
-    if (threadIdx.x < NTL) flag[threadIdx.x] = 0;
     __syncthreads();
     const int s = s0 + threadIdx.x;
-    const float best = v[threadIdx.x + nt];
     bool sel = false;
-    if (s < N) {
-        const float m = RECHECK_MARGIN;
-        if (best >= th2 * (1.f - m)) {
-            float wmax = best, other = -1.f;
-            for (int d = -nt; d <= nt; ++d) {
-                if (d == 0) continue;
-                const float u = v[threadIdx.x + nt + d];
-                wmax = fmaxf(wmax, u);
-                other = fmaxf(other, u);
-            }
-            const bool near_thr = fabsf(best - th2) <= m * th2;
-            const bool near_tmpl = cf2[s] >= best * (1.f - m);
-            const bool near_peak = best >= wmax * (1.f - m) && other >= best * (1.f - m);
-            sel = near_thr || near_tmpl || near_peak;
+    if (s >= nt && s < N - nt) {
+        const float lo = lo_s[threadIdx.x + nt], hi = hi_s[threadIdx.x + nt];
+        if (hi > th2 && (lo <= th2 || ch[s] >= lo)) sel = true;
+        for (int d = -nt; d <= nt && !sel; ++d) {
+            if (d == 0) continue;
+            const float lv = lo_s[threadIdx.x + nt + d], hv = hi_s[threadIdx.x + nt + d];
+            if ((hi > th2 || hv > th2) && hv >= lo && hi >= lv) sel = true;
         }
     }
     const unsigned bal = __ballot_sync(0xffffffffu, sel);
-    if (bal) {
-        if ((threadIdx.x & 31) == 0) atomicAdd(count + 2, __popc(bal));
-        flag[threadIdx.x / RECHECK_TILE] = 1;
+    const int lane = threadIdx.x & 31;
+    int base = 0;
+    if (lane == 0 && bal) {
+        base = atomicAdd(count, __popc(bal));
+        atomicAdd(count + 2, __popc(bal));
     }
-    __syncthreads();
-    if (threadIdx.x < NTL) {
-        int sl = -1;
-        if (flag[threadIdx.x]) {
-            sl = atomicAdd(count, 1);
-            tiles[sl] = s0 / RECHECK_TILE + threadIdx.x;
-        }
-        slot[threadIdx.x] = sl;
-    }
-    __syncthreads();
-    const int sl = slot[threadIdx.x / RECHECK_TILE];
-    if (sl >= 0) {
-        const int64_t r = (int64_t)sl * RECHECK_TILE + threadIdx.x % RECHECK_TILE;
-        pre_cf[r] = (s < N) ? best : 0.f;
-        pre_im[r] = (s < N) ? imax[s] : 0;
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (sel) {
+        const int i = base + __popc(bal & ((1u << lane) - 1u));
+        cols[i] = s;
+        pre_cf[i] = cfmax[s];
+        pre_im[i] = imax[s];
     }
 }
 
-cudaError_t launch_recheck_select(const float* cfmax, const float* cf2, const int32_t* imax, int32_t N, int32_t nt,
-                                  float th2, int32_t* tiles, float* pre_cf, int32_t* pre_im, int32_t* count,
-                                  cudaStream_t s) {
-    if (nt > 256) return cudaErrorInvalidValue;
+cudaError_t launch_recheck_select(const float* cf_lo, const float* cf_hi, const float* ch, const float* cfmax,
+                                  const int32_t* imax, int32_t N, int32_t nt, float th2, int32_t* cols, float* pre_cf,
+                                  int32_t* pre_im, int32_t* count, cudaStream_t s) {
+    if (nt > RS_MAX_NT) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(count, 0, 4 * sizeof(int32_t), s);
     if (e != cudaSuccess) return e;
-    k_recheck_select<<<(N + RS_TILE - 1) / RS_TILE, RS_TILE, 0, s>>>(cfmax, cf2, imax, N, nt, th2, tiles, pre_cf,
-                                                                    pre_im, count);
+    k_recheck_select<<<(N + RS_COLS - 1) / RS_COLS, RS_COLS, 0, s>>>(cf_lo, cf_hi, ch, cfmax, imax, N, nt, th2, cols,
+                                                                    pre_cf, pre_im, count);
     return cudaGetLastError();
+}
+
+// FP32 projection of the listed columns into rows 0.. of hi / lo (tf32 split),
+// with k_pca_proj_t's arithmetic: every output sums its (zero-padded) taps in
+// ascending order with one fmaf each, so the rows equal the FP32 path's.
+template <int KPC>
+__global__ void __launch_bounds__(128) k_pca_proj_cols(const float* __restrict__ X, int64_t ldx, int32_t C, int64_t N,
+                                                       const float* __restrict__ wpca, int32_t nt, int32_t ntp,
+                                                       const int32_t* __restrict__ cols,
+                                                       const int32_t* __restrict__ count, float* __restrict__ hi,
+                                                       float* __restrict__ lo, int64_t ldk) {
+    extern __shared__ float ws[];  // [KPC][ntp]
+    const int i = blockIdx.x;
+    if (i >= *count) return;
+    const int64_t s = cols[i];
+    for (int e = threadIdx.x; e < KPC * ntp; e += blockDim.x) {
+        const int k = e / ntp, m = e % ntp;
+        ws[e] = (m < nt) ? wpca[k * nt + m] : 0.f;
+    }
+    __syncthreads();
+    const int half = nt / 2;
+    for (int c = threadIdx.x; c < C; c += blockDim.x) {
+        const float* xr = X + (int64_t)c * ldx;
+        float acc[KPC];
+#pragma unroll
+        for (int k = 0; k < KPC; ++k) acc[k] = 0.f;
+        for (int m = 0; m < ntp; ++m) {
+            const int64_t g = s - half + m;
+            const float xv = (g >= 0 && g < N) ? xr[g] : 0.f;
+#pragma unroll
+            for (int k = 0; k < KPC; ++k) acc[k] = fmaf(ws[k * ntp + m], xv, acc[k]);
+        }
+        const int64_t o = (int64_t)i * ldk + (int64_t)c * KPC;
+#pragma unroll
+        for (int k = 0; k < KPC; ++k) {
+            const float h = tf32_rna(acc[k]);
+            hi[o + k] = h;
+            lo[o + k] = __fsub_rn(acc[k], h);
+        }
+    }
+}
+
+template <int KPC>
+static cudaError_t launch_cols(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t nt,
+                               const int32_t* cols, const int32_t* count, float* hi, float* lo, int64_t ldk,
+                               cudaStream_t s) {
+    const int ntp = (nt + 7) & ~7;
+    const size_t smem = sizeof(float) * KPC * ntp;
+    if (smem > 48 * 1024) return cudaErrorInvalidValue;
+    k_pca_proj_cols<KPC><<<(unsigned)N, 128, smem, s>>>(X, ldx, C, N, wpca, nt, ntp, cols, count, hi, lo, ldk);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pca_proj_cols_tf32(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
+                                      int32_t nt, const int32_t* cols, const int32_t* count, float* hi, float* lo,
+                                      int64_t ldk, cudaStream_t s) {
+    switch (K) {
+        case 1: return launch_cols<1>(X, ldx, C, N, wpca, nt, cols, count, hi, lo, ldk, s);
+        case 2: return launch_cols<2>(X, ldx, C, N, wpca, nt, cols, count, hi, lo, ldk, s);
+        case 3: return launch_cols<3>(X, ldx, C, N, wpca, nt, cols, count, hi, lo, ldk, s);
+        case 4: return launch_cols<4>(X, ldx, C, N, wpca, nt, cols, count, hi, lo, ldk, s);
+        case 5: return launch_cols<5>(X, ldx, C, N, wpca, nt, cols, count, hi, lo, ldk, s);
+        case 6: return launch_cols<6>(X, ldx, C, N, wpca, nt, cols, count, hi, lo, ldk, s);
+        case 7: return launch_cols<7>(X, ldx, C, N, wpca, nt, cols, count, hi, lo, ldk, s);
+        case 8: return launch_cols<8>(X, ldx, C, N, wpca, nt, cols, count, hi, lo, ldk, s);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 // Decisions the FP32 re-check changed: the best template, or the side of the
 // threshold the column maximum falls on.
 __global__ void k_recheck_flips(const float* __restrict__ cfmax, const int32_t* __restrict__ imax,
-                                const int32_t* __restrict__ tiles, const float* __restrict__ pre_cf,
-                                const int32_t* __restrict__ pre_im, const int32_t* __restrict__ count, int32_t N,
-                                float th2, int32_t* flips) {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= count[0] * RECHECK_TILE) return;
-    const int s = tiles[r / RECHECK_TILE] * RECHECK_TILE + r % RECHECK_TILE;
-    if (s >= N) return;
-    if (imax[s] != pre_im[r] || ((cfmax[s] > th2) != (pre_cf[r] > th2))) atomicAdd(flips, 1);
+                                const int32_t* __restrict__ cols, const float* __restrict__ pre_cf,
+                                const int32_t* __restrict__ pre_im, const int32_t* __restrict__ count, float th2,
+                                int32_t* flips) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count[0]) return;
+    const int s = cols[i];
+    if (imax[s] != pre_im[i] || ((cfmax[s] > th2) != (pre_cf[i] > th2))) atomicAdd(flips, 1);
 }
 
-cudaError_t launch_recheck_flips(const float* cfmax, const int32_t* imax, const int32_t* tiles, const float* pre_cf,
+cudaError_t launch_recheck_flips(const float* cfmax, const int32_t* imax, const int32_t* cols, const float* pre_cf,
                                  const int32_t* pre_im, int32_t* count, int32_t N, float th2, cudaStream_t s) {
-    const int rows = (N + RECHECK_TILE - 1) / RECHECK_TILE * RECHECK_TILE;
-    k_recheck_flips<<<(rows + 255) / 256, 256, 0, s>>>(cfmax, imax, tiles, pre_cf, pre_im, count, N, th2, count + 1);
+    k_recheck_flips<<<(N + 255) / 256, 256, 0, s>>>(cfmax, imax, cols, pre_cf, pre_im, count, th2, count + 1);
+    return cudaGetLastError();
+}
+
+// un[t] = ||hi[t, :] + lo[t, :]|| (rows of the tf32-split template operand,
+// summed in double, rounded up): the template norms of the BF16 error bound
+__global__ void k_row_norms(const float* __restrict__ hi, const float* __restrict__ lo, int32_t T, int64_t ld,
+                            float* __restrict__ un) {
+    const int t = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (t >= T) return;
+    double q = 0.0;
+    for (int64_t e = lane; e < ld; e += 32) {
+        const double v = (double)hi[t * ld + e] + (double)lo[t * ld + e];
+        q += v * v;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) q += __shfl_xor_sync(0xffffffffu, q, o);
+    if (lane == 0) un[t] = __double2float_ru(__dsqrt_ru(q));
+}
+
+cudaError_t launch_row_norms(const float* hi, const float* lo, int32_t T, int64_t ld, float* un, cudaStream_t s) {
+    k_row_norms<<<(T + 7) / 8, 256, 0, s>>>(hi, lo, T, ld, un);
     return cudaGetLastError();
 }
 

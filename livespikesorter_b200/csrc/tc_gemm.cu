@@ -70,6 +70,14 @@ struct Args {
     int pass_w;               // templates per pass (<= MAX_NP)
     unsigned long long* keys; // split mode: one work item per (sample tile, pass); column maxima are
                               // combined as atomicMax of (Cf bits << 32 | ~t) (null: a CTA owns whole rows)
+    // error bounds (BF16 path): |B - B_fp32| <= eps * un[t] * sqrt(pn2[s]) per score; per column
+    // the epilogue writes cf_lo (lower bound of the best template's Cf), cf_hi (upper bound of
+    // the column maximum) and, in cf2, the largest upper bound of any other template
+    const float* un;
+    const float* pn2;
+    float eps;
+    float* cf_lo;
+    float* cf_hi;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -239,6 +247,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
     float* s_nm = reinterpret_cast<float*>(tmem_slot + 4);
     float* s_inv = s_nm + a.Tpad;
+    float* s_un = s_inv + a.Tpad;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t s0 = smem_u32(smem);
@@ -265,6 +274,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         const float v = (t < a.T) ? a.nm[t] : 1.f;
         s_nm[t] = v;
         s_inv[t] = __frcp_rn(v);
+        s_un[t] = (a.un && t < a.T) ? a.un[t] : 0.f;
     }
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
@@ -397,8 +407,13 @@ __global__ void __launch_bounds__(THREADS, 1)
             const int n = (a.rowmap && gr < rows) ? a.rowmap[gr / a.map_rows] * a.map_rows + gr % a.map_rows : gr;
             const bool valid = gr < rows && n < a.ncols;
             const bool edge = (n < a.nt) || (n >= a.ncols - a.nt);
-            const bool second = a.cf2 != nullptr;
+            const bool bounds = a.un != nullptr;
+            const bool second = a.cf2 != nullptr && !bounds;
             ColMax m;
+            // bound of this column's score errors per unit template norm
+            const float epsp = (bounds && valid) ? __fmul_ru(a.eps, __fsqrt_ru(a.pn2[n])) : 0.f;
+            float lo_best = 0.f, hi1 = 0.f, hi2 = 0.f;
+            int thi1 = -1;
             for (int p = pb; p < pe; ++p) {
                 const int np = min(PW, a.Tpad - p * PW);
                 if (!mbar_wait(accf_bar(acc), acc_ph[acc], abort_flag, a.status)) { ok = false; break; }
@@ -418,6 +433,24 @@ __global__ void __launch_bounds__(THREADS, 1)
                                 if (!edge) {
                                     if (second) m.consider<true>(v, s_nm[t], s_inv[t], t);
                                     else m.consider<false>(v, s_nm[t], s_inv[t], t);
+                                    if (bounds) {
+                                        // Cf of the FP32 path lies in [lo, hi]: B within +-dB,
+                                        // directed rounding, then a margin for the
+                                        // reciprocal and the rounded squares
+                                        const float dB = __fmul_ru(epsp, s_un[t]);
+                                        const float bh = fmaxf(__fadd_ru(v, dB), 0.f);
+                                        const float bl = fmaxf(__fsub_rd(v, dB), 0.f);
+                                        const float hi = __fmul_ru(__fmul_ru(__fmul_ru(bh, bh), s_inv[t]), 1.000001f);
+                                        const float lo = __fmul_rd(__fmul_rd(__fmul_rd(bl, bl), s_inv[t]), 0.999999f);
+                                        if (m.bi == t) lo_best = lo;  // t just became the best
+                                        if (hi > hi1) {
+                                            hi2 = hi1;
+                                            hi1 = hi;
+                                            thi1 = t;
+                                        } else {
+                                            hi2 = fmaxf(hi2, hi);
+                                        }
+                                    }
                                 }
                             }
                         }
@@ -438,6 +471,11 @@ __global__ void __launch_bounds__(THREADS, 1)
                     a.cfmax[n] = edge ? 0.f : m.best;
                     a.imax[n] = edge ? 0 : m.bi;
                     if (second) a.cf2[n] = edge ? 0.f : m.second;
+                    if (bounds) {
+                        a.cf2[n] = edge ? 0.f : ((thi1 == m.bi) ? hi2 : hi1);
+                        a.cf_lo[n] = edge ? 0.f : lo_best;
+                        a.cf_hi[n] = edge ? 0.f : hi1;
+                    }
                 }
             }
         }
@@ -514,11 +552,11 @@ TcPlan tc_plan(int T, bool tf32, int pass_w) {
     p.b_rows = b_rows;
     const size_t row = tf32 ? 64 : 128, parts = tf32 ? 2 : 1;
     const size_t stage = parts * (tc::BM * row + (size_t)b_rows * row);
-    const size_t tail = 8 * (2 * 4 + 5) + 16 + 8 * (size_t)p.Tpad;
+    const size_t tail = 8 * (2 * 4 + 5) + 16 + 12 * (size_t)p.Tpad;
     const size_t budget = 227 * 1024 - 1024 - tail;
     p.stages = (int)std::min<size_t>(4, budget / stage);
     p.nacc = (np0 <= 256) ? 2 : 1;
-    p.smem = 1024 + (size_t)p.stages * stage + 8 * (2 * p.stages + 5) + 16 + 8 * (size_t)p.Tpad;
+    p.smem = 1024 + (size_t)p.stages * stage + 8 * (2 * p.stages + 5) + 16 + 12 * (size_t)p.Tpad;
     p.kblock = tf32 ? 16 : 64;
     return p;
 }
@@ -568,6 +606,12 @@ static cudaError_t launch_tc(const void* A, const void* Alo, int64_t ldk, int N,
     a.cf2 = ex.cf2;
     a.pass_w = p.pass_w;
     a.keys = split ? ex.keys : nullptr;
+    a.un = split ? nullptr : ex.un;
+    a.pn2 = ex.pn2;
+    a.eps = ex.eps;
+    a.cf_lo = ex.cf_lo;
+    a.cf_hi = ex.cf_hi;
+    if (a.un && (!a.pn2 || !a.cf2 || !a.cf_lo || !a.cf_hi || ex.rowmap)) return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(tc::k_score_tc<TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
     if (e != cudaSuccess) return e;
     const int items = split ? ntiles * ((p.Tpad + p.pass_w - 1) / p.pass_w) : ntiles;
