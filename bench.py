@@ -503,8 +503,7 @@ def bf16_report(s16, s32, rows_d, drifts, ids, nb):
     nbat = len(ids)
     return {'agreement_vs_fp32': common / max(n32, n16, 1), 'spikes_fp32': n32, 'spikes_bf16': n16,
             'common': common, 'recheck_near_columns_per_batch': near / nbat,
-            'recheck_rescored_columns_per_batch': rescored / nbat, 'recheck_flips_per_batch': flips / nbat,
-            'batch_samples': setup.NT}
+            'recheck_rescored_columns_per_batch': rescored / nbat, 'recheck_flips_per_batch': flips / nbat}
 
 
 def oracle_batch(setup, rec, ib, ns=None):

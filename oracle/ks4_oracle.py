@@ -145,13 +145,14 @@ def prepare_matching(wPCA: torch.Tensor, U: torch.Tensor, nt: int) -> torch.Tens
 def run_matching(X: torch.Tensor, U: torch.Tensor, ctc: torch.Tensor, wPCA: torch.Tensor,
                  Th: float, nt: int, dtype=torch.float32, B: torch.Tensor | None = None,
                  nm: torch.Tensor | None = None, max_rounds: int = 100,
-                 capacity: int = 100000, return_rounds=False):
+                 capacity: int = 100000, return_rounds=False, return_field=False):
     """``run_matching`` restated (template_matching.py:128-202).
 
     ``B`` optionally injects the score field (so the rounds can be checked in
     isolation from the score GEMM's rounding); ``nm`` likewise injects the
-    template energies.  Returns ``(st int64 [n,2], amps [n,1], Xres [C,N])`` and,
-    with ``return_rounds``, the round index of every spike.
+    template energies.  Returns ``(st int64 [n,2], amps [n,1], Xres [C,N])``,
+    with ``return_rounds`` also the round index of every spike, and with
+    ``return_field`` the score field left after the last round.
     """
     X = X.to(dtype)
     U = U.to(dtype)
@@ -197,9 +198,8 @@ def run_matching(X: torch.Tensor, U: torch.Tensor, ctc: torch.Tensor, wPCA: torc
         for j in range(n):
             Xres[:, iX[j::n] + tiwave] -= amp[j::n] * torch.einsum('ijk, jl -> kil', U[iY[j::n, 0]], W)
             B[:, iX[j::n] + trange] -= amp[j::n] * ctc[:, iY[j::n, 0], :]
-    if return_rounds:
-        return st[:k], amps[:k], Xres, rounds[:k]
-    return st[:k], amps[:k], Xres
+    out = (st[:k], amps[:k], Xres) + ((rounds[:k],) if return_rounds else ()) + ((B,) if return_field else ())
+    return out
 
 
 def score_field(X: torch.Tensor, U: torch.Tensor, wPCA: torch.Tensor, nt: int,

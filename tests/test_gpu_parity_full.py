@@ -47,19 +47,29 @@ def _oracle(setup, rec, ib, dtype=torch.float32):
     return X, st, amps, Xres, rounds
 
 
-def _report(setup, X, st_o, rounds_o, got, i):
-    """Margins of the first differing decision, and what the FP64 oracle picks."""
+def _report(setup, X, st_o, rounds_o, x_gpu, y_gpu, i):
+    """Margins of the first differing decision on the oracle's own score field
+    at the start of that round (FP32), and what the FP64 oracle picks."""
     nt = setup.nt
     U = setup.U
+    r = int(rounds_o[min(i, len(rounds_o) - 1)])
+    out = ko.run_matching(X, U, setup.ctc, setup.wPCA, setup.Th, nt, max_rounds=r, return_field=True)
+    Br = out[-1].double()
     nm = (U.double() ** 2).sum(-1).sum(-1)
-    B = ko.score_field(X, U, setup.wPCA, nt, dtype=torch.float64)
-    m = ko.margin_report(B, nm, setup.Th, nt)
-    x = int(st_o[i, 0]) if i < len(st_o) else int(got[i, 0]) - setup.NT
+    Cf = torch.relu(Br) ** 2 / nm[:, None]
+    Cf[:, :nt] = 0
+    Cf[:, -nt:] = 0
+    x = int(st_o[i, 0]) if i < len(st_o) else int(x_gpu)
+    col = Cf[:, x]
+    top = torch.topk(col, 2)
+    win = torch.cat([Cf[:, max(0, x - nt):x].max(0).values, Cf[:, x + 1:x + nt + 1].max(0).values])
     st64, _, _ = ko.run_matching(X, U, setup.ctc, setup.wPCA, setup.Th, nt, dtype=torch.float64)
-    return (f'first difference at spike {i} (oracle round {int(rounds_o[i]) if i < len(rounds_o) else "-"}): '
-            f'oracle {st_o[i].tolist() if i < len(st_o) else None}, GPU {got[i].tolist() if i < len(got) else None}; '
-            f'round-1 margins at column {x}: Cf - Th^2 = {float(m["threshold_gap"][x]):.3e}, '
-            f'best - runner-up = {float(m["runner_up_gap"][x]):.3e}; FP64 oracle: {len(st64)} spikes, '
+    return (f'first difference at spike {i} (oracle round {r}): oracle (x, y) = '
+            f'{st_o[i].tolist() if i < len(st_o) else None}, GPU (x, y) = ({int(x_gpu)}, {int(y_gpu)}); '
+            f'oracle field at the start of round {r}, column {x}: best {int(top.indices[0])} Cf {float(top.values[0]):.6e}, '
+            f'runner-up {int(top.indices[1])} Cf {float(top.values[1]):.6e} (relative gap '
+            f'{float((top.values[0] - top.values[1]) / top.values[0]):.3e}), GPU template Cf {float(col[int(y_gpu)]):.6e}, '
+            f'largest other column in the window {float(win.max()):.6e}; FP64 oracle: {len(st64)} spikes, '
             f'{"same" if len(st64) == len(st_o) and torch.equal(st64, st_o) else "different"} sequence as FP32')
 
 
@@ -84,10 +94,12 @@ def _check_batches(T, dup, seed):
         if got.shape != want.shape or not np.array_equal(got, want):
             n = min(len(got), len(want))
             i = int(np.nonzero((got[:n] != want[:n]).any(1))[0][0]) if (got[:n] != want[:n]).any() else n
-            # records of batch 0 drop negative times: map back to matching order
+            # records of batch 0 drop negative times: map back to matching order and columns
             off = 0 if ib != 0 else int(((st[:, 0] - nt - nt // 2 + setup.nt0min) < 0).sum())
+            gi = min(i, len(got) - 1)
+            x_gpu = got[gi, 0] - (ib * NT - nt // 2 + setup.nt0min) + nt
             pytest.fail(f'T={T} batch {ib}: {len(got)} GPU vs {len(want)} oracle spikes; '
-                        + _report(setup, X, st, rounds, torch.from_numpy(got), min(i + off, len(st) - 1)))
+                        + _report(setup, X, st, rounds, x_gpu, got[gi, 1], min(i + off, len(st) - 1)))
         a = r['amplitude'].numpy().astype(np.float64)
         b = ref[:, 2]
         rel = np.abs(a - b) / np.maximum(np.abs(b), 1e-6)
@@ -96,14 +108,6 @@ def _check_batches(T, dup, seed):
         assert np.abs(r['pc'].numpy() - tf).max() <= PC_TOL * np.abs(tf).max(), ib
         total += len(got)
     return total
-
-
-def test_fp32_spike_set_identical_at_384ch_400_templates_with_drift():
-    assert _check_batches(400, dup=False, seed=41) > 15000
-
-
-def test_fp32_spike_set_identical_at_384ch_800_templates_near_duplicates():
-    assert _check_batches(800, dup=True, seed=43) > 30000
 
 
 @pytest.mark.parametrize('T, dup', [(400, False), (800, True)])
@@ -128,3 +132,11 @@ def test_rounds_bit_exact_on_given_scores_at_384ch(T, dup):
     assert torch.equal(amps.cpu(), amps_o)
     stats = s.stats()
     assert 0 < stats['mp_items_updated'] < 0.6 * stats['mp_items'], stats
+
+
+def test_fp32_spike_set_identical_at_384ch_400_templates_with_drift():
+    assert _check_batches(400, dup=False, seed=41) > 15000
+
+
+def test_fp32_spike_set_identical_at_384ch_800_templates_near_duplicates():
+    assert _check_batches(800, dup=True, seed=43) > 30000
