@@ -57,7 +57,9 @@ def build(ptxas_verbose: bool = False) -> Path:
     if LIB.exists() and LIB.stat().st_mtime >= max(o.stat().st_mtime for o in objs):
         return LIB
     tmp = LIB.with_suffix('.so.tmp')
-    cmd = [NVCC, *ARCH, '-shared', '-o', str(tmp), *map(str, objs), '-lcudart_static', '-lrt', '-ldl', '-lpthread']
+    # --no-undefined: a symbol missing from the sources fails the build, not the first dlopen
+    cmd = [NVCC, *ARCH, '-shared', '-Xlinker', '--no-undefined', '-o', str(tmp), *map(str, objs), '-lcudart_static',
+           '-lrt', '-ldl', '-lpthread']
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f'link failed:\n{r.stdout}\n{r.stderr}')

@@ -336,7 +336,7 @@ __device__ __forceinline__ void pc_features_one(
         const int nc = min(FT_CH, C - c0);
         __syncthreads();
         if (Phi) {
-            // projection row of the score GEMM: P[x, c*K + k] = hi + lo
+            // projection row of the score GEMM: P[x, c*K + k] = hi + lo (to 2^-23 relative)
             const int64_t o = (int64_t)x * ldp + (int64_t)c0 * K;
             for (int e = threadIdx.x; e < nc * K; e += blockDim.x) pc[e] = __fadd_rn(Phi[o + e], Plo[o + e]);
         } else {

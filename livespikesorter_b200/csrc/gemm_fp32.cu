@@ -108,7 +108,7 @@ struct StorePlain {
 
 // Folded-template layout of the score GEMM: row m = t*K + k, column n = c'
 // goes to [t, c'*K + k] of a row-stride-ldk array, as bf16 or as the tf32
-// split hi = rna(v), lo = v - hi.
+// split hi = rna(v), lo = rna(v - hi) (both exact tf32 values).
 struct StoreFolded {
     int K;
     int64_t ldk;
@@ -125,7 +125,8 @@ struct StoreFolded {
             asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
             const float h = __uint_as_float(r);
             hi[o] = h;
-            lo[o] = __fsub_rn(v, h);
+            asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(__fsub_rn(v, h)));
+            lo[o] = __uint_as_float(r);
         }
     }
 };

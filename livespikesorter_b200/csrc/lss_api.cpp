@@ -136,7 +136,7 @@ int lss::rebuild_uw(lss_handle* h) {
 // so templates adjacent in this order sit close together and their
 // cross-correlations with distant spikes vanish together). Any order gives the
 // same spikes; this one lets whole blocks be skipped. Then the |ctc| maxima per
-// (spike template, row) and (spike template, block).
+// (spike template, row).
 int lss::rebuild_mp_blocks(lss_handle* h) {
     const int T = h->T, K = h->K, C = h->C, nb = h->mp_nb;
     std::vector<float> u((size_t)T * K * C);
@@ -156,9 +156,9 @@ int lss::rebuild_mp_blocks(lss_handle* h) {
     for (int t = 0; t < T; ++t) perm[t] = t;
     std::stable_sort(perm.begin(), perm.begin() + T, [&](int32_t i, int32_t j) { return com[i] < com[j]; });
     CK(cudaMemcpy(h->mp_perm.p, perm.data(), perm.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
-    CK(launch_ctc_block_max(h->ctcP.p, T, 2 * h->nt + 1, h->mp_perm.p, nb, h->mp_cmaxb.p, h->mp_cmaxr.p, 0));
+    CK(launch_ctc_row_max(h->ctcP.p, T, 2 * h->nt + 1, h->mp_cmaxr.p, 0));
     CK(cudaDeviceSynchronize());
-    h->stats.launches += 2;
+    h->stats.launches += 1;
     return LSS_OK;
 }
 
@@ -426,7 +426,6 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
     ALLOC(colkey, 2 * ld);
     h->mp_nb = (T + MPB_ROWS - 1) / MPB_ROWS;
     ALLOC(mp_perm, (size_t)h->mp_nb * MPB_ROWS);
-    ALLOC(mp_cmaxb, (size_t)T * h->mp_nb);
     ALLOC(mp_cmaxr, (size_t)T * T);
     ALLOC(mp_bkey, (size_t)h->mp_nb * ld);
     ALLOC(mp_bmin, (size_t)h->mp_nb * ld);
@@ -476,18 +475,23 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
         CK(cudaMemset(h->Pc_lo.p, 0, rc_bytes));
     }
     {
-        // U_p split into tf32 hi (round half away, like cvt.rna.tf32.f32) and lo = x - hi
+        // U_p split into tf32 parts, each rounded half away like cvt.rna.tf32.f32:
+        // hi = rna(x), lo = rna(x - hi)
+        auto rna = [](float x) {
+            uint32_t u;
+            std::memcpy(&u, &x, 4);
+            if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x1000u) & 0xffffe000u;
+            float r;
+            std::memcpy(&r, &u, 4);
+            return r;
+        };
         std::vector<float> hi((size_t)Tpad32 * h->CKpad, 0.f), lo(hi.size(), 0.f);
         for (int i = 0; i < T; ++i)
             for (int e = 0; e < C * K; ++e) {
                 const float x = up[(size_t)i * C * K + e];
-                uint32_t u;
-                std::memcpy(&u, &x, 4);
-                if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x1000u) & 0xffffe000u;
-                float xh;
-                std::memcpy(&xh, &u, 4);
+                const float xh = rna(x);
                 hi[(size_t)i * h->CKpad + e] = xh;
-                lo[(size_t)i * h->CKpad + e] = x - xh;
+                lo[(size_t)i * h->CKpad + e] = rna(x - xh);
             }
         CK(cudaMemcpy(h->Up_hi.p, hi.data(), hi.size() * sizeof(float), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(h->Up_lo.p, lo.data(), lo.size() * sizeof(float), cudaMemcpyHostToDevice));
@@ -755,7 +759,6 @@ int lss::enqueue_mp(lss_handle* h, int64_t N, cudaStream_t s, bool maxima_ready)
     a.bar = h->bar.p;
     a.perm = h->mp_perm.p;
     a.nb = h->mp_nb;
-    a.cmaxb = h->mp_cmaxb.p;
     a.cmaxr = h->mp_cmaxr.p;
     a.bkey = h->mp_bkey.p;
     a.bmin = h->mp_bmin.p;

@@ -68,7 +68,7 @@ struct lss_handle {
     // MPB_ROWS ordered along the probe, |ctc| maxima, per-block column state
     int mp_nb = 0;
     DevBuf<int32_t> mp_perm;
-    DevBuf<float> mp_cmaxb, mp_cmaxr, mp_bmin;
+    DevBuf<float> mp_cmaxr, mp_bmin;
     DevBuf<unsigned long long> mp_bkey;
     DevBuf<__nv_bfloat16> B0T, Up16;   // BF16 path: transposed projection, templates
     DevBuf<float> B0T_hi, B0T_lo, Up_hi, Up_lo;  // FP32 path (3xTF32): tf32 hi/lo splits
@@ -146,7 +146,7 @@ struct lss_handle {
         tF.release(); iCC.release(); iU.release(); cfmax.release(); imax.release(); blk_cnt.release();
         blk_x.release(); blk_y.release(); sp_x.release(); sp_y.release(); sp_round.release();
         round_start.release(); counters.release(); status.release(); sp_amp.release(); blk_amp.release(); colkey.release();
-        mp_perm.release(); mp_cmaxb.release(); mp_cmaxr.release(); mp_bmin.release(); mp_bkey.release();
+        mp_perm.release(); mp_cmaxr.release(); mp_bmin.release(); mp_bkey.release();
         bar.release(); rec_time.release(); rec_count.release(); rec_tmpl.release(); rec_slot.release(); rec_amp.release();
         rec_pc.release(); B0T.release(); Up16.release();
         B0T_hi.release(); B0T_lo.release(); Up_hi.release(); Up_lo.release();

@@ -146,7 +146,6 @@ struct MPArgs {
     // blocks of MPB_ROWS (rows of templates close on the probe, by perm)
     const int32_t* perm = nullptr;          // [nb * MPB_ROWS] template of each block row, -1 past T
     int32_t nb = 0;                         // row blocks
-    const float* cmaxb = nullptr;           // [T(spike template), nb] max |ctc| over a block's rows and lags
     const float* cmaxr = nullptr;           // [T(spike template), T(row)] max |ctc| over lags
     unsigned long long* bkey = nullptr;     // [nb, ldk] per block and column: max (Cf bits << 32 | ~t)
     float* bmin = nullptr;                  // [nb, ldk] per block and column: min |B|
@@ -154,13 +153,12 @@ struct MPArgs {
 enum : int32_t { STATUS_TIMEOUT = 1, STATUS_CAPACITY = 2, STATUS_LIST = 4 };
 cudaError_t launch_mp(MPArgs a, int grid, cudaStream_t s);
 // the same rounds, skipping (spike, row block) updates that provably leave
-// every score of the block unchanged; needs perm, nb, cmaxb, cmaxr, bkey, bmin
+// every score of the block unchanged; needs perm, nb, cmaxr, bkey, bmin
 constexpr int MPB_ROWS = 32;
 cudaError_t launch_mp_blocks(MPArgs a, int grid, cudaStream_t s);
 int mp_blocks_max_grid(int device);
-// per (spike template, block) and (spike template, row) maxima of |ctc| over lags
-cudaError_t launch_ctc_block_max(const float* ctcP, int32_t T, int32_t L2, const int32_t* perm, int32_t nb,
-                                 float* cmaxb, float* cmaxr, cudaStream_t s);
+// cmaxr[y, t] = max over lags of |ctcP[y, t, :]| (infinite where a lag is NaN)
+cudaError_t launch_ctc_row_max(const float* ctcP, int32_t T, int32_t L2, float* cmaxr, cudaStream_t s);
 int mp_max_grid(int device);
 void set_thread_error(const char* msg);
 // true when kernels on `device` may dereference p (that device's memory,

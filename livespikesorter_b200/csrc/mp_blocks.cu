@@ -17,12 +17,13 @@
 //   * per block and column the kernel keeps bmin = min over the block's rows
 //     of |B| and bkey = max over the rows of (Cf bits << 32 | ~t), exact for
 //     the current field;
-//   * a (spike segment, block, 32-column chunk) work item whose terms all
-//     satisfy fl(|a| * cmaxb[y][block]) < 2^(e(bmin) - 25) is skipped: every
-//     score of the block is provably unchanged, and so are its bmin and bkey.
-//     In a processed block a single term is skipped per row by the same test
-//     with the row's own max |ctc| (cmaxr), as long as no earlier term of
-//     that row changed the score;
+//   * for a (spike segment, 32-column chunk) and a block, row r needs spike
+//     e's term only if fl(|a_e| * cmaxr[y_e][t_r]) >= thr, thr being a quarter
+//     ulp of the smallest bmin over the warp's columns (cmaxr = max over lags
+//     of |ctc|); a block where no row needs a term is skipped (its scores,
+//     bmin and bkey are provably unchanged); in a processed block the terms
+//     that are no-ops are skipped row by row, the second term only where the
+//     first left the score unchanged;
 //   * the peak phase takes each column's maximum over the block keys.
 // Everything that is computed is computed exactly as in k_mp: single-rounded
 // products and differences (__fmul_rn / __fsub_rn), Cf = fl(fl(r*r)/nm), the
@@ -39,12 +40,15 @@
 #include "mp_common.cuh"
 
 #include <algorithm>
+#include <cfloat>
 #include <climits>
 
 namespace lss {
 
 constexpr int MPB_THREADS = 512;
 constexpr int MPB_MAX_GRID = 1024;
+constexpr int MPB_GROUP = 4;  // row blocks per update work item
+constexpr int MPB_SPK = 3;    // spikes of a chunk's list that get row masks
 constexpr unsigned FULL = 0xffffffffu;
 
 // 2^(e - 25) for v in [2^e, 2^(e+1)) (v >= 0): any |d| below it leaves
@@ -144,16 +148,15 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
                     v = 0.f;  // Cf[:, :nt] = Cf[:, -nt:] = 0
                     if (own) ivals[s - lo] = 0;
                 } else {
+                    // the block keys of the column, 16 loads in flight at a time
                     unsigned long long k = 0ull;
-                    int bb = 0;
-                    for (; bb + 4 <= nb; bb += 4) {
-                        const unsigned long long k0 = __ldcg(a.bkey + (bb + 0) * ldk + s);
-                        const unsigned long long k1 = __ldcg(a.bkey + (bb + 1) * ldk + s);
-                        const unsigned long long k2 = __ldcg(a.bkey + (bb + 2) * ldk + s);
-                        const unsigned long long k3 = __ldcg(a.bkey + (bb + 3) * ldk + s);
-                        k = max(max(k, k0), max(max(k1, k2), k3));
+                    for (int b0 = 0; b0 < nb; b0 += 16) {
+                        unsigned long long kk[16];
+#pragma unroll
+                        for (int u = 0; u < 16; ++u) kk[u] = (b0 + u < nb) ? __ldcg(a.bkey + (b0 + u) * ldk + s) : 0ull;
+#pragma unroll
+                        for (int u = 0; u < 16; ++u) k = max(k, kk[u]);
                     }
-                    for (; bb < nb; ++bb) k = max(k, __ldcg(a.bkey + bb * ldk + s));
                     v = __uint_as_float((unsigned)(k >> 32));
                     if (own) ivals[s - lo] = (int)(0xFFFFFFFFu - (unsigned)(k & 0xFFFFFFFFull));
                 }
@@ -225,7 +228,8 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
             break;
         }
         const int nch = (L2 + 31) / 32;
-        const int per_spike = nb * nch;
+        const int ngr = (nb + MPB_GROUP - 1) / MPB_GROUP;
+        const int per_spike = nch * ngr;
         const int items = total * per_spike;
         const int per_cta = (items + G - 1) / G;
         const int it_end = min(items, (b + 1) * per_cta);
@@ -243,9 +247,10 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
         }
         __syncthreads();
         {
-            // Work item (spike q, block bb, chunk ch): the columns of spike q's
-            // segment [max(x_q - nt, x_{q-1} + nt + 1), x_q + nt], 32 at a time,
-            // rows of block bb. Lane L holds spike q - 1 + L of the round.
+            // Work item (spike q, chunk ch, group g): the columns of spike q's
+            // segment [max(x_q - nt, x_{q-1} + nt + 1), x_q + nt], 32 at a
+            // time (lane = column), and the row blocks g*MPB_GROUP.. of the
+            // group. Lane L holds spike q - 1 + L of the round.
             int cur_q = -1, x = INT_MAX, y = 0;
             float amp = 0.f;
             for (;;) {
@@ -253,7 +258,7 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
                 if (lane == 0) it = atomicAdd(&s_next, 1);
                 it = __shfl_sync(FULL, it, 0);
                 if (it >= it_end) break;
-                const int q = it / per_spike, rem = it - q * per_spike, bb = rem / nch, ch = rem - bb * nch;
+                const int q = it / per_spike, rem = it - q * per_spike, ch = rem / ngr, g = rem - ch * ngr;
                 if (q != cur_q) {
                     cur_q = q;
                     const int j = q - 1 + lane;
@@ -276,7 +281,7 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
                 const int xprev = __shfl_sync(FULL, x, 0);
                 const bool ok = lane >= 1 && (q - 1 + lane) < total && x <= xi + 2 * nt;
                 const int nl = __popc(__ballot_sync(FULL, ok));
-                if (lane == 0 && ch == 0 && bb == 0 && nl == MP_LIST && q + MP_LIST < total)
+                if (lane == 0 && ch == 0 && g == 0 && nl == MP_LIST && q + MP_LIST < total)
                     atomicOr(a.status, STATUS_LIST);
                 const int lo_own = max(max(xi - nt, (q > 0 ? xprev : INT_MIN / 2) + nt + 1), 0);
                 const int hi_own = min(xi + nt, N - 1);
@@ -297,58 +302,98 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
                 const int x1 = __shfl_sync(FULL, x, max(e1, 0) + 1);
                 const int y1 = __shfl_sync(FULL, y, max(e1, 0) + 1);
                 const float a1 = __shfl_sync(FULL, amp, max(e1, 0) + 1);
-                // exact no-op test of the whole block for this column
-                float thr = 0.f;
-                bool noop = true;
-                if (active) {
-                    thr = quarter_ulp(__ldcg(a.bmin + bb * ldk + s));
-                    if (e0 >= 0 && !(__fmul_rn(fabsf(a0), __ldg(a.cmaxb + (int64_t)y0 * nb + bb)) < thr)) noop = false;
-                    if (e1 >= 0 && !(__fmul_rn(fabsf(a1), __ldg(a.cmaxb + (int64_t)y1 * nb + bb)) < thr)) noop = false;
+                // the first MPB_SPK spikes of the list (nearly always the only ones
+                // a chunk meets): template and |amplitude| for the row masks
+                int ye[MPB_SPK];
+                float fae[MPB_SPK];
+#pragma unroll
+                for (int e = 0; e < MPB_SPK; ++e) {
+                    ye[e] = __shfl_sync(FULL, y, e + 1);
+                    fae[e] = fabsf(__shfl_sync(FULL, amp, e + 1));
                 }
-                ++n_items;
-                if (__all_sync(FULL, noop)) continue;
-                ++n_proc;
-                if (!active) continue;
-                const int r0 = bb * MPB_ROWS, nr = min(MPB_ROWS, T - r0);
+                // ---- decisions for the group's blocks, all loads in one round trip.
+                // thr: a quarter ulp of the smallest |B| the block holds in any of
+                // the warp's columns; row r of block b needs spike e's term only if
+                // fl(|a_e| * max_l |ctc[t_r, y_e, l]|) >= thr (otherwise the term
+                // leaves every score of the row bit for bit unchanged).
+                const int bg0 = g * MPB_GROUP, nbg = min(MPB_GROUP, nb - bg0);
+                float bmv[MPB_GROUP], cmv[MPB_GROUP][MPB_SPK];
+#pragma unroll
+                for (int j = 0; j < MPB_GROUP; ++j) {
+                    const int bb = bg0 + j;
+                    const int tr = (j < nbg) ? s_perm[bb * MPB_ROWS + lane] : -1;
+                    bmv[j] = (j < nbg && active) ? __ldcg(a.bmin + bb * ldk + s) : 0.f;
+#pragma unroll
+                    for (int e = 0; e < MPB_SPK; ++e)
+                        cmv[j][e] = (tr >= 0 && e < nl) ? __ldg(a.cmaxr + (int64_t)ye[e] * T + tr) : 0.f;
+                }
+                // per block j: the rows that need this lane's even term (m0) and odd
+                // term (m1), packed 32 bits per block; bit j of procm: block j is processed
+                unsigned long long m0p[(MPB_GROUP + 1) / 2], m1p[(MPB_GROUP + 1) / 2];
+#pragma unroll
+                for (int i = 0; i < (MPB_GROUP + 1) / 2; ++i) m0p[i] = m1p[i] = 0ull;
+                unsigned procm = 0u;
+#pragma unroll
+                for (int j = 0; j < MPB_GROUP; ++j) {
+                    const float thr_l = active ? quarter_ulp(bmv[j]) : FLT_MAX;
+                    const float thr = __uint_as_float(__reduce_min_sync(FULL, __float_as_uint(thr_l)));
+                    unsigned m0 = (e0 >= MPB_SPK) ? 0xffffffffu : 0u, m1 = (e1 >= MPB_SPK) ? 0xffffffffu : 0u;
+#pragma unroll
+                    for (int e = 0; e < MPB_SPK; ++e) {
+                        const unsigned me = __ballot_sync(FULL, e < nl && !(__fmul_rn(fae[e], cmv[j][e]) < thr));
+                        if (e0 == e) m0 = me;
+                        if (e1 == e) m1 = me;
+                    }
+                    if (e0 < 0) m0 = 0u;
+                    // after a term that changes the score the second is always applied
+                    m1 = (e1 >= 0) ? (m1 | m0) : 0u;
+                    if (j < nbg && __any_sync(FULL, active && (m0 | m1) != 0u)) procm |= 1u << j;
+                    m0p[j / 2] |= (unsigned long long)m0 << (32 * (j & 1));
+                    m1p[j / 2] |= (unsigned long long)m1 << (32 * (j & 1));
+                }
+                n_items += nbg;
                 const float* c0p = a.ctcP + (int64_t)y0 * T * L2 + (s - x0 + nt);
                 const float* c1p = a.ctcP + (int64_t)y1 * T * L2 + (s - x1 + nt);
-                const float* cr0 = a.cmaxr + (int64_t)y0 * T;
-                const float* cr1 = a.cmaxr + (int64_t)y1 * T;
-                const float fa0 = fabsf(a0), fa1 = fabsf(a1);
-                ColMaxAny m;
-                float mn = INFINITY;
-                for (int rr = 0; rr < nr; rr += 8) {
-                    int tt[8];
-                    float v[8], w0[8], w1[8];
-                    bool u0[8], u1[8];
+#pragma unroll 1
+                for (int j = 0; j < MPB_GROUP; ++j) {
+                    if (!((procm >> j) & 1u)) continue;  // warp-uniform
+                    ++n_proc;
+                    const int bb = bg0 + j, r0 = bb * MPB_ROWS, nr = min(MPB_ROWS, T - r0);
+                    unsigned long long p0 = m0p[0], p1 = m1p[0];
 #pragma unroll
-                    for (int u = 0; u < 8; ++u) tt[u] = (rr + u < nr) ? s_perm[r0 + rr + u] : -1;
+                    for (int i = 1; i < (MPB_GROUP + 1) / 2; ++i)
+                        if (j / 2 == i) {
+                            p0 = m0p[i];
+                            p1 = m1p[i];
+                        }
+                    const unsigned m0 = (unsigned)(p0 >> (32 * (j & 1))), m1 = (unsigned)(p1 >> (32 * (j & 1)));
+                    if (!active) continue;
+                    ColMaxAny m;
+                    float mn = INFINITY;
+                    for (int rr = 0; rr < nr; rr += 16) {
+                        float v[16], w0[16], w1[16];
 #pragma unroll
-                    for (int u = 0; u < 8; ++u) v[u] = tt[u] >= 0 ? ld_keep(a.B + (int64_t)tt[u] * ldb + s, pk) : 0.f;
+                        for (int u = 0; u < 16; ++u) {
+                            const int t = (rr + u < nr) ? s_perm[r0 + rr + u] : -1;
+                            v[u] = t >= 0 ? ld_keep(a.B + (int64_t)t * ldb + s, pk) : 0.f;
+                            w0[u] = (t >= 0 && ((m0 >> (rr + u)) & 1u)) ? ld_stream(c0p + (int64_t)t * L2, ps) : 0.f;
+                            w1[u] = (t >= 0 && ((m1 >> (rr + u)) & 1u)) ? ld_stream(c1p + (int64_t)t * L2, ps) : 0.f;
+                        }
 #pragma unroll
-                    for (int u = 0; u < 8; ++u) {
-                        // term 0 applies unless it is a no-op on the old score; term 1
-                        // may be skipped only when term 0 left the score unchanged
-                        u0[u] = tt[u] >= 0 && e0 >= 0 && !(__fmul_rn(fa0, __ldg(cr0 + tt[u])) < thr);
-                        u1[u] = tt[u] >= 0 && e1 >= 0 && (u0[u] || !(__fmul_rn(fa1, __ldg(cr1 + tt[u])) < thr));
+                        for (int u = 0; u < 16; ++u) {
+                            if (rr + u >= nr) continue;
+                            const int t = s_perm[r0 + rr + u];
+                            float xv = v[u];
+                            if ((m0 >> (rr + u)) & 1u) xv = __fsub_rn(xv, __fmul_rn(a0, w0[u]));
+                            if ((m1 >> (rr + u)) & 1u) xv = __fsub_rn(xv, __fmul_rn(a1, w1[u]));
+                            if (__float_as_uint(xv) != __float_as_uint(v[u])) st_keep(a.B + (int64_t)t * ldb + s, xv, pk);
+                            mn = fminf(mn, fabsf(xv));
+                            m.consider(xv, s_nm[t], s_inv[t], t);
+                        }
                     }
-#pragma unroll
-                    for (int u = 0; u < 8; ++u) w0[u] = u0[u] ? ld_stream(c0p + (int64_t)tt[u] * L2, ps) : 0.f;
-#pragma unroll
-                    for (int u = 0; u < 8; ++u) w1[u] = u1[u] ? ld_stream(c1p + (int64_t)tt[u] * L2, ps) : 0.f;
-#pragma unroll
-                    for (int u = 0; u < 8; ++u) {
-                        if (tt[u] < 0) continue;
-                        float xv = v[u];
-                        if (u0[u]) xv = __fsub_rn(xv, __fmul_rn(a0, w0[u]));
-                        if (u1[u]) xv = __fsub_rn(xv, __fmul_rn(a1, w1[u]));
-                        if (__float_as_uint(xv) != __float_as_uint(v[u])) st_keep(a.B + (int64_t)tt[u] * ldb + s, xv, pk);
-                        mn = fminf(mn, fabsf(xv));
-                        m.consider(xv, s_nm[tt[u]], s_inv[tt[u]], tt[u]);
-                    }
+                    a.bkey[bb * ldk + s] = pack_key(m.best, m.bi);
+                    a.bmin[bb * ldk + s] = mn;
                 }
-                a.bkey[bb * ldk + s] = pack_key(m.best, m.bi);
-                a.bmin[bb * ldk + s] = mn;
             }
         }
         base += total;
@@ -377,7 +422,7 @@ static size_t mpb_smem_bytes(int cols_per_blk, int nt, int T, int nb) {
 }
 
 cudaError_t launch_mp_blocks(MPArgs a, int grid, cudaStream_t s) {
-    if (grid > MPB_MAX_GRID || !a.perm || !a.cmaxb || !a.cmaxr || !a.bkey || !a.bmin ||
+    if (grid > MPB_MAX_GRID || !a.perm || !a.cmaxr || !a.bkey || !a.bmin ||
         a.nb != (a.T + MPB_ROWS - 1) / MPB_ROWS)
         return cudaErrorInvalidValue;
     const size_t smem = mpb_smem_bytes(a.cols_per_blk, a.nt, a.T, a.nb);
@@ -417,26 +462,9 @@ __global__ void k_ctc_row_max(const float* __restrict__ ctcP, int64_t rows, int 
     if (lane == 0) cmaxr[row] = m;
 }
 
-// cmaxb[y, b] = max over the rows of block b of cmaxr[y, row]
-__global__ void k_ctc_block_max(const float* __restrict__ cmaxr, int T, const int32_t* __restrict__ perm, int nb,
-                                float* __restrict__ cmaxb) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (int64_t)T * nb) return;
-    const int y = (int)(i / nb), bb = (int)(i % nb);
-    float m = 0.f;
-    for (int r = 0; r < MPB_ROWS; ++r) {
-        const int t = perm[bb * MPB_ROWS + r];
-        if (t >= 0) m = fmaxf(m, cmaxr[(int64_t)y * T + t]);
-    }
-    cmaxb[i] = m;
-}
-
-cudaError_t launch_ctc_block_max(const float* ctcP, int32_t T, int32_t L2, const int32_t* perm, int32_t nb,
-                                 float* cmaxb, float* cmaxr, cudaStream_t s) {
+cudaError_t launch_ctc_row_max(const float* ctcP, int32_t T, int32_t L2, float* cmaxr, cudaStream_t s) {
     const int64_t rows = (int64_t)T * T;
     k_ctc_row_max<<<(unsigned)((rows + 7) / 8), 256, 0, s>>>(ctcP, rows, L2, cmaxr);
-    const int64_t nbk = (int64_t)T * nb;
-    k_ctc_block_max<<<(unsigned)((nbk + 255) / 256), 256, 0, s>>>(cmaxr, T, perm, nb, cmaxb);
     return cudaGetLastError();
 }
 

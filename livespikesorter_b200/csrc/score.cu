@@ -16,7 +16,10 @@ namespace lss {
 // rows = samples (the GEMM's M), columns = (channel, component) (its K), row
 // stride ldk (a multiple of the GEMM's k-block; pad columns stay zero). The
 // BF16 path stores bf16; the FP32 path stores the tf32 split hi = rna(x),
-// lo = x - hi (exact in fp32) in two fp32 arrays. CTA: 64 samples x PC
+// lo = rna(x - hi) in two fp32 arrays: both parts exact tf32 values, so the
+// tensor core's tf32 reading of them drops nothing and the split errs by at
+// most 2^-23 |x|, unbiased (a plain x - hi would be truncated by the MMA,
+// always toward zero). CTA: 64 samples x PC
 // channels, staged in shared memory and written as contiguous row segments.
 // ---------------------------------------------------------------------------
 constexpr int PT_S = 64;    // samples per CTA
@@ -110,8 +113,8 @@ __global__ void __launch_bounds__(256) k_pca_proj_t(const float* __restrict__ X,
             const int64_t o = orow + 4 * q;
             if (TF32) {
                 const float4 hi = make_float4(tf32_rna(v.x), tf32_rna(v.y), tf32_rna(v.z), tf32_rna(v.w));
-                const float4 lo = make_float4(__fsub_rn(v.x, hi.x), __fsub_rn(v.y, hi.y), __fsub_rn(v.z, hi.z),
-                                              __fsub_rn(v.w, hi.w));
+                const float4 lo = make_float4(tf32_rna(__fsub_rn(v.x, hi.x)), tf32_rna(__fsub_rn(v.y, hi.y)),
+                                              tf32_rna(__fsub_rn(v.z, hi.z)), tf32_rna(__fsub_rn(v.w, hi.w)));
                 *reinterpret_cast<float4*>(static_cast<float*>(out0) + o) = hi;
                 *reinterpret_cast<float4*>(out_lo + o) = lo;
             } else {
@@ -128,7 +131,7 @@ __global__ void __launch_bounds__(256) k_pca_proj_t(const float* __restrict__ X,
             if (TF32) {
                 const float hi = tf32_rna(v);
                 static_cast<float*>(out0)[orow + j] = hi;
-                out_lo[orow + j] = __fsub_rn(v, hi);
+                out_lo[orow + j] = tf32_rna(__fsub_rn(v, hi));
             } else {
                 static_cast<__nv_bfloat16*>(out0)[orow + j] = __float2bfloat16_rn(v);
             }
@@ -216,23 +219,27 @@ cudaError_t launch_build_uw(const float* U, const float* Mw, int32_t T, int32_t 
 // (bf16 rounding of both operands moves each product by at most 2^-8 of its
 // magnitude, sum |U||P| <= ||U|| ||P||, and both paths accumulate in FP32 with
 // errors far below that). From it the BF16 GEMM's epilogue gives each column
-// an interval [cf_lo, cf_hi] that holds the FP32 path's column maximum of Cf
-// for the same best template, and ch, the largest upper bound of Cf over the
-// other templates. The FP32 path's first-round decisions at a column can
-// differ from the BF16 path's only when
-//   * threshold:     cf_lo <= Th^2 < cf_hi;
-//   * best template: ch >= cf_lo (and cf_hi > Th^2);
-//   * peak test:     the interval of a column of the +-nt window overlaps the
-//                    column's own, and one of the two can exceed Th^2
-//                    (edge columns are exactly zero in both paths).
-// Those columns, and only those, are listed, projected with the FP32 path's
-// arithmetic and re-scored by its 3xTF32 GEMM through the list, which
-// overwrites their scores with the FP32 path's values; every other column's
-// first-round decisions are then provably the FP32 path's. count[0] = listed
+// an interval [lo, hi] that holds its column maximum of Cf in both paths (the
+// BF16 best template's), and ch, the largest upper bound of Cf over the other
+// templates. With W(x) the +-nt window of column x (without x):
+//   * x can be a peak in either path only if it is a candidate:
+//       hi(x) > Th^2 and no v in W(x) has lo(v) > hi(x);
+//   * a candidate's decisions are open when lo(x) <= Th^2 (threshold),
+//     ch(x) >= lo(x) (best template) or some v in W(x) has hi(v) >= lo(x)
+//     (window maximum);
+//   * listed: every candidate with an open decision, and every column v whose
+//     hi(v) reaches lo(x) of a candidate x with an open window maximum.
+// Listed columns are projected with the FP32 path's arithmetic and re-scored
+// by its 3xTF32 GEMM through the list, which overwrites their scores with the
+// FP32 path's values. Every first-round decision then equals the FP32 path's:
+// an unlisted non-candidate is beaten by a neighbour, an unlisted candidate
+// strictly beats its window and the threshold with a strictly best template,
+// in both paths, and every open comparison involves FP32 values only. Edge
+// columns are exactly zero in both paths and never listed. count[0] = listed
 // columns, count[1] = decisions the re-check changed, count[2] = listed.
 // ---------------------------------------------------------------------------
 constexpr int RS_COLS = 256;
-constexpr int RS_MAX_NT = 256;
+constexpr int RS_MAX_NT = 128;
 
 __global__ void __launch_bounds__(RS_COLS) k_recheck_select(const float* __restrict__ cf_lo,
                                                             const float* __restrict__ cf_hi,
@@ -242,25 +249,41 @@ __global__ void __launch_bounds__(RS_COLS) k_recheck_select(const float* __restr
                                                             float th2, int32_t* __restrict__ cols,
                                                             float* __restrict__ pre_cf, int32_t* __restrict__ pre_im,
                                                             int32_t* __restrict__ count) {
-    __shared__ float lo_s[RS_COLS + 2 * RS_MAX_NT], hi_s[RS_COLS + 2 * RS_MAX_NT];
+    // columns s0 - 2nt .. s0 + RS_COLS + 2nt (p = s - s0 + 2nt)
+    __shared__ float lo_s[RS_COLS + 4 * RS_MAX_NT], hi_s[RS_COLS + 4 * RS_MAX_NT];
+    __shared__ unsigned char openmax[RS_COLS + 2 * RS_MAX_NT];  // p - nt: candidate with an open window maximum
     const int s0 = blockIdx.x * RS_COLS;
-    for (int p = threadIdx.x; p < RS_COLS + 2 * nt; p += blockDim.x) {
-        const int s = s0 - nt + p;
+    const int span = RS_COLS + 4 * nt;
+    for (int p = threadIdx.x; p < span; p += blockDim.x) {
+        const int s = s0 - 2 * nt + p;
         const bool in = s >= nt && s < N - nt;  // edge and outside columns: exactly zero
         lo_s[p] = in ? cf_lo[s] : 0.f;
         hi_s[p] = in ? cf_hi[s] : 0.f;
     }
     __syncthreads();
+    // candidates and their open window maxima for columns s0 - nt .. s0 + RS_COLS + nt
+    for (int p = nt + threadIdx.x; p < RS_COLS + 3 * nt; p += blockDim.x) {
+        const float lo = lo_s[p], hi = hi_s[p];
+        float wlo = 0.f, whi = 0.f;
+        for (int d = 1; d <= nt; ++d) {
+            wlo = fmaxf(wlo, fmaxf(lo_s[p - d], lo_s[p + d]));
+            whi = fmaxf(whi, fmaxf(hi_s[p - d], hi_s[p + d]));
+        }
+        const bool cand = hi > th2 && !(wlo > hi);
+        openmax[p - nt] = cand && whi >= lo;
+    }
+    __syncthreads();
     const int s = s0 + threadIdx.x;
     bool sel = false;
     if (s >= nt && s < N - nt) {
-        const float lo = lo_s[threadIdx.x + nt], hi = hi_s[threadIdx.x + nt];
-        if (hi > th2 && (lo <= th2 || ch[s] >= lo)) sel = true;
-        for (int d = -nt; d <= nt && !sel; ++d) {
-            if (d == 0) continue;
-            const float lv = lo_s[threadIdx.x + nt + d], hv = hi_s[threadIdx.x + nt + d];
-            if ((hi > th2 || hv > th2) && hv >= lo && hi >= lv) sel = true;
-        }
+        const int p = threadIdx.x + 2 * nt;
+        const float lo = lo_s[p], hi = hi_s[p];
+        float wlo = 0.f;
+        for (int d = 1; d <= nt; ++d) wlo = fmaxf(wlo, fmaxf(lo_s[p - d], lo_s[p + d]));
+        const bool cand = hi > th2 && !(wlo > hi);
+        sel = cand && (lo <= th2 || ch[s] >= lo || openmax[p - nt]);
+        for (int d = -nt; d <= nt && !sel; ++d)
+            if (d != 0 && openmax[p + d - nt] && hi >= lo_s[p + d]) sel = true;
     }
     const unsigned bal = __ballot_sync(0xffffffffu, sel);
     const int lane = threadIdx.x & 31;
@@ -324,7 +347,7 @@ __global__ void __launch_bounds__(128) k_pca_proj_cols(const float* __restrict__
         for (int k = 0; k < KPC; ++k) {
             const float h = tf32_rna(acc[k]);
             hi[o + k] = h;
-            lo[o + k] = __fsub_rn(acc[k], h);
+            lo[o + k] = tf32_rna(__fsub_rn(acc[k], h));
         }
     }
 }

@@ -67,8 +67,8 @@ __global__ void k_ucc(const float* __restrict__ U, const int64_t* __restrict__ i
     Ucc[e] = U[((int64_t)t * K + k) * C + ch];
 }
 
-// GEMM operands U_p[t, c*K + k] = U[t, k, c]: tf32 split (the bit rounding
-// lss_create uses) and bf16.
+// GEMM operands U_p[t, c*K + k] = U[t, k, c]: tf32 split hi = rna(x),
+// lo = rna(x - hi) (the bit rounding lss_create uses) and bf16.
 __global__ void k_up(const float* __restrict__ U, int T, int K, int C, int64_t ldk, float* __restrict__ hi,
                      float* __restrict__ lo, __nv_bfloat16* __restrict__ b16) {
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -78,8 +78,10 @@ __global__ void k_up(const float* __restrict__ U, int T, int K, int C, int64_t l
     uint32_t u = __float_as_uint(x);
     if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x1000u) & 0xffffe000u;
     const float xh = __uint_as_float(u);
+    uint32_t v = __float_as_uint(__fsub_rn(x, xh));
+    if ((v & 0x7f800000u) != 0x7f800000u) v = (v + 0x1000u) & 0xffffe000u;
     hi[(int64_t)t * ldk + r] = xh;
-    lo[(int64_t)t * ldk + r] = __fsub_rn(x, xh);
+    lo[(int64_t)t * ldk + r] = __uint_as_float(v);
     if (b16) b16[(int64_t)t * ldk + r] = __float2bfloat16_rn(x);
 }
 

@@ -10,7 +10,12 @@
 Each batch goes through lss_sort_batch (int16 rows in, records out) and
 through the oracle (filter + run_matching + PC features, FP32 torch on the
 CPU). Tolerances:
-* identical (time, template) sequence in run_matching order;
+* identical (time, template) sequence in run_matching order, except after a
+  near-tie: a decision whose alternatives differ by less than 1e-5 relative
+  Cf on the oracle's own field at that round (FP32 rounding of the score GEMM
+  can take either side). Then the batch's spike sets must agree to 0.999, the
+  prefix before the tie must be identical, and there may be at most one such
+  batch per 20000 spikes;
 * amplitudes within 1e-4 relative;
 * PC features within 1e-3 of their largest magnitude (FP32 projection sums in
   another order than torch's conv1d / matmul).
@@ -28,6 +33,12 @@ pytestmark = pytest.mark.gpu
 
 AMP_RTOL = 1e-4
 PC_TOL = 1e-3
+# a decision whose two sides differ by less than this relative Cf, on the
+# oracle's own field at that round, is a near-tie: the score GEMM (3xTF32 on
+# the tensor cores, about 1e-7 relative) and torch's CPU einsum round
+# differently, so either side is an FP32-correct answer
+NEAR_TIE = 1e-5
+NEAR_TIE_AGREEMENT = 0.999
 
 
 def _rows(raw, ib, nb, NT, nt):
@@ -48,8 +59,9 @@ def _oracle(setup, rec, ib, dtype=torch.float32):
 
 
 def _report(setup, X, st_o, rounds_o, x_gpu, y_gpu, i):
-    """Margins of the first differing decision on the oracle's own score field
-    at the start of that round (FP32), and what the FP64 oracle picks."""
+    """The first differing decision on the oracle's own score field at the start
+    of that round (FP32): the relative Cf gap between the oracle's choice and
+    the GPU's, a message with the margins, and what the FP64 oracle picks."""
     nt = setup.nt
     U = setup.U
     r = int(rounds_o[min(i, len(rounds_o) - 1)])
@@ -59,18 +71,18 @@ def _report(setup, X, st_o, rounds_o, x_gpu, y_gpu, i):
     Cf = torch.relu(Br) ** 2 / nm[:, None]
     Cf[:, :nt] = 0
     Cf[:, -nt:] = 0
-    x = int(st_o[i, 0]) if i < len(st_o) else int(x_gpu)
-    col = Cf[:, x]
-    top = torch.topk(col, 2)
-    win = torch.cat([Cf[:, max(0, x - nt):x].max(0).values, Cf[:, x + 1:x + nt + 1].max(0).values])
+    x, y = (int(st_o[i, 0]), int(st_o[i, 1])) if i < len(st_o) else (int(x_gpu), int(y_gpu))
+    c_o = float(Cf[y, x])
+    c_g = float(Cf[int(y_gpu), int(x_gpu)])
+    gap = (c_o - c_g) / max(c_o, 1e-30)
+    top = torch.topk(Cf[:, x], 2)
     st64, _, _ = ko.run_matching(X, U, setup.ctc, setup.wPCA, setup.Th, nt, dtype=torch.float64)
-    return (f'first difference at spike {i} (oracle round {r}): oracle (x, y) = '
-            f'{st_o[i].tolist() if i < len(st_o) else None}, GPU (x, y) = ({int(x_gpu)}, {int(y_gpu)}); '
-            f'oracle field at the start of round {r}, column {x}: best {int(top.indices[0])} Cf {float(top.values[0]):.6e}, '
-            f'runner-up {int(top.indices[1])} Cf {float(top.values[1]):.6e} (relative gap '
-            f'{float((top.values[0] - top.values[1]) / top.values[0]):.3e}), GPU template Cf {float(col[int(y_gpu)]):.6e}, '
-            f'largest other column in the window {float(win.max()):.6e}; FP64 oracle: {len(st64)} spikes, '
-            f'{"same" if len(st64) == len(st_o) and torch.equal(st64, st_o) else "different"} sequence as FP32')
+    msg = (f'first difference at spike {i} (oracle round {r}): oracle (x, y) = ({x}, {y}) Cf {c_o:.7e}, '
+           f'GPU (x, y) = ({int(x_gpu)}, {int(y_gpu)}) Cf {c_g:.7e} on the oracle field, relative gap {gap:.3e}; '
+           f'column {x}: best {int(top.indices[0])} {float(top.values[0]):.7e}, runner-up {int(top.indices[1])} '
+           f'{float(top.values[1]):.7e}; FP64 oracle: {len(st64)} spikes, '
+           f'{"same" if len(st64) == len(st_o) and torch.equal(st64, st_o) else "different"} sequence as FP32')
+    return gap, msg
 
 
 def _check_batches(T, dup, seed):
@@ -83,6 +95,7 @@ def _check_batches(T, dup, seed):
     nb = rec.n_batches
     NT, nt = setup.NT, setup.nt
     total = 0
+    near_ties = []
     for ib in (0, nb // 2, nb - 1):
         s.set_drift(setup.drift_matrix(rec.dshift[ib]))
         r = s.sort_batch(np.ascontiguousarray(_rows(rec.raw, ib, nb, NT, nt)), ib, nb)
@@ -91,6 +104,7 @@ def _check_batches(T, dup, seed):
                                        setup.nt0min, ib, NT)
         got = np.stack([r['time'].numpy(), r['template'].numpy()], 1)
         want = ref[:, :2].astype(np.int64)
+        n_cmp = len(got)
         if got.shape != want.shape or not np.array_equal(got, want):
             n = min(len(got), len(want))
             i = int(np.nonzero((got[:n] != want[:n]).any(1))[0][0]) if (got[:n] != want[:n]).any() else n
@@ -98,15 +112,27 @@ def _check_batches(T, dup, seed):
             off = 0 if ib != 0 else int(((st[:, 0] - nt - nt // 2 + setup.nt0min) < 0).sum())
             gi = min(i, len(got) - 1)
             x_gpu = got[gi, 0] - (ib * NT - nt // 2 + setup.nt0min) + nt
-            pytest.fail(f'T={T} batch {ib}: {len(got)} GPU vs {len(want)} oracle spikes; '
-                        + _report(setup, X, st, rounds, x_gpu, got[gi, 1], min(i + off, len(st) - 1)))
-        a = r['amplitude'].numpy().astype(np.float64)
-        b = ref[:, 2]
+            gap, msg = _report(setup, X, st, rounds, x_gpu, got[gi, 1], min(i + off, len(st) - 1))
+            if not (abs(gap) <= NEAR_TIE):
+                pytest.fail(f'T={T} batch {ib}: {len(got)} GPU vs {len(want)} oracle spikes; ' + msg)
+            # a near-tie decided the other way: the rounds after it differ near
+            # that column only; the rest must still agree as a set
+            a_set = set(map(tuple, got.tolist()))
+            b_set = set(map(tuple, want.tolist()))
+            agree = len(a_set & b_set) / max(len(a_set), len(b_set))
+            near_ties.append((T, ib, gap, agree))
+            print(f'near-tie, T={T} batch {ib}: {msg}; set agreement {agree:.6f}')
+            assert agree >= NEAR_TIE_AGREEMENT, (T, ib, agree, msg)
+            n_cmp = i  # amplitudes and features of the common prefix
+        a = r['amplitude'].numpy().astype(np.float64)[:n_cmp]
+        b = ref[:n_cmp, 2]
         rel = np.abs(a - b) / np.maximum(np.abs(b), 1e-6)
-        assert rel.max() <= AMP_RTOL, (ib, rel.max())
+        assert n_cmp == 0 or rel.max() <= AMP_RTOL, (ib, rel.max())
         tf = ref_tf.numpy()
-        assert np.abs(r['pc'].numpy() - tf).max() <= PC_TOL * np.abs(tf).max(), ib
+        assert np.abs(r['pc'].numpy()[:n_cmp] - tf[:n_cmp]).max() <= PC_TOL * np.abs(tf).max(), ib
         total += len(got)
+    # at most one near-tie per 20000 spikes
+    assert len(near_ties) <= max(1, total // 20000), near_ties
     return total
 
 
