@@ -394,10 +394,11 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
             g_create_err = "event creation failed";
             return LSS_ERR_CUDA;
         }
-    } else {
-        ALLOC(B0T_hi, (size_t)h->N * h->CKpad);
-        ALLOC(B0T_lo, (size_t)h->N * h->CKpad);
     }
+    // FP32 projection rows: the FP32 path's GEMM operand; the BF16 path keeps
+    // the rows of its spikes' columns there for the PC features
+    ALLOC(B0T_hi, (size_t)h->N * h->CKpad);
+    ALLOC(B0T_lo, (size_t)h->N * h->CKpad);
     // tf32 template splits: the FP32 path's scores, and the BF16 path's re-check
     const int Tpad32 = tc_plan(T, true).Tpad;
     ALLOC(Up_hi, (size_t)Tpad32 * h->CKpad);
@@ -495,10 +496,8 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
             }
         CK(cudaMemcpy(h->Up_hi.p, hi.data(), hi.size() * sizeof(float), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(h->Up_lo.p, lo.data(), lo.size() * sizeof(float), cudaMemcpyHostToDevice));
-        if (!bf16) {
-            CK(cudaMemset(h->B0T_hi.p, 0, (size_t)h->N * h->CKpad * sizeof(float)));
-            CK(cudaMemset(h->B0T_lo.p, 0, (size_t)h->N * h->CKpad * sizeof(float)));
-        }
+        CK(cudaMemset(h->B0T_hi.p, 0, (size_t)h->N * h->CKpad * sizeof(float)));
+        CK(cudaMemset(h->B0T_lo.p, 0, (size_t)h->N * h->CKpad * sizeof(float)));
     }
     CK(cudaMemcpy(h->nm.p, nmv.data(), T * sizeof(float), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->wave.p, wave.data(), wave.size() * sizeof(float), cudaMemcpyHostToDevice));
@@ -691,8 +690,8 @@ int lss::run_scores(lss_handle* h, const float* X, int64_t ldx, int64_t N, float
         const float th2 = h->cfg.th_learned * h->cfg.th_learned;
         CK(launch_recheck_select(h->cf_lo.p, h->cf_hi.p, h->cf2.p, h->cfmax.p, h->imax.p, (int)N, h->nt, th2,
                                  h->rc_cols.p, h->pre_cf.p, h->pre_im.p, h->rc_count.p, s));
-        CK(launch_pca_proj_cols_tf32(X, ldx, h->C, N, h->wpca.p, h->K, h->nt, h->rc_cols.p, h->rc_count.p, h->Pc_hi.p,
-                                     h->Pc_lo.p, h->CKpad, s));
+        CK(launch_pca_proj_cols_tf32(X, ldx, h->C, N, h->wpca.p, h->K, h->nt, h->rc_cols.p, h->rc_count.p, (int)N,
+                                     h->Pc_hi.p, h->Pc_lo.p, h->CKpad, 0, s));
         TcExtra ex2;
         ex2.rowmap = h->rc_cols.p;
         ex2.map_rows = 1;
@@ -1115,11 +1114,17 @@ static int sort_batch_impl(lss_handle* h, const int16_t* raw, int64_t n_rows, in
     const int32_t n_bound = h->cfg.max_spikes;
     h->mark(8, s);
     if (need_tf) {
+        if (bf16) {
+            // FP32 projection rows of the spikes' columns, as the FP32 path has them
+            CK(launch_pca_proj_cols_tf32(Xh, h->ld, h->C, h->N, h->wpca.p, h->K, h->nt, h->sp_x.p, h->counters.p,
+                                         n_bound, h->B0T_hi.p, h->B0T_lo.p, h->CKpad, 1, s));
+            h->stats.launches += 1;
+        }
         const int grid = std::min(n_bound, 16 * h->sm_count);
         CK(launch_pc_features_folded(Xh, h->ld, h->C, h->nt, h->K, h->nC, h->T, h->wpca.p, h->Mw.p, h->U.p, h->R.p,
                                      h->iCC.p, h->iU.p, h->Ucc.p, h->sp_x.p, h->sp_y.p, h->sp_amp.p,
-                                     h->round_start.p, 0, grid, h->counters.p, h->tF.p, h->status.p,
-                                     bf16 ? nullptr : h->B0T_hi.p, bf16 ? nullptr : h->B0T_lo.p, h->CKpad, s));
+                                     h->round_start.p, 0, grid, h->counters.p, h->tF.p, h->status.p, h->B0T_hi.p,
+                                     h->B0T_lo.p, h->CKpad, s));
         h->stats.launches += 1;
     }
     h->mark(9, s);

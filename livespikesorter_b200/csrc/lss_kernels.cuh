@@ -106,9 +106,11 @@ constexpr float BF16_SCORE_EPS = 0.0078125f;  // 2^-7: |B16 - B32| <= eps ||U_t|
 cudaError_t launch_recheck_select(const float* cf_lo, const float* cf_hi, const float* ch, const float* cfmax,
                                   const int32_t* imax, int32_t N, int32_t nt, float th2, int32_t* cols, float* pre_cf,
                                   int32_t* pre_im, int32_t* count, cudaStream_t s);
+// FP32 projection rows (tf32 split) of the columns cols[0 .. *count) (at most
+// max_cols): row i of hi / lo, or row cols[i] when scatter is set
 cudaError_t launch_pca_proj_cols_tf32(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
-                                      int32_t nt, const int32_t* cols, const int32_t* count, float* hi, float* lo,
-                                      int64_t ldk, cudaStream_t s);
+                                      int32_t nt, const int32_t* cols, const int32_t* count, int32_t max_cols, float* hi,
+                                      float* lo, int64_t ldk, int32_t scatter, cudaStream_t s);
 cudaError_t launch_recheck_flips(const float* cfmax, const int32_t* imax, const int32_t* cols, const float* pre_cf,
                                  const int32_t* pre_im, int32_t* count, int32_t N, float th2, cudaStream_t s);
 // un[t] = ||hi[t, :] + lo[t, :]|| over rows of length ld

@@ -8,6 +8,8 @@
 
 #include <cuda_bf16.h>
 
+#include <algorithm>
+
 namespace lss {
 
 // ---------------------------------------------------------------------------
@@ -312,25 +314,27 @@ cudaError_t launch_recheck_select(const float* cf_lo, const float* cf_hi, const 
     return cudaGetLastError();
 }
 
-// FP32 projection of the listed columns into rows 0.. of hi / lo (tf32 split),
-// with k_pca_proj_t's arithmetic: every output sums its (zero-padded) taps in
-// ascending order with one fmaf each, so the rows equal the FP32 path's.
+// FP32 projection of the listed columns (tf32 split), with k_pca_proj_t's
+// arithmetic: every output sums its (zero-padded) taps in ascending order with
+// one fmaf each, so the rows equal the FP32 path's. Column cols[i] goes to row
+// i (scatter = 0) or to row cols[i] (scatter = 1: a batch-sized array).
 template <int KPC>
 __global__ void __launch_bounds__(128) k_pca_proj_cols(const float* __restrict__ X, int64_t ldx, int32_t C, int64_t N,
                                                        const float* __restrict__ wpca, int32_t nt, int32_t ntp,
                                                        const int32_t* __restrict__ cols,
                                                        const int32_t* __restrict__ count, float* __restrict__ hi,
-                                                       float* __restrict__ lo, int64_t ldk) {
+                                                       float* __restrict__ lo, int64_t ldk, int32_t scatter) {
     extern __shared__ float ws[];  // [KPC][ntp]
-    const int i = blockIdx.x;
-    if (i >= *count) return;
-    const int64_t s = cols[i];
     for (int e = threadIdx.x; e < KPC * ntp; e += blockDim.x) {
         const int k = e / ntp, m = e % ntp;
         ws[e] = (m < nt) ? wpca[k * nt + m] : 0.f;
     }
     __syncthreads();
+    const int n = *count;
     const int half = nt / 2;
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    const int64_t s = cols[i];
+    const int64_t row = scatter ? s : (int64_t)i;
     for (int c = threadIdx.x; c < C; c += blockDim.x) {
         const float* xr = X + (int64_t)c * ldx;
         float acc[KPC];
@@ -342,7 +346,7 @@ __global__ void __launch_bounds__(128) k_pca_proj_cols(const float* __restrict__
 #pragma unroll
             for (int k = 0; k < KPC; ++k) acc[k] = fmaf(ws[k * ntp + m], xv, acc[k]);
         }
-        const int64_t o = (int64_t)i * ldk + (int64_t)c * KPC;
+        const int64_t o = row * ldk + (int64_t)c * KPC;
 #pragma unroll
         for (int k = 0; k < KPC; ++k) {
             const float h = tf32_rna(acc[k]);
@@ -350,31 +354,36 @@ __global__ void __launch_bounds__(128) k_pca_proj_cols(const float* __restrict__
             lo[o + k] = tf32_rna(__fsub_rn(acc[k], h));
         }
     }
+    }
 }
 
 template <int KPC>
 static cudaError_t launch_cols(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t nt,
-                               const int32_t* cols, const int32_t* count, float* hi, float* lo, int64_t ldk,
-                               cudaStream_t s) {
+                               const int32_t* cols, const int32_t* count, int32_t max_cols, float* hi, float* lo,
+                               int64_t ldk, int32_t scatter, cudaStream_t s) {
     const int ntp = (nt + 7) & ~7;
     const size_t smem = sizeof(float) * KPC * ntp;
     if (smem > 48 * 1024) return cudaErrorInvalidValue;
-    k_pca_proj_cols<KPC><<<(unsigned)N, 128, smem, s>>>(X, ldx, C, N, wpca, nt, ntp, cols, count, hi, lo, ldk);
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = std::max(1, std::min(max_cols, 16 * sms));
+    k_pca_proj_cols<KPC><<<grid, 128, smem, s>>>(X, ldx, C, N, wpca, nt, ntp, cols, count, hi, lo, ldk, scatter);
     return cudaGetLastError();
 }
 
 cudaError_t launch_pca_proj_cols_tf32(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
-                                      int32_t nt, const int32_t* cols, const int32_t* count, float* hi, float* lo,
-                                      int64_t ldk, cudaStream_t s) {
+                                      int32_t nt, const int32_t* cols, const int32_t* count, int32_t max_cols, float* hi,
+                                      float* lo, int64_t ldk, int32_t scatter, cudaStream_t s) {
     switch (K) {
-        case 1: return launch_cols<1>(X, ldx, C, N, wpca, nt, cols, count, hi, lo, ldk, s);
-        case 2: return launch_cols<2>(X, ldx, C, N, wpca, nt, cols, count, hi, lo, ldk, s);
-        case 3: return launch_cols<3>(X, ldx, C, N, wpca, nt, cols, count, hi, lo, ldk, s);
-        case 4: return launch_cols<4>(X, ldx, C, N, wpca, nt, cols, count, hi, lo, ldk, s);
-        case 5: return launch_cols<5>(X, ldx, C, N, wpca, nt, cols, count, hi, lo, ldk, s);
-        case 6: return launch_cols<6>(X, ldx, C, N, wpca, nt, cols, count, hi, lo, ldk, s);
-        case 7: return launch_cols<7>(X, ldx, C, N, wpca, nt, cols, count, hi, lo, ldk, s);
-        case 8: return launch_cols<8>(X, ldx, C, N, wpca, nt, cols, count, hi, lo, ldk, s);
+        case 1: return launch_cols<1>(X, ldx, C, N, wpca, nt, cols, count, max_cols, hi, lo, ldk, scatter, s);
+        case 2: return launch_cols<2>(X, ldx, C, N, wpca, nt, cols, count, max_cols, hi, lo, ldk, scatter, s);
+        case 3: return launch_cols<3>(X, ldx, C, N, wpca, nt, cols, count, max_cols, hi, lo, ldk, scatter, s);
+        case 4: return launch_cols<4>(X, ldx, C, N, wpca, nt, cols, count, max_cols, hi, lo, ldk, scatter, s);
+        case 5: return launch_cols<5>(X, ldx, C, N, wpca, nt, cols, count, max_cols, hi, lo, ldk, scatter, s);
+        case 6: return launch_cols<6>(X, ldx, C, N, wpca, nt, cols, count, max_cols, hi, lo, ldk, scatter, s);
+        case 7: return launch_cols<7>(X, ldx, C, N, wpca, nt, cols, count, max_cols, hi, lo, ldk, scatter, s);
+        case 8: return launch_cols<8>(X, ldx, C, N, wpca, nt, cols, count, max_cols, hi, lo, ldk, scatter, s);
         default: return cudaErrorInvalidValue;
     }
 }

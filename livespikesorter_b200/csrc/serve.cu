@@ -216,11 +216,15 @@ int enqueue_stream_batch(Probe* p) {
     if (rc) return p->fail(rc, h->err);
     const bool bf16 = h->cfg.precision == LSS_PREC_BF16_RECHECK;
     if (p->feat > 0) {
+        if (bf16)  // FP32 projection rows of the spikes' columns, as the FP32 path has them
+            PCK(launch_pca_proj_cols_tf32(Xh, h->ld, h->C, h->N, h->wpca.p, h->K, h->nt, h->sp_x.p, h->counters.p,
+                                          (int)std::min<int64_t>(p->cap, h->cfg.max_spikes), h->B0T_hi.p, h->B0T_lo.p,
+                                          h->CKpad, 1, s));
         const int grid = (int)std::min<int64_t>(p->cap, 2 * (int64_t)h->sm_count);
         PCK(launch_pc_features_folded(Xh, h->ld, h->C, h->nt, h->K, h->nC, h->T, h->wpca.p, h->Mw.p, h->U.p,
                                       h->R.p, h->iCC.p, h->iU.p, h->Ucc.p, h->sp_x.p, h->sp_y.p, h->sp_amp.p,
-                                      h->round_start.p, 0, grid, h->counters.p, h->tF.p, h->status.p,
-                                      bf16 ? nullptr : h->B0T_hi.p, bf16 ? nullptr : h->B0T_lo.p, h->CKpad, s));
+                                      h->round_start.p, 0, grid, h->counters.p, h->tF.p, h->status.p, h->B0T_hi.p,
+                                      h->B0T_lo.p, h->CKpad, s));
     }
     RecordClock rclk;
     rclk.ibatch_dev = p->state.p;
@@ -350,6 +354,12 @@ int harvest_one(Probe* p, std::unique_lock<std::mutex>& lk, bool wait) {
         r.clu.assign(p->o_clu.p + k * p->cap, p->o_clu.p + k * p->cap + n);
     }
     p->lat_ms.push_back((double)(sl.emit_ns - sl.arrival_ns) * 1e-6);
+    // the host and device clocks drift apart by a few ppm: each batch brackets
+    // the offset between launch - t_begin (the device began after the host
+    // launched) and emit - t_end (the host saw completion after the device
+    // ended); the estimate is pulled into that bracket when it has drifted out
+    p->gpu_offset_ns = std::max(p->gpu_offset_ns, sl.launch_ns - mail.t_begin);
+    p->gpu_offset_ns = std::min(p->gpu_offset_ns, sl.emit_ns - mail.t_end);
     const int64_t beg = mail.t_begin + p->gpu_offset_ns, end = mail.t_end + p->gpu_offset_ns;
     const double parts[4] = {(double)(sl.launch_ns - sl.arrival_ns) * 1e-6, (double)(beg - sl.launch_ns) * 1e-6,
                              (double)(end - beg) * 1e-6, (double)(sl.emit_ns - end) * 1e-6};

@@ -33,10 +33,10 @@ pytestmark = pytest.mark.gpu
 
 AMP_RTOL = 1e-4
 PC_TOL = 1e-3
-# a decision whose two sides differ by less than this relative Cf, on the
-# oracle's own field at that round, is a near-tie: the score GEMM (3xTF32 on
-# the tensor cores, about 1e-7 relative) and torch's CPU einsum round
-# differently, so either side is an FP32-correct answer
+# a GPU pick that another column of its window (or another template) beats by
+# less than this relative Cf on the oracle's own field at that round is a
+# near-tie: the score GEMM (3xTF32 on the tensor cores) and torch's CPU einsum
+# round differently, so either side is an FP32-correct answer
 NEAR_TIE = 1e-5
 NEAR_TIE_AGREEMENT = 0.999
 
@@ -59,9 +59,11 @@ def _oracle(setup, rec, ib, dtype=torch.float32):
 
 
 def _report(setup, X, st_o, rounds_o, x_gpu, y_gpu, i):
-    """The first differing decision on the oracle's own score field at the start
-    of that round (FP32): the relative Cf gap between the oracle's choice and
-    the GPU's, a message with the margins, and what the FP64 oracle picks."""
+    """The first differing decision, judged on the oracle's own score field at
+    the start of that round (FP32): how far the GPU's pick (x, y) is from being
+    a valid pick there (relative Cf by which another column of its +-nt window,
+    or another template at x, beats it; <= 0 means valid), a message with the
+    margins, and what the FP64 oracle picks."""
     nt = setup.nt
     U = setup.U
     r = int(rounds_o[min(i, len(rounds_o) - 1)])
@@ -71,16 +73,16 @@ def _report(setup, X, st_o, rounds_o, x_gpu, y_gpu, i):
     Cf = torch.relu(Br) ** 2 / nm[:, None]
     Cf[:, :nt] = 0
     Cf[:, -nt:] = 0
-    x, y = (int(st_o[i, 0]), int(st_o[i, 1])) if i < len(st_o) else (int(x_gpu), int(y_gpu))
-    c_o = float(Cf[y, x])
-    c_g = float(Cf[int(y_gpu), int(x_gpu)])
-    gap = (c_o - c_g) / max(c_o, 1e-30)
-    top = torch.topk(Cf[:, x], 2)
+    cmax = Cf.max(0).values
+    xg, yg = int(x_gpu), int(y_gpu)
+    c_g = float(Cf[yg, xg])
+    wmax = float(cmax[max(0, xg - nt):xg + nt + 1].max())
+    gap = (wmax - c_g) / max(c_g, 1e-30)
+    x, y = (int(st_o[i, 0]), int(st_o[i, 1])) if i < len(st_o) else (xg, yg)
     st64, _, _ = ko.run_matching(X, U, setup.ctc, setup.wPCA, setup.Th, nt, dtype=torch.float64)
-    msg = (f'first difference at spike {i} (oracle round {r}): oracle (x, y) = ({x}, {y}) Cf {c_o:.7e}, '
-           f'GPU (x, y) = ({int(x_gpu)}, {int(y_gpu)}) Cf {c_g:.7e} on the oracle field, relative gap {gap:.3e}; '
-           f'column {x}: best {int(top.indices[0])} {float(top.values[0]):.7e}, runner-up {int(top.indices[1])} '
-           f'{float(top.values[1]):.7e}; FP64 oracle: {len(st64)} spikes, '
+    msg = (f'first difference at spike {i} (oracle round {r}): oracle (x, y) = ({x}, {y}) Cf {float(Cf[y, x]):.7e}, '
+           f'GPU (x, y) = ({xg}, {yg}) Cf {c_g:.7e} on the oracle field, best of its window {wmax:.7e}, '
+           f'relative gap {gap:.3e}; FP64 oracle: {len(st64)} spikes, '
            f'{"same" if len(st64) == len(st_o) and torch.equal(st64, st_o) else "different"} sequence as FP32')
     return gap, msg
 
@@ -113,7 +115,7 @@ def _check_batches(T, dup, seed):
             gi = min(i, len(got) - 1)
             x_gpu = got[gi, 0] - (ib * NT - nt // 2 + setup.nt0min) + nt
             gap, msg = _report(setup, X, st, rounds, x_gpu, got[gi, 1], min(i + off, len(st) - 1))
-            if not (abs(gap) <= NEAR_TIE):
+            if not (gap <= NEAR_TIE):
                 pytest.fail(f'T={T} batch {ib}: {len(got)} GPU vs {len(want)} oracle spikes; ' + msg)
             # a near-tie decided the other way: the rounds after it differ near
             # that column only; the rest must still agree as a set
@@ -123,13 +125,20 @@ def _check_batches(T, dup, seed):
             near_ties.append((T, ib, gap, agree))
             print(f'near-tie, T={T} batch {ib}: {msg}; set agreement {agree:.6f}')
             assert agree >= NEAR_TIE_AGREEMENT, (T, ib, agree, msg)
-            n_cmp = i  # amplitudes and features of the common prefix
+            n_cmp = i  # amplitudes of the common prefix
         a = r['amplitude'].numpy().astype(np.float64)[:n_cmp]
         b = ref[:n_cmp, 2]
         rel = np.abs(a - b) / np.maximum(np.abs(b), 1e-6)
         assert n_cmp == 0 or rel.max() <= AMP_RTOL, (ib, rel.max())
+        # PC features of the common prefix, except spikes within 2nt of a spike
+        # that differs (their residual windows hold the other side of the tie)
         tf = ref_tf.numpy()
-        assert np.abs(r['pc'].numpy()[:n_cmp] - tf[:n_cmp]).max() <= PC_TOL * np.abs(tf).max(), ib
+        keep = np.ones(n_cmp, bool)
+        if n_cmp < len(got):
+            diff_t = np.concatenate([got[n_cmp:, 0], want[n_cmp:, 0]])
+            near = np.abs(got[:n_cmp, 0][:, None] - diff_t[None, :]).min(1) <= 2 * nt
+            keep &= ~near
+        assert np.abs(r['pc'].numpy()[:n_cmp][keep] - tf[:n_cmp][keep]).max() <= PC_TOL * np.abs(tf).max(), ib
         total += len(got)
     # at most one near-tie per 20000 spikes
     assert len(near_ties) <= max(1, total // 20000), near_ties

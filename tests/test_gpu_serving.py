@@ -115,8 +115,9 @@ def test_realtime_latency_is_reported():
         assert parts.shape == (st.n_blocks, 4)
         assert np.allclose(parts.sum(1), lat, rtol=0, atol=1e-6)
         assert np.all(parts[:, 0] >= 0) and np.all(parts[:, 2] > 0)
-        # device times mapped to the host clock: the offset's error is a few us
-        assert np.all(parts[:, 1] > -0.05) and np.all(parts[:, 3] > -0.05)
+        # device times mapped to the host clock (offset re-anchored on every
+        # batch's own launch / completion bracket): no part is negative
+        assert np.all(parts >= 0), parts[(parts < 0).any(1)][:3]
     assert out['wall_s'] >= 0.35
 
 
