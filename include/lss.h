@@ -166,6 +166,14 @@ int  lss_match(lss_handle* h, const float* X_dev, int64_t N, int64_t* st_dev, fl
 int  lss_match_scores(lss_handle* h, const float* B_dev, int64_t N, int64_t* st_dev,
                       float* amps_dev, int64_t capacity, int64_t* n_spikes, void* stream);
 
+/* Which kernel runs the matching-pursuit rounds of this handle (identical
+ * spikes, amplitudes and score field either way; a performance choice, no
+ * counterpart in the reference): 0 = every template row of every spike window
+ * is updated (default); 1 = template rows are grouped in blocks along the probe
+ * and a block whose update provably leaves every score unchanged (terms below
+ * a quarter ulp of the block's smallest score) is skipped. */
+int  lss_set_round_kernel(lss_handle* h, int32_t skip_blocks);
+
 /* The same matching-pursuit rounds for callers that cannot allocate device
  * memory (an acquisition host that owns the GPU's memory, a process whose
  * memory another allocator reserved up front, a real-time loop that must not

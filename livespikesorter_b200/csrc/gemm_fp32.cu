@@ -107,19 +107,23 @@ struct StorePlain {
 };
 
 // Folded-template layout of the score GEMM: row m = t*K + k, column n = c'
-// goes to [t, c'*K + k] of a row-stride-ldk array, as bf16 or as the tf32
-// split hi = rna(v), lo = rna(v - hi) (both exact tf32 values).
+// goes to [t, c'*K + k] of a row-stride-ldk array, as the bf16 split
+// hi = bf16(v), lo = bf16(v - hi) or as the tf32 split hi = rna(v),
+// lo = rna(v - hi) (both exact tf32 values).
 struct StoreFolded {
     int K;
     int64_t ldk;
     __nv_bfloat16* out16;
+    __nv_bfloat16* out16lo;
     float* hi;
     float* lo;
     __device__ void operator()(int m, int n, float v) const {
         const int t = m / K, k = m - (m / K) * K;
         const int64_t o = (int64_t)t * ldk + (int64_t)n * K + k;
         if (out16) {
-            out16[o] = __float2bfloat16_rn(v);
+            const __nv_bfloat16 h = __float2bfloat16_rn(v);
+            out16[o] = h;
+            if (out16lo) out16lo[o] = __float2bfloat16_rn(__fsub_rn(v, __bfloat162float(h)));
         } else {
             uint32_t r;
             asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
@@ -200,10 +204,10 @@ cudaError_t launch_sgemm(const float* A, int64_t lda, const float* B, int64_t ld
 }
 
 cudaError_t launch_sgemm_folded(const float* U, const float* Mw, int32_t T, int32_t K, int32_t C, int64_t ldk,
-                                __nv_bfloat16* out16, float* hi, float* lo, cudaStream_t s) {
+                                __nv_bfloat16* out16, __nv_bfloat16* out16lo, float* hi, float* lo, cudaStream_t s) {
     // rows t*K + k of U [T, K, C] (row-major, stride C) times Mw [C, C]
     dim3 grid((C + SBN - 1) / SBN, (T * K + SBM - 1) / SBM);
-    k_sgemm64<StoreFolded><<<grid, 256, 0, s>>>(U, C, Mw, C, T * K, C, C, StoreFolded{K, ldk, out16, hi, lo});
+    k_sgemm64<StoreFolded><<<grid, 256, 0, s>>>(U, C, Mw, C, T * K, C, C, StoreFolded{K, ldk, out16, out16lo, hi, lo});
     return cudaGetLastError();
 }
 

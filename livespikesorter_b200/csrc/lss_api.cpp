@@ -114,10 +114,10 @@ int lss::rebuild_uw(lss_handle* h) {
     const int C = h->C;
     // templates with the whitening folded in, for lss_sort_batch
     const bool bf16 = h->cfg.precision == LSS_PREC_BF16_RECHECK;
-    CK(launch_build_uw(h->U.p, h->Mw.p, h->T, h->K, C, h->CKpad, nullptr, h->Uw_hi.p, h->Uw_lo.p, 0));
+    CK(launch_build_uw(h->U.p, h->Mw.p, h->T, h->K, C, h->CKpad, nullptr, nullptr, h->Uw_hi.p, h->Uw_lo.p, 0));
     h->stats.launches += 1;
     if (bf16) {
-        CK(launch_build_uw(h->U.p, h->Mw.p, h->T, h->K, C, h->CKpad, h->Uw16.p, nullptr, nullptr, 0));
+        CK(launch_build_uw(h->U.p, h->Mw.p, h->T, h->K, C, h->CKpad, h->Uw16.p, h->Uw16lo.p, nullptr, nullptr, 0));
         // template norms of the BF16 error bound, for the folded and the plain operand
         CK(launch_row_norms(h->Uw_hi.p, h->Uw_lo.p, h->T, h->CKpad, h->un_w.p, 0));
         CK(launch_row_norms(h->Up_hi.p, h->Up_lo.p, h->T, h->CKpad, h->un_p.p, 0));
@@ -334,7 +334,8 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
 
     // one CTA per >= 32 columns (a serving loop lowers it further so that
     // its probes' rounds kernels fit on the device together)
-    h->mp_grid = std::min<int>(mp_blocks_max_grid(cfg->device), (int)std::max<int64_t>(1, (h->N + 31) / 32));
+    h->mp_grid = std::min<int>(std::min(mp_blocks_max_grid(cfg->device), mp_max_grid(cfg->device)),
+                               (int)std::max<int64_t>(1, (h->N + 31) / 32));
     cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, cfg->device);
     h->CKpad = (C * K + 63) / 64 * 64;
     const int64_t cap = cfg->max_spikes;
@@ -358,19 +359,22 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
     ALLOC(Xh, (size_t)C * ld);
     ALLOC(X, (size_t)C * ld);
     const bool bf16 = cfg->precision == LSS_PREC_BF16_RECHECK;
-    const TcPlan plan = tc_plan(T, !bf16);
+    const TcPlan plan = tc_plan(T, bf16 ? TC_BF16X3 : TC_TF32X3);
     if (plan.stages < 2) {
         g_create_err = "too many templates for the tensor-core score GEMM's shared memory";
         return LSS_ERR_ARG;
     }
     if (bf16) {
-        if (tc_plan(T, true).stages < 2) {
+        if (tc_plan(T, TC_TF32X3).stages < 2) {
             g_create_err = "too many templates for the FP32 re-check GEMM's shared memory";
             return LSS_ERR_ARG;
         }
         ALLOC(B0T, (size_t)h->N * h->CKpad);
+        ALLOC(B0T16lo, (size_t)h->N * h->CKpad);
         ALLOC(Up16, (size_t)plan.Tpad * h->CKpad);
+        ALLOC(Up16lo, (size_t)plan.Tpad * h->CKpad);
         ALLOC(Uw16, (size_t)plan.Tpad * h->CKpad);
+        ALLOC(Uw16lo, (size_t)plan.Tpad * h->CKpad);
         // FP32 re-check of open decisions: projection rows of the listed columns, bookkeeping
         const size_t rc_rows = (size_t)(h->N + 127) / 128 * 128;
         ALLOC(Pc_hi, rc_rows * h->CKpad);
@@ -400,7 +404,7 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
     ALLOC(B0T_hi, (size_t)h->N * h->CKpad);
     ALLOC(B0T_lo, (size_t)h->N * h->CKpad);
     // tf32 template splits: the FP32 path's scores, and the BF16 path's re-check
-    const int Tpad32 = tc_plan(T, true).Tpad;
+    const int Tpad32 = tc_plan(T, TC_TF32X3).Tpad;
     ALLOC(Up_hi, (size_t)Tpad32 * h->CKpad);
     ALLOC(Up_lo, (size_t)Tpad32 * h->CKpad);
     ALLOC(Uw_hi, (size_t)Tpad32 * h->CKpad);
@@ -465,12 +469,19 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
     CK(cudaMemcpy(h->chan_map.p, cmap.data(), C * sizeof(int32_t), cudaMemcpyHostToDevice));
     if (!taps.empty()) CK(cudaMemcpy(h->taps.p, taps.data(), taps.size() * sizeof(float), cudaMemcpyHostToDevice));
     if (bf16) {
-        // U_p in bf16, [Tpad, CKpad] with zero padding
-        std::vector<__nv_bfloat16> u16((size_t)plan.Tpad * h->CKpad, __float2bfloat16(0.f));
+        // U_p as the bf16 split hi = bf16(x), lo = bf16(x - hi), [Tpad, CKpad] with zero padding
+        std::vector<__nv_bfloat16> u16((size_t)plan.Tpad * h->CKpad, __float2bfloat16(0.f)), u16lo(u16);
         for (int i = 0; i < T; ++i)
-            for (int e = 0; e < C * K; ++e) u16[(size_t)i * h->CKpad + e] = __float2bfloat16(up[(size_t)i * C * K + e]);
+            for (int e = 0; e < C * K; ++e) {
+                const float x = up[(size_t)i * C * K + e];
+                const __nv_bfloat16 hb = __float2bfloat16(x);
+                u16[(size_t)i * h->CKpad + e] = hb;
+                u16lo[(size_t)i * h->CKpad + e] = __float2bfloat16(x - __bfloat162float(hb));
+            }
         CK(cudaMemcpy(h->Up16.p, u16.data(), u16.size() * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h->Up16lo.p, u16lo.data(), u16lo.size() * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice));
         CK(cudaMemset(h->B0T.p, 0, (size_t)h->N * h->CKpad * sizeof(__nv_bfloat16)));
+        CK(cudaMemset(h->B0T16lo.p, 0, (size_t)h->N * h->CKpad * sizeof(__nv_bfloat16)));
         const size_t rc_bytes = (size_t)(h->N + 127) / 128 * 128 * h->CKpad * sizeof(float);
         CK(cudaMemset(h->Pc_hi.p, 0, rc_bytes));
         CK(cudaMemset(h->Pc_lo.p, 0, rc_bytes));
@@ -537,7 +548,10 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
                 }
         CK(cudaMemcpy(h->R.p, r.data(), r.size() * sizeof(float), cudaMemcpyHostToDevice));
     }
-    if (bf16) CK(cudaMemset(h->Uw16.p, 0, (size_t)plan.Tpad * h->CKpad * sizeof(__nv_bfloat16)));
+    if (bf16) {
+        CK(cudaMemset(h->Uw16.p, 0, (size_t)plan.Tpad * h->CKpad * sizeof(__nv_bfloat16)));
+        CK(cudaMemset(h->Uw16lo.p, 0, (size_t)plan.Tpad * h->CKpad * sizeof(__nv_bfloat16)));
+    }
     CK(cudaMemset(h->Uw_hi.p, 0, (size_t)Tpad32 * h->CKpad * sizeof(float)));
     CK(cudaMemset(h->Uw_lo.p, 0, (size_t)Tpad32 * h->CKpad * sizeof(float)));
     if (nC > 0) {
@@ -586,6 +600,13 @@ int lss_get_stats(const lss_handle* h, lss_stats* out) {
         out->recheck_flips = h->rc_host[1];
         out->recheck_rescored = h->rc_host[0];
     }
+    return LSS_OK;
+}
+
+int lss_set_round_kernel(lss_handle* h, int32_t skip_blocks) {
+    if (!h || (skip_blocks != 0 && skip_blocks != 1)) return LSS_ERR_ARG;
+    if (h->streaming) return h->fail(LSS_ERR_STATE, "handle is owned by a serving loop");
+    h->mp_skip = skip_blocks != 0;
     return LSS_OK;
 }
 
@@ -673,17 +694,21 @@ int lss::run_ingest(lss_handle* h, const int16_t* src, const IngestMap& map, flo
 int lss::run_scores(lss_handle* h, const float* X, int64_t ldx, int64_t N, float* B, cudaStream_t s,
                    bool* maxima_ready, bool folded) {
     if (h->cfg.precision == LSS_PREC_BF16_RECHECK) {
-        CK(launch_pca_proj_t(X, ldx, h->C, N, h->wpca.p, h->K, h->nt, h->B0T.p, h->CKpad, s, h->pn2.p));
+        CK(launch_pca_proj_t(X, ldx, h->C, N, h->wpca.p, h->K, h->nt, h->B0T.p, h->B0T16lo.p, h->CKpad, s, h->pn2.p));
         h->mark(5, s);
         TcExtra ex;
         ex.cf2 = h->cf2.p;
         ex.un = folded ? h->un_w.p : h->un_p.p;
         ex.pn2 = h->pn2.p;
-        ex.eps = BF16_SCORE_EPS;
+        // |B - B_fp32| <= eps ||U_t|| ||P_s||: 3 * 2^-18 for the dropped lo*lo term
+        // and the rounding of the lo parts, plus FP32 accumulation over CKpad
+        // terms in both paths (CKpad * 2^-24 each)
+        ex.eps = (float)(3.0 * std::ldexp(1.0, -18) * 1.01 + 2.0 * h->CKpad * std::ldexp(1.0, -24));
         ex.cf_lo = h->cf_lo.p;
         ex.cf_hi = h->cf_hi.p;
-        CK(launch_score_tc(h->B0T.p, h->CKpad, (int)N, folded ? h->Uw16.p : h->Up16.p, h->T, h->CKpad, h->nm.p, B,
-                           h->ld, h->cfmax.p, h->imax.p, h->nt, h->status.p, h->sm_count, s, ex));
+        CK(launch_score_tc_bf16x3(h->B0T.p, h->B0T16lo.p, h->CKpad, (int)N, folded ? h->Uw16.p : h->Up16.p,
+                                  folded ? h->Uw16lo.p : h->Up16lo.p, h->T, h->CKpad, h->nm.p, B, h->ld, h->cfmax.p,
+                                  h->imax.p, h->nt, h->status.p, h->sm_count, s, ex));
         // FP32 re-check of the columns whose first-round decisions the BF16
         // error bound leaves open; the column list and its length stay on the
         // device
@@ -756,17 +781,23 @@ int lss::enqueue_mp(lss_handle* h, int64_t N, cudaStream_t s, bool maxima_ready)
     a.counters = h->counters.p;
     a.status = h->status.p;
     a.bar = h->bar.p;
-    a.perm = h->mp_perm.p;
-    a.nb = h->mp_nb;
-    a.cmaxr = h->mp_cmaxr.p;
-    a.bkey = h->mp_bkey.p;
-    a.bmin = h->mp_bmin.p;
     const int G = h->mp_grid;
     a.cols_per_blk = (int)((N + G - 1) / G);
-    a.init_cols = 1;  // the rounds take their block maxima from the field itself
     if (!maxima_ready) CK(cudaMemsetAsync(h->status.p, 0, sizeof(int32_t), s));
     CK(cudaMemsetAsync(h->counters.p, 0, 4 * sizeof(int32_t), s));
-    CK(launch_mp_blocks(a, G, s));
+    if (h->mp_skip) {
+        a.perm = h->mp_perm.p;
+        a.nb = h->mp_nb;
+        a.cmaxr = h->mp_cmaxr.p;
+        a.bkey = h->mp_bkey.p;
+        a.bmin = h->mp_bmin.p;
+        a.init_cols = 1;  // the rounds take their block maxima from the field itself
+        CK(launch_mp_blocks(a, G, s));
+    } else {
+        a.init_cols = maxima_ready ? 0 : 1;
+        CK(cudaMemsetAsync(h->colkey.p, 0, 2 * h->ld * sizeof(unsigned long long), s));
+        CK(launch_mp(a, G, s));
+    }
     h->stats.launches += 1;
     return LSS_OK;
 }

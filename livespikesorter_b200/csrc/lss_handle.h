@@ -66,13 +66,15 @@ struct lss_handle {
     DevBuf<unsigned long long> colkey;
     // block-skipping rounds (mp_blocks.cu): template rows in blocks of
     // MPB_ROWS ordered along the probe, |ctc| maxima, per-block column state
+    bool mp_skip = false;                        // rounds kernel: block-skipping (mp_blocks.cu) or full (mp.cu)
     int mp_nb = 0;
     DevBuf<int32_t> mp_perm;
     DevBuf<float> mp_cmaxr, mp_bmin;
     DevBuf<unsigned long long> mp_bkey;
-    DevBuf<__nv_bfloat16> B0T, Up16;   // BF16 path: transposed projection, templates
+    // BF16 path (BF16x3 GEMM): projection and templates as bf16 hi / lo splits
+    DevBuf<__nv_bfloat16> B0T, B0T16lo, Up16, Up16lo;
     DevBuf<float> B0T_hi, B0T_lo, Up_hi, Up_lo;  // FP32 path (3xTF32): tf32 hi/lo splits
-    DevBuf<__nv_bfloat16> Uw16;                  // templates with the whitening folded in (BF16 path)
+    DevBuf<__nv_bfloat16> Uw16, Uw16lo;          // templates with the whitening folded in (BF16 path)
     DevBuf<float> Uw_hi, Uw_lo;                  // ... (FP32 path)
     DevBuf<float> U, R;                          // U [T,K,C]; R [K,K,2nt-1] basis lag correlations
     DevBuf<float2> hpH, hpTw;                    // highpass spectrum and twiddles (FFT form)
@@ -148,9 +150,9 @@ struct lss_handle {
         round_start.release(); counters.release(); status.release(); sp_amp.release(); blk_amp.release(); colkey.release();
         mp_perm.release(); mp_cmaxr.release(); mp_bmin.release(); mp_bkey.release();
         bar.release(); rec_time.release(); rec_count.release(); rec_tmpl.release(); rec_slot.release(); rec_amp.release();
-        rec_pc.release(); B0T.release(); Up16.release();
+        rec_pc.release(); B0T.release(); B0T16lo.release(); Up16.release(); Up16lo.release();
         B0T_hi.release(); B0T_lo.release(); Up_hi.release(); Up_lo.release();
-        Uw16.release(); Uw_hi.release(); Uw_lo.release(); U.release(); R.release(); hpH.release(); hpTw.release();
+        Uw16.release(); Uw16lo.release(); Uw_hi.release(); Uw_lo.release(); U.release(); R.release(); hpH.release(); hpTw.release();
         cf2.release(); cf_lo.release(); cf_hi.release(); pre_cf.release(); Pc_hi.release(); Pc_lo.release();
         pn2.release(); un_w.release(); un_p.release(); rc_cols.release(); pre_im.release();
         rc_count.release();

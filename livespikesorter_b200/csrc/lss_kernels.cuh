@@ -42,13 +42,15 @@ cudaError_t launch_sgemm(const float* A, int64_t lda, const float* B, int64_t ld
 // rows t*K + k of U [T, K, C] times Mw [C, C], stored as the score GEMM's
 // folded templates ([t, c'*K + k], bf16 or tf32 hi/lo)
 cudaError_t launch_sgemm_folded(const float* U, const float* Mw, int32_t T, int32_t K, int32_t C, int64_t ldk,
-                                __nv_bfloat16* out16, float* hi, float* lo, cudaStream_t s);
+                                __nv_bfloat16* out16, __nv_bfloat16* out16lo, float* hi, float* lo, cudaStream_t s);
 
 // ---- temporal basis projection (score.cu) ----
 // transposed bf16 variant for the tensor-core GEMM: B0T[s, c*K + k], row stride ldk
-// norm2 (optional, [N]): ||B0T[s, :]||^2 of the FP32 values before bf16 rounding
+// bf16 split (hi, lo = bf16(x - hi)) of the projection for the BF16x3 GEMM;
+// norm2 (optional, [N]): ||B0T[s, :]||^2 of the FP32 values before rounding
 cudaError_t launch_pca_proj_t(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
-                              int32_t nt, __nv_bfloat16* B0T, int64_t ldk, cudaStream_t s, float* norm2 = nullptr);
+                              int32_t nt, __nv_bfloat16* B0T_hi, __nv_bfloat16* B0T_lo, int64_t ldk, cudaStream_t s,
+                              float* norm2 = nullptr);
 
 // ---- tensor-core score GEMM (tc_gemm.cu) ----
 struct TcPlan {
@@ -61,7 +63,9 @@ struct TcPlan {
     int kblock;    // K elements per pipeline stage
     int pass_w;    // templates per pass
 };
-TcPlan tc_plan(int T, bool tf32, int pass_w = 512);
+// element kinds of the score GEMM (tc_gemm.cu)
+enum TcOp : int { TC_BF16 = 0, TC_TF32X3 = 1, TC_BF16X3 = 2 };
+TcPlan tc_plan(int T, int op, int pass_w = 512);
 // Optional epilogue behaviour of the score GEMM.
 struct TcExtra {
     // GEMM row r scores sample rowmap[r / map_rows] * map_rows + r % map_rows
@@ -86,6 +90,13 @@ struct TcExtra {
 cudaError_t launch_score_tc(const __nv_bfloat16* B0T, int64_t ldk, int N, const __nv_bfloat16* Up, int T, int CKpad,
                             const float* nm, float* Bout, int64_t ldb, float* cfmax, int32_t* imax, int nt,
                             int32_t* status, int grid, cudaStream_t s, const TcExtra& ex = TcExtra());
+// BF16x3: operands split into bf16 hi = bf16(x), lo = bf16(x - hi); three bf16
+// MMAs per k-step (hi*hi, hi*lo, lo*hi) with FP32 accumulation, about 2^-16
+// relative per product
+cudaError_t launch_score_tc_bf16x3(const __nv_bfloat16* B0T_hi, const __nv_bfloat16* B0T_lo, int64_t ldk, int N,
+                                   const __nv_bfloat16* Up_hi, const __nv_bfloat16* Up_lo, int T, int CKpad,
+                                   const float* nm, float* Bout, int64_t ldb, float* cfmax, int32_t* imax, int nt,
+                                   int32_t* status, int grid, cudaStream_t s, const TcExtra& ex = TcExtra());
 // FP32-class variant (3xTF32): operands split into tf32 hi + lo parts stored as fp32.
 cudaError_t launch_score_tc_tf32x3(const float* B0T_hi, const float* B0T_lo, int64_t ldk, int N, const float* Up_hi,
                                    const float* Up_lo, int T, int CKpad, const float* nm, float* Bout, int64_t ldb,
@@ -95,14 +106,13 @@ cudaError_t launch_score_tc_tf32x3(const float* B0T_hi, const float* B0T_lo, int
 cudaError_t launch_pca_proj_t_tf32(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
                                    int32_t nt, float* hi, float* lo, int64_t ldk, cudaStream_t s);
 
-// U_w[t, c'*K + k] = sum_c U[t,k,c] Mw[c,c'] in GEMM layout: bf16 (out16) or tf32 hi/lo
+// U_w[t, c'*K + k] = sum_c U[t,k,c] Mw[c,c'] in GEMM layout: bf16 split (out16, out16lo) or tf32 hi/lo
 cudaError_t launch_build_uw(const float* U, const float* Mw, int32_t T, int32_t K, int32_t C, int64_t ldk,
-                            __nv_bfloat16* out16, float* hi, float* lo, cudaStream_t s);
+                            __nv_bfloat16* out16, __nv_bfloat16* out16lo, float* hi, float* lo, cudaStream_t s);
 
 // FP32 re-check of the BF16 path (score.cu): columns whose first-round
 // decisions the BF16 error bound leaves open, their FP32 projection rows and
 // the count of decisions the re-check changed
-constexpr float BF16_SCORE_EPS = 0.0078125f;  // 2^-7: |B16 - B32| <= eps ||U_t|| ||P_s||
 cudaError_t launch_recheck_select(const float* cf_lo, const float* cf_hi, const float* ch, const float* cfmax,
                                   const int32_t* imax, int32_t N, int32_t nt, float th2, int32_t* cols, float* pre_cf,
                                   int32_t* pre_im, int32_t* count, cudaStream_t s);

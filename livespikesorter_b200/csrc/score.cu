@@ -38,7 +38,7 @@ __device__ __forceinline__ float tf32_rna(float x) {
 template <int KPC, int PC, bool TF32, int NTP>
 __global__ void __launch_bounds__(256) k_pca_proj_t(const float* __restrict__ X, int64_t ldx, int32_t C, int64_t N,
                                                     const float* __restrict__ wpca, int32_t nt, void* __restrict__ out0,
-                                                    float* __restrict__ out_lo, int64_t ldk,
+                                                    void* __restrict__ out_lo, int64_t ldk,
                                                     const int32_t* __restrict__ tiles, const int32_t* __restrict__ ntiles,
                                                     float* __restrict__ norm2) {
     extern __shared__ float sm[];
@@ -118,13 +118,19 @@ __global__ void __launch_bounds__(256) k_pca_proj_t(const float* __restrict__ X,
                 const float4 lo = make_float4(tf32_rna(__fsub_rn(v.x, hi.x)), tf32_rna(__fsub_rn(v.y, hi.y)),
                                               tf32_rna(__fsub_rn(v.z, hi.z)), tf32_rna(__fsub_rn(v.w, hi.w)));
                 *reinterpret_cast<float4*>(static_cast<float*>(out0) + o) = hi;
-                *reinterpret_cast<float4*>(out_lo + o) = lo;
+                *reinterpret_cast<float4*>(static_cast<float*>(out_lo) + o) = lo;
             } else {
-                __nv_bfloat16* d = static_cast<__nv_bfloat16*>(out0) + o;
-                d[0] = __float2bfloat16_rn(v.x);
-                d[1] = __float2bfloat16_rn(v.y);
-                d[2] = __float2bfloat16_rn(v.z);
-                d[3] = __float2bfloat16_rn(v.w);
+                // bf16 split: hi = bf16(x), lo = bf16(x - hi), 4 values per 8-byte store
+                const float vv[4] = {v.x, v.y, v.z, v.w};
+                __align__(8) __nv_bfloat16 hb[4], lb[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    hb[u] = __float2bfloat16_rn(vv[u]);
+                    lb[u] = __float2bfloat16_rn(__fsub_rn(vv[u], __bfloat162float(hb[u])));
+                }
+                *reinterpret_cast<uint2*>(static_cast<__nv_bfloat16*>(out0) + o) = *reinterpret_cast<const uint2*>(hb);
+                if (out_lo)
+                    *reinterpret_cast<uint2*>(static_cast<__nv_bfloat16*>(out_lo) + o) = *reinterpret_cast<const uint2*>(lb);
             }
         }
         // tail (seg not a multiple of 4)
@@ -133,9 +139,12 @@ __global__ void __launch_bounds__(256) k_pca_proj_t(const float* __restrict__ X,
             if (TF32) {
                 const float hi = tf32_rna(v);
                 static_cast<float*>(out0)[orow + j] = hi;
-                out_lo[orow + j] = tf32_rna(__fsub_rn(v, hi));
+                static_cast<float*>(out_lo)[orow + j] = tf32_rna(__fsub_rn(v, hi));
             } else {
-                static_cast<__nv_bfloat16*>(out0)[orow + j] = __float2bfloat16_rn(v);
+                const __nv_bfloat16 h = __float2bfloat16_rn(v);
+                static_cast<__nv_bfloat16*>(out0)[orow + j] = h;
+                if (out_lo)
+                    static_cast<__nv_bfloat16*>(out_lo)[orow + j] = __float2bfloat16_rn(__fsub_rn(v, __bfloat162float(h)));
             }
         }
         if (norm2) {
@@ -151,7 +160,7 @@ __global__ void __launch_bounds__(256) k_pca_proj_t(const float* __restrict__ X,
 
 template <int KPC, bool TF32>
 static cudaError_t launch_pjt(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t nt,
-                              void* out0, float* out_lo, int64_t ldk, const int32_t* tiles, const int32_t* ntiles,
+                              void* out0, void* out_lo, int64_t ldk, const int32_t* tiles, const int32_t* ntiles,
                               float* norm2, cudaStream_t s) {
     constexpr int PC = 32;
     const int ntp = (nt + 7) & ~7;
@@ -171,7 +180,7 @@ static cudaError_t launch_pjt(const float* X, int64_t ldx, int32_t C, int64_t N,
 
 template <bool TF32>
 static cudaError_t pjt_dispatch(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
-                                int32_t nt, void* out0, float* out_lo, int64_t ldk, const int32_t* tiles,
+                                int32_t nt, void* out0, void* out_lo, int64_t ldk, const int32_t* tiles,
                                 const int32_t* ntiles, float* norm2, cudaStream_t s) {
     if (norm2) {
         const cudaError_t e = cudaMemsetAsync(norm2, 0, sizeof(float) * N, s);
@@ -191,8 +200,9 @@ static cudaError_t pjt_dispatch(const float* X, int64_t ldx, int32_t C, int64_t 
 }
 
 cudaError_t launch_pca_proj_t(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
-                              int32_t nt, __nv_bfloat16* B0T, int64_t ldk, cudaStream_t s, float* norm2) {
-    return pjt_dispatch<false>(X, ldx, C, N, wpca, K, nt, B0T, nullptr, ldk, nullptr, nullptr, norm2, s);
+                              int32_t nt, __nv_bfloat16* B0T_hi, __nv_bfloat16* B0T_lo, int64_t ldk, cudaStream_t s,
+                              float* norm2) {
+    return pjt_dispatch<false>(X, ldx, C, N, wpca, K, nt, B0T_hi, B0T_lo, ldk, nullptr, nullptr, norm2, s);
 }
 
 cudaError_t launch_pca_proj_t_tf32(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
@@ -209,8 +219,8 @@ cudaError_t launch_pca_proj_t_tf32(const float* X, int64_t ldx, int32_t C, int64
 // product is the 64x64-tile FP32 GEMM with a store into that layout; every
 // output sums over c in order.
 cudaError_t launch_build_uw(const float* U, const float* Mw, int32_t T, int32_t K, int32_t C, int64_t ldk,
-                            __nv_bfloat16* out16, float* hi, float* lo, cudaStream_t s) {
-    return launch_sgemm_folded(U, Mw, T, K, C, ldk, out16, hi, lo, s);
+                            __nv_bfloat16* out16, __nv_bfloat16* out16lo, float* hi, float* lo, cudaStream_t s) {
+    return launch_sgemm_folded(U, Mw, T, K, C, ldk, out16, out16lo, hi, lo, s);
 }
 
 

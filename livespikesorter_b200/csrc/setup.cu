@@ -68,9 +68,10 @@ __global__ void k_ucc(const float* __restrict__ U, const int64_t* __restrict__ i
 }
 
 // GEMM operands U_p[t, c*K + k] = U[t, k, c]: tf32 split hi = rna(x),
-// lo = rna(x - hi) (the bit rounding lss_create uses) and bf16.
+// lo = rna(x - hi) (the bit rounding lss_create uses) and the bf16 split
+// hi = bf16(x), lo = bf16(x - hi).
 __global__ void k_up(const float* __restrict__ U, int T, int K, int C, int64_t ldk, float* __restrict__ hi,
-                     float* __restrict__ lo, __nv_bfloat16* __restrict__ b16) {
+                     float* __restrict__ lo, __nv_bfloat16* __restrict__ b16, __nv_bfloat16* __restrict__ b16lo) {
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= (int64_t)T * C * K) return;
     const int t = (int)(e / ((int64_t)C * K)), r = (int)(e % ((int64_t)C * K)), c = r / K, k = r % K;
@@ -82,7 +83,11 @@ __global__ void k_up(const float* __restrict__ U, int T, int K, int C, int64_t l
     if ((v & 0x7f800000u) != 0x7f800000u) v = (v + 0x1000u) & 0xffffe000u;
     hi[(int64_t)t * ldk + r] = xh;
     lo[(int64_t)t * ldk + r] = __uint_as_float(v);
-    if (b16) b16[(int64_t)t * ldk + r] = __float2bfloat16_rn(x);
+    if (b16) {
+        const __nv_bfloat16 hb = __float2bfloat16_rn(x);
+        b16[(int64_t)t * ldk + r] = hb;
+        b16lo[(int64_t)t * ldk + r] = __float2bfloat16_rn(__fsub_rn(x, __bfloat162float(hb)));
+    }
 }
 
 // wave[t, c, m] = sum_k U[t, k, c] wPCA[k, m] (double, k order)
@@ -270,7 +275,7 @@ int lss_set_templates(lss_handle* h, const float* U, const float* wPCA) {
     const int64_t nup = (int64_t)T * C * K;
     const bool bf16 = h->cfg.precision == LSS_PREC_BF16_RECHECK;
     k_up<<<(unsigned)((nup + 255) / 256), 256, 0, s>>>(h->U.p, T, K, C, h->CKpad, h->Up_hi.p, h->Up_lo.p,
-                                                       bf16 ? h->Up16.p : nullptr);
+                                                       bf16 ? h->Up16.p : nullptr, bf16 ? h->Up16lo.p : nullptr);
     const int64_t nw = (int64_t)T * C * nt;
     k_wave<<<(unsigned)((nw + 255) / 256), 256, 0, s>>>(h->U.p, h->wpca.p, T, K, C, nt, h->wave.p);
     const int M = T * K;

@@ -35,20 +35,26 @@ constexpr int MAX_NP = 512;           // templates per pass (TMEM columns)
 constexpr int SPLIT_W = 128;          // templates per work item in split mode
 constexpr int THREADS = 192;
 
-// Element kinds of the score GEMM.
-//  BF16 : one MMA term, 128-byte rows (64 bf16 per k-block), 128B swizzle.
+// Element kinds of the score GEMM (TcOp).
+//  BF16  : one MMA term, 128-byte rows (64 bf16 per k-block), 128B swizzle.
 //  TF32x3: FP32-class accuracy from tf32 splits x = hi + lo:
-//         D += A_hi B_hi + A_hi B_lo + A_lo B_hi, 64-byte rows (16 floats per
-//         k-block), 64B swizzle; A and B each have a hi and a lo tile.
-template <bool TF32>
+//          D += A_hi B_hi + A_hi B_lo + A_lo B_hi, 64-byte rows (16 floats per
+//          k-block), 64B swizzle; A and B each have a hi and a lo tile.
+//  BF16x3: the same three terms with bf16 splits hi = bf16(x), lo = bf16(x - hi)
+//          (about 2^-16 relative per product), 64-byte rows (32 bf16 per
+//          k-block), 64B swizzle: half the operand bytes and tensor time of
+//          TF32x3.
+template <int OP>
 struct Kind {
-    static constexpr uint32_t ROW = TF32 ? 64u : 128u;       // bytes per operand row in a stage
-    static constexpr int BKE = TF32 ? 16 : 64;               // elements per k-block
-    static constexpr int SUB = 2 * (TF32 ? 1 : 2);           // 32-byte MMA K steps per k-block
-    static constexpr int PARTS = TF32 ? 2 : 1;               // hi (+ lo) tiles per operand
-    static constexpr uint32_t A_TILE = BM * ROW;             // bytes of one A tile
-    static constexpr uint32_t ATOM = 8 * ROW;                // swizzle atom (8 rows)
-    static constexpr uint64_t LAYOUT = TF32 ? 4 : 2;         // UMMA layout: SWIZZLE_64B / SWIZZLE_128B
+    static constexpr bool SPLIT = OP != TC_BF16;                   // hi and lo tiles per operand
+    static constexpr uint32_t ROW = SPLIT ? 64u : 128u;            // bytes per operand row in a stage
+    static constexpr int BKE = OP == TC_TF32X3 ? 16 : (OP == TC_BF16X3 ? 32 : 64);  // elements per k-block
+    static constexpr int SUB = ROW / 32;                           // 32-byte MMA K steps per k-block
+    static constexpr int PARTS = SPLIT ? 2 : 1;
+    static constexpr uint32_t A_TILE = BM * ROW;                   // bytes of one A tile
+    static constexpr uint32_t ATOM = 8 * ROW;                      // swizzle atom (8 rows)
+    static constexpr uint64_t LAYOUT = SPLIT ? 4 : 2;              // UMMA layout: SWIZZLE_64B / SWIZZLE_128B
+    static constexpr uint32_t FMT = OP == TC_TF32X3 ? 2u : 1u;     // operand format: TF32 (2) or BF16 (1)
 };
 
 struct Args {
@@ -146,25 +152,25 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
 }
 
 // K-major operand with swizzled rows: 8-row atoms of ATOM bytes.
-template <bool TF32>
+template <int OP>
 __device__ __forceinline__ uint64_t operand_desc(uint32_t addr) {
-    using KD = Kind<TF32>;
+    using KD = Kind<OP>;
     return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(KD::ATOM >> 4) << 32) |
            ((uint64_t)1 << 46) | (KD::LAYOUT << 61);
 }
 
 // Instruction descriptor: F32 accumulator, BF16 (1) or TF32 (2) operands,
 // both K-major, M = 128.
-template <bool TF32>
+template <int OP>
 __device__ __forceinline__ uint32_t instr_desc(int n) {
-    const uint32_t fmt = TF32 ? 2u : 1u;
+    const uint32_t fmt = Kind<OP>::FMT;
     return (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
 }
 
-template <bool TF32>
+template <int OP>
 __device__ __forceinline__ void mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
                                     uint32_t accumulate) {
-    if constexpr (TF32) {
+    if constexpr (OP == TC_TF32X3) {
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
             "setp.ne.b32 p, %4, 0;\n\t"
@@ -230,12 +236,12 @@ struct ColMax {
     }
 };
 
-// Stage layout: [A_hi | A_lo] [B_hi rows | B_lo rows] (lo tiles only for TF32x3).
-template <bool TF32>
+// Stage layout: [A_hi | A_lo] [B_hi rows | B_lo rows] (lo tiles only for the split kinds).
+template <int OP>
 __global__ void __launch_bounds__(THREADS, 1)
     k_score_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmAlo,
                const __grid_constant__ CUtensorMap tmB, const __grid_constant__ CUtensorMap tmBlo, Args a) {
-    using KD = Kind<TF32>;
+    using KD = Kind<OP>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const uint32_t a_bytes = KD::PARTS * KD::A_TILE;
@@ -316,11 +322,11 @@ __global__ void __launch_bounds__(THREADS, 1)
                         const int kx = kb * KD::BKE;
                         mbar_expect_tx(full_bar(stage), bytes);
                         tma_load_2d(sa, &tmA, kx, tile * BM, full_bar(stage));
-                        if (TF32) tma_load_2d(sa + KD::A_TILE, &tmAlo, kx, tile * BM, full_bar(stage));
+                        if (KD::SPLIT) tma_load_2d(sa + KD::A_TILE, &tmAlo, kx, tile * BM, full_bar(stage));
                         for (int bx = 0; bx < nbox; ++bx) {
                             const int row = p * PW + bx * a.box_rows;
                             tma_load_2d(sb + bx * a.box_rows * KD::ROW, &tmB, kx, row, full_bar(stage));
-                            if (TF32) tma_load_2d(sb + b_part + bx * a.box_rows * KD::ROW, &tmBlo, kx, row, full_bar(stage));
+                            if (KD::SPLIT) tma_load_2d(sb + b_part + bx * a.box_rows * KD::ROW, &tmBlo, kx, row, full_bar(stage));
                         }
                         last_ph[stage] = ph;
                         pending[stage] = true;
@@ -357,20 +363,20 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
                         for (int ks = 0; ks < KD::SUB; ++ks) {
                             const uint32_t ko = ks * 32;
-                            const uint64_t ad = operand_desc<TF32>(sa + ko);
+                            const uint64_t ad = operand_desc<OP>(sa + ko);
                             for (int c = 0; c < np; c += 256) {
                                 const int n = min(256, np - c);
-                                const uint32_t idesc = instr_desc<TF32>(n);
-                                const uint64_t bd = operand_desc<TF32>(sb + (uint32_t)c * KD::ROW + ko);
+                                const uint32_t idesc = instr_desc<OP>(n);
+                                const uint64_t bd = operand_desc<OP>(sb + (uint32_t)c * KD::ROW + ko);
                                 const uint32_t acc_on = (kb | ks) != 0;
-                                if (TF32) {
-                                    const uint64_t adl = operand_desc<TF32>(sa + KD::A_TILE + ko);
-                                    const uint64_t bdl = operand_desc<TF32>(sb + b_part + (uint32_t)c * KD::ROW + ko);
-                                    mma<TF32>(dcol + (uint32_t)c, adl, bd, idesc, acc_on);   // A_lo B_hi
-                                    mma<TF32>(dcol + (uint32_t)c, ad, bdl, idesc, 1u);      // A_hi B_lo
-                                    mma<TF32>(dcol + (uint32_t)c, ad, bd, idesc, 1u);       // A_hi B_hi
+                                if (KD::SPLIT) {
+                                    const uint64_t adl = operand_desc<OP>(sa + KD::A_TILE + ko);
+                                    const uint64_t bdl = operand_desc<OP>(sb + b_part + (uint32_t)c * KD::ROW + ko);
+                                    mma<OP>(dcol + (uint32_t)c, adl, bd, idesc, acc_on);   // A_lo B_hi
+                                    mma<OP>(dcol + (uint32_t)c, ad, bdl, idesc, 1u);      // A_hi B_lo
+                                    mma<OP>(dcol + (uint32_t)c, ad, bd, idesc, 1u);       // A_hi B_hi
                                 } else {
-                                    mma<TF32>(dcol + (uint32_t)c, ad, bd, idesc, acc_on);
+                                    mma<OP>(dcol + (uint32_t)c, ad, bd, idesc, acc_on);
                                 }
                             }
                         }
@@ -518,27 +524,29 @@ static PFN_encodeTiled get_encode() {
     return fn;
 }
 
-// 2-D tensor [rows, cols] (cols contiguous, row pitch in elements) of bf16 or
-// fp32, box [box_rows, one swizzled row] with 128B (bf16) or 64B (fp32) swizzle.
+// 2-D tensor [rows, cols] (cols contiguous, row pitch in elements) of the
+// kind's element type, box [box_rows, one swizzled row]: 128 B rows with 128B
+// swizzle (BF16) or 64 B rows with 64B swizzle (TF32x3, BF16x3).
 static bool make_map(CUtensorMap* m, const void* base, int64_t rows, int64_t cols, int64_t pitch, int box_rows,
-                     bool f32) {
+                     int op) {
     PFN_encodeTiled enc = get_encode();
     if (!enc) return false;
+    const bool f32 = op == TC_TF32X3;
     const int64_t esz = f32 ? 4 : 2;
     if ((reinterpret_cast<uintptr_t>(base) & 15) || ((pitch * esz) & 15) || box_rows < 8 || box_rows > 256 ||
         (box_rows & 7))
         return false;
     cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
     cuuint64_t strides[1] = {(cuuint64_t)(pitch * esz)};
-    cuuint32_t box[2] = {f32 ? 16u : 64u, (cuuint32_t)box_rows};
+    cuuint32_t box[2] = {(cuuint32_t)(op == TC_BF16 ? 64 : 64 / esz), (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1u, 1u};
     return enc(m, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base),
                dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-               f32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+               op == TC_BF16 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-TcPlan tc_plan(int T, bool tf32, int pass_w) {
+TcPlan tc_plan(int T, int op, int pass_w) {
     TcPlan p{};
     p.Tpad = (T + 15) / 16 * 16;
     p.pass_w = std::min(pass_w, tc::MAX_NP);
@@ -550,18 +558,18 @@ TcPlan tc_plan(int T, bool tf32, int pass_w) {
         b_rows = std::max(b_rows, (np + p.box_rows - 1) / p.box_rows * p.box_rows);
     }
     p.b_rows = b_rows;
-    const size_t row = tf32 ? 64 : 128, parts = tf32 ? 2 : 1;
+    const size_t row = op == TC_BF16 ? 128 : 64, parts = op == TC_BF16 ? 1 : 2;
     const size_t stage = parts * (tc::BM * row + (size_t)b_rows * row);
     const size_t tail = 8 * (2 * 4 + 5) + 16 + 12 * (size_t)p.Tpad;
     const size_t budget = 227 * 1024 - 1024 - tail;
     p.stages = (int)std::min<size_t>(4, budget / stage);
     p.nacc = (np0 <= 256) ? 2 : 1;
     p.smem = 1024 + (size_t)p.stages * stage + 8 * (2 * p.stages + 5) + 16 + 12 * (size_t)p.Tpad;
-    p.kblock = tf32 ? 16 : 64;
+    p.kblock = op == TC_TF32X3 ? 16 : (op == TC_BF16X3 ? 32 : 64);
     return p;
 }
 
-template <bool TF32>
+template <int OP>
 static cudaError_t launch_tc(const void* A, const void* Alo, int64_t ldk, int N, const void* Bm, const void* Blo, int T,
                              int CKpad, const float* nm, float* Bout, int64_t ldb, float* cfmax, int32_t* imax, int nt,
                              int32_t* status, int grid, cudaStream_t s, const TcExtra& ex) {
@@ -570,14 +578,14 @@ static cudaError_t launch_tc(const void* A, const void* Alo, int64_t ldk, int N,
     // column maxima are then combined through 64-bit keys.
     const int ntiles = (N + tc::BM - 1) / tc::BM;
     const bool split = ex.keys && !ex.cf2 && !ex.rowmap && 2 * ntiles < grid && T > tc::SPLIT_W;
-    const TcPlan p = tc_plan(T, TF32, split ? tc::SPLIT_W : tc::MAX_NP);
+    const TcPlan p = tc_plan(T, OP, split ? tc::SPLIT_W : tc::MAX_NP);
     if (p.stages < 2 || CKpad % p.kblock) return cudaErrorInvalidValue;
     CUtensorMap ma, malo, mb, mblo;
-    if (!make_map(&ma, A, N, CKpad, ldk, tc::BM, TF32) || !make_map(&mb, Bm, p.Tpad, CKpad, CKpad, p.box_rows, TF32))
+    if (!make_map(&ma, A, N, CKpad, ldk, tc::BM, OP) || !make_map(&mb, Bm, p.Tpad, CKpad, CKpad, p.box_rows, OP))
         return cudaErrorInvalidValue;
-    if (TF32) {
-        if (!make_map(&malo, Alo, N, CKpad, ldk, tc::BM, true) ||
-            !make_map(&mblo, Blo, p.Tpad, CKpad, CKpad, p.box_rows, true))
+    if (tc::Kind<OP>::SPLIT) {
+        if (!make_map(&malo, Alo, N, CKpad, ldk, tc::BM, OP) ||
+            !make_map(&mblo, Blo, p.Tpad, CKpad, CKpad, p.box_rows, OP))
             return cudaErrorInvalidValue;
     } else {
         malo = ma;
@@ -612,14 +620,14 @@ static cudaError_t launch_tc(const void* A, const void* Alo, int64_t ldk, int N,
     a.cf_lo = ex.cf_lo;
     a.cf_hi = ex.cf_hi;
     if (a.un && (!a.pn2 || !a.cf2 || !a.cf_lo || !a.cf_hi || ex.rowmap)) return cudaErrorInvalidValue;
-    cudaError_t e = cudaFuncSetAttribute(tc::k_score_tc<TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
+    cudaError_t e = cudaFuncSetAttribute(tc::k_score_tc<OP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
     if (e != cudaSuccess) return e;
     const int items = split ? ntiles * ((p.Tpad + p.pass_w - 1) / p.pass_w) : ntiles;
     if (split) {
         e = cudaMemsetAsync(ex.keys, 0, (size_t)N * sizeof(unsigned long long), s);
         if (e != cudaSuccess) return e;
     }
-    tc::k_score_tc<TF32><<<std::min(grid, items), tc::THREADS, p.smem, s>>>(ma, malo, mb, mblo, a);
+    tc::k_score_tc<OP><<<std::min(grid, items), tc::THREADS, p.smem, s>>>(ma, malo, mb, mblo, a);
     if (split) tc::k_keys_to_maxima<<<(N + 255) / 256, 256, 0, s>>>(ex.keys, N, cfmax, imax);
     return cudaGetLastError();
 }
@@ -627,16 +635,24 @@ static cudaError_t launch_tc(const void* A, const void* Alo, int64_t ldk, int N,
 cudaError_t launch_score_tc(const __nv_bfloat16* B0T, int64_t ldk, int N, const __nv_bfloat16* Up, int T, int CKpad,
                             const float* nm, float* Bout, int64_t ldb, float* cfmax, int32_t* imax, int nt,
                             int32_t* status, int grid, cudaStream_t s, const TcExtra& ex) {
-    return launch_tc<false>(B0T, nullptr, ldk, N, Up, nullptr, T, CKpad, nm, Bout, ldb, cfmax, imax, nt, status, grid, s,
-                            ex);
+    return launch_tc<TC_BF16>(B0T, nullptr, ldk, N, Up, nullptr, T, CKpad, nm, Bout, ldb, cfmax, imax, nt, status, grid,
+                              s, ex);
+}
+
+cudaError_t launch_score_tc_bf16x3(const __nv_bfloat16* B0T_hi, const __nv_bfloat16* B0T_lo, int64_t ldk, int N,
+                                   const __nv_bfloat16* Up_hi, const __nv_bfloat16* Up_lo, int T, int CKpad,
+                                   const float* nm, float* Bout, int64_t ldb, float* cfmax, int32_t* imax, int nt,
+                                   int32_t* status, int grid, cudaStream_t s, const TcExtra& ex) {
+    return launch_tc<TC_BF16X3>(B0T_hi, B0T_lo, ldk, N, Up_hi, Up_lo, T, CKpad, nm, Bout, ldb, cfmax, imax, nt, status,
+                                grid, s, ex);
 }
 
 cudaError_t launch_score_tc_tf32x3(const float* B0T_hi, const float* B0T_lo, int64_t ldk, int N, const float* Up_hi,
                                    const float* Up_lo, int T, int CKpad, const float* nm, float* Bout, int64_t ldb,
                                    float* cfmax, int32_t* imax, int nt, int32_t* status, int grid, cudaStream_t s,
                                    const TcExtra& ex) {
-    return launch_tc<true>(B0T_hi, B0T_lo, ldk, N, Up_hi, Up_lo, T, CKpad, nm, Bout, ldb, cfmax, imax, nt, status, grid,
-                           s, ex);
+    return launch_tc<TC_TF32X3>(B0T_hi, B0T_lo, ldk, N, Up_hi, Up_lo, T, CKpad, nm, Bout, ldb, cfmax, imax, nt, status,
+                                grid, s, ex);
 }
 
 }  // namespace lss

@@ -333,6 +333,11 @@ class Sorter:
         """Forget the last kept time per cluster (a new stream)."""
         self._check(self._lib.lss_reset_postprocess(self._h))
 
+    def set_round_kernel(self, skip_blocks: bool):
+        """Rounds kernel: skip provably unchanged template-row blocks (True) or
+        update every row (False, the default); the results are identical."""
+        self._check(self._lib.lss_set_round_kernel(self._h, int(bool(skip_blocks))))
+
     def set_profiling(self, on: bool = True):
         self._check(self._lib.lss_set_profiling(self._h, int(on)))
 

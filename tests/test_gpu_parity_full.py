@@ -148,8 +148,9 @@ def _check_batches(T, dup, seed):
 @pytest.mark.parametrize('T, dup', [(400, False), (800, True)])
 def test_rounds_bit_exact_on_given_scores_at_384ch(T, dup):
     """The rounds alone on the oracle's own score field of a 384-channel batch:
-    spikes and amplitudes bit-identical to the oracle's run_matching, with most
-    template-row blocks skipped as exact no-ops."""
+    spikes and amplitudes bit-identical to the oracle's run_matching with both
+    rounds kernels (every row updated; provably unchanged template-row blocks
+    skipped, where most blocks are skipped)."""
     from livespikesorter_b200 import synth
     from livespikesorter_b200.sorter import Sorter
     setup, rec = synth.config(2 if dup else 1, duration_s=4.0, seed=47, T=T)
@@ -161,10 +162,12 @@ def test_rounds_bit_exact_on_given_scores_at_384ch(T, dup):
     nm = (setup.U ** 2).sum(-1).sum(-1)
     st_o, amps_o, _ = ko.run_matching(X, setup.U, setup.ctc, setup.wPCA, setup.Th, nt, B=B, nm=nm)
     s = Sorter.from_setup(setup, nm=nm)
-    st, amps = s.match_scores(B.cuda())
     assert len(st_o) > 5000
-    assert torch.equal(st.cpu(), st_o)
-    assert torch.equal(amps.cpu(), amps_o)
+    for skip in (False, True):
+        s.set_round_kernel(skip)
+        st, amps = s.match_scores(B.cuda())
+        assert torch.equal(st.cpu(), st_o), skip
+        assert torch.equal(amps.cpu(), amps_o), skip
     stats = s.stats()
     assert 0 < stats['mp_items_updated'] < 0.6 * stats['mp_items'], stats
 

@@ -1,6 +1,9 @@
 """FP32 re-check of the BF16 score path.
 
-Every BF16 score is within 2^-7 ||U_t|| ||P_s|| of the FP32 path's. From that
+The BF16 path splits both GEMM operands into bf16 parts (hi = bf16(x),
+lo = bf16(x - hi)) and accumulates three bf16 MMAs in FP32; its scores are
+within about 2^-11 ||U_t|| ||P_s|| of the FP32 path's (the tests check the
+looser 2^-7). From that
 bound the BF16 GEMM gives each column an interval for the FP32 path's best Cf
 and an upper bound for every other template; columns whose first-round
 decisions the intervals leave open (threshold, best template, or the max-pool
