@@ -327,43 +327,50 @@ cudaError_t launch_recheck_select(const float* cf_lo, const float* cf_hi, const 
 // FP32 projection of the listed columns (tf32 split), with k_pca_proj_t's
 // arithmetic: every output sums its (zero-padded) taps in ascending order with
 // one fmaf each, so the rows equal the FP32 path's. Column cols[i] goes to row
-// i (scatter = 0) or to row cols[i] (scatter = 1: a batch-sized array).
+// i (scatter = 0) or to row cols[i] (scatter = 1: a batch-sized array). A CTA
+// takes a column at a time and stages its window of PCOL_CH channels x ntp
+// samples in shared memory with coalesced loads before the dot products.
+constexpr int PCOL_CH = 64;
 template <int KPC>
-__global__ void __launch_bounds__(128) k_pca_proj_cols(const float* __restrict__ X, int64_t ldx, int32_t C, int64_t N,
+__global__ void __launch_bounds__(256) k_pca_proj_cols(const float* __restrict__ X, int64_t ldx, int32_t C, int64_t N,
                                                        const float* __restrict__ wpca, int32_t nt, int32_t ntp,
                                                        const int32_t* __restrict__ cols,
                                                        const int32_t* __restrict__ count, float* __restrict__ hi,
                                                        float* __restrict__ lo, int64_t ldk, int32_t scatter) {
-    extern __shared__ float ws[];  // [KPC][ntp]
+    extern __shared__ float sm[];
+    float* ws = sm;                   // [KPC][ntp]
+    float* xs = sm + KPC * ntp;       // [PCOL_CH][ntp + 1]
+    const int xw = ntp + 1;
     for (int e = threadIdx.x; e < KPC * ntp; e += blockDim.x) {
         const int k = e / ntp, m = e % ntp;
         ws[e] = (m < nt) ? wpca[k * nt + m] : 0.f;
     }
-    __syncthreads();
     const int n = *count;
     const int half = nt / 2;
     for (int i = blockIdx.x; i < n; i += gridDim.x) {
-    const int64_t s = cols[i];
-    const int64_t row = scatter ? s : (int64_t)i;
-    for (int c = threadIdx.x; c < C; c += blockDim.x) {
-        const float* xr = X + (int64_t)c * ldx;
-        float acc[KPC];
-#pragma unroll
-        for (int k = 0; k < KPC; ++k) acc[k] = 0.f;
-        for (int m = 0; m < ntp; ++m) {
-            const int64_t g = s - half + m;
-            const float xv = (g >= 0 && g < N) ? xr[g] : 0.f;
-#pragma unroll
-            for (int k = 0; k < KPC; ++k) acc[k] = fmaf(ws[k * ntp + m], xv, acc[k]);
+        const int64_t s = cols[i];
+        const int64_t row = scatter ? s : (int64_t)i;
+        for (int c0 = 0; c0 < C; c0 += PCOL_CH) {
+            const int nc = min(PCOL_CH, C - c0);
+            __syncthreads();
+            for (int e = threadIdx.x; e < nc * ntp; e += blockDim.x) {
+                const int c = e / ntp, m = e % ntp;
+                const int64_t g = s - half + m;
+                xs[c * xw + m] = (g >= 0 && g < N) ? X[(int64_t)(c0 + c) * ldx + g] : 0.f;
+            }
+            __syncthreads();
+            for (int e = threadIdx.x; e < nc * KPC; e += blockDim.x) {
+                const int c = e / KPC, k = e % KPC;
+                const float* xr = xs + c * xw;
+                const float* wk = ws + k * ntp;
+                float acc = 0.f;
+                for (int m = 0; m < ntp; ++m) acc = fmaf(wk[m], xr[m], acc);
+                const int64_t o = row * ldk + (int64_t)(c0 + c) * KPC + k;
+                const float h = tf32_rna(acc);
+                hi[o] = h;
+                lo[o] = tf32_rna(__fsub_rn(acc, h));
+            }
         }
-        const int64_t o = row * ldk + (int64_t)c * KPC;
-#pragma unroll
-        for (int k = 0; k < KPC; ++k) {
-            const float h = tf32_rna(acc[k]);
-            hi[o + k] = h;
-            lo[o + k] = tf32_rna(__fsub_rn(acc[k], h));
-        }
-    }
     }
 }
 
@@ -372,13 +379,13 @@ static cudaError_t launch_cols(const float* X, int64_t ldx, int32_t C, int64_t N
                                const int32_t* cols, const int32_t* count, int32_t max_cols, float* hi, float* lo,
                                int64_t ldk, int32_t scatter, cudaStream_t s) {
     const int ntp = (nt + 7) & ~7;
-    const size_t smem = sizeof(float) * KPC * ntp;
+    const size_t smem = sizeof(float) * ((size_t)KPC * ntp + (size_t)PCOL_CH * (ntp + 1));
     if (smem > 48 * 1024) return cudaErrorInvalidValue;
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int grid = std::max(1, std::min(max_cols, 16 * sms));
-    k_pca_proj_cols<KPC><<<grid, 128, smem, s>>>(X, ldx, C, N, wpca, nt, ntp, cols, count, hi, lo, ldk, scatter);
+    const int grid = std::max(1, std::min(max_cols, 8 * sms));
+    k_pca_proj_cols<KPC><<<grid, 256, smem, s>>>(X, ldx, C, N, wpca, nt, ntp, cols, count, hi, lo, ldk, scatter);
     return cudaGetLastError();
 }
 

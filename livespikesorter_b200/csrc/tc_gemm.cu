@@ -578,7 +578,13 @@ static cudaError_t launch_tc(const void* A, const void* Alo, int64_t ldk, int N,
     // column maxima are then combined through 64-bit keys.
     const int ntiles = (N + tc::BM - 1) / tc::BM;
     const bool split = ex.keys && !ex.cf2 && !ex.rowmap && 2 * ntiles < grid && T > tc::SPLIT_W;
-    const TcPlan p = tc_plan(T, OP, split ? tc::SPLIT_W : tc::MAX_NP);
+    // templates in passes of at most 256 TMEM columns (equal widths): two
+    // accumulators alternate, so one pass's epilogue drains while the next
+    // pass's MMAs run, and the smaller stages leave room for four of them
+    const int tpad = (T + 15) / 16 * 16;
+    const int npass = (tpad + 255) / 256;
+    const int even_w = ((tpad + npass - 1) / npass + 15) / 16 * 16;
+    const TcPlan p = tc_plan(T, OP, split ? tc::SPLIT_W : even_w);
     if (p.stages < 2 || CKpad % p.kblock) return cudaErrorInvalidValue;
     CUtensorMap ma, malo, mb, mblo;
     if (!make_map(&ma, A, N, CKpad, ldk, tc::BM, OP) || !make_map(&mb, Bm, p.Tpad, CKpad, CKpad, p.box_rows, OP))
