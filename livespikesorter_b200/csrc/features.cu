@@ -15,6 +15,11 @@
 
 namespace lss {
 
+// projection-row element as float: the FP32 path's tf32 parts or the BF16
+// path's bf16 parts (hi + lo is the projection to 2^-23 or 2^-17 relative)
+__device__ __forceinline__ float pval(const float* p) { return *p; }
+__device__ __forceinline__ float pval(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+
 constexpr int XR_COLS = 128;
 constexpr int XR_CH = 32;
 constexpr int XR_LIST_MAX = 1024;
@@ -232,13 +237,14 @@ constexpr int FT_CH = 64;
 constexpr int FT_LIST = 512;
 constexpr int FT_NQ = 32;  // neighbours per staged chunk
 
+template <typename PT>
 __device__ __forceinline__ void pc_features_one(
     int i, int rounds, const float* __restrict__ Xh, int64_t ldx, int32_t C, int32_t nt, int32_t K, int32_t nC,
     int32_t T, const float* __restrict__ wpca, const float* __restrict__ Mw, const float* __restrict__ U,
     const float* __restrict__ R, const int64_t* __restrict__ iCC, const int64_t* __restrict__ iU,
     const float* __restrict__ Ucc, const int32_t* __restrict__ sp_x, const int32_t* __restrict__ sp_y,
     const float* __restrict__ sp_amp, const int32_t* __restrict__ round_start, float* __restrict__ tF,
-    int32_t* status, const float* __restrict__ Phi, const float* __restrict__ Plo, int64_t ldp) {
+    int32_t* status, const PT* __restrict__ Phi, const PT* __restrict__ Plo, int64_t ldp) {
     extern __shared__ float sm[];
     const int ntp = nt + 1;
     float* ws = sm;                          // [K][nt]
@@ -315,7 +321,7 @@ __device__ __forceinline__ void pc_features_one(
         float* red = mwr + nC * C;         // [4*nC*K]
         __syncthreads();
         const int64_t o = (int64_t)x * ldp;
-        for (int e = threadIdx.x; e < C * K; e += blockDim.x) prow[e] = __fadd_rn(Phi[o + e], Plo[o + e]);
+        for (int e = threadIdx.x; e < C * K; e += blockDim.x) prow[e] = __fadd_rn(pval(Phi + o + e), pval(Plo + o + e));
         for (int e = threadIdx.x; e < nC * C; e += blockDim.x) {
             const int j = e / C, c = e % C;
             mwr[e] = Mw[(int64_t)s_ch[j] * C + c];
@@ -338,7 +344,7 @@ __device__ __forceinline__ void pc_features_one(
         if (Phi) {
             // projection row of the score GEMM: P[x, c*K + k] = hi + lo (to 2^-23 relative)
             const int64_t o = (int64_t)x * ldp + (int64_t)c0 * K;
-            for (int e = threadIdx.x; e < nc * K; e += blockDim.x) pc[e] = __fadd_rn(Phi[o + e], Plo[o + e]);
+            for (int e = threadIdx.x; e < nc * K; e += blockDim.x) pc[e] = __fadd_rn(pval(Phi + o + e), pval(Plo + o + e));
         } else {
             for (int e = threadIdx.x; e < nc * nt; e += blockDim.x) {
                 const int c = e / nt, m = e % nt;
@@ -408,14 +414,14 @@ __device__ __forceinline__ void pc_features_one(
 // partial sums are combined by a butterfly, then each lane owns one or two
 // features for the neighbour corrections (list order) and the amp * Ucc term.
 constexpr int FW_LIST = 256;  // neighbours per spike (all rounds, within +-nt)
-template <int KPC, int NCC>
+template <int KPC, int NCC, typename PT>
 __global__ void __launch_bounds__(256, 2) k_pc_features_warp(
     int32_t C, int32_t nt, int32_t T, const float* __restrict__ Mw, const float* __restrict__ U,
     const float* __restrict__ R, const int64_t* __restrict__ iCC, const int64_t* __restrict__ iU,
     const float* __restrict__ Ucc, const int32_t* __restrict__ sp_x, const int32_t* __restrict__ sp_y,
     const float* __restrict__ sp_amp, const int32_t* __restrict__ round_start, int32_t rounds, int32_t n,
-    const int32_t* __restrict__ counters, float* __restrict__ tF, int32_t* status, const float* __restrict__ Phi,
-    const float* __restrict__ Plo, int64_t ldp) {
+    const int32_t* __restrict__ counters, float* __restrict__ tF, int32_t* status, const PT* __restrict__ Phi,
+    const PT* __restrict__ Plo, int64_t ldp) {
     constexpr int F = NCC * KPC;
     __shared__ int s_lx[8][FW_LIST], s_ly[8][FW_LIST];
     __shared__ float s_la[8][FW_LIST];
@@ -443,7 +449,7 @@ __global__ void __launch_bounds__(256, 2) k_pc_features_warp(
         for (int c = lane; c < C; c += 32) {
             float pv[KPC];
 #pragma unroll
-            for (int k = 0; k < KPC; ++k) pv[k] = __fadd_rn(Phi[o + c * KPC + k], Plo[o + c * KPC + k]);
+            for (int k = 0; k < KPC; ++k) pv[k] = __fadd_rn(pval(Phi + o + c * KPC + k), pval(Plo + o + c * KPC + k));
 #pragma unroll
             for (int j = 0; j < NCC; ++j) {
                 const float mv = __ldg(Mw + (int64_t)ch[j] * C + c);
@@ -534,14 +540,15 @@ __global__ void __launch_bounds__(256, 2) k_pc_features_warp(
 // CTA per spike, grid-stride over the spikes; with counters != null the spike
 // and round counts are read from the matching pursuit's device counters
 // (graph-captured batches, whose launch does not know them).
+template <typename PT>
 __global__ void __launch_bounds__(256) k_pc_features_folded(
     const float* __restrict__ Xh, int64_t ldx, int32_t C, int32_t nt, int32_t K, int32_t nC, int32_t T,
     const float* __restrict__ wpca, const float* __restrict__ Mw, const float* __restrict__ U,
     const float* __restrict__ R, const int64_t* __restrict__ iCC, const int64_t* __restrict__ iU,
     const float* __restrict__ Ucc, const int32_t* __restrict__ sp_x, const int32_t* __restrict__ sp_y,
     const float* __restrict__ sp_amp, const int32_t* __restrict__ round_start, int32_t rounds, int32_t n,
-    const int32_t* __restrict__ counters, float* __restrict__ tF, int32_t* status, const float* __restrict__ Phi,
-    const float* __restrict__ Plo, int64_t ldp) {
+    const int32_t* __restrict__ counters, float* __restrict__ tF, int32_t* status, const PT* __restrict__ Phi,
+    const PT* __restrict__ Plo, int64_t ldp) {
     if (counters) {
         n = counters[0];
         rounds = counters[1];
@@ -553,19 +560,20 @@ __global__ void __launch_bounds__(256) k_pc_features_folded(
     }
 }
 
-cudaError_t launch_pc_features_folded(const float* Xh, int64_t ldx, int32_t C, int32_t nt, int32_t K, int32_t nC,
-                                      int32_t T, const float* wpca, const float* Mw, const float* U, const float* R,
-                                      const int64_t* iCC, const int64_t* iU, const float* Ucc, const int32_t* sp_x,
-                                      const int32_t* sp_y, const float* sp_amp, const int32_t* round_start,
-                                      int32_t rounds, int32_t n, const int32_t* counters, float* tF,
-                                      int32_t* status, const float* Phi, const float* Plo, int64_t ldp,
-                                      cudaStream_t s) {
+template <typename PT>
+static cudaError_t launch_pcf(const float* Xh, int64_t ldx, int32_t C, int32_t nt, int32_t K, int32_t nC, int32_t T,
+                              const float* wpca, const float* Mw, const float* U, const float* R, const int64_t* iCC,
+                              const int64_t* iU, const float* Ucc, const int32_t* sp_x, const int32_t* sp_y,
+                              const float* sp_amp, const int32_t* round_start, int32_t rounds, int32_t n,
+                              const int32_t* counters, float* tF, int32_t* status, const PT* Phi, const PT* Plo,
+                              int64_t ldp, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
     if (Phi && K == 6 && nC == 10) {
         // warp per spike; n: the spike count or (counters) the grid bound in spikes
         const int grid = (n + 7) / 8;
-        k_pc_features_warp<6, 10><<<grid, 256, 0, s>>>(C, nt, T, Mw, U, R, iCC, iU, Ucc, sp_x, sp_y, sp_amp,
-                                                       round_start, rounds, n, counters, tF, status, Phi, Plo, ldp);
+        k_pc_features_warp<6, 10, PT><<<grid, 256, 0, s>>>(C, nt, T, Mw, U, R, iCC, iU, Ucc, sp_x, sp_y, sp_amp,
+                                                           round_start, rounds, n, counters, tF, status, Phi, Plo,
+                                                           ldp);
         return cudaGetLastError();
     }
     if (nC * K > 256) return cudaErrorInvalidValue;  // one (j, k) per thread
@@ -574,11 +582,29 @@ cudaError_t launch_pc_features_folded(const float* Xh, int64_t ldx, int32_t C, i
                                           (size_t)C * K + (size_t)nC * C + 4 * (size_t)nC * K);
     const size_t smem = sizeof(float) * (front + (size_t)nC * K + (size_t)FT_NQ * nC * K);
     if (smem > 48 * 1024)
-        cudaFuncSetAttribute(k_pc_features_folded, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_pc_features_folded<PT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     // n: the spike count, or (counters != null) the grid size
-    k_pc_features_folded<<<n, 256, smem, s>>>(Xh, ldx, C, nt, K, nC, T, wpca, Mw, U, R, iCC, iU, Ucc, sp_x, sp_y,
-                                              sp_amp, round_start, rounds, n, counters, tF, status, Phi, Plo, ldp);
+    k_pc_features_folded<PT><<<n, 256, smem, s>>>(Xh, ldx, C, nt, K, nC, T, wpca, Mw, U, R, iCC, iU, Ucc, sp_x,
+                                                  sp_y, sp_amp, round_start, rounds, n, counters, tF, status, Phi, Plo,
+                                                  ldp);
     return cudaGetLastError();
+}
+
+cudaError_t launch_pc_features_folded(const float* Xh, int64_t ldx, int32_t C, int32_t nt, int32_t K, int32_t nC,
+                                      int32_t T, const float* wpca, const float* Mw, const float* U, const float* R,
+                                      const int64_t* iCC, const int64_t* iU, const float* Ucc, const int32_t* sp_x,
+                                      const int32_t* sp_y, const float* sp_amp, const int32_t* round_start,
+                                      int32_t rounds, int32_t n, const int32_t* counters, float* tF,
+                                      int32_t* status, const void* Phi, const void* Plo, int32_t p_bf16, int64_t ldp,
+                                      cudaStream_t s) {
+    if (p_bf16)
+        return launch_pcf<__nv_bfloat16>(Xh, ldx, C, nt, K, nC, T, wpca, Mw, U, R, iCC, iU, Ucc, sp_x, sp_y, sp_amp,
+                                         round_start, rounds, n, counters, tF, status,
+                                         static_cast<const __nv_bfloat16*>(Phi),
+                                         static_cast<const __nv_bfloat16*>(Plo), ldp, s);
+    return launch_pcf<float>(Xh, ldx, C, nt, K, nC, T, wpca, Mw, U, R, iCC, iU, Ucc, sp_x, sp_y, sp_amp, round_start,
+                             rounds, n, counters, tF, status, static_cast<const float*>(Phi),
+                             static_cast<const float*>(Plo), ldp, s);
 }
 
 // acc |= *st (errors of asynchronous batches, collected until lss_sync)

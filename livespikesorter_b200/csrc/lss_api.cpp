@@ -398,11 +398,10 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
             g_create_err = "event creation failed";
             return LSS_ERR_CUDA;
         }
+    } else {
+        ALLOC(B0T_hi, (size_t)h->N * h->CKpad);
+        ALLOC(B0T_lo, (size_t)h->N * h->CKpad);
     }
-    // FP32 projection rows: the FP32 path's GEMM operand; the BF16 path keeps
-    // the rows of its spikes' columns there for the PC features
-    ALLOC(B0T_hi, (size_t)h->N * h->CKpad);
-    ALLOC(B0T_lo, (size_t)h->N * h->CKpad);
     // tf32 template splits: the FP32 path's scores, and the BF16 path's re-check
     const int Tpad32 = tc_plan(T, TC_TF32X3).Tpad;
     ALLOC(Up_hi, (size_t)Tpad32 * h->CKpad);
@@ -507,8 +506,10 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
             }
         CK(cudaMemcpy(h->Up_hi.p, hi.data(), hi.size() * sizeof(float), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(h->Up_lo.p, lo.data(), lo.size() * sizeof(float), cudaMemcpyHostToDevice));
-        CK(cudaMemset(h->B0T_hi.p, 0, (size_t)h->N * h->CKpad * sizeof(float)));
-        CK(cudaMemset(h->B0T_lo.p, 0, (size_t)h->N * h->CKpad * sizeof(float)));
+        if (!bf16) {
+            CK(cudaMemset(h->B0T_hi.p, 0, (size_t)h->N * h->CKpad * sizeof(float)));
+            CK(cudaMemset(h->B0T_lo.p, 0, (size_t)h->N * h->CKpad * sizeof(float)));
+        }
     }
     CK(cudaMemcpy(h->nm.p, nmv.data(), T * sizeof(float), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->wave.p, wave.data(), wave.size() * sizeof(float), cudaMemcpyHostToDevice));
@@ -1145,17 +1146,14 @@ static int sort_batch_impl(lss_handle* h, const int16_t* raw, int64_t n_rows, in
     const int32_t n_bound = h->cfg.max_spikes;
     h->mark(8, s);
     if (need_tf) {
-        if (bf16) {
-            // FP32 projection rows of the spikes' columns, as the FP32 path has them
-            CK(launch_pca_proj_cols_tf32(Xh, h->ld, h->C, h->N, h->wpca.p, h->K, h->nt, h->sp_x.p, h->counters.p,
-                                         n_bound, h->B0T_hi.p, h->B0T_lo.p, h->CKpad, 1, s));
-            h->stats.launches += 1;
-        }
+        // the projection rows of the score GEMM: tf32 parts (FP32 path) or bf16 parts (BF16 path)
         const int grid = std::min(n_bound, 16 * h->sm_count);
         CK(launch_pc_features_folded(Xh, h->ld, h->C, h->nt, h->K, h->nC, h->T, h->wpca.p, h->Mw.p, h->U.p, h->R.p,
                                      h->iCC.p, h->iU.p, h->Ucc.p, h->sp_x.p, h->sp_y.p, h->sp_amp.p,
-                                     h->round_start.p, 0, grid, h->counters.p, h->tF.p, h->status.p, h->B0T_hi.p,
-                                     h->B0T_lo.p, h->CKpad, s));
+                                     h->round_start.p, 0, grid, h->counters.p, h->tF.p, h->status.p,
+                                     bf16 ? (const void*)h->B0T.p : (const void*)h->B0T_hi.p,
+                                     bf16 ? (const void*)h->B0T16lo.p : (const void*)h->B0T_lo.p, bf16 ? 1 : 0,
+                                     h->CKpad, s));
         h->stats.launches += 1;
     }
     h->mark(9, s);

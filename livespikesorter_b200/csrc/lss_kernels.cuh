@@ -154,7 +154,6 @@ struct MPArgs {
     unsigned int* bar;        // [2] grid barrier count / generation, zero at launch
     int32_t cols_per_blk;     // W
     int32_t init_cols;        // 1: compute column maxima of B before round 0
-    int32_t ring_stages = 0;  // mp.cu: stages of 8 rows in each warp's shared-memory copy ring (set by launch_mp)
     // block-skipping rounds (mp_blocks.cu) only: template rows are grouped in
     // blocks of MPB_ROWS (rows of templates close on the probe, by perm)
     const int32_t* perm = nullptr;          // [nb * MPB_ROWS] template of each block row, -1 past T
@@ -235,13 +234,14 @@ cudaError_t launch_records(const int32_t* sp_x, const int32_t* sp_y, const float
                            int32_t* out_tmpl, float* out_amp, float* out_pc, int64_t capacity, int64_t* out_count,
                            cudaStream_t s);
 // PC features from the highpassed batch (or, when Phi is given, the projection rows
-// P = Phi + Plo [N, ldp] of the score GEMM) and the folded whitening (no residual array)
+// P = Phi + Plo [N, ldp] of the score GEMM: fp32 tf32 parts, or bf16 parts when
+// p_bf16) and the folded whitening (no residual array)
 cudaError_t launch_pc_features_folded(const float* Xh, int64_t ldx, int32_t C, int32_t nt, int32_t K, int32_t nC,
                                       int32_t T, const float* wpca, const float* Mw, const float* U, const float* R,
                                       const int64_t* iCC, const int64_t* iU, const float* Ucc, const int32_t* sp_x,
                                       const int32_t* sp_y, const float* sp_amp, const int32_t* round_start,
                                       int32_t rounds, int32_t n, const int32_t* counters, float* tF,
-                                      int32_t* status, const float* Phi, const float* Plo, int64_t ldp,
+                                      int32_t* status, const void* Phi, const void* Plo, int32_t p_bf16, int64_t ldp,
                                       cudaStream_t s);
 cudaError_t launch_st_out(const int32_t* sp_x, const int32_t* sp_y, const float* sp_amp, int32_t n,
                           int64_t* st, float* amps, cudaStream_t s);

@@ -45,7 +45,6 @@ namespace lss {
 
 constexpr int MP_THREADS = 512;
 static_assert(MP_LIST == 31, "MSG_MP_LIST names the list length");
-constexpr int MP_RING_STAGE = 3 * 8 * 32;  // floats of one ring stage: 8 rows x (score, ctc, ctc) x 32 lanes
 constexpr int MP_MAX_GRID = 1024;
 // U-phase work items: at least MP_ITEMS_PER_WARP items per warp and at most
 // MP_ROWS_PER_ITEM template rows per item (whole 8-row batches)
@@ -72,8 +71,6 @@ __global__ void __launch_bounds__(MP_THREADS, 1) k_mp(MPArgs a) {
     int* ivals = reinterpret_cast<int*>(smem + W + 2 * nt);   // [W]
     float* s_nm = smem + 2 * W + 2 * nt;                       // [T]
     float* s_inv = s_nm + T;                                   // [T]
-    const int NS = a.ring_stages;                              // 0: rows through registers
-    float* ring = s_inv + ((T + 3) & ~3);                      // [MP_THREADS / 32][NS][MP_RING_STAGE]
     for (int t = tid; t < T; t += MP_THREADS) {
         const float v = __ldg(a.nm + t);
         s_nm[t] = v;
@@ -283,50 +280,6 @@ __global__ void __launch_bounds__(MP_THREADS, 1) k_mp(MPArgs a) {
                 const float* p0 = c0p ? c0p + (int64_t)t0 * L2 : nullptr;
                 const float* p1 = c1p ? c1p + (int64_t)t0 * L2 : nullptr;
                 const int64_t ldb = a.ldb;
-                if (NS > 0) {
-                    // rows move through this warp's ring of NS stages of 8 rows
-                    // (score, even term's ctc, odd term's ctc) by asynchronous
-                    // copies, NS - 1 stages in flight while one is updated; each
-                    // lane copies and reads its own column only
-                    float* wr = ring + (size_t)warp * NS * MP_RING_STAGE + lane;
-                    const int nbat = (t1 - t0 + 7) / 8;
-                    auto issue = [&](int bt) {
-                        if (bt < nbat) {
-                            float* st = wr + (bt % NS) * MP_RING_STAGE;
-                            const int r0 = bt * 8;
-#pragma unroll
-                            for (int u = 0; u < 8; ++u)
-                                if (t0 + r0 + u < t1) {
-                                    cp_async4(st + u * 32, bp + (int64_t)(r0 + u) * ldb, pk);
-                                    if (p0) cp_async4(st + (8 + u) * 32, p0 + (int64_t)(r0 + u) * L2, ps);
-                                    if (p1) cp_async4(st + (16 + u) * 32, p1 + (int64_t)(r0 + u) * L2, ps);
-                                }
-                        }
-                        cp_async_commit();
-                    };
-                    for (int bt = 0; bt < NS - 1; ++bt) issue(bt);
-                    for (int bt = 0; bt < nbat; ++bt) {
-                        // all but the NS - 2 newest groups are complete: batch bt has landed
-                        if (NS == 4) cp_async_wait<2>();
-                        else if (NS == 3) cp_async_wait<1>();
-                        else cp_async_wait<0>();
-                        const float* st = wr + (bt % NS) * MP_RING_STAGE;
-                        const int r0 = bt * 8;
-#pragma unroll
-                        for (int u = 0; u < 8; ++u) {
-                            const int t = t0 + r0 + u;
-                            if (t < t1) {
-                                float xv = st[u * 32];
-                                if (p0) xv = __fsub_rn(xv, __fmul_rn(a0, st[(8 + u) * 32]));
-                                if (p1) xv = __fsub_rn(xv, __fmul_rn(a1, st[(16 + u) * 32]));
-                                st_keep(bp + (int64_t)(r0 + u) * ldb, xv, pk);
-                                if (!edge) m.consider(xv, s_nm[t], s_inv[t], t);
-                            }
-                        }
-                        issue(bt + NS - 1);  // into the stage batch bt - 1 used
-                    }
-                    cp_async_wait<0>();
-                } else {
                 int t = t0;
                 // software pipelined: the next eight rows' loads are issued
                 // before the current eight are updated (the rows of a column
@@ -378,7 +331,6 @@ __global__ void __launch_bounds__(MP_THREADS, 1) k_mp(MPArgs a) {
                     st_keep(bp, xv, pk);
                     if (!edge) m.consider(xv, s_nm[t], s_inv[t], t);
                 }
-                }
                 if (!edge && t1 > t0) atomicMax(knext + s, pack_key(m.best, m.bi));
             }
         }
@@ -401,27 +353,14 @@ int mp_max_grid(int device) {
     return std::min(sms * occ, MP_MAX_GRID);
 }
 
-size_t mp_smem_bytes(int cols_per_blk, int nt, int T, int stages) {
+size_t mp_smem_bytes(int cols_per_blk, int nt, int T) {
     return sizeof(float) * ((size_t)cols_per_blk + 2 * nt) + sizeof(int) * (size_t)cols_per_blk +
-           sizeof(float) * ((size_t)T + ((T + 3) & ~3)) + 16 +
-           sizeof(float) * (size_t)(MP_THREADS / 32) * stages * MP_RING_STAGE;
+           sizeof(float) * 2 * (size_t)T + 16;
 }
 
 cudaError_t launch_mp(MPArgs a, int grid, cudaStream_t s) {
     if (grid > MP_MAX_GRID) return cudaErrorInvalidValue;
-    // the deepest copy ring (4, 3 or 2 stages) that fits the shared memory
-    // left beside the kernel's static arrays; none: rows through registers
-    int dev = 0, optin = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    const size_t budget = (size_t)optin > 8192 ? (size_t)optin - 8192 : 0;  // static arrays (s_pref ...)
-    a.ring_stages = 0;
-    for (int st = 4; st >= 2; --st)
-        if (mp_smem_bytes(a.cols_per_blk, a.nt, a.T, st) <= budget) {
-            a.ring_stages = st;
-            break;
-        }
-    const size_t smem = mp_smem_bytes(a.cols_per_blk, a.nt, a.T, a.ring_stages);
+    const size_t smem = mp_smem_bytes(a.cols_per_blk, a.nt, a.T);
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k_mp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;

@@ -75,16 +75,6 @@ __device__ __forceinline__ float ld_stream(const float* a, uint64_t pol) {
 }
 
 
-// 4-byte asynchronous copies global -> shared (LDGSTS) with an L2 policy;
-// each thread waits for its own groups (cp.async.wait_group)
-__device__ __forceinline__ void cp_async4(float* dst, const float* src, uint64_t pol) {
-    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
-    asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "l"(pol) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
-
 __device__ __forceinline__ float cf_of(float b, float nmv) {
     const float r = fmaxf(b, 0.f);
     return __fdiv_rn(__fmul_rn(r, r), nmv);

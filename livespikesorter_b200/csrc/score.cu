@@ -338,12 +338,12 @@ __global__ void __launch_bounds__(256) k_pca_proj_cols(const float* __restrict__
                                                        const int32_t* __restrict__ count, float* __restrict__ hi,
                                                        float* __restrict__ lo, int64_t ldk, int32_t scatter) {
     extern __shared__ float sm[];
-    float* ws = sm;                   // [KPC][ntp]
-    float* xs = sm + KPC * ntp;       // [PCOL_CH][ntp + 1]
-    const int xw = ntp + 1;
+    const int xw = ntp + 1;           // odd row strides: no bank conflicts across k or c
+    float* ws = sm;                   // [KPC][ntp + 1]
+    float* xs = sm + KPC * xw;        // [PCOL_CH][ntp + 1]
     for (int e = threadIdx.x; e < KPC * ntp; e += blockDim.x) {
         const int k = e / ntp, m = e % ntp;
-        ws[e] = (m < nt) ? wpca[k * nt + m] : 0.f;
+        ws[k * xw + m] = (m < nt) ? wpca[k * nt + m] : 0.f;
     }
     const int n = *count;
     const int half = nt / 2;
@@ -362,7 +362,7 @@ __global__ void __launch_bounds__(256) k_pca_proj_cols(const float* __restrict__
             for (int e = threadIdx.x; e < nc * KPC; e += blockDim.x) {
                 const int c = e / KPC, k = e % KPC;
                 const float* xr = xs + c * xw;
-                const float* wk = ws + k * ntp;
+                const float* wk = ws + k * xw;
                 float acc = 0.f;
                 for (int m = 0; m < ntp; ++m) acc = fmaf(wk[m], xr[m], acc);
                 const int64_t o = row * ldk + (int64_t)(c0 + c) * KPC + k;
@@ -379,7 +379,7 @@ static cudaError_t launch_cols(const float* X, int64_t ldx, int32_t C, int64_t N
                                const int32_t* cols, const int32_t* count, int32_t max_cols, float* hi, float* lo,
                                int64_t ldk, int32_t scatter, cudaStream_t s) {
     const int ntp = (nt + 7) & ~7;
-    const size_t smem = sizeof(float) * ((size_t)KPC * ntp + (size_t)PCOL_CH * (ntp + 1));
+    const size_t smem = sizeof(float) * ((size_t)KPC * (ntp + 1) + (size_t)PCOL_CH * (ntp + 1));
     if (smem > 48 * 1024) return cudaErrorInvalidValue;
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);

@@ -216,15 +216,13 @@ int enqueue_stream_batch(Probe* p) {
     if (rc) return p->fail(rc, h->err);
     const bool bf16 = h->cfg.precision == LSS_PREC_BF16_RECHECK;
     if (p->feat > 0) {
-        if (bf16)  // FP32 projection rows of the spikes' columns, as the FP32 path has them
-            PCK(launch_pca_proj_cols_tf32(Xh, h->ld, h->C, h->N, h->wpca.p, h->K, h->nt, h->sp_x.p, h->counters.p,
-                                          (int)std::min<int64_t>(p->cap, h->cfg.max_spikes), h->B0T_hi.p, h->B0T_lo.p,
-                                          h->CKpad, 1, s));
         const int grid = (int)std::min<int64_t>(p->cap, 2 * (int64_t)h->sm_count);
         PCK(launch_pc_features_folded(Xh, h->ld, h->C, h->nt, h->K, h->nC, h->T, h->wpca.p, h->Mw.p, h->U.p,
                                       h->R.p, h->iCC.p, h->iU.p, h->Ucc.p, h->sp_x.p, h->sp_y.p, h->sp_amp.p,
-                                      h->round_start.p, 0, grid, h->counters.p, h->tF.p, h->status.p, h->B0T_hi.p,
-                                      h->B0T_lo.p, h->CKpad, s));
+                                      h->round_start.p, 0, grid, h->counters.p, h->tF.p, h->status.p,
+                                      bf16 ? (const void*)h->B0T.p : (const void*)h->B0T_hi.p,
+                                      bf16 ? (const void*)h->B0T16lo.p : (const void*)h->B0T_lo.p, bf16 ? 1 : 0,
+                                      h->CKpad, s));
     }
     RecordClock rclk;
     rclk.ibatch_dev = p->state.p;

@@ -15,7 +15,7 @@ CPU). Tolerances:
   Cf on the oracle's own field at that round (FP32 rounding of the score GEMM
   can take either side). Then the batch's spike sets must agree to 0.999, the
   prefix before the tie must be identical, and there may be at most one such
-  batch per 20000 spikes;
+  batch per 10000 spikes;
 * amplitudes within 1e-4 relative;
 * PC features within 1e-3 of their largest magnitude (FP32 projection sums in
   another order than torch's conv1d / matmul).
@@ -141,8 +141,8 @@ def _check_batches(T, dup, seed):
         if keep.any():
             assert np.abs(r['pc'].numpy()[:n_cmp][keep] - tf[:n_cmp][keep]).max() <= PC_TOL * np.abs(tf).max(), ib
         total += len(got)
-    # at most one near-tie per 20000 spikes
-    assert len(near_ties) <= max(1, total // 20000), near_ties
+    # at most one near-tie batch per 10000 spikes
+    assert len(near_ties) <= max(1, total // 10000), near_ties
     return total
 
 
