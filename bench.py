@@ -293,6 +293,7 @@ def run_b200(args):
     tot_h, per_h, seen = timed_e2e(K, W)
     tot_s, per_s, _ = timed(K, W, host=True)
     stages, spikes, rounds = profiled(min(K, 2 * len(ids)))
+    phases = s.stats()['mp_phases_ms']
     rec_s = setup.NT / FS
     value = world * K * rec_s / (tot / 1e3)
     e2e = world * K * rec_s / (tot_h / 1e3)
@@ -341,7 +342,8 @@ def run_b200(args):
         'latency_ms_p50': float(np.percentile(per, 50)), 'latency_ms_p99': float(np.percentile(per, 99)),
         'roofline': roof, 'roofline_path': path_roofline(setup, float(np.mean(spikes)), T, value / world, hbm, tfl, src),
         'gpu_launches': int(launches), 'clocks': clocks,
-        'stage_ms': mean_st, 'spikes_per_batch': float(np.mean(spikes)), 'rounds_per_batch': float(np.mean(rounds)),
+        'stage_ms': mean_st, 'mp_phases_ms': phases,
+        'spikes_per_batch': float(np.mean(spikes)), 'rounds_per_batch': float(np.mean(rounds)),
         'step_ms': [round(float(v), 3) for v in per],
     }
     if not args.no_extras:
@@ -352,6 +354,18 @@ def run_b200(args):
             out['fp32_path'] = {'value': world * K * rec_s / (t32 / 1e3), 'unit': 'rec-s/s',
                                 'ms_per_step': t32 / K, 'stage_ms': st32,
                                 'api': 'lss_set_drift + lss_sort_batch_async, device-resident rows, same batches'}
+        # the two rounds kernels on the same batches (identical results): every
+        # row updated, or provably unchanged template-row blocks skipped
+        kernels = {}
+        for skip in (False, True):
+            s32.set_round_kernel(skip)
+            tk, stk = device_resident_rate(s32, rows_d, drifts, ids, nb, K, W, stream, dist, local)
+            st_k = s32.stats()
+            kernels['skip_blocks' if skip else 'full'] = {
+                'rec_s_per_s': world * K * rec_s / (tk / 1e3), 'mp_ms': stk['mp_ms'], 'phases_ms': stk['mp_phases_ms'],
+                'update_items': st_k['mp_items'], 'update_items_changed': st_k['mp_items_updated']}
+        s32.set_round_kernel(False)
+        out['round_kernels_fp32'] = kernels
         if args.precision == 'bf16':
             out['bf16'] = bf16_report(s, s32, rows_d, drifts, ids, nb)
             out['bf16']['score_err_fp64'] = fp64_score_error(s, s32, setup, rows_d[0], drifts[0], ids[0], nb)
@@ -403,13 +417,15 @@ def device_resident_rate(s, rows_d, drifts, ids, nb, K, W, stream, dist, local):
     torch.cuda.synchronize()
     tot = max_over_ranks(float(e0.elapsed_time(e1)), dist, f'cuda:{local}')
     s.set_profiling(True)
-    st = []
+    st, ph = [], []
     for i in range(2):
         s.set_drift(drifts[i % len(ids)])
         s.sort_batch(rows_d[i % len(ids)], ids[i % len(ids)], nb, on_device=True)
         st.append(s.stage_times())
+        ph.append(s.stats()['mp_phases_ms'])
     s.set_profiling(False)
     stages = {k: float(np.mean([x[k] for x in st])) for k in st[0]}
+    stages['mp_phases_ms'] = {k: float(np.mean([x[k] for x in ph])) for k in ph[0]}
     return tot, stages
 
 

@@ -241,6 +241,12 @@ typedef struct lss_stats {
      * any score: the others were skipped as exact no-ops */
     int64_t mp_items;
     int64_t mp_items_updated;
+    /* the rounds' time split, per CTA of the rounds kernel (mean over CTAs,
+     * summed over the rounds of the last synchronous batch): peak phase,
+     * waiting at the grid barrier after it, update phase, waiting after it;
+     * and the slowest CTA's peak and update totals */
+    int64_t mp_peak_ns, mp_peak_wait_ns, mp_update_ns, mp_update_wait_ns;
+    int64_t mp_peak_max_ns, mp_update_max_ns;
 } lss_stats;
 int  lss_get_stats(const lss_handle* h, lss_stats* out);
 

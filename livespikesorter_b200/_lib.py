@@ -57,7 +57,9 @@ class LssPostConfig(ct.Structure):
 class LssStats(ct.Structure):
     _fields_ = [('rounds', ct.c_int32), ('spikes', ct.c_int64), ('recheck_columns', ct.c_int64),
                 ('recheck_flips', ct.c_int64), ('launches', ct.c_int64), ('recheck_rescored', ct.c_int64),
-                ('mp_items', ct.c_int64), ('mp_items_updated', ct.c_int64)]
+                ('mp_items', ct.c_int64), ('mp_items_updated', ct.c_int64),
+                ('mp_peak_ns', ct.c_int64), ('mp_peak_wait_ns', ct.c_int64), ('mp_update_ns', ct.c_int64),
+                ('mp_update_wait_ns', ct.c_int64), ('mp_peak_max_ns', ct.c_int64), ('mp_update_max_ns', ct.c_int64)]
 
 
 STAGES = ('h2d_ms', 'ingest_ms', 'highpass_ms', 'whiten_ms', 'project_ms', 'score_ms', 'mp_ms', 'xres_ms',

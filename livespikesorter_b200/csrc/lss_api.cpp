@@ -432,6 +432,7 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
     ALLOC(mp_perm, (size_t)h->mp_nb * MPB_ROWS);
     ALLOC(mp_cmaxr, (size_t)T * T);
     ALLOC(mp_bkey, (size_t)h->mp_nb * ld);
+    ALLOC(mp_phase, 6);
     ALLOC(mp_bmin, (size_t)h->mp_nb * ld);
     ALLOC(blk_cnt, 4096);
     ALLOC(blk_x, ld);
@@ -786,6 +787,8 @@ int lss::enqueue_mp(lss_handle* h, int64_t N, cudaStream_t s, bool maxima_ready)
     a.cols_per_blk = (int)((N + G - 1) / G);
     if (!maxima_ready) CK(cudaMemsetAsync(h->status.p, 0, sizeof(int32_t), s));
     CK(cudaMemsetAsync(h->counters.p, 0, 4 * sizeof(int32_t), s));
+    CK(cudaMemsetAsync(h->mp_phase.p, 0, 6 * sizeof(unsigned long long), s));
+    a.phase = h->mp_phase.p;
     if (h->mp_skip) {
         a.perm = h->mp_perm.p;
         a.nb = h->mp_nb;
@@ -810,6 +813,7 @@ static int run_mp(lss_handle* h, int64_t N, int32_t* n_out, int32_t* rounds_out,
     if (rc) return rc;
     int32_t hc[4], st = 0;
     CK(cudaMemcpyAsync(hc, h->counters.p, sizeof(hc), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(h->mp_phase_host, h->mp_phase.p, sizeof(h->mp_phase_host), cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(&st, h->status.p, sizeof(st), cudaMemcpyDeviceToHost, s));
     h->mark(7, s);
     CK(cudaStreamSynchronize(s));
@@ -823,6 +827,7 @@ static int run_mp(lss_handle* h, int64_t N, int32_t* n_out, int32_t* rounds_out,
     h->stats.spikes = hc[0];
     h->stats.mp_items_updated = hc[2];
     h->stats.mp_items = hc[3];
+    h->set_phase_stats();
     return LSS_OK;
 }
 
@@ -1194,6 +1199,7 @@ static int sort_batch_impl(lss_handle* h, const int16_t* raw, int64_t n_rows, in
     CK(cudaMemcpyAsync(&count, h->rec_count.p, sizeof(count), cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(&st, h->status.p, sizeof(st), cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(hc, h->counters.p, sizeof(hc), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(h->mp_phase_host, h->mp_phase.p, sizeof(h->mp_phase_host), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     if (st & STATUS_TIMEOUT) return h->fail(LSS_ERR_TIMEOUT, "a bounded device-side wait timed out");
     if (st & STATUS_CAPACITY) return h->fail(LSS_ERR_CAPACITY, "more than max_spikes spikes in one batch");
@@ -1203,6 +1209,7 @@ static int sort_batch_impl(lss_handle* h, const int16_t* raw, int64_t n_rows, in
     h->stats.rounds = hc[1];
     h->stats.mp_items_updated = hc[2];
     h->stats.mp_items = hc[3];
+    h->set_phase_stats();
     out->count = count;
     if (count > cap) return h->fail(LSS_ERR_CAPACITY, "record capacity smaller than the spike count");
     if (!out->on_device && count > 0) {

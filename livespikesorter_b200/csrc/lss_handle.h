@@ -71,6 +71,7 @@ struct lss_handle {
     DevBuf<int32_t> mp_perm;
     DevBuf<float> mp_cmaxr, mp_bmin;
     DevBuf<unsigned long long> mp_bkey;
+    DevBuf<unsigned long long> mp_phase;         // [6] phase clock of the rounds kernel
     // BF16 path (BF16x3 GEMM): projection and templates as bf16 hi / lo splits
     DevBuf<__nv_bfloat16> B0T, B0T16lo, Up16, Up16lo;
     DevBuf<float> B0T_hi, B0T_lo, Up_hi, Up_lo;  // FP32 path (3xTF32): tf32 hi/lo splits
@@ -122,6 +123,17 @@ struct lss_handle {
     cudaEvent_t up_done[2] = {}, raw_free[2] = {};
     int raw_next = 0;
 
+    unsigned long long mp_phase_host[6] = {};    // host copy of mp_phase after a synchronous batch
+    void set_phase_stats() {
+        const int64_t g = std::max(1, mp_grid);
+        stats.mp_peak_ns = (int64_t)(mp_phase_host[0] / g);
+        stats.mp_peak_wait_ns = (int64_t)(mp_phase_host[1] / g);
+        stats.mp_update_ns = (int64_t)(mp_phase_host[2] / g);
+        stats.mp_update_wait_ns = (int64_t)(mp_phase_host[3] / g);
+        stats.mp_peak_max_ns = (int64_t)mp_phase_host[4];
+        stats.mp_update_max_ns = (int64_t)mp_phase_host[5];
+    }
+
     int fail(int code, const std::string& m) {
         err = m;
         return code;
@@ -148,7 +160,7 @@ struct lss_handle {
         tF.release(); iCC.release(); iU.release(); cfmax.release(); imax.release(); blk_cnt.release();
         blk_x.release(); blk_y.release(); sp_x.release(); sp_y.release(); sp_round.release();
         round_start.release(); counters.release(); status.release(); sp_amp.release(); blk_amp.release(); colkey.release();
-        mp_perm.release(); mp_cmaxr.release(); mp_bmin.release(); mp_bkey.release();
+        mp_perm.release(); mp_cmaxr.release(); mp_phase.release(); mp_bmin.release(); mp_bkey.release();
         bar.release(); rec_time.release(); rec_count.release(); rec_tmpl.release(); rec_slot.release(); rec_amp.release();
         rec_pc.release(); B0T.release(); B0T16lo.release(); Up16.release(); Up16lo.release();
         B0T_hi.release(); B0T_lo.release(); Up_hi.release(); Up_lo.release();

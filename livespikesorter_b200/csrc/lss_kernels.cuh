@@ -154,6 +154,7 @@ struct MPArgs {
     unsigned int* bar;        // [2] grid barrier count / generation, zero at launch
     int32_t cols_per_blk;     // W
     int32_t init_cols;        // 1: compute column maxima of B before round 0
+    unsigned long long* phase = nullptr;    // [6] phase clock of the rounds (PhaseClock), zero at launch; may be null
     // block-skipping rounds (mp_blocks.cu) only: template rows are grouped in
     // blocks of MPB_ROWS (rows of templates close on the probe, by perm)
     const int32_t* perm = nullptr;          // [nb * MPB_ROWS] template of each block row, -1 past T

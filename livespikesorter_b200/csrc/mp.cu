@@ -89,6 +89,8 @@ __global__ void __launch_bounds__(MP_THREADS, 1) k_mp(MPArgs a) {
         }
     }
     if (!grid_sync(a.bar, a.status)) return;
+    PhaseClock clk;
+    if (tid == 0) clk.start();
     int base = 0;
     int r = 0;
     for (; r < a.max_rounds; ++r) {
@@ -151,7 +153,9 @@ __global__ void __launch_bounds__(MP_THREADS, 1) k_mp(MPArgs a) {
         }
         __syncthreads();
         if (tid == 0) a.blk_cnt[b] = s_cnt;
+        if (tid == 0) clk.lap(0);
         if (!grid_sync(a.bar, a.status)) return;
+        if (tid == 0) clk.lap(1);
 
         // ---- U: global order of the round's spikes, records, score update
         {
@@ -335,7 +339,13 @@ __global__ void __launch_bounds__(MP_THREADS, 1) k_mp(MPArgs a) {
             }
         }
         base += total;
+        if (tid == 0) clk.lap(2);
         if (!grid_sync(a.bar, a.status)) return;
+        if (tid == 0) clk.lap(3);
+    }
+    if (tid == 0) {
+        clk.lap(2);  // the last round's update phase, or its empty tail
+        clk.flush(a.phase);
     }
     if (b == 0 && tid == 0) {
         a.counters[0] = base;

@@ -132,6 +132,8 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
         }
     }
     if (!grid_sync(a.bar, a.status)) return;
+    PhaseClock clk;
+    if (tid == 0) clk.start();
 
     int base = 0;
     int r = 0;
@@ -196,7 +198,9 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
         }
         __syncthreads();
         if (tid == 0) a.blk_cnt[b] = s_cnt;
+        if (tid == 0) clk.lap(0);
         if (!grid_sync(a.bar, a.status)) return;
+        if (tid == 0) clk.lap(1);
 
         // ---- U: global order of the round's spikes, records, block updates
         {
@@ -397,11 +401,17 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
             }
         }
         base += total;
+        if (tid == 0) clk.lap(2);
         if (!grid_sync(a.bar, a.status)) return;
+        if (tid == 0) clk.lap(3);
     }
     if (lane == 0 && n_items) {
         atomicAdd(a.counters + 2, n_proc);
         atomicAdd(a.counters + 3, n_items);
+    }
+    if (tid == 0) {
+        clk.lap(2);  // the last round's update phase, or its empty tail
+        clk.flush(a.phase);
     }
     if (b == 0 && tid == 0) {
         a.counters[0] = base;

@@ -75,6 +75,31 @@ __device__ __forceinline__ float ld_stream(const float* a, uint64_t pol) {
 }
 
 
+// Phase clock of the rounds (thread 0 of each CTA): time in the peak phase,
+// waiting at the grid barrier after it, in the update phase and waiting after
+// it, summed over the rounds; added to phase[0..3] (sums over CTAs) with the
+// slowest CTA's peak and update totals in phase[4], phase[5].
+struct PhaseClock {
+    unsigned long long t = 0, acc[4] = {0, 0, 0, 0};
+    __device__ __forceinline__ static unsigned long long now() {
+        unsigned long long v;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(v));
+        return v;
+    }
+    __device__ __forceinline__ void start() { t = now(); }
+    __device__ __forceinline__ void lap(int i) {
+        const unsigned long long u = now();
+        acc[i] += u - t;
+        t = u;
+    }
+    __device__ __forceinline__ void flush(unsigned long long* phase) const {
+        if (!phase) return;
+        for (int i = 0; i < 4; ++i) atomicAdd(phase + i, acc[i]);
+        atomicMax(phase + 4, acc[0]);
+        atomicMax(phase + 5, acc[2]);
+    }
+};
+
 __device__ __forceinline__ float cf_of(float b, float nmv) {
     const float r = fmaxf(b, 0.f);
     return __fdiv_rn(__fmul_rn(r, r), nmv);
