@@ -34,8 +34,9 @@
 // Round structure, work split and bounded grid barriers follow k_mp: the peak
 // phase owns W consecutive columns per CTA; the update phase prefix-sums the
 // per-CTA peak counts for the round's time order; update work items are
-// split into contiguous ranges per CTA and handed to warps through a shared
-// counter; every wait is bounded (STATUS_TIMEOUT).
+// strided over all warps of the grid, and a warp runs the rows of an item's
+// processed blocks through one software pipeline; every wait is bounded
+// (STATUS_TIMEOUT).
 #include "lss_kernels.cuh"
 #include "mp_common.cuh"
 
@@ -83,7 +84,7 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
     extern __shared__ float smem[];
     __shared__ int s_pref[MPB_MAX_GRID + 1];
     __shared__ int s_wcnt[MPB_THREADS / 32];
-    __shared__ int s_cnt, s_total, s_next;
+    __shared__ int s_cnt, s_total;
 
     const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
@@ -235,8 +236,6 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
         const int ngr = (nb + MPB_GROUP - 1) / MPB_GROUP;
         const int per_spike = nch * ngr;
         const int items = total * per_spike;
-        const int per_cta = (items + G - 1) / G;
-        const int it_end = min(items, (b + 1) * per_cta);
         {
             const int cnt = s_pref[b + 1] - s_pref[b];
             for (int k = tid; k < cnt; k += MPB_THREADS) {
@@ -247,40 +246,40 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
                 if (a.sp_round) a.sp_round[i] = r;
             }
             if (b == 0 && tid == 0) a.round_start[r] = base;
-            if (tid == 0) s_next = b * per_cta;
         }
-        __syncthreads();
         {
-            // Work item (spike q, chunk ch, group g): the columns of spike q's
-            // segment [max(x_q - nt, x_{q-1} + nt + 1), x_q + nt], 32 at a
-            // time (lane = column), and the row blocks g*MPB_GROUP.. of the
-            // group. Lane L holds spike q - 1 + L of the round.
-            int cur_q = -1, x = INT_MAX, y = 0;
-            float amp = 0.f;
-            for (;;) {
-                int it = 0;
-                if (lane == 0) it = atomicAdd(&s_next, 1);
-                it = __shfl_sync(FULL, it, 0);
-                if (it >= it_end) break;
-                const int q = it / per_spike, rem = it - q * per_spike, ch = rem / ngr, g = rem - ch * ngr;
-                if (q != cur_q) {
-                    cur_q = q;
-                    const int j = q - 1 + lane;
-                    x = INT_MAX;
-                    y = 0;
-                    amp = 0.f;
-                    if (j >= 0 && j < total) {
-                        int lo2 = 0, hi2 = G;  // region c with s_pref[c] <= j < s_pref[c+1]
-                        while (hi2 - lo2 > 1) {
-                            const int m = (lo2 + hi2) >> 1;
-                            if (s_pref[m] <= j) lo2 = m; else hi2 = m;
-                        }
-                        const int idx = lo2 * W + (j - s_pref[lo2]);
-                        x = __ldcg(a.blk_x + idx);
-                        y = __ldcg(a.blk_y + idx);
-                        amp = __ldcg(a.blk_amp + idx);
+            // Work items (spike q, chunk ch, group g), strided over all warps
+            // of the grid: the columns of spike q's segment
+            // [max(x_q - nt, x_{q-1} + nt + 1), x_q + nt], 32 at a time (lane =
+            // column), and the row blocks g*MPB_GROUP.. of the group. Lane L
+            // holds spike q - 1 + L of the round; the next item's spikes are
+            // fetched while the current one is processed.
+            const int wid = b * (MPB_THREADS / 32) + warp, wtot = G * (MPB_THREADS / 32);
+            auto fetch = [&](int it2, int& fx, int& fy, float& fa) {
+                const int j = it2 / per_spike - 1 + lane;
+                fx = INT_MAX;
+                fy = 0;
+                fa = 0.f;
+                if (it2 < items && j >= 0 && j < total) {
+                    int lo2 = 0, hi2 = G;  // region c with s_pref[c] <= j < s_pref[c+1]
+                    while (hi2 - lo2 > 1) {
+                        const int m = (lo2 + hi2) >> 1;
+                        if (s_pref[m] <= j) lo2 = m; else hi2 = m;
                     }
+                    const int idx = lo2 * W + (j - s_pref[lo2]);
+                    fx = __ldcg(a.blk_x + idx);
+                    fy = __ldcg(a.blk_y + idx);
+                    fa = __ldcg(a.blk_amp + idx);
                 }
+            };
+            int nx, ny;
+            float na;
+            fetch(wid, nx, ny, na);
+            for (int it = wid; it < items; it += wtot) {
+                const int x = nx, y = ny;
+                const float amp = na;
+                fetch(it + wtot, nx, ny, na);
+                const int q = it / per_spike, rem = it - q * per_spike, ch = rem / ngr, g = rem - ch * ngr;
                 const int xi = __shfl_sync(FULL, x, 1);
                 const int xprev = __shfl_sync(FULL, x, 0);
                 const bool ok = lane >= 1 && (q - 1 + lane) < total && x <= xi + 2 * nt;
@@ -358,11 +357,12 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
                 n_items += nbg;
                 const float* c0p = a.ctcP + (int64_t)y0 * T * L2 + (s - x0 + nt);
                 const float* c1p = a.ctcP + (int64_t)y1 * T * L2 + (s - x1 + nt);
-#pragma unroll 1
-                for (int j = 0; j < MPB_GROUP; ++j) {
-                    if (!((procm >> j) & 1u)) continue;  // warp-uniform
-                    ++n_proc;
-                    const int bb = bg0 + j, r0 = bb * MPB_ROWS, nr = min(MPB_ROWS, T - r0);
+                n_proc += __popc(procm);
+                if (!active || procm == 0u) continue;
+                // the processed blocks' rows in 8-row batches through one
+                // software pipeline: the next batch's loads are issued before
+                // the current batch is updated, across block boundaries
+                auto masks = [&](int j, unsigned& m0, unsigned& m1) {
                     unsigned long long p0 = m0p[0], p1 = m1p[0];
 #pragma unroll
                     for (int i = 1; i < (MPB_GROUP + 1) / 2; ++i)
@@ -370,33 +370,71 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
                             p0 = m0p[i];
                             p1 = m1p[i];
                         }
-                    const unsigned m0 = (unsigned)(p0 >> (32 * (j & 1))), m1 = (unsigned)(p1 >> (32 * (j & 1)));
-                    if (!active) continue;
-                    ColMaxAny m;
-                    float mn = INFINITY;
-                    for (int rr = 0; rr < nr; rr += 16) {
-                        float v[16], w0[16], w1[16];
+                    m0 = (unsigned)(p0 >> (32 * (j & 1)));
+                    m1 = (unsigned)(p1 >> (32 * (j & 1)));
+                };
+                // batch k of the sequence: block j = k-th set bit group, rows rb*8..
+                const int nbt = __popc(procm) * (MPB_ROWS / 8);
+                auto batch_of = [&](int k, int& j, int& rb) {
+                    int left = k / (MPB_ROWS / 8);
+                    unsigned pm = procm;
+                    for (int i = 0; i < left; ++i) pm &= pm - 1u;
+                    j = __ffs(pm) - 1;
+                    rb = k % (MPB_ROWS / 8);
+                };
+                float v[8], w0[8], w1[8];
+                auto load = [&](int k, float (&lv)[8], float (&l0)[8], float (&l1)[8]) {
+                    int j, rb;
+                    batch_of(k, j, rb);
+                    unsigned m0, m1;
+                    masks(j, m0, m1);
+                    const int r0 = (bg0 + j) * MPB_ROWS, nr = min(MPB_ROWS, T - r0);
 #pragma unroll
-                        for (int u = 0; u < 16; ++u) {
-                            const int t = (rr + u < nr) ? s_perm[r0 + rr + u] : -1;
-                            v[u] = t >= 0 ? ld_keep(a.B + (int64_t)t * ldb + s, pk) : 0.f;
-                            w0[u] = (t >= 0 && ((m0 >> (rr + u)) & 1u)) ? ld_stream(c0p + (int64_t)t * L2, ps) : 0.f;
-                            w1[u] = (t >= 0 && ((m1 >> (rr + u)) & 1u)) ? ld_stream(c1p + (int64_t)t * L2, ps) : 0.f;
-                        }
+                    for (int u = 0; u < 8; ++u) {
+                        const int rr = rb * 8 + u;
+                        const int t = rr < nr ? s_perm[r0 + rr] : -1;
+                        lv[u] = t >= 0 ? ld_keep(a.B + (int64_t)t * ldb + s, pk) : 0.f;
+                        l0[u] = (t >= 0 && ((m0 >> rr) & 1u)) ? ld_stream(c0p + (int64_t)t * L2, ps) : 0.f;
+                        l1[u] = (t >= 0 && ((m1 >> rr) & 1u)) ? ld_stream(c1p + (int64_t)t * L2, ps) : 0.f;
+                    }
+                };
+                load(0, v, w0, w1);
+                ColMaxAny m;
+                float mn = INFINITY;
+                for (int k = 0; k < nbt; ++k) {
+                    float nv[8], nw0[8], nw1[8];
+                    if (k + 1 < nbt) load(k + 1, nv, nw0, nw1);
+                    int j, rb;
+                    batch_of(k, j, rb);
+                    unsigned m0, m1;
+                    masks(j, m0, m1);
+                    const int bb = bg0 + j, r0 = bb * MPB_ROWS, nr = min(MPB_ROWS, T - r0);
 #pragma unroll
-                        for (int u = 0; u < 16; ++u) {
-                            if (rr + u >= nr) continue;
-                            const int t = s_perm[r0 + rr + u];
-                            float xv = v[u];
-                            if ((m0 >> (rr + u)) & 1u) xv = __fsub_rn(xv, __fmul_rn(a0, w0[u]));
-                            if ((m1 >> (rr + u)) & 1u) xv = __fsub_rn(xv, __fmul_rn(a1, w1[u]));
-                            if (__float_as_uint(xv) != __float_as_uint(v[u])) st_keep(a.B + (int64_t)t * ldb + s, xv, pk);
-                            mn = fminf(mn, fabsf(xv));
-                            m.consider(xv, s_nm[t], s_inv[t], t);
+                    for (int u = 0; u < 8; ++u) {
+                        const int rr = rb * 8 + u;
+                        if (rr >= nr) continue;
+                        const int t = s_perm[r0 + rr];
+                        float xv = v[u];
+                        if ((m0 >> rr) & 1u) xv = __fsub_rn(xv, __fmul_rn(a0, w0[u]));
+                        if ((m1 >> rr) & 1u) xv = __fsub_rn(xv, __fmul_rn(a1, w1[u]));
+                        if (__float_as_uint(xv) != __float_as_uint(v[u])) st_keep(a.B + (int64_t)t * ldb + s, xv, pk);
+                        mn = fminf(mn, fabsf(xv));
+                        m.consider(xv, s_nm[t], s_inv[t], t);
+                    }
+                    if (rb == MPB_ROWS / 8 - 1) {  // last batch of the block: its key and minimum
+                        a.bkey[bb * ldk + s] = pack_key(m.best, m.bi);
+                        a.bmin[bb * ldk + s] = mn;
+                        m = ColMaxAny();
+                        mn = INFINITY;
+                    }
+                    if (k + 1 < nbt) {
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) {
+                            v[u] = nv[u];
+                            w0[u] = nw0[u];
+                            w1[u] = nw1[u];
                         }
                     }
-                    a.bkey[bb * ldk + s] = pack_key(m.best, m.bi);
-                    a.bmin[bb * ldk + s] = mn;
                 }
             }
         }
