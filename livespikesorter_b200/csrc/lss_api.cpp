@@ -433,6 +433,7 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
     ALLOC(mp_cmaxr, (size_t)T * T);
     ALLOC(mp_bkey, (size_t)h->mp_nb * ld);
     ALLOC(mp_phase, 6);
+    ALLOC(mp_work, cfg->max_rounds + 1);
     ALLOC(mp_bmin, (size_t)h->mp_nb * ld);
     ALLOC(blk_cnt, 4096);
     ALLOC(blk_x, ld);
@@ -795,7 +796,9 @@ int lss::enqueue_mp(lss_handle* h, int64_t N, cudaStream_t s, bool maxima_ready)
         a.cmaxr = h->mp_cmaxr.p;
         a.bkey = h->mp_bkey.p;
         a.bmin = h->mp_bmin.p;
+        a.work = h->mp_work.p;
         a.init_cols = 1;  // the rounds take their block maxima from the field itself
+        CK(cudaMemsetAsync(h->mp_work.p, 0, (h->cfg.max_rounds + 1) * sizeof(unsigned int), s));
         CK(launch_mp_blocks(a, G, s));
     } else {
         a.init_cols = maxima_ready ? 0 : 1;

@@ -34,9 +34,9 @@
 // Round structure, work split and bounded grid barriers follow k_mp: the peak
 // phase owns W consecutive columns per CTA; the update phase prefix-sums the
 // per-CTA peak counts for the round's time order; update work items are
-// strided over all warps of the grid, and a warp runs the rows of an item's
-// processed blocks through one software pipeline; every wait is bounded
-// (STATUS_TIMEOUT).
+// handed to warps a few at a time from a global counter per round, and a warp
+// runs the rows of an item's processed blocks through one software pipeline;
+// every wait is bounded (STATUS_TIMEOUT).
 #include "lss_kernels.cuh"
 #include "mp_common.cuh"
 
@@ -50,6 +50,7 @@ constexpr int MPB_THREADS = 512;
 constexpr int MPB_MAX_GRID = 1024;
 constexpr int MPB_GROUP = 4;  // row blocks per update work item
 constexpr int MPB_SPK = 3;    // spikes of a chunk's list that get row masks
+constexpr int MPB_GRAB = 4;   // update work items a warp takes from the round's counter at a time
 constexpr unsigned FULL = 0xffffffffu;
 
 // 2^(e - 25) for v in [2^e, 2^(e+1)) (v >= 0): any |d| below it leaves
@@ -248,19 +249,19 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
             if (b == 0 && tid == 0) a.round_start[r] = base;
         }
         {
-            // Work items (spike q, chunk ch, group g), strided over all warps
-            // of the grid: the columns of spike q's segment
-            // [max(x_q - nt, x_{q-1} + nt + 1), x_q + nt], 32 at a time (lane =
-            // column), and the row blocks g*MPB_GROUP.. of the group. Lane L
-            // holds spike q - 1 + L of the round; the next item's spikes are
-            // fetched while the current one is processed.
-            const int wid = b * (MPB_THREADS / 32) + warp, wtot = G * (MPB_THREADS / 32);
-            auto fetch = [&](int it2, int& fx, int& fy, float& fa) {
-                const int j = it2 / per_spike - 1 + lane;
+            // Work items (spike q, chunk ch, group g): the columns of spike q's
+            // segment [max(x_q - nt, x_{q-1} + nt + 1), x_q + nt], 32 at a time
+            // (lane = column), and the row blocks g*MPB_GROUP.. of the group.
+            // Their cost varies from nothing to MPB_GROUP processed blocks, so
+            // warps take MPB_GRAB consecutive items at a time from the round's
+            // global counter (the next grab is in flight while a grab is
+            // worked). Lane L holds spike q - 1 + L of the round.
+            auto fetch = [&](int q2, int& fx, int& fy, float& fa) {
+                const int j = q2 - 1 + lane;
                 fx = INT_MAX;
                 fy = 0;
                 fa = 0.f;
-                if (it2 < items && j >= 0 && j < total) {
+                if (j >= 0 && j < total) {
                     int lo2 = 0, hi2 = G;  // region c with s_pref[c] <= j < s_pref[c+1]
                     while (hi2 - lo2 > 1) {
                         const int m = (lo2 + hi2) >> 1;
@@ -272,14 +273,22 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
                     fa = __ldcg(a.blk_amp + idx);
                 }
             };
-            int nx, ny;
-            float na;
-            fetch(wid, nx, ny, na);
-            for (int it = wid; it < items; it += wtot) {
-                const int x = nx, y = ny;
-                const float amp = na;
-                fetch(it + wtot, nx, ny, na);
+            int x = INT_MAX, y = 0, cur_q = -1;
+            float amp = 0.f;
+            unsigned grab = 0;
+            if (lane == 0) grab = atomicAdd(a.work + r, 1u);
+            grab = __shfl_sync(FULL, grab, 0);
+            for (;;) {
+                const int it0 = (int)grab * MPB_GRAB;
+                if (it0 >= items) break;
+                unsigned next = 0;
+                if (lane == 0) next = atomicAdd(a.work + r, 1u);
+                for (int it = it0; it < min(items, it0 + MPB_GRAB); ++it) {
                 const int q = it / per_spike, rem = it - q * per_spike, ch = rem / ngr, g = rem - ch * ngr;
+                if (q != cur_q) {
+                    cur_q = q;
+                    fetch(q, x, y, amp);
+                }
                 const int xi = __shfl_sync(FULL, x, 1);
                 const int xprev = __shfl_sync(FULL, x, 0);
                 const bool ok = lane >= 1 && (q - 1 + lane) < total && x <= xi + 2 * nt;
@@ -436,6 +445,8 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
                         }
                     }
                 }
+                }
+                grab = __shfl_sync(FULL, next, 0);
             }
         }
         base += total;
@@ -470,7 +481,7 @@ static size_t mpb_smem_bytes(int cols_per_blk, int nt, int T, int nb) {
 }
 
 cudaError_t launch_mp_blocks(MPArgs a, int grid, cudaStream_t s) {
-    if (grid > MPB_MAX_GRID || !a.perm || !a.cmaxr || !a.bkey || !a.bmin ||
+    if (grid > MPB_MAX_GRID || !a.perm || !a.cmaxr || !a.bkey || !a.bmin || !a.work ||
         a.nb != (a.T + MPB_ROWS - 1) / MPB_ROWS)
         return cudaErrorInvalidValue;
     const size_t smem = mpb_smem_bytes(a.cols_per_blk, a.nt, a.T, a.nb);
