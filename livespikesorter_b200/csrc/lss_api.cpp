@@ -158,6 +158,26 @@ int lss::rebuild_mp_blocks(lss_handle* h) {
     CK(cudaMemcpy(h->mp_perm.p, perm.data(), perm.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
     CK(launch_ctc_row_max(h->ctcP.p, T, 2 * h->nt + 1, h->mp_cmaxr.p, 0));
     CK(cudaDeviceSynchronize());
+    // each spike template's band of row blocks: blocks holding a row t whose
+    // max |ctc| reaches 2^-30 ||U_t|| (about where a unit-amplitude term stops
+    // being a no-op on noise-level scores); used only to balance the work
+    {
+        std::vector<float> cm((size_t)T * T), nmv(T);
+        CK(cudaMemcpy(cm.data(), h->mp_cmaxr.p, cm.size() * sizeof(float), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(nmv.data(), h->nm.p, T * sizeof(float), cudaMemcpyDeviceToHost));
+        std::vector<int32_t> blo(T, 1), bhi(T, 0);
+        for (int y = 0; y < T; ++y)
+            for (int i = 0; i < T; ++i) {
+                const int t = perm[i];
+                if (cm[(size_t)y * T + t] >= std::ldexp(1.0, -30) * std::sqrt((double)nmv[t])) {
+                    const int bb = i / MPB_ROWS;
+                    if (blo[y] > bhi[y]) blo[y] = bb;
+                    bhi[y] = bb;
+                }
+            }
+        CK(cudaMemcpy(h->mp_band_lo.p, blo.data(), T * sizeof(int32_t), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h->mp_band_hi.p, bhi.data(), T * sizeof(int32_t), cudaMemcpyHostToDevice));
+    }
     h->stats.launches += 1;
     return LSS_OK;
 }
@@ -433,7 +453,8 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
     ALLOC(mp_cmaxr, (size_t)T * T);
     ALLOC(mp_bkey, (size_t)h->mp_nb * ld);
     ALLOC(mp_phase, 6);
-    ALLOC(mp_work, cfg->max_rounds + 1);
+    ALLOC(mp_band_lo, T);
+    ALLOC(mp_band_hi, T);
     ALLOC(mp_bmin, (size_t)h->mp_nb * ld);
     ALLOC(blk_cnt, 4096);
     ALLOC(blk_x, ld);
@@ -796,9 +817,9 @@ int lss::enqueue_mp(lss_handle* h, int64_t N, cudaStream_t s, bool maxima_ready)
         a.cmaxr = h->mp_cmaxr.p;
         a.bkey = h->mp_bkey.p;
         a.bmin = h->mp_bmin.p;
-        a.work = h->mp_work.p;
+        a.band_lo = h->mp_band_lo.p;
+        a.band_hi = h->mp_band_hi.p;
         a.init_cols = 1;  // the rounds take their block maxima from the field itself
-        CK(cudaMemsetAsync(h->mp_work.p, 0, (h->cfg.max_rounds + 1) * sizeof(unsigned int), s));
         CK(launch_mp_blocks(a, G, s));
     } else {
         a.init_cols = maxima_ready ? 0 : 1;

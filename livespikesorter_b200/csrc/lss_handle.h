@@ -72,7 +72,7 @@ struct lss_handle {
     DevBuf<float> mp_cmaxr, mp_bmin;
     DevBuf<unsigned long long> mp_bkey;
     DevBuf<unsigned long long> mp_phase;         // [6] phase clock of the rounds kernel
-    DevBuf<unsigned int> mp_work;                // [max_rounds + 1] work counters of the block-skipping rounds
+    DevBuf<int32_t> mp_band_lo, mp_band_hi;      // [T] row-block band of each spike template (work estimate)
     // BF16 path (BF16x3 GEMM): projection and templates as bf16 hi / lo splits
     DevBuf<__nv_bfloat16> B0T, B0T16lo, Up16, Up16lo;
     DevBuf<float> B0T_hi, B0T_lo, Up_hi, Up_lo;  // FP32 path (3xTF32): tf32 hi/lo splits
@@ -161,7 +161,7 @@ struct lss_handle {
         tF.release(); iCC.release(); iU.release(); cfmax.release(); imax.release(); blk_cnt.release();
         blk_x.release(); blk_y.release(); sp_x.release(); sp_y.release(); sp_round.release();
         round_start.release(); counters.release(); status.release(); sp_amp.release(); blk_amp.release(); colkey.release();
-        mp_perm.release(); mp_cmaxr.release(); mp_phase.release(); mp_work.release(); mp_bmin.release(); mp_bkey.release();
+        mp_perm.release(); mp_cmaxr.release(); mp_phase.release(); mp_band_lo.release(); mp_band_hi.release(); mp_bmin.release(); mp_bkey.release();
         bar.release(); rec_time.release(); rec_count.release(); rec_tmpl.release(); rec_slot.release(); rec_amp.release();
         rec_pc.release(); B0T.release(); B0T16lo.release(); Up16.release(); Up16lo.release();
         B0T_hi.release(); B0T_lo.release(); Up_hi.release(); Up_lo.release();

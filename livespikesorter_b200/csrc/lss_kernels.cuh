@@ -162,7 +162,8 @@ struct MPArgs {
     const float* cmaxr = nullptr;           // [T(spike template), T(row)] max |ctc| over lags
     unsigned long long* bkey = nullptr;     // [nb, ldk] per block and column: max (Cf bits << 32 | ~t)
     float* bmin = nullptr;                  // [nb, ldk] per block and column: min |B|
-    unsigned int* work = nullptr;           // [max_rounds + 1] update work counters, zero at launch
+    const int32_t* band_lo = nullptr;       // [T] first / last row block a spike template's ctc can reach
+    const int32_t* band_hi = nullptr;       //     (a cost estimate for the work split only)
 };
 enum : int32_t { STATUS_TIMEOUT = 1, STATUS_CAPACITY = 2, STATUS_LIST = 4 };
 cudaError_t launch_mp(MPArgs a, int grid, cudaStream_t s);

@@ -34,9 +34,10 @@
 // Round structure, work split and bounded grid barriers follow k_mp: the peak
 // phase owns W consecutive columns per CTA; the update phase prefix-sums the
 // per-CTA peak counts for the round's time order; update work items are
-// handed to warps a few at a time from a global counter per round, and a warp
-// runs the rows of an item's processed blocks through one software pipeline;
-// every wait is bounded (STATUS_TIMEOUT).
+// split into per-CTA slices of equal estimated cost (template bands) and
+// handed to the CTA's warps through a shared counter, and a warp runs the
+// rows of an item's processed blocks through one software pipeline; every
+// wait is bounded (STATUS_TIMEOUT).
 #include "lss_kernels.cuh"
 #include "mp_common.cuh"
 
@@ -50,7 +51,7 @@ constexpr int MPB_THREADS = 512;
 constexpr int MPB_MAX_GRID = 1024;
 constexpr int MPB_GROUP = 4;  // row blocks per update work item
 constexpr int MPB_SPK = 3;    // spikes of a chunk's list that get row masks
-constexpr int MPB_GRAB = 4;   // update work items a warp takes from the round's counter at a time
+constexpr int MPB_MAX_SPK = 2048;  // spikes per round the cost-balanced split holds (else: equal item counts)
 constexpr unsigned FULL = 0xffffffffu;
 
 // 2^(e - 25) for v in [2^e, 2^(e+1)) (v >= 0): any |d| below it leaves
@@ -85,7 +86,7 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
     extern __shared__ float smem[];
     __shared__ int s_pref[MPB_MAX_GRID + 1];
     __shared__ int s_wcnt[MPB_THREADS / 32];
-    __shared__ int s_cnt, s_total;
+    __shared__ int s_cnt, s_total, s_next, s_end;
 
     const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
@@ -99,6 +100,8 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
     float* s_nm = smem + 2 * W + 2 * nt;                      // [T]
     float* s_inv = s_nm + T;                                  // [T]
     int* s_perm = reinterpret_cast<int*>(s_inv + T);          // [nb * MPB_ROWS]
+    int* s_cost = s_perm + nb * MPB_ROWS;                     // [MPB_MAX_SPK] spike costs, then their prefix
+    int* s_band = s_cost + MPB_MAX_SPK;                       // [MPB_MAX_SPK] band lo | hi << 16 per spike
     for (int t = tid; t < T; t += MPB_THREADS) {
         const float v = __ldg(a.nm + t);
         s_nm[t] = v;
@@ -248,14 +251,86 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
             }
             if (b == 0 && tid == 0) a.round_start[r] = base;
         }
+        // ---- this CTA's share of the update items, balanced by estimated cost:
+        // an item (spike q, chunk ch, group g) costs 1 (its decisions) plus 4
+        // per block of the group inside spike q's template band (the blocks
+        // its cross-correlations can reach); every CTA prefix-sums the spikes'
+        // costs and takes the items of an equal slice of the total
+        if (total <= MPB_MAX_SPK) {
+            for (int q = tid; q < total; q += MPB_THREADS) {
+                int lo2 = 0, hi2 = G;
+                while (hi2 - lo2 > 1) {
+                    const int m = (lo2 + hi2) >> 1;
+                    if (s_pref[m] <= q) lo2 = m; else hi2 = m;
+                }
+                const int y = __ldcg(a.blk_y + lo2 * W + (q - s_pref[lo2]));
+                const int bl = __ldg(a.band_lo + y), bh = __ldg(a.band_hi + y);
+                s_band[q] = (bl & 0xFFFF) | (bh << 16);
+                s_cost[q] = nch * (ngr + 4 * max(0, bh - bl + 1));
+            }
+            __syncthreads();
+            // inclusive prefix of s_cost[0, total): 4 consecutive entries per thread
+            {
+                int v4[4], sum = 0;
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int q = 4 * tid + u;
+                    v4[u] = q < total ? s_cost[q] : 0;
+                    sum += v4[u];
+                }
+                const int inc = warp_inc_scan(sum, lane);
+                if (lane == 31) s_wcnt[warp] = inc;
+                __syncthreads();
+                if (warp == 0) {
+                    const int wc = (lane < MPB_THREADS / 32) ? s_wcnt[lane] : 0;
+                    const int winc = warp_inc_scan(wc, lane);
+                    if (lane < MPB_THREADS / 32) s_wcnt[lane] = winc - wc;
+                }
+                __syncthreads();
+                int run = s_wcnt[warp] + inc - sum;
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int q = 4 * tid + u;
+                    run += v4[u];
+                    if (q < total) s_cost[q] = run;
+                }
+            }
+            __syncthreads();
+            if (tid == 0) {
+                const int64_t ctot = s_cost[total - 1];
+                // first item whose cumulative cost exceeds c
+                auto item_at = [&](int64_t c) -> int {
+                    if (c >= ctot) return items;
+                    int lo2 = 0, hi2 = total - 1;  // first q with s_cost[q] > c
+                    while (lo2 < hi2) {
+                        const int m = (lo2 + hi2) >> 1;
+                        if (s_cost[m] > c) hi2 = m; else lo2 = m + 1;
+                    }
+                    int64_t acc = lo2 > 0 ? s_cost[lo2 - 1] : 0;
+                    const int bl = s_band[lo2] & 0xFFFF, bh = s_band[lo2] >> 16;
+                    for (int k = 0; k < per_spike; ++k) {
+                        const int g0 = (k % ngr) * MPB_GROUP;
+                        acc += 1 + 4 * max(0, min(bh, g0 + MPB_GROUP - 1) - max(bl, g0) + 1);
+                        if (acc > c) return lo2 * per_spike + k;
+                    }
+                    return (lo2 + 1) * per_spike;
+                };
+                s_next = item_at(ctot * b / G);
+                s_end = (b == G - 1) ? items : item_at(ctot * (b + 1) / G);
+            }
+        } else if (tid == 0) {
+            const int per_cta = (items + G - 1) / G;
+            s_next = min(items, b * per_cta);
+            s_end = min(items, (b + 1) * per_cta);
+        }
+        __syncthreads();
         {
             // Work items (spike q, chunk ch, group g): the columns of spike q's
             // segment [max(x_q - nt, x_{q-1} + nt + 1), x_q + nt], 32 at a time
-            // (lane = column), and the row blocks g*MPB_GROUP.. of the group.
-            // Their cost varies from nothing to MPB_GROUP processed blocks, so
-            // warps take MPB_GRAB consecutive items at a time from the round's
-            // global counter (the next grab is in flight while a grab is
-            // worked). Lane L holds spike q - 1 + L of the round.
+            // (lane = column), and the row blocks g*MPB_GROUP.. of the group;
+            // the CTA's warps take them from a shared counter. Lane L holds
+            // spike q - 1 + L of the round.
+            const int it_end = s_end;
             auto fetch = [&](int q2, int& fx, int& fy, float& fa) {
                 const int j = q2 - 1 + lane;
                 fx = INT_MAX;
@@ -275,15 +350,11 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
             };
             int x = INT_MAX, y = 0, cur_q = -1;
             float amp = 0.f;
-            unsigned grab = 0;
-            if (lane == 0) grab = atomicAdd(a.work + r, 1u);
-            grab = __shfl_sync(FULL, grab, 0);
             for (;;) {
-                const int it0 = (int)grab * MPB_GRAB;
-                if (it0 >= items) break;
-                unsigned next = 0;
-                if (lane == 0) next = atomicAdd(a.work + r, 1u);
-                for (int it = it0; it < min(items, it0 + MPB_GRAB); ++it) {
+                int it = 0;
+                if (lane == 0) it = atomicAdd(&s_next, 1);
+                it = __shfl_sync(FULL, it, 0);
+                if (it >= it_end) break;
                 const int q = it / per_spike, rem = it - q * per_spike, ch = rem / ngr, g = rem - ch * ngr;
                 if (q != cur_q) {
                     cur_q = q;
@@ -445,8 +516,6 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
                         }
                     }
                 }
-                }
-                grab = __shfl_sync(FULL, next, 0);
             }
         }
         base += total;
@@ -477,11 +546,11 @@ int mp_blocks_max_grid(int device) {
 
 static size_t mpb_smem_bytes(int cols_per_blk, int nt, int T, int nb) {
     return sizeof(float) * ((size_t)cols_per_blk + 2 * nt) + sizeof(int) * (size_t)cols_per_blk +
-           sizeof(float) * 2 * (size_t)T + sizeof(int) * (size_t)nb * MPB_ROWS + 16;
+           sizeof(float) * 2 * (size_t)T + sizeof(int) * (size_t)nb * MPB_ROWS + sizeof(int) * 2 * MPB_MAX_SPK + 16;
 }
 
 cudaError_t launch_mp_blocks(MPArgs a, int grid, cudaStream_t s) {
-    if (grid > MPB_MAX_GRID || !a.perm || !a.cmaxr || !a.bkey || !a.bmin || !a.work ||
+    if (grid > MPB_MAX_GRID || !a.perm || !a.cmaxr || !a.bkey || !a.bmin || !a.band_lo || !a.band_hi ||
         a.nb != (a.T + MPB_ROWS - 1) / MPB_ROWS)
         return cudaErrorInvalidValue;
     const size_t smem = mpb_smem_bytes(a.cols_per_blk, a.nt, a.T, a.nb);
