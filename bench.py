@@ -314,9 +314,9 @@ def run_b200(args):
     if top == 'mp_ms':
         ach = mp_bytes / (mean_st['mp_ms'] / 1e3) / 1e9
         roof = {'kernel': 'k_mp (matching pursuit)', 'bound': 'hbm', 'achieved': ach, 'peak': hbm, 'unit': 'GB/s',
-                'frac': ach / hbm, 'traffic': profile_traffic('k_mp_384ch_400t.md') if T == 400 else None,
+                'frac': ach / hbm, 'traffic': profile_traffic(f'k_mp_384ch_{T}t.md'),
                 'traffic_source': 'ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of this workload '
-                                  '(profiles/k_mp_384ch_400t.md)',
+                                  f'(profiles/k_mp_384ch_{T}t.md)',
                 'algorithmic_bytes': mp_bytes, 'peak_source': src}
     else:
         ach = gemm_flops / (mean_st['score_ms'] / 1e3) / 1e12

@@ -89,7 +89,8 @@ __global__ void __launch_bounds__(MP_THREADS, 1) k_mp(MPArgs a) {
         }
     }
     if (!grid_sync(a.bar, a.status)) return;
-    PhaseClock clk;
+    __shared__ unsigned long long s_clk[5];
+    PhaseClock clk{s_clk};
     if (tid == 0) clk.start();
     int base = 0;
     int r = 0;
@@ -287,27 +288,17 @@ __global__ void __launch_bounds__(MP_THREADS, 1) k_mp(MPArgs a) {
                 int t = t0;
                 // software pipelined: the next eight rows' loads are issued
                 // before the current eight are updated (the rows of a column
-                // belong to this lane alone)
-                float v[8], w0[8], w1[8];
-                if (t + 8 <= t1) {
+                // belong to this lane alone); two buffers used alternately, so
+                // no register copy has to wait for loads in flight
+                auto issue = [&](int dt, float (&lv)[8], float (&l0)[8], float (&l1)[8]) {
 #pragma unroll
-                    for (int u = 0; u < 8; ++u) v[u] = ld_keep(bp + u * ldb, pk);
+                    for (int u = 0; u < 8; ++u) lv[u] = ld_keep(bp + (dt + u) * ldb, pk);
 #pragma unroll
-                    for (int u = 0; u < 8; ++u) w0[u] = p0 ? ld_stream(p0 + u * L2, ps) : 0.f;
+                    for (int u = 0; u < 8; ++u) l0[u] = p0 ? ld_stream(p0 + (dt + u) * L2, ps) : 0.f;
 #pragma unroll
-                    for (int u = 0; u < 8; ++u) w1[u] = p1 ? ld_stream(p1 + u * L2, ps) : 0.f;
-                }
-                for (; t + 8 <= t1; t += 8) {
-                    float nv[8], nw0[8], nw1[8];
-                    const bool more = t + 16 <= t1;
-                    if (more) {
-#pragma unroll
-                        for (int u = 0; u < 8; ++u) nv[u] = ld_keep(bp + (8 + u) * ldb, pk);
-#pragma unroll
-                        for (int u = 0; u < 8; ++u) nw0[u] = p0 ? ld_stream(p0 + (8 + u) * L2, ps) : 0.f;
-#pragma unroll
-                        for (int u = 0; u < 8; ++u) nw1[u] = p1 ? ld_stream(p1 + (8 + u) * L2, ps) : 0.f;
-                    }
+                    for (int u = 0; u < 8; ++u) l1[u] = p1 ? ld_stream(p1 + (dt + u) * L2, ps) : 0.f;
+                };
+                auto update = [&](const float (&v)[8], const float (&w0)[8], const float (&w1)[8]) {
 #pragma unroll
                     for (int u = 0; u < 8; ++u) {
                         float xv = v[u];
@@ -319,14 +310,16 @@ __global__ void __launch_bounds__(MP_THREADS, 1) k_mp(MPArgs a) {
                     bp += 8 * ldb;
                     if (p0) p0 += 8 * L2;
                     if (p1) p1 += 8 * L2;
-                    if (more) {
-#pragma unroll
-                        for (int u = 0; u < 8; ++u) {
-                            v[u] = nv[u];
-                            w0[u] = nw0[u];
-                            w1[u] = nw1[u];
-                        }
-                    }
+                    t += 8;
+                };
+                float va[8], w0a[8], w1a[8], vb[8], w0b[8], w1b[8];
+                if (t + 8 <= t1) issue(0, va, w0a, w1a);
+                while (t + 8 <= t1) {
+                    if (t + 16 <= t1) issue(8, vb, w0b, w1b);
+                    update(va, w0a, w1a);
+                    if (t + 8 > t1) break;
+                    if (t + 16 <= t1) issue(8, va, w0a, w1a);
+                    update(vb, w0b, w1b);
                 }
                 for (; t < t1; ++t, bp += ldb) {
                     float xv = ld_keep(bp, pk);

@@ -137,7 +137,8 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
         }
     }
     if (!grid_sync(a.bar, a.status)) return;
-    PhaseClock clk;
+    __shared__ unsigned long long s_clk[5];
+    PhaseClock clk{s_clk};
     if (tid == 0) clk.start();
 
     int base = 0;

@@ -79,24 +79,29 @@ __device__ __forceinline__ float ld_stream(const float* a, uint64_t pol) {
 // waiting at the grid barrier after it, in the update phase and waiting after
 // it, summed over the rounds; added to phase[0..3] (sums over CTAs) with the
 // slowest CTA's peak and update totals in phase[4], phase[5].
+// The clock lives in shared memory (s: time of the last lap, then the four
+// sums), so that no register is held for it across the rounds.
 struct PhaseClock {
-    unsigned long long t = 0, acc[4] = {0, 0, 0, 0};
+    unsigned long long* s;  // [5] shared
     __device__ __forceinline__ static unsigned long long now() {
         unsigned long long v;
         asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(v));
         return v;
     }
-    __device__ __forceinline__ void start() { t = now(); }
+    __device__ __forceinline__ void start() {
+        s[0] = now();
+        for (int i = 1; i < 5; ++i) s[i] = 0;
+    }
     __device__ __forceinline__ void lap(int i) {
         const unsigned long long u = now();
-        acc[i] += u - t;
-        t = u;
+        s[1 + i] += u - s[0];
+        s[0] = u;
     }
     __device__ __forceinline__ void flush(unsigned long long* phase) const {
         if (!phase) return;
-        for (int i = 0; i < 4; ++i) atomicAdd(phase + i, acc[i]);
-        atomicMax(phase + 4, acc[0]);
-        atomicMax(phase + 5, acc[2]);
+        for (int i = 0; i < 4; ++i) atomicAdd(phase + i, s[1 + i]);
+        atomicMax(phase + 4, s[1]);
+        atomicMax(phase + 5, s[3]);
     }
 };
 

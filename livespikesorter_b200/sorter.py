@@ -296,9 +296,9 @@ class Sorter:
         return dict(rounds=s.rounds, spikes=s.spikes, recheck_columns=s.recheck_columns,
                     recheck_flips=s.recheck_flips, recheck_rescored=s.recheck_rescored, launches=s.launches,
                     mp_items=s.mp_items, mp_items_updated=s.mp_items_updated,
-                    mp_phases_ms={k: getattr(s, k) * 1e-6 for k in ('mp_peak_ns', 'mp_peak_wait_ns', 'mp_update_ns',
-                                                                       'mp_update_wait_ns', 'mp_peak_max_ns',
-                                                                       'mp_update_max_ns')})
+                    mp_phases_ms={k[3:-3]: getattr(s, k) * 1e-6 for k in ('mp_peak_ns', 'mp_peak_wait_ns',
+                                                                             'mp_update_ns', 'mp_update_wait_ns',
+                                                                             'mp_peak_max_ns', 'mp_update_max_ns')})
 
     def set_templates(self, U, wPCA=None):
         """Swap in new templates (same shapes) and optionally a new temporal
