@@ -155,29 +155,14 @@ int lss::rebuild_mp_blocks(lss_handle* h) {
     std::vector<int32_t> perm((size_t)nb * MPB_ROWS, -1);
     for (int t = 0; t < T; ++t) perm[t] = t;
     std::stable_sort(perm.begin(), perm.begin() + T, [&](int32_t i, int32_t j) { return com[i] < com[j]; });
+    std::vector<int32_t> rowof(T);
+    for (int r = 0; r < T; ++r) rowof[perm[r]] = r;
     CK(cudaMemcpy(h->mp_perm.p, perm.data(), perm.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
-    CK(launch_ctc_row_max(h->ctcP.p, T, 2 * h->nt + 1, h->mp_cmaxr.p, 0));
+    CK(cudaMemcpy(h->mp_rowof.p, rowof.data(), T * sizeof(int32_t), cudaMemcpyHostToDevice));
+    // the rounds read each spike template's ctc rows in the score rows' order
+    CK(launch_permute_ctc(h->ctcP.p, h->mp_perm.p, T, 2 * h->nt + 1, h->mp_ctcq.p, 0));
+    CK(launch_ctc_row_max(h->mp_ctcq.p, T, 2 * h->nt + 1, h->mp_cmaxr.p, 0));
     CK(cudaDeviceSynchronize());
-    // each spike template's band of row blocks: blocks holding a row t whose
-    // max |ctc| reaches 2^-30 ||U_t|| (about where a unit-amplitude term stops
-    // being a no-op on noise-level scores); used only to balance the work
-    {
-        std::vector<float> cm((size_t)T * T), nmv(T);
-        CK(cudaMemcpy(cm.data(), h->mp_cmaxr.p, cm.size() * sizeof(float), cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(nmv.data(), h->nm.p, T * sizeof(float), cudaMemcpyDeviceToHost));
-        std::vector<int32_t> blo(T, 1), bhi(T, 0);
-        for (int y = 0; y < T; ++y)
-            for (int i = 0; i < T; ++i) {
-                const int t = perm[i];
-                if (cm[(size_t)y * T + t] >= std::ldexp(1.0, -30) * std::sqrt((double)nmv[t])) {
-                    const int bb = i / MPB_ROWS;
-                    if (blo[y] > bhi[y]) blo[y] = bb;
-                    bhi[y] = bb;
-                }
-            }
-        CK(cudaMemcpy(h->mp_band_lo.p, blo.data(), T * sizeof(int32_t), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(h->mp_band_hi.p, bhi.data(), T * sizeof(int32_t), cudaMemcpyHostToDevice));
-    }
     h->stats.launches += 1;
     return LSS_OK;
 }
@@ -451,10 +436,13 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
     h->mp_nb = (T + MPB_ROWS - 1) / MPB_ROWS;
     ALLOC(mp_perm, (size_t)h->mp_nb * MPB_ROWS);
     ALLOC(mp_cmaxr, (size_t)T * T);
+    ALLOC(mp_rowof, T);
+    ALLOC(mp_ctcq, (size_t)T * T * L2);
     ALLOC(mp_bkey, (size_t)h->mp_nb * ld);
     ALLOC(mp_phase, 6);
-    ALLOC(mp_band_lo, T);
-    ALLOC(mp_band_hi, T);
+    // 4 int4 per list entry
+    ALLOC(mp_ent, (size_t)mp_blocks_list_entries(ld, nt, T, h->mp_grid) * 4);
+    ALLOC(mp_ent_cnt, (size_t)h->mp_grid);
     ALLOC(mp_bmin, (size_t)h->mp_nb * ld);
     ALLOC(blk_cnt, 4096);
     ALLOC(blk_x, ld);
@@ -716,7 +704,8 @@ int lss::run_ingest(lss_handle* h, const int16_t* src, const IngestMap& map, flo
 }
 
 int lss::run_scores(lss_handle* h, const float* X, int64_t ldx, int64_t N, float* B, cudaStream_t s,
-                   bool* maxima_ready, bool folded) {
+                   bool* maxima_ready, bool folded, bool rows_for_mp) {
+    const int32_t* rowof = (rows_for_mp && h->mp_skip) ? h->mp_rowof.p : nullptr;
     if (h->cfg.precision == LSS_PREC_BF16_RECHECK) {
         CK(launch_pca_proj_t(X, ldx, h->C, N, h->wpca.p, h->K, h->nt, h->B0T.p, h->B0T16lo.p, h->CKpad, s, h->pn2.p));
         h->mark(5, s);
@@ -730,6 +719,7 @@ int lss::run_scores(lss_handle* h, const float* X, int64_t ldx, int64_t N, float
         ex.eps = (float)(3.0 * std::ldexp(1.0, -18) * 1.01 + 2.0 * h->CKpad * std::ldexp(1.0, -24));
         ex.cf_lo = h->cf_lo.p;
         ex.cf_hi = h->cf_hi.p;
+        ex.rowof = rowof;
         CK(launch_score_tc_bf16x3(h->B0T.p, h->B0T16lo.p, h->CKpad, (int)N, folded ? h->Uw16.p : h->Up16.p,
                                   folded ? h->Uw16lo.p : h->Up16lo.p, h->T, h->CKpad, h->nm.p, B, h->ld, h->cfmax.p,
                                   h->imax.p, h->nt, h->status.p, h->sm_count, s, ex));
@@ -746,6 +736,7 @@ int lss::run_scores(lss_handle* h, const float* X, int64_t ldx, int64_t N, float
         ex2.map_rows = 1;
         ex2.count_dev = h->rc_count.p;
         ex2.ncols = (int)N;
+        ex2.rowof = rowof;
         const int max_rows = (int)((N + 127) / 128 * 128);
         CK(launch_score_tc_tf32x3(h->Pc_hi.p, h->Pc_lo.p, h->CKpad, max_rows, folded ? h->Uw_hi.p : h->Up_hi.p,
                                   folded ? h->Uw_lo.p : h->Up_lo.p, h->T, h->CKpad, h->nm.p, B, h->ld, h->cfmax.p,
@@ -767,6 +758,7 @@ int lss::run_scores(lss_handle* h, const float* X, int64_t ldx, int64_t N, float
     h->mark(5, s);
     TcExtra ex;
     ex.keys = h->colkey.p;  // free until the rounds start (they clear it)
+    ex.rowof = rowof;
     CK(launch_score_tc_tf32x3(h->B0T_hi.p, h->B0T_lo.p, h->CKpad, (int)N, folded ? h->Uw_hi.p : h->Up_hi.p,
                               folded ? h->Uw_lo.p : h->Up_lo.p, h->T, h->CKpad, h->nm.p, B, h->ld, h->cfmax.p,
                               h->imax.p, h->nt, h->status.p, h->sm_count, s, ex));
@@ -817,8 +809,10 @@ int lss::enqueue_mp(lss_handle* h, int64_t N, cudaStream_t s, bool maxima_ready)
         a.cmaxr = h->mp_cmaxr.p;
         a.bkey = h->mp_bkey.p;
         a.bmin = h->mp_bmin.p;
-        a.band_lo = h->mp_band_lo.p;
-        a.band_hi = h->mp_band_hi.p;
+        a.ctcP = h->mp_ctcq.p;
+        a.ment = h->mp_ent.p;
+        a.ment_cnt = h->mp_ent_cnt.p;
+        a.ment_cap = (int32_t)std::min<int64_t>(h->mp_ent.n / 4 / G, INT32_MAX);
         a.init_cols = 1;  // the rounds take their block maxima from the field itself
         CK(launch_mp_blocks(a, G, s));
     } else {
@@ -1003,7 +997,7 @@ int lss_scores(lss_handle* h, const float* X_dev, int64_t N, float* B_dev, void*
     CK(cudaMemcpy2DAsync(h->X.p, h->ld * sizeof(float), X_dev, N * sizeof(float), N * sizeof(float), h->C,
                          cudaMemcpyDeviceToDevice, s));
     CK(cudaMemsetAsync(h->status.p, 0, sizeof(int32_t), s));
-    int rc = run_scores(h, h->X.p, h->ld, N, h->B.p, s);
+    int rc = run_scores(h, h->X.p, h->ld, N, h->B.p, s, nullptr, false, /*rows_for_mp=*/false);
     if (rc) return rc;
     CK(cudaMemcpy2DAsync(B_dev, N * sizeof(float), h->B.p, h->ld * sizeof(float), N * sizeof(float), h->T,
                          cudaMemcpyDeviceToDevice, s));
@@ -1064,8 +1058,13 @@ int lss_match_scores(lss_handle* h, const float* B_dev, int64_t N, int64_t* st_d
     CK(cudaSetDevice(h->cfg.device));
     cudaStream_t s = (cudaStream_t)stream;
     CK(wait_mixing(h, s));
-    CK(cudaMemcpy2DAsync(h->B.p, h->ld * sizeof(float), B_dev, N * sizeof(float), N * sizeof(float), h->T,
-                         cudaMemcpyDeviceToDevice, s));
+    if (h->mp_skip) {  // the block-skipping rounds read the rows in probe order
+        CK(launch_gather_rows(B_dev, N, h->mp_perm.p, h->T, N, h->B.p, h->ld, s));
+        h->stats.launches += 1;
+    } else {
+        CK(cudaMemcpy2DAsync(h->B.p, h->ld * sizeof(float), B_dev, N * sizeof(float), N * sizeof(float), h->T,
+                             cudaMemcpyDeviceToDevice, s));
+    }
     CK(cudaMemsetAsync(h->status.p, 0, sizeof(int32_t), s));
     return match_common(h, N, nullptr, st_dev, amps_dev, nullptr, capacity, n_spikes, s);
 }

@@ -72,7 +72,10 @@ struct lss_handle {
     DevBuf<float> mp_cmaxr, mp_bmin;
     DevBuf<unsigned long long> mp_bkey;
     DevBuf<unsigned long long> mp_phase;         // [6] phase clock of the rounds kernel
-    DevBuf<int32_t> mp_band_lo, mp_band_hi;      // [T] row-block band of each spike template (work estimate)
+    DevBuf<int4> mp_ent;                         // block-skipping rounds: per-CTA lists of blocks to process
+    DevBuf<int32_t> mp_ent_cnt;                  // [grid] entries per list
+    DevBuf<int32_t> mp_rowof;                    // [T] score row of each template in probe order
+    DevBuf<float> mp_ctcq;                       // [T, T, 2nt+1] ctc rows in probe order
     // BF16 path (BF16x3 GEMM): projection and templates as bf16 hi / lo splits
     DevBuf<__nv_bfloat16> B0T, B0T16lo, Up16, Up16lo;
     DevBuf<float> B0T_hi, B0T_lo, Up_hi, Up_lo;  // FP32 path (3xTF32): tf32 hi/lo splits
@@ -161,7 +164,7 @@ struct lss_handle {
         tF.release(); iCC.release(); iU.release(); cfmax.release(); imax.release(); blk_cnt.release();
         blk_x.release(); blk_y.release(); sp_x.release(); sp_y.release(); sp_round.release();
         round_start.release(); counters.release(); status.release(); sp_amp.release(); blk_amp.release(); colkey.release();
-        mp_perm.release(); mp_cmaxr.release(); mp_phase.release(); mp_band_lo.release(); mp_band_hi.release(); mp_bmin.release(); mp_bkey.release();
+        mp_perm.release(); mp_cmaxr.release(); mp_phase.release(); mp_ent.release(); mp_ent_cnt.release(); mp_rowof.release(); mp_ctcq.release(); mp_bmin.release(); mp_bkey.release();
         bar.release(); rec_time.release(); rec_count.release(); rec_tmpl.release(); rec_slot.release(); rec_amp.release();
         rec_pc.release(); B0T.release(); B0T16lo.release(); Up16.release(); Up16lo.release();
         B0T_hi.release(); B0T_lo.release(); Up_hi.release(); Up_lo.release();
@@ -196,9 +199,10 @@ namespace lss {
 int run_ingest(lss_handle* h, const int16_t* src, const IngestMap& map, float* Xout, cudaStream_t s,
                const float** pre_out);
 // Projection and score GEMM of X [C, ldx] into B; *maxima_ready when the
-// column maxima were fused into the GEMM.
+// column maxima were fused into the GEMM. rows_for_mp: B rows in the order
+// the selected rounds kernel reads (probe order for the block-skipping one).
 int run_scores(lss_handle* h, const float* X, int64_t ldx, int64_t N, float* B, cudaStream_t s,
-               bool* maxima_ready = nullptr, bool folded = false);
+               bool* maxima_ready = nullptr, bool folded = false, bool rows_for_mp = true);
 // Whitening-folded template operands from U and Mw (after a template or drift change).
 int rebuild_uw(lss_handle* h);
 // Orders stream s after the last template / drift rebuild (no host wait).

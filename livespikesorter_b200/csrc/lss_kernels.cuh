@@ -84,6 +84,9 @@ struct TcExtra {
     float eps = 0.f;
     float* cf_lo = nullptr;
     float* cf_hi = nullptr;
+    // score rows in another order: template t's row of B is rowof[t] (the
+    // block-skipping rounds keep rows in probe order); null: row t
+    const int32_t* rowof = nullptr;
 };
 // B[t, s] (row stride ldb) = sum_kk B0T[s, kk] * Up[t, kk] with B0T [N, ldk] and Up [Tpad, CKpad]
 // bf16, CKpad a multiple of 64; also writes the column maxima cfmax/imax of Cf.
@@ -155,15 +158,18 @@ struct MPArgs {
     int32_t cols_per_blk;     // W
     int32_t init_cols;        // 1: compute column maxima of B before round 0
     unsigned long long* phase = nullptr;    // [6] phase clock of the rounds (PhaseClock), zero at launch; may be null
-    // block-skipping rounds (mp_blocks.cu) only: template rows are grouped in
-    // blocks of MPB_ROWS (rows of templates close on the probe, by perm)
-    const int32_t* perm = nullptr;          // [nb * MPB_ROWS] template of each block row, -1 past T
+    // block-skipping rounds (mp_blocks.cu) only: the score rows of B are in
+    // probe order (row r holds template perm[r]) and grouped in blocks of
+    // MPB_ROWS; ctcP then points at ctcQ [T(spike template), T(row), 2nt+1]
+    const int32_t* perm = nullptr;          // [nb * MPB_ROWS] template of each row, -1 past T
     int32_t nb = 0;                         // row blocks
     const float* cmaxr = nullptr;           // [T(spike template), T(row)] max |ctc| over lags
     unsigned long long* bkey = nullptr;     // [nb, ldk] per block and column: max (Cf bits << 32 | ~t)
     float* bmin = nullptr;                  // [nb, ldk] per block and column: min |B|
-    const int32_t* band_lo = nullptr;       // [T] first / last row block a spike template's ctc can reach
-    const int32_t* band_hi = nullptr;       //     (a cost estimate for the work split only)
+    int4* ment = nullptr;                   // [G * ment_cap * 4] per-CTA lists of blocks to process (64-byte
+                                            // entries); null: blocks are processed where they are decided
+    int32_t* ment_cnt = nullptr;            // [G] entries per list
+    int32_t ment_cap = 0;                   // entries per list
 };
 enum : int32_t { STATUS_TIMEOUT = 1, STATUS_CAPACITY = 2, STATUS_LIST = 4 };
 cudaError_t launch_mp(MPArgs a, int grid, cudaStream_t s);
@@ -172,8 +178,17 @@ cudaError_t launch_mp(MPArgs a, int grid, cudaStream_t s);
 constexpr int MPB_ROWS = 32;
 cudaError_t launch_mp_blocks(MPArgs a, int grid, cudaStream_t s);
 int mp_blocks_max_grid(int device);
+// entries the lists of a grid of `grid` CTAs hold in all (ment_cap = that / grid
+// keeps every round of at most (N + nt) / (nt + 1) peaks in list mode)
+int64_t mp_blocks_list_entries(int64_t N, int nt, int T, int grid);
 // cmaxr[y, t] = max over lags of |ctcP[y, t, :]| (infinite where a lag is NaN)
 cudaError_t launch_ctc_row_max(const float* ctcP, int32_t T, int32_t L2, float* cmaxr, cudaStream_t s);
+// ctcQ[y, r, :] = ctcP[y, perm[r], :] (the block-skipping rounds' copy, rows in probe order)
+cudaError_t launch_permute_ctc(const float* ctcP, const int32_t* perm, int32_t T, int32_t L2, float* ctcQ,
+                               cudaStream_t s);
+// dst row r = src row perm[r], N columns
+cudaError_t launch_gather_rows(const float* src, int64_t lds, const int32_t* perm, int32_t rows, int64_t N,
+                               float* dst, int64_t ldd, cudaStream_t s);
 int mp_max_grid(int device);
 void set_thread_error(const char* msg);
 // true when kernels on `device` may dereference p (that device's memory,

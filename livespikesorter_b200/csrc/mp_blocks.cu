@@ -31,13 +31,19 @@
 // interleaved passes per round (last even spike's term, then the last odd
 // spike's, per element).
 //
-// Round structure, work split and bounded grid barriers follow k_mp: the peak
-// phase owns W consecutive columns per CTA; the update phase prefix-sums the
-// per-CTA peak counts for the round's time order; update work items are
-// split into per-CTA slices of equal estimated cost (template bands) and
-// handed to the CTA's warps through a shared counter, and a warp runs the
-// rows of an item's processed blocks through one software pipeline; every
-// wait is bounded (STATUS_TIMEOUT).
+// Score rows are kept in probe order (row r holds template perm[r]; the score
+// GEMM writes them so, and ctc comes as a copy with each spike template's
+// rows in that order), so a block's rows are contiguous.
+//
+// Round structure and bounded grid barriers follow k_mp: the peak phase owns
+// W consecutive columns per CTA; the update phase prefix-sums the per-CTA
+// peak counts for the round's time order. The update then runs in two steps
+// split by a grid barrier: the decisions for every (spike segment, 32-column
+// chunk, group of blocks) item, an equal range of items per warp, append the
+// blocks to process to their CTA's list; then every warp takes an equal range
+// of all lists' entries and streams their rows through a ring of stages in
+// shared memory filled by asynchronous copies a few batches ahead. Every wait
+// is bounded (STATUS_TIMEOUT).
 #include "lss_kernels.cuh"
 #include "mp_common.cuh"
 
@@ -51,7 +57,9 @@ constexpr int MPB_THREADS = 512;
 constexpr int MPB_MAX_GRID = 1024;
 constexpr int MPB_GROUP = 4;  // row blocks per update work item
 constexpr int MPB_SPK = 3;    // spikes of a chunk's list that get row masks
-constexpr int MPB_MAX_SPK = 2048;  // spikes per round the cost-balanced split holds (else: equal item counts)
+constexpr int WPB = MPB_THREADS / 32;  // warps per CTA
+constexpr int BPB = MPB_ROWS / 8;     // 8-row batches per block
+static_assert(MPB_SPK == 3, "list entries hold three spikes");
 constexpr unsigned FULL = 0xffffffffu;
 
 // 2^(e - 25) for v in [2^e, 2^(e+1)) (v >= 0): any |d| below it leaves
@@ -62,34 +70,40 @@ __device__ __forceinline__ float quarter_ulp(float v) {
     return (e > 25u && e < 255u) ? __uint_as_float((e - 25u) << 23) : 0.f;
 }
 
-// Running max of Cf over rows visited in any order: larger Cf first, smaller
-// template index on ties (torch.max's first index). The correctly rounded
-// quotient is formed only for candidates (see ColMax in mp_common.cuh).
-struct ColMaxAny {
+// Running max of Cf over score rows in probe order (row r holds template
+// perm[r]): larger Cf first, smaller template index on ties (torch.max's
+// first index). The correctly rounded quotient is formed only for candidates
+// (see ColMax in mp_common.cuh).
+struct ColMaxRows {
     float best = -1.f;
     float thr = -1.f;
-    int bi = INT_MAX;
-    __device__ __forceinline__ void consider(float b, float nmv, float inv, int t) {
-        const float r = fmaxf(b, 0.f);
-        const float sq = __fmul_rn(r, r);
+    int br = -1;
+    __device__ __forceinline__ void consider(float b, float nmv, float inv, int r, const int* perm) {
+        const float x = fmaxf(b, 0.f);
+        const float sq = __fmul_rn(x, x);
         if (__fmul_rn(sq, inv) < thr) return;
         const float cf = __fdiv_rn(sq, nmv);
-        if (cf > best || (cf == best && t < bi)) {
+        if (cf > best || (cf == best && perm[r] < perm[br])) {
             best = cf;
-            bi = t;
+            br = r;
             thr = (cf >= 1e-30f) ? __fmul_rd(cf, 0.99999952316f) : -1.f;
         }
     }
+    __device__ __forceinline__ unsigned long long key(const int* perm) const {
+        return pack_key(best, br >= 0 ? perm[br] : 0);
+    }
 };
 
+template <int NST>
 __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
     extern __shared__ float smem[];
     __shared__ int s_pref[MPB_MAX_GRID + 1];
     __shared__ int s_wcnt[MPB_THREADS / 32];
-    __shared__ int s_cnt, s_total, s_next, s_end;
+    __shared__ int s_cnt, s_total, s_ecnt;
 
     const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
+    const int NW = G * WPB, gw = b * WPB + warp;  // warps of the grid, this warp's rank
     const int N = a.N, T = a.T, nt = a.nt, L2 = 2 * nt + 1, nb = a.nb;
     const int W = a.cols_per_blk;
     const int lo = min(N, b * W), hi = min(N, lo + W);
@@ -97,17 +111,24 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
 
     float* vals = smem;                                       // [W + 2nt]
     int* ivals = reinterpret_cast<int*>(smem + W + 2 * nt);  // [W]
-    float* s_nm = smem + 2 * W + 2 * nt;                      // [T]
-    float* s_inv = s_nm + T;                                  // [T]
+    // score rows are in probe order: row r holds template perm[r], template t
+    // is row s_rowof[t]; nm and 1/nm by row
+    float* s_nm = smem + 2 * W + 2 * nt;                      // [T] by row
+    float* s_inv = s_nm + T;                                  // [T] by row
     int* s_perm = reinterpret_cast<int*>(s_inv + T);          // [nb * MPB_ROWS]
-    int* s_cost = s_perm + nb * MPB_ROWS;                     // [MPB_MAX_SPK] spike costs, then their prefix
-    int* s_band = s_cost + MPB_MAX_SPK;                       // [MPB_MAX_SPK] band lo | hi << 16 per spike
-    for (int t = tid; t < T; t += MPB_THREADS) {
-        const float v = __ldg(a.nm + t);
-        s_nm[t] = v;
-        s_inv[t] = __frcp_rn(v);
+    int* s_rowof = s_perm + nb * MPB_ROWS;                    // [T]
+    // per warp: NST stages of 3 x 8 rows x 32 columns (16-byte aligned)
+    float* ring = smem + ((2 * W + 2 * nt + 2 * T + nb * MPB_ROWS + T + 3) & ~3);
+    for (int i = tid; i < nb * MPB_ROWS; i += MPB_THREADS) {
+        const int t = __ldg(a.perm + i);
+        s_perm[i] = t;
+        if (i < T) {
+            const float v = __ldg(a.nm + t);
+            s_nm[i] = v;
+            s_inv[i] = __frcp_rn(v);
+            s_rowof[t] = i;
+        }
     }
-    for (int i = tid; i < nb * MPB_ROWS; i += MPB_THREADS) s_perm[i] = __ldg(a.perm + i);
     __syncthreads();
     const uint64_t pk = policy_keep(), ps = policy_stream();
 
@@ -117,22 +138,21 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
         for (int w = tid; w < ncol * nb; w += MPB_THREADS) {
             const int bb = w / ncol, s = lo + (w - bb * ncol);
             const int r0 = bb * MPB_ROWS, nr = min(MPB_ROWS, T - r0);
-            ColMaxAny m;
+            ColMaxRows m;
             float mn = INFINITY;
             for (int r = 0; r < nr; r += 16) {
                 float v[16];
 #pragma unroll
                 for (int u = 0; u < 16; ++u)
-                    v[u] = (r + u < nr) ? ld_keep(a.B + (int64_t)s_perm[r0 + r + u] * ldb + s, pk) : 0.f;
+                    v[u] = (r + u < nr) ? ld_keep(a.B + (int64_t)(r0 + r + u) * ldb + s, pk) : 0.f;
 #pragma unroll
                 for (int u = 0; u < 16; ++u)
                     if (r + u < nr) {
-                        const int t = s_perm[r0 + r + u];
                         mn = fminf(mn, fabsf(v[u]));
-                        m.consider(v[u], s_nm[t], s_inv[t], t);
+                        m.consider(v[u], s_nm[r0 + r + u], s_inv[r0 + r + u], r0 + r + u, s_perm);
                     }
             }
-            a.bkey[bb * ldk + s] = pack_key(m.best, m.bi);
+            a.bkey[bb * ldk + s] = m.key(s_perm);
             a.bmin[bb * ldk + s] = mn;
         }
     }
@@ -171,7 +191,10 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
             }
             vals[p] = v;
         }
-        if (tid == 0) s_cnt = 0;
+        if (tid == 0) {
+            s_cnt = 0;
+            s_ecnt = 0;
+        }
         __syncthreads();
         for (int c0 = lo; c0 < hi; c0 += MPB_THREADS) {
             const int s = c0 + tid;
@@ -197,7 +220,8 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
                 const int y = ivals[s - lo];
                 a.blk_x[lo + k] = s;
                 a.blk_y[lo + k] = y;
-                a.blk_amp[lo + k] = __fdiv_rn(__ldcg(a.B + (int64_t)y * ldb + s), s_nm[y]);
+                const int ry = s_rowof[y];
+                a.blk_amp[lo + k] = __fdiv_rn(__ldcg(a.B + (int64_t)ry * ldb + s), s_nm[ry]);
             }
             __syncthreads();
             if (tid == 0) s_cnt += s_total;
@@ -209,19 +233,20 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
         if (tid == 0) clk.lap(1);
 
         // ---- U: global order of the round's spikes, records, block updates
-        {
+        // s_pref[c] = sum of cnt[0, c) over the grid's CTAs, s_pref[G] = total
+        auto prefix_counts = [&](const int32_t* cnt) {
             int carry = 0;
             for (int c0 = 0; c0 < G; c0 += MPB_THREADS) {
                 const int i = c0 + tid;
-                const int c = (i < G) ? __ldcg(a.blk_cnt + i) : 0;
+                const int c = (i < G) ? __ldcg(cnt + i) : 0;
                 const int inc = warp_inc_scan(c, lane);
                 if (lane == 31) s_wcnt[warp] = inc;
                 __syncthreads();
                 if (warp == 0) {
-                    const int wc = (lane < MPB_THREADS / 32) ? s_wcnt[lane] : 0;
+                    const int wc = (lane < WPB) ? s_wcnt[lane] : 0;
                     const int winc = warp_inc_scan(wc, lane);
-                    if (lane < MPB_THREADS / 32) s_wcnt[lane] = winc - wc;
-                    if (lane == MPB_THREADS / 32 - 1) s_total = winc;
+                    if (lane < WPB) s_wcnt[lane] = winc - wc;
+                    if (lane == WPB - 1) s_total = winc;
                 }
                 __syncthreads();
                 if (i < G) s_pref[i] = carry + s_wcnt[warp] + inc - c;
@@ -230,7 +255,8 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
             }
             if (tid == 0) s_pref[G] = carry;
             __syncthreads();
-        }
+        };
+        prefix_counts(a.blk_cnt);
         const int total = s_pref[G];
         if (total == 0) break;
         if (base + total > a.capacity) {
@@ -252,86 +278,20 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
             }
             if (b == 0 && tid == 0) a.round_start[r] = base;
         }
-        // ---- this CTA's share of the update items, balanced by estimated cost:
-        // an item (spike q, chunk ch, group g) costs 1 (its decisions) plus 4
-        // per block of the group inside spike q's template band (the blocks
-        // its cross-correlations can reach); every CTA prefix-sums the spikes'
-        // costs and takes the items of an equal slice of the total
-        if (total <= MPB_MAX_SPK) {
-            for (int q = tid; q < total; q += MPB_THREADS) {
-                int lo2 = 0, hi2 = G;
-                while (hi2 - lo2 > 1) {
-                    const int m = (lo2 + hi2) >> 1;
-                    if (s_pref[m] <= q) lo2 = m; else hi2 = m;
-                }
-                const int y = __ldcg(a.blk_y + lo2 * W + (q - s_pref[lo2]));
-                const int bl = __ldg(a.band_lo + y), bh = __ldg(a.band_hi + y);
-                s_band[q] = (bl & 0xFFFF) | (bh << 16);
-                s_cost[q] = nch * (ngr + 4 * max(0, bh - bl + 1));
-            }
-            __syncthreads();
-            // inclusive prefix of s_cost[0, total): 4 consecutive entries per thread
-            {
-                int v4[4], sum = 0;
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int q = 4 * tid + u;
-                    v4[u] = q < total ? s_cost[q] : 0;
-                    sum += v4[u];
-                }
-                const int inc = warp_inc_scan(sum, lane);
-                if (lane == 31) s_wcnt[warp] = inc;
-                __syncthreads();
-                if (warp == 0) {
-                    const int wc = (lane < MPB_THREADS / 32) ? s_wcnt[lane] : 0;
-                    const int winc = warp_inc_scan(wc, lane);
-                    if (lane < MPB_THREADS / 32) s_wcnt[lane] = winc - wc;
-                }
-                __syncthreads();
-                int run = s_wcnt[warp] + inc - sum;
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int q = 4 * tid + u;
-                    run += v4[u];
-                    if (q < total) s_cost[q] = run;
-                }
-            }
-            __syncthreads();
-            if (tid == 0) {
-                const int64_t ctot = s_cost[total - 1];
-                // first item whose cumulative cost exceeds c
-                auto item_at = [&](int64_t c) -> int {
-                    if (c >= ctot) return items;
-                    int lo2 = 0, hi2 = total - 1;  // first q with s_cost[q] > c
-                    while (lo2 < hi2) {
-                        const int m = (lo2 + hi2) >> 1;
-                        if (s_cost[m] > c) hi2 = m; else lo2 = m + 1;
-                    }
-                    int64_t acc = lo2 > 0 ? s_cost[lo2 - 1] : 0;
-                    const int bl = s_band[lo2] & 0xFFFF, bh = s_band[lo2] >> 16;
-                    for (int k = 0; k < per_spike; ++k) {
-                        const int g0 = (k % ngr) * MPB_GROUP;
-                        acc += 1 + 4 * max(0, min(bh, g0 + MPB_GROUP - 1) - max(bl, g0) + 1);
-                        if (acc > c) return lo2 * per_spike + k;
-                    }
-                    return (lo2 + 1) * per_spike;
-                };
-                s_next = item_at(ctot * b / G);
-                s_end = (b == G - 1) ? items : item_at(ctot * (b + 1) / G);
-            }
-        } else if (tid == 0) {
-            const int per_cta = (items + G - 1) / G;
-            s_next = min(items, b * per_cta);
-            s_end = min(items, (b + 1) * per_cta);
-        }
-        __syncthreads();
+        // Work items (spike q, chunk ch, group g): the columns of spike q's
+        // segment [max(x_q - nt, x_{q-1} + nt + 1), x_q + nt], 32 at a time
+        // (lane = column), and the row blocks g*MPB_GROUP.. of the group; an
+        // equal range of consecutive items per warp of the grid. An item's
+        // decisions name the blocks to process; in list mode each becomes an
+        // entry of the CTA's list and the lists are processed after a grid
+        // barrier, an equal share of all entries per warp (decisions take one
+        // round trip per item, a processed block four batches of rows, so
+        // separating them balances both); otherwise the item's blocks are
+        // processed where they are decided.
+        const bool use_list =
+            a.ment != nullptr && (int64_t)((items + NW - 1) / NW) * WPB * MPB_GROUP <= (int64_t)a.ment_cap;
         {
-            // Work items (spike q, chunk ch, group g): the columns of spike q's
-            // segment [max(x_q - nt, x_{q-1} + nt + 1), x_q + nt], 32 at a time
-            // (lane = column), and the row blocks g*MPB_GROUP.. of the group;
-            // the CTA's warps take them from a shared counter. Lane L holds
-            // spike q - 1 + L of the round.
-            const int it_end = s_end;
+            // lane L holds spike q - 1 + L of the round
             auto fetch = [&](int q2, int& fx, int& fy, float& fa) {
                 const int j = q2 - 1 + lane;
                 fx = INT_MAX;
@@ -351,11 +311,8 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
             };
             int x = INT_MAX, y = 0, cur_q = -1;
             float amp = 0.f;
-            for (;;) {
-                int it = 0;
-                if (lane == 0) it = atomicAdd(&s_next, 1);
-                it = __shfl_sync(FULL, it, 0);
-                if (it >= it_end) break;
+            const int it_hi = (int)((int64_t)items * (gw + 1) / NW);
+            for (int it = (int)((int64_t)items * gw / NW); it < it_hi; ++it) {
                 const int q = it / per_spike, rem = it - q * per_spike, ch = rem / ngr, g = rem - ch * ngr;
                 if (q != cur_q) {
                     cur_q = q;
@@ -380,12 +337,6 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
                         if ((q + e) & 1) e1 = e; else e0 = e;
                     }
                 }
-                const int x0 = __shfl_sync(FULL, x, max(e0, 0) + 1);
-                const int y0 = __shfl_sync(FULL, y, max(e0, 0) + 1);
-                const float a0 = __shfl_sync(FULL, amp, max(e0, 0) + 1);
-                const int x1 = __shfl_sync(FULL, x, max(e1, 0) + 1);
-                const int y1 = __shfl_sync(FULL, y, max(e1, 0) + 1);
-                const float a1 = __shfl_sync(FULL, amp, max(e1, 0) + 1);
                 // the first MPB_SPK spikes of the list (nearly always the only ones
                 // a chunk meets): template and |amplitude| for the row masks
                 int ye[MPB_SPK];
@@ -398,125 +349,305 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
                 // ---- decisions for the group's blocks, all loads in one round trip.
                 // thr: a quarter ulp of the smallest |B| the block holds in any of
                 // the warp's columns; row r of block b needs spike e's term only if
-                // fl(|a_e| * max_l |ctc[t_r, y_e, l]|) >= thr (otherwise the term
+                // fl(|a_e| * max_l |ctc[r, y_e, l]|) >= thr (otherwise the term
                 // leaves every score of the row bit for bit unchanged).
                 const int bg0 = g * MPB_GROUP, nbg = min(MPB_GROUP, nb - bg0);
                 float bmv[MPB_GROUP], cmv[MPB_GROUP][MPB_SPK];
 #pragma unroll
                 for (int j = 0; j < MPB_GROUP; ++j) {
                     const int bb = bg0 + j;
-                    const int tr = (j < nbg) ? s_perm[bb * MPB_ROWS + lane] : -1;
+                    const int tr = (j < nbg && bb * MPB_ROWS + lane < T) ? bb * MPB_ROWS + lane : -1;
                     bmv[j] = (j < nbg && active) ? __ldcg(a.bmin + bb * ldk + s) : 0.f;
 #pragma unroll
                     for (int e = 0; e < MPB_SPK; ++e)
                         cmv[j][e] = (tr >= 0 && e < nl) ? __ldg(a.cmaxr + (int64_t)ye[e] * T + tr) : 0.f;
                 }
-                // per block j: the rows that need this lane's even term (m0) and odd
-                // term (m1), packed 32 bits per block; bit j of procm: block j is processed
-                unsigned long long m0p[(MPB_GROUP + 1) / 2], m1p[(MPB_GROUP + 1) / 2];
+                // me[j][e]: the rows of block j that need spike e's term (lane =
+                // row in the ballot); per column, the rows that need its even term
+                // (m0) and its odd term (m1); bit j of procm: block j is processed
+                unsigned me[MPB_GROUP][MPB_SPK];
+                auto masks = [&](int j, unsigned& m0, unsigned& m1) {
+                    m0 = (e0 >= MPB_SPK) ? FULL : 0u;
+                    m1 = (e1 >= MPB_SPK) ? FULL : 0u;
 #pragma unroll
-                for (int i = 0; i < (MPB_GROUP + 1) / 2; ++i) m0p[i] = m1p[i] = 0ull;
+                    for (int jj = 0; jj < MPB_GROUP; ++jj)
+                        if (jj == j) {
+#pragma unroll
+                            for (int e = 0; e < MPB_SPK; ++e) {
+                                if (e0 == e) m0 = me[jj][e];
+                                if (e1 == e) m1 = me[jj][e];
+                            }
+                        }
+                    if (e0 < 0) m0 = 0u;
+                    // after a term that changes the score the second is always applied
+                    m1 = (e1 >= 0) ? (m1 | m0) : 0u;
+                };
                 unsigned procm = 0u;
 #pragma unroll
                 for (int j = 0; j < MPB_GROUP; ++j) {
                     const float thr_l = active ? quarter_ulp(bmv[j]) : FLT_MAX;
                     const float thr = __uint_as_float(__reduce_min_sync(FULL, __float_as_uint(thr_l)));
-                    unsigned m0 = (e0 >= MPB_SPK) ? 0xffffffffu : 0u, m1 = (e1 >= MPB_SPK) ? 0xffffffffu : 0u;
 #pragma unroll
-                    for (int e = 0; e < MPB_SPK; ++e) {
-                        const unsigned me = __ballot_sync(FULL, e < nl && !(__fmul_rn(fae[e], cmv[j][e]) < thr));
-                        if (e0 == e) m0 = me;
-                        if (e1 == e) m1 = me;
-                    }
-                    if (e0 < 0) m0 = 0u;
-                    // after a term that changes the score the second is always applied
-                    m1 = (e1 >= 0) ? (m1 | m0) : 0u;
-                    if (j < nbg && __any_sync(FULL, active && (m0 | m1) != 0u)) procm |= 1u << j;
-                    m0p[j / 2] |= (unsigned long long)m0 << (32 * (j & 1));
-                    m1p[j / 2] |= (unsigned long long)m1 << (32 * (j & 1));
-                }
-                n_items += nbg;
-                const float* c0p = a.ctcP + (int64_t)y0 * T * L2 + (s - x0 + nt);
-                const float* c1p = a.ctcP + (int64_t)y1 * T * L2 + (s - x1 + nt);
-                n_proc += __popc(procm);
-                if (!active || procm == 0u) continue;
-                // the processed blocks' rows in 8-row batches through one
-                // software pipeline: the next batch's loads are issued before
-                // the current batch is updated, across block boundaries
-                auto masks = [&](int j, unsigned& m0, unsigned& m1) {
-                    unsigned long long p0 = m0p[0], p1 = m1p[0];
-#pragma unroll
-                    for (int i = 1; i < (MPB_GROUP + 1) / 2; ++i)
-                        if (j / 2 == i) {
-                            p0 = m0p[i];
-                            p1 = m1p[i];
-                        }
-                    m0 = (unsigned)(p0 >> (32 * (j & 1)));
-                    m1 = (unsigned)(p1 >> (32 * (j & 1)));
-                };
-                // batch k of the sequence: block j = k-th set bit group, rows rb*8..
-                const int nbt = __popc(procm) * (MPB_ROWS / 8);
-                auto batch_of = [&](int k, int& j, int& rb) {
-                    int left = k / (MPB_ROWS / 8);
-                    unsigned pm = procm;
-                    for (int i = 0; i < left; ++i) pm &= pm - 1u;
-                    j = __ffs(pm) - 1;
-                    rb = k % (MPB_ROWS / 8);
-                };
-                float v[8], w0[8], w1[8];
-                auto load = [&](int k, float (&lv)[8], float (&l0)[8], float (&l1)[8]) {
-                    int j, rb;
-                    batch_of(k, j, rb);
+                    for (int e = 0; e < MPB_SPK; ++e)
+                        me[j][e] = __ballot_sync(FULL, e < nl && !(__fmul_rn(fae[e], cmv[j][e]) < thr));
                     unsigned m0, m1;
                     masks(j, m0, m1);
-                    const int r0 = (bg0 + j) * MPB_ROWS, nr = min(MPB_ROWS, T - r0);
+                    if (j < nbg && __any_sync(FULL, active && (m0 | m1) != 0u)) procm |= 1u << j;
+                }
+                n_items += nbg;
+                n_proc += __popc(procm);
+                if (procm == 0u) continue;
+                if (use_list && __all_sync(FULL, e0 < MPB_SPK && e1 < MPB_SPK)) {
+                    // one entry per processed block: chunk, block, the first
+                    // MPB_SPK spikes of the list and their row masks
+                    int slot = 0;
+                    if (lane == 0) slot = atomicAdd(&s_ecnt, __popc(procm));
+                    slot = __shfl_sync(FULL, slot, 0);
+                    int xe[MPB_SPK];
+                    float ae[MPB_SPK];
 #pragma unroll
-                    for (int u = 0; u < 8; ++u) {
-                        const int rr = rb * 8 + u;
-                        const int t = rr < nr ? s_perm[r0 + rr] : -1;
-                        lv[u] = t >= 0 ? ld_keep(a.B + (int64_t)t * ldb + s, pk) : 0.f;
-                        l0[u] = (t >= 0 && ((m0 >> rr) & 1u)) ? ld_stream(c0p + (int64_t)t * L2, ps) : 0.f;
-                        l1[u] = (t >= 0 && ((m1 >> rr) & 1u)) ? ld_stream(c1p + (int64_t)t * L2, ps) : 0.f;
+                    for (int e = 0; e < MPB_SPK; ++e) {
+                        xe[e] = __shfl_sync(FULL, x, e + 1);
+                        ae[e] = __shfl_sync(FULL, amp, e + 1);
                     }
-                };
-                load(0, v, w0, w1);
-                ColMaxAny m;
-                float mn = INFINITY;
-                for (int k = 0; k < nbt; ++k) {
-                    float nv[8], nw0[8], nw1[8];
-                    if (k + 1 < nbt) load(k + 1, nv, nw0, nw1);
-                    int j, rb;
-                    batch_of(k, j, rb);
+                    int4* dst = a.ment + ((int64_t)b * a.ment_cap + slot) * 4;
+                    int k = 0;
+#pragma unroll
+                    for (int j = 0; j < MPB_GROUP; ++j) {
+                        if (!((procm >> j) & 1u)) continue;
+                        int4 w;
+                        if (lane == 0)
+                            w = make_int4(lo_own + ch * 32, hi_own, bg0 + j, min(nl, MPB_SPK) | ((q & 1) << 8));
+                        else if (lane == 1)
+                            w = make_int4((int)me[j][0], (int)me[j][1], (int)me[j][2], xe[0]);
+                        else if (lane == 2)
+                            w = make_int4(xe[1], xe[2], ye[0], ye[1]);
+                        else
+                            w = make_int4(ye[2], __float_as_int(ae[0]), __float_as_int(ae[1]), __float_as_int(ae[2]));
+                        if (lane < 4) __stcg(dst + 4 * k + lane, w);
+                        ++k;
+                    }
+                    continue;
+                }
+                // not listed (a spike list longer than the entries hold, or lists
+                // too short for the round): the processed blocks' rows here, 8 at
+                // a time
+                const int x0 = __shfl_sync(FULL, x, max(e0, 0) + 1);
+                const int y0 = __shfl_sync(FULL, y, max(e0, 0) + 1);
+                const float a0 = __shfl_sync(FULL, amp, max(e0, 0) + 1);
+                const int x1 = __shfl_sync(FULL, x, max(e1, 0) + 1);
+                const int y1 = __shfl_sync(FULL, y, max(e1, 0) + 1);
+                const float a1 = __shfl_sync(FULL, amp, max(e1, 0) + 1);
+                const float* c0p = a.ctcP + (int64_t)y0 * T * L2 + (s - x0 + nt);
+                const float* c1p = a.ctcP + (int64_t)y1 * T * L2 + (s - x1 + nt);
+                for (int j = 0; j < nbg; ++j) {
+                    if (!((procm >> j) & 1u)) continue;
                     unsigned m0, m1;
                     masks(j, m0, m1);
                     const int bb = bg0 + j, r0 = bb * MPB_ROWS, nr = min(MPB_ROWS, T - r0);
+                    ColMaxRows m;
+                    float mn = INFINITY;
+                    for (int rb = 0; rb < BPB; ++rb) {
+                        float v[8], w0[8], w1[8];
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) {
+                            const int rr = rb * 8 + u;
+                            const bool ld = active && rr < nr;
+                            const int64_t t = r0 + rr;
+                            v[u] = ld ? ld_keep(a.B + t * ldb + s, pk) : 0.f;
+                            w0[u] = (ld && ((m0 >> rr) & 1u)) ? ld_stream(c0p + t * L2, ps) : 0.f;
+                            w1[u] = (ld && ((m1 >> rr) & 1u)) ? ld_stream(c1p + t * L2, ps) : 0.f;
+                        }
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) {
+                            const int rr = rb * 8 + u;
+                            if (!active || rr >= nr) continue;
+                            const int t = r0 + rr;
+                            float xv = v[u];
+                            if ((m0 >> rr) & 1u) xv = __fsub_rn(xv, __fmul_rn(a0, w0[u]));
+                            if ((m1 >> rr) & 1u) xv = __fsub_rn(xv, __fmul_rn(a1, w1[u]));
+                            if (__float_as_uint(xv) != __float_as_uint(v[u]))
+                                st_keep(a.B + (int64_t)t * ldb + s, xv, pk);
+                            mn = fminf(mn, fabsf(xv));
+                            m.consider(xv, s_nm[t], s_inv[t], t, s_perm);
+                        }
+                    }
+                    if (active) {
+                        a.bkey[bb * ldk + s] = m.key(s_perm);
+                        a.bmin[bb * ldk + s] = mn;
+                    }
+                }
+            }
+        }
+        if (use_list) {
+            // ---- the CTAs' lists: an equal range of all entries per warp, their
+            // rows fetched NST - 1 batches ahead into this warp's ring in shared
+            // memory (asynchronous copies, no registers held for rows in flight)
+            __syncthreads();
+            if (tid == 0) {
+                a.ment_cnt[b] = s_ecnt;
+                clk.lap(2);
+            }
+            if (!grid_sync(a.bar, a.status)) return;
+            if (tid == 0) clk.lap(3);
+            prefix_counts(a.ment_cnt);
+            const int n = s_pref[G];
+            const int e_lo = (int)((int64_t)n * gw / NW), e_hi = (int)((int64_t)n * (gw + 1) / NW);
+            if (e_lo < e_hi) {
+                struct Ent {
+                    int4 w0, w1, w2, w3;
+                };
+                // this lane's column of an entry: its row masks, terms and ctc rows
+                struct St {
+                    int s, bb;  // s < 0: the lane's column is past the chunk's segment
+                    unsigned m0, m1;
+                    float a0, a1;
+                    const float* c0p;
+                    const float* c1p;
+                };
+                auto ld_ent = [&](int e, Ent& E) {
+                    int lo2 = 0, hi2 = G;  // list c with s_pref[c] <= e < s_pref[c+1]
+                    while (hi2 - lo2 > 1) {
+                        const int m = (lo2 + hi2) >> 1;
+                        if (s_pref[m] <= e) lo2 = m; else hi2 = m;
+                    }
+                    const int4* p = a.ment + ((int64_t)lo2 * a.ment_cap + (e - s_pref[lo2])) * 4;
+                    E.w0 = __ldcg(p);
+                    E.w1 = __ldcg(p + 1);
+                    E.w2 = __ldcg(p + 2);
+                    E.w3 = __ldcg(p + 3);
+                };
+                auto make = [&](const Ent& E, St& S) {
+                    const int col = E.w0.x + lane;
+                    const bool act = col <= E.w0.y;
+                    S.s = act ? col : -1;
+                    S.bb = E.w0.z;
+                    const int nlq = E.w0.w & 0xFF, qp = (E.w0.w >> 8) & 1;
+                    const int xs[MPB_SPK] = {E.w1.w, E.w2.x, E.w2.y};
+                    const int ys[MPB_SPK] = {E.w2.z, E.w2.w, E.w3.x};
+                    const float as[MPB_SPK] = {__int_as_float(E.w3.y), __int_as_float(E.w3.z), __int_as_float(E.w3.w)};
+                    const unsigned ms[MPB_SPK] = {(unsigned)E.w1.x, (unsigned)E.w1.y, (unsigned)E.w1.z};
+                    int e0 = -1, e1 = -1;
+#pragma unroll
+                    for (int e = 0; e < MPB_SPK; ++e)
+                        if (e < nlq && act && xs[e] <= col + nt) {
+                            if ((qp + e) & 1) e1 = e; else e0 = e;
+                        }
+                    unsigned m0 = 0u, m1 = 0u;
+                    int x0 = xs[0], y0 = ys[0], x1 = xs[0], y1 = ys[0];
+                    float a0 = as[0], a1 = as[0];
+#pragma unroll
+                    for (int e = 0; e < MPB_SPK; ++e) {
+                        if (e0 == e) {
+                            m0 = ms[e];
+                            x0 = xs[e];
+                            y0 = ys[e];
+                            a0 = as[e];
+                        }
+                        if (e1 == e) {
+                            m1 = ms[e];
+                            x1 = xs[e];
+                            y1 = ys[e];
+                            a1 = as[e];
+                        }
+                    }
+                    S.m0 = m0;
+                    S.m1 = (e1 >= 0) ? (m1 | m0) : 0u;
+                    S.a0 = a0;
+                    S.a1 = a1;
+                    S.c0p = a.ctcP + (int64_t)y0 * T * L2 + (col - x0 + nt);
+                    S.c1p = a.ctcP + (int64_t)y1 * T * L2 + (col - x1 + nt);
+                };
+                // this warp's ring of NST stages in shared memory, stage =
+                // [B rows | even-term ctc rows | odd-term ctc rows][8][32 lanes]
+                const uint32_t ring_s = (uint32_t)__cvta_generic_to_shared(ring + warp * NST * 3 * 8 * 32);
+                const float* ring_w = ring + warp * NST * 3 * 8 * 32 + lane;
+                auto issue = [&](const St& S, int rb, int stage) {
+                    const int r0 = S.bb * MPB_ROWS, nr = min(MPB_ROWS, T - r0);
+                    const bool act = S.s >= 0;
+                    const uint32_t d = ring_s + (uint32_t)(stage * 3 * 8 * 32 + lane) * 4u;
 #pragma unroll
                     for (int u = 0; u < 8; ++u) {
                         const int rr = rb * 8 + u;
-                        if (rr >= nr) continue;
-                        const int t = s_perm[r0 + rr];
-                        float xv = v[u];
-                        if ((m0 >> rr) & 1u) xv = __fsub_rn(xv, __fmul_rn(a0, w0[u]));
-                        if ((m1 >> rr) & 1u) xv = __fsub_rn(xv, __fmul_rn(a1, w1[u]));
-                        if (__float_as_uint(xv) != __float_as_uint(v[u])) st_keep(a.B + (int64_t)t * ldb + s, xv, pk);
-                        mn = fminf(mn, fabsf(xv));
-                        m.consider(xv, s_nm[t], s_inv[t], t);
+                        const bool ld = act && rr < nr;
+                        const int64_t t = r0 + rr;
+                        cp_async4_if(d + (uint32_t)u * 128u, a.B + t * ldb + S.s, ld, pk);
+                        cp_async4_if(d + (uint32_t)(8 + u) * 128u, S.c0p + t * L2, ld && ((S.m0 >> rr) & 1u), ps);
+                        cp_async4_if(d + (uint32_t)(16 + u) * 128u, S.c1p + t * L2, ld && ((S.m1 >> rr) & 1u), ps);
                     }
-                    if (rb == MPB_ROWS / 8 - 1) {  // last batch of the block: its key and minimum
-                        a.bkey[bb * ldk + s] = pack_key(m.best, m.bi);
-                        a.bmin[bb * ldk + s] = mn;
-                        m = ColMaxAny();
+                };
+                Ent En;
+                St scur, siss;  // the entry being updated, the entry being fetched
+                ld_ent(e_lo, En);
+                make(En, siss);
+                scur = siss;
+                if (e_lo + 1 < e_hi) ld_ent(e_lo + 1, En);
+                const int nbt = (e_hi - e_lo) * BPB;
+                // flat batch j of the warp's entries into stage j % NST; the
+                // fetch runs NST - 1 batches ahead of the update (less than one
+                // entry, so at most two entries are live)
+                static_assert(NST - 1 < BPB, "the fetch may run at most one entry ahead");
+                auto fetch_batch = [&](int j) {
+                    const int rb = j % BPB;
+                    if (rb == 0 && j > 0) {
+                        make(En, siss);
+                        const int e2 = e_lo + j / BPB + 1;
+                        if (e2 < e_hi) ld_ent(e2, En);
+                    }
+                    issue(siss, rb, j % NST);
+                };
+#pragma unroll
+                for (int j = 0; j < NST - 1; ++j) {
+                    if (j < nbt) fetch_batch(j);
+                    cp_async_commit();
+                }
+                ColMaxRows m;
+                float mn = INFINITY;
+                for (int k = 0; k < nbt; ++k) {
+                    if (k + NST - 1 < nbt) fetch_batch(k + NST - 1);
+                    cp_async_commit();
+                    cp_async_wait<NST - 1>();  // batch k has landed (this lane's own copies)
+                    const int rb = k % BPB;
+                    if (rb == 0 && k > 0) scur = siss;
+                    const float* stg = ring_w + (k % NST) * 3 * 8 * 32;
+                    const int r0 = scur.bb * MPB_ROWS, nr = min(MPB_ROWS, T - r0);
+                    const bool act = scur.s >= 0;
+                    // the eight rows' updates without branches (selects and
+                    // predicated stores; rows not fetched are never selected),
+                    // then the rare Cf candidates
+                    float xs[8], ap[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        const int rr = rb * 8 + u;
+                        const bool okr = act && rr < nr;
+                        const int t = r0 + rr;
+                        const float v = stg[u * 32], w0 = stg[(8 + u) * 32], w1 = stg[(16 + u) * 32];
+                        const float y0 = __fsub_rn(v, __fmul_rn(scur.a0, w0));
+                        const float xa = ((scur.m0 >> rr) & 1u) ? y0 : v;
+                        const float y1 = __fsub_rn(xa, __fmul_rn(scur.a1, w1));
+                        const float xv = ((scur.m1 >> rr) & 1u) ? y1 : xa;
+                        st_keep_if(a.B + (int64_t)t * ldb + scur.s, xv,
+                                   okr && __float_as_uint(xv) != __float_as_uint(v), pk);
+                        mn = okr ? fminf(mn, fabsf(xv)) : mn;
+                        const float rl = fmaxf(xv, 0.f);
+                        ap[u] = okr ? __fmul_rn(__fmul_rn(rl, rl), s_inv[min(t, T - 1)]) : -INFINITY;
+                        xs[u] = xv;
+                    }
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        const int t = r0 + rb * 8 + u;
+                        if (ap[u] >= m.thr) m.consider(xs[u], s_nm[t], s_inv[t], t, s_perm);
+                    }
+                    if (rb == BPB - 1) {  // the entry's block: its key and minimum in this column
+                        if (act) {
+                            a.bkey[scur.bb * ldk + scur.s] = m.key(s_perm);
+                            a.bmin[scur.bb * ldk + scur.s] = mn;
+                        }
+                        m = ColMaxRows();
                         mn = INFINITY;
                     }
-                    if (k + 1 < nbt) {
-#pragma unroll
-                        for (int u = 0; u < 8; ++u) {
-                            v[u] = nv[u];
-                            w0[u] = nw0[u];
-                            w1[u] = nw1[u];
-                        }
-                    }
                 }
+                cp_async_wait<0>();
             }
         }
         base += total;
@@ -545,22 +676,17 @@ int mp_blocks_max_grid(int device) {
     return std::min(sms, MPB_MAX_GRID);
 }
 
-static size_t mpb_smem_bytes(int cols_per_blk, int nt, int T, int nb) {
-    return sizeof(float) * ((size_t)cols_per_blk + 2 * nt) + sizeof(int) * (size_t)cols_per_blk +
-           sizeof(float) * 2 * (size_t)T + sizeof(int) * (size_t)nb * MPB_ROWS + sizeof(int) * 2 * MPB_MAX_SPK + 16;
+static size_t mpb_smem_bytes(int cols_per_blk, int nt, int T, int nb, int nst) {
+    const size_t base = ((size_t)2 * cols_per_blk + 2 * nt + 3 * (size_t)T + (size_t)nb * MPB_ROWS + 3) & ~(size_t)3;
+    return sizeof(float) * (base + (size_t)WPB * nst * 3 * 8 * 32);
 }
 
-cudaError_t launch_mp_blocks(MPArgs a, int grid, cudaStream_t s) {
-    if (grid > MPB_MAX_GRID || !a.perm || !a.cmaxr || !a.bkey || !a.bmin || !a.band_lo || !a.band_hi ||
-        a.nb != (a.T + MPB_ROWS - 1) / MPB_ROWS)
-        return cudaErrorInvalidValue;
-    const size_t smem = mpb_smem_bytes(a.cols_per_blk, a.nt, a.T, a.nb);
+template <int NST>
+static cudaError_t launch_nst(const MPArgs& a, int grid, size_t smem, cudaStream_t s) {
     if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(k_mp_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = cudaFuncSetAttribute(k_mp_blocks<NST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    cudaError_t e = cudaMemsetAsync(a.bar, 0, 2 * sizeof(unsigned int), s);
-    if (e != cudaSuccess) return e;
     cudaLaunchConfig_t lc = {};
     lc.gridDim = dim3(grid);
     lc.blockDim = dim3(MPB_THREADS);
@@ -571,7 +697,80 @@ cudaError_t launch_mp_blocks(MPArgs a, int grid, cudaStream_t s) {
     attr[0].val.cooperative = 1;
     lc.attrs = attr;
     lc.numAttrs = 1;
-    return cudaLaunchKernelEx(&lc, k_mp_blocks, a);
+    return cudaLaunchKernelEx(&lc, k_mp_blocks<NST>, a);
+}
+
+int64_t mp_blocks_list_entries(int64_t N, int nt, int T, int grid) {
+    // the rounds' largest peak count when peaks are nt + 1 apart, its items,
+    // the largest share of one CTA, MPB_GROUP entries per item
+    const int64_t peaks = (N + nt) / (nt + 1);
+    const int64_t items = peaks * ((2 * nt + 1 + 31) / 32) * (((T + MPB_ROWS - 1) / MPB_ROWS + MPB_GROUP - 1) / MPB_GROUP);
+    const int64_t nw = (int64_t)std::max(grid, 1) * WPB;
+    return (int64_t)std::max(grid, 1) * ((items + nw - 1) / nw) * WPB * MPB_GROUP;
+}
+
+cudaError_t launch_mp_blocks(MPArgs a, int grid, cudaStream_t s) {
+    if (grid > MPB_MAX_GRID || !a.perm || !a.cmaxr || !a.bkey || !a.bmin || (a.ment && (!a.ment_cnt || a.ment_cap < 0)) ||
+        a.nb != (a.T + MPB_ROWS - 1) / MPB_ROWS)
+        return cudaErrorInvalidValue;
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e != cudaSuccess) return e;
+    cudaFuncAttributes fa{};
+    e = cudaFuncGetAttributes(&fa, k_mp_blocks<2>);
+    if (e != cudaSuccess) return e;
+    const size_t room = (size_t)optin - fa.sharedSizeBytes;
+    // the deepest ring of fetched rows that fits (4, 3 or 2 stages per warp)
+    int nst = 4;
+    while (nst > 2 && mpb_smem_bytes(a.cols_per_blk, a.nt, a.T, a.nb, nst) > room) --nst;
+    const size_t smem = mpb_smem_bytes(a.cols_per_blk, a.nt, a.T, a.nb, nst);
+    if (smem > room) return cudaErrorInvalidValue;
+    e = cudaMemsetAsync(a.bar, 0, 2 * sizeof(unsigned int), s);
+    if (e != cudaSuccess) return e;
+    if (nst == 4) return launch_nst<4>(a, grid, smem, s);
+    if (nst == 3) return launch_nst<3>(a, grid, smem, s);
+    return launch_nst<2>(a, grid, smem, s);
+}
+
+// ctcQ[y, r, :] = ctcP[y, perm[r], :]: each spike template's cross-correlation
+// rows in the score rows' probe order (a warp per row, lags by lane)
+__global__ void k_permute_ctc(const float* __restrict__ ctcP, const int32_t* __restrict__ perm, int T, int L2,
+                              float* __restrict__ ctcQ) {
+    const int64_t row = (int64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (row >= (int64_t)T * T) return;
+    const int64_t y = row / T;
+    const int r = (int)(row - y * T);
+    const float* src = ctcP + (y * T + __ldg(perm + r)) * L2;
+    float* dst = ctcQ + row * L2;
+    for (int l = lane; l < L2; l += 32) dst[l] = __ldg(src + l);
+}
+
+cudaError_t launch_permute_ctc(const float* ctcP, const int32_t* perm, int32_t T, int32_t L2, float* ctcQ,
+                               cudaStream_t s) {
+    const int64_t rows = (int64_t)T * T;
+    k_permute_ctc<<<(unsigned)((rows + 7) / 8), 256, 0, s>>>(ctcP, perm, T, L2, ctcQ);
+    return cudaGetLastError();
+}
+
+// dst row r = src row perm[r] (N columns each)
+__global__ void k_gather_rows(const float* __restrict__ src, int64_t lds, const int32_t* __restrict__ perm,
+                              int64_t N, float* __restrict__ dst, int64_t ldd) {
+    const int r = blockIdx.y;
+    const float* sp = src + (int64_t)__ldg(perm + r) * lds;
+    float* dp = dst + (int64_t)r * ldd;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x)
+        dp[n] = __ldg(sp + n);
+}
+
+cudaError_t launch_gather_rows(const float* src, int64_t lds, const int32_t* perm, int32_t rows, int64_t N,
+                               float* dst, int64_t ldd, cudaStream_t s) {
+    if (rows <= 0 || N <= 0) return cudaSuccess;
+    const unsigned gx = (unsigned)std::min<int64_t>((N + 255) / 256, 64);
+    k_gather_rows<<<dim3(gx, (unsigned)rows), 256, 0, s>>>(src, lds, perm, N, dst, ldd);
+    return cudaGetLastError();
 }
 
 // cmaxr[y, t] = max over lags of |ctcP[y, t, :]| (one warp per row); a NaN

@@ -75,6 +75,33 @@ __device__ __forceinline__ float ld_stream(const float* a, uint64_t pol) {
 }
 
 
+// Predicated store (no branch around it), so that the rows of a batch stay
+// in one basic block and their chains interleave.
+__device__ __forceinline__ void st_keep_if(float* a, float v, bool p, uint64_t pol) {
+    asm volatile(
+        "{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %2, 0;\n\t"
+        "@q st.global.cg.L2::cache_hint.f32 [%0], %1, %3;\n\t}" ::"l"(a),
+        "f"(v), "r"((int)p), "l"(pol)
+        : "memory");
+}
+// Asynchronous 4-byte copy global -> shared (skipped where p is false), and
+// its group commit / wait. The copies go through L1 (cp.async of 4 bytes has
+// only the .ca form); rows that other CTAs updated in an earlier round are
+// visible because every round ends at a grid barrier whose gpu-scope fences
+// order those writes before this CTA's later reads.
+__device__ __forceinline__ void cp_async4_if(uint32_t dst, const float* src, bool p, uint64_t pol) {
+    asm volatile(
+        "{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %2, 0;\n\t"
+        "@q cp.async.ca.shared.global.L2::cache_hint [%0], [%1], 4, %3;\n\t}" ::"r"(dst),
+        "l"(src), "r"((int)p), "l"(pol)
+        : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // Phase clock of the rounds (thread 0 of each CTA): time in the peak phase,
 // waiting at the grid barrier after it, in the update phase and waiting after
 // it, summed over the rounds; added to phase[0..3] (sums over CTAs) with the

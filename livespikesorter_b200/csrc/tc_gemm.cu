@@ -71,6 +71,7 @@ struct Args {
     const int32_t* rowmap;    // GEMM row r scores sample rowmap[r / map_rows] * map_rows + r % map_rows (null: r)
     int map_rows;
     const int32_t* count_dev; // rows = min(N, count_dev[0] * map_rows) (null: N)
+    const int32_t* rowof;     // template t's score row is Bout row rowof[t] (null: t)
     int ncols;                // samples in the batch (edge columns are the first/last nt)
     float* cf2;               // runner-up Cf of each column (null: not tracked)
     int pass_w;               // templates per pass (<= MAX_NP)
@@ -435,7 +436,8 @@ __global__ void __launch_bounds__(THREADS, 1)
                             const int t = t0 + j;
                             if (t < a.T) {
                                 const float v = __uint_as_float(r[j]);
-                                st_keep(a.Bout + (int64_t)t * a.ldb + n, v, pol);
+                                const int orow = a.rowof ? __ldg(a.rowof + t) : t;
+                                st_keep(a.Bout + (int64_t)orow * a.ldb + n, v, pol);
                                 if (!edge) {
                                     if (second) m.consider<true>(v, s_nm[t], s_inv[t], t);
                                     else m.consider<false>(v, s_nm[t], s_inv[t], t);
@@ -616,6 +618,7 @@ static cudaError_t launch_tc(const void* A, const void* Alo, int64_t ldk, int N,
     a.rowmap = ex.rowmap;
     a.map_rows = ex.map_rows;
     a.count_dev = ex.count_dev;
+    a.rowof = ex.rowof;
     a.ncols = ex.rowmap ? ex.ncols : N;
     a.cf2 = ex.cf2;
     a.pass_w = p.pass_w;
