@@ -357,6 +357,7 @@ def run_b200(args):
         # the two rounds kernels on the same batches (identical results): every
         # row updated, or provably unchanged template-row blocks skipped
         kernels = {}
+        default_skip = s32.round_kernel()
         for skip in (False, True):
             s32.set_round_kernel(skip)
             tk, stk = device_resident_rate(s32, rows_d, drifts, ids, nb, K, W, stream, dist, local)
@@ -364,7 +365,7 @@ def run_b200(args):
             kernels['skip_blocks' if skip else 'full'] = {
                 'rec_s_per_s': world * K * rec_s / (tk / 1e3), 'mp_ms': stk['mp_ms'], 'phases_ms': stk['mp_phases_ms'],
                 'update_items': st_k['mp_items'], 'update_items_changed': st_k['mp_items_updated']}
-        s32.set_round_kernel(False)
+        s32.set_round_kernel(default_skip)
         out['round_kernels_fp32'] = kernels
         if args.precision == 'bf16':
             out['bf16'] = bf16_report(s, s32, rows_d, drifts, ids, nb)

@@ -169,10 +169,14 @@ int  lss_match_scores(lss_handle* h, const float* B_dev, int64_t N, int64_t* st_
 /* Which kernel runs the matching-pursuit rounds of this handle (identical
  * spikes, amplitudes and score field either way; a performance choice, no
  * counterpart in the reference): 0 = every template row of every spike window
- * is updated (default); 1 = template rows are grouped in blocks along the probe
- * and a block whose update provably leaves every score unchanged (terms below
- * a quarter ulp of the block's smallest score) is skipped. */
+ * is updated; 1 = template rows are grouped in blocks along the probe and a
+ * block whose update provably leaves every score unchanged (terms below a
+ * quarter ulp of the block's smallest score) is skipped. The default is 1 from
+ * 600 templates up (measured on a B200, 384 channels: 7.40 vs 7.75 ms of rounds
+ * per 2-s batch at 800 templates, 2.43 vs 2.15 ms at 400), else 0. */
 int  lss_set_round_kernel(lss_handle* h, int32_t skip_blocks);
+/* The handle's rounds kernel (1: block-skipping, 0: every row). */
+int  lss_get_round_kernel(const lss_handle* h, int32_t* skip_blocks);
 
 /* The same matching-pursuit rounds for callers that cannot allocate device
  * memory (an acquisition host that owns the GPU's memory, a process whose

@@ -17,7 +17,7 @@ LSS_PREC_FP32, LSS_PREC_BF16_RECHECK = 0, 1
 EXPORTS = ('lss_create', 'lss_create_from_dir', 'lss_destroy', 'lss_last_error', 'lss_get_config',
            'lss_set_drift', 'lss_filter', 'lss_match', 'lss_match_scores', 'lss_scores',
            'lss_sort_batch', 'lss_get_stats', 'lss_set_profiling', 'lss_get_stage_times',
-           'lss_mp_rounds_noalloc', 'lss_set_round_kernel', 'lss_server_create', 'lss_server_destroy', 'lss_server_admit',
+           'lss_mp_rounds_noalloc', 'lss_set_round_kernel', 'lss_get_round_kernel', 'lss_server_create', 'lss_server_destroy', 'lss_server_admit',
            'lss_server_push', 'lss_server_poll', 'lss_server_release', 'lss_server_set_drift',
            'lss_server_latency', 'lss_server_memory', 'lss_recon_forward', 'lss_recon_backward',
            'lss_set_postprocess', 'lss_reset_postprocess', 'lss_format_spike_lines', 'lss_serialize_payload',
@@ -107,6 +107,7 @@ def load() -> ct.CDLL:
         'lss_set_profiling': ([P, I32], ct.c_int),
         'lss_get_stage_times': ([P, ct.POINTER(LssStageTimes)], ct.c_int),
         'lss_set_round_kernel': ([P, I32], ct.c_int),
+        'lss_get_round_kernel': ([P, ct.POINTER(ct.c_int32)], ct.c_int),
         'lss_mp_rounds_noalloc': ([P, I64, I32, I32, I32, ct.c_float, P, P, I32, I32, P, P, P,
                                    ct.POINTER(I32), ct.POINTER(I32), P], ct.c_int),
         'lss_server_create': ([I32, I64, I32, ct.POINTER(P)], ct.c_int),

@@ -434,6 +434,9 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
     ALLOC(imax, ld);
     ALLOC(colkey, 2 * ld);
     h->mp_nb = (T + MPB_ROWS - 1) / MPB_ROWS;
+    // the block-skipping rounds pay off from a few hundred templates on (more
+    // rows per block far from a spike); below, updating every row is faster
+    h->mp_skip = T >= 600;
     ALLOC(mp_perm, (size_t)h->mp_nb * MPB_ROWS);
     ALLOC(mp_cmaxr, (size_t)T * T);
     ALLOC(mp_rowof, T);
@@ -622,6 +625,12 @@ int lss_set_round_kernel(lss_handle* h, int32_t skip_blocks) {
     return LSS_OK;
 }
 
+int lss_get_round_kernel(const lss_handle* h, int32_t* skip_blocks) {
+    if (!h || !skip_blocks) return LSS_ERR_ARG;
+    *skip_blocks = h->mp_skip ? 1 : 0;
+    return LSS_OK;
+}
+
 int lss_set_drift(lss_handle* h, const float* M) {
     if (!h) return LSS_ERR_ARG;
     if (h->streaming) return h->fail(LSS_ERR_STATE, "handle is owned by a serving loop");
@@ -737,6 +746,7 @@ int lss::run_scores(lss_handle* h, const float* X, int64_t ldx, int64_t N, float
         ex2.count_dev = h->rc_count.p;
         ex2.ncols = (int)N;
         ex2.rowof = rowof;
+        ex2.keys = h->colkey.p;  // templates split over CTAs; free until the rounds start (they clear it)
         const int max_rows = (int)((N + 127) / 128 * 128);
         CK(launch_score_tc_tf32x3(h->Pc_hi.p, h->Pc_lo.p, h->CKpad, max_rows, folded ? h->Uw_hi.p : h->Up_hi.p,
                                   folded ? h->Uw_lo.p : h->Up_lo.p, h->T, h->CKpad, h->nm.p, B, h->ld, h->cfmax.p,
@@ -749,7 +759,7 @@ int lss::run_scores(lss_handle* h, const float* X, int64_t ldx, int64_t N, float
             h->rc_pending = true;
             h->last_scored = N;
         }
-        h->stats.launches += 6;
+        h->stats.launches += 7;
         h->mark(6, s);
         if (maxima_ready) *maxima_ready = true;
         return LSS_OK;

@@ -33,6 +33,7 @@ namespace tc {
 constexpr int BM = 128;               // samples per tile
 constexpr int MAX_NP = 512;           // templates per pass (TMEM columns)
 constexpr int SPLIT_W = 128;          // templates per work item in split mode
+constexpr int MAPPED_SPLIT_W = 64;    // ... for a re-check of a few mapped rows
 constexpr int THREADS = 192;
 
 // Element kinds of the score GEMM (TcOp).
@@ -507,6 +508,18 @@ __global__ void k_keys_to_maxima(const unsigned long long* __restrict__ keys, in
     imax[n] = (int32_t)(~(uint32_t)k);
 }
 
+// The same for the mapped columns of a re-check (rowmap, count on the device).
+__global__ void k_keys_to_maxima_mapped(const unsigned long long* __restrict__ keys, const int32_t* __restrict__ rowmap,
+                                        const int32_t* __restrict__ count_dev, int map_rows, int max_rows,
+                                        float* __restrict__ cfmax, int32_t* __restrict__ imax) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= min(max_rows, count_dev[0] * map_rows)) return;
+    const int n = rowmap[i / map_rows] * map_rows + i % map_rows;
+    const unsigned long long k = keys[n];
+    cfmax[n] = __uint_as_float((uint32_t)(k >> 32));
+    imax[n] = (int32_t)(~(uint32_t)k);
+}
+
 }  // namespace tc
 
 // ---------------------------------------------------------------- host side
@@ -578,15 +591,18 @@ static cudaError_t launch_tc(const void* A, const void* Alo, int64_t ldk, int N,
     // Few sample tiles (short streaming batches): one work item per (tile,
     // pass of SPLIT_W templates) so that more SMs share the templates; the
     // column maxima are then combined through 64-bit keys.
+    // A re-check of mapped rows (rowmap, count on the device) is usually one
+    // or two tiles: its templates are split the same way, in narrower passes.
     const int ntiles = (N + tc::BM - 1) / tc::BM;
-    const bool split = ex.keys && !ex.cf2 && !ex.rowmap && 2 * ntiles < grid && T > tc::SPLIT_W;
+    const bool split_map = ex.keys && ex.rowmap && ex.count_dev && !ex.cf2 && !ex.un && T > tc::MAPPED_SPLIT_W;
+    const bool split = split_map || (ex.keys && !ex.cf2 && !ex.rowmap && 2 * ntiles < grid && T > tc::SPLIT_W);
     // templates in passes of at most 256 TMEM columns (equal widths): two
     // accumulators alternate, so one pass's epilogue drains while the next
     // pass's MMAs run, and the smaller stages leave room for four of them
     const int tpad = (T + 15) / 16 * 16;
     const int npass = (tpad + 255) / 256;
     const int even_w = ((tpad + npass - 1) / npass + 15) / 16 * 16;
-    const TcPlan p = tc_plan(T, OP, split ? tc::SPLIT_W : even_w);
+    const TcPlan p = tc_plan(T, OP, split_map ? tc::MAPPED_SPLIT_W : (split ? tc::SPLIT_W : even_w));
     if (p.stages < 2 || CKpad % p.kblock) return cudaErrorInvalidValue;
     CUtensorMap ma, malo, mb, mblo;
     if (!make_map(&ma, A, N, CKpad, ldk, tc::BM, OP) || !make_map(&mb, Bm, p.Tpad, CKpad, CKpad, p.box_rows, OP))
@@ -633,11 +649,15 @@ static cudaError_t launch_tc(const void* A, const void* Alo, int64_t ldk, int N,
     if (e != cudaSuccess) return e;
     const int items = split ? ntiles * ((p.Tpad + p.pass_w - 1) / p.pass_w) : ntiles;
     if (split) {
-        e = cudaMemsetAsync(ex.keys, 0, (size_t)N * sizeof(unsigned long long), s);
+        e = cudaMemsetAsync(ex.keys, 0, (size_t)(split_map ? ex.ncols : N) * sizeof(unsigned long long), s);
         if (e != cudaSuccess) return e;
     }
     tc::k_score_tc<OP><<<std::min(grid, items), tc::THREADS, p.smem, s>>>(ma, malo, mb, mblo, a);
-    if (split) tc::k_keys_to_maxima<<<(N + 255) / 256, 256, 0, s>>>(ex.keys, N, cfmax, imax);
+    if (split_map)
+        tc::k_keys_to_maxima_mapped<<<(N + 255) / 256, 256, 0, s>>>(ex.keys, ex.rowmap, ex.count_dev, ex.map_rows, N,
+                                                                    cfmax, imax);
+    else if (split)
+        tc::k_keys_to_maxima<<<(N + 255) / 256, 256, 0, s>>>(ex.keys, N, cfmax, imax);
     return cudaGetLastError();
 }
 

@@ -338,8 +338,16 @@ class Sorter:
 
     def set_round_kernel(self, skip_blocks: bool):
         """Rounds kernel: skip provably unchanged template-row blocks (True) or
-        update every row (False, the default); the results are identical."""
+        update every row (False); the results are identical. The default is
+        True from 600 templates up."""
         self._check(self._lib.lss_set_round_kernel(self._h, int(bool(skip_blocks))))
+
+    def round_kernel(self) -> bool:
+        """True when the rounds skip provably unchanged template-row blocks."""
+        import ctypes
+        v = ctypes.c_int32(0)
+        self._check(self._lib.lss_get_round_kernel(self._h, ctypes.byref(v)))
+        return bool(v.value)
 
     def set_profiling(self, on: bool = True):
         self._check(self._lib.lss_set_profiling(self._h, int(on)))
