@@ -40,9 +40,10 @@
 // peak counts for the round's time order. The update then runs in two steps
 // split by a grid barrier: the decisions for every (spike segment, 32-column
 // chunk, group of blocks) item, an equal range of items per warp, append the
-// blocks to process to their CTA's list; then every warp takes an equal range
-// of all lists' entries and streams their rows through a ring of stages in
-// shared memory filled by asynchronous copies a few batches ahead. Every wait
+// blocks to process to their CTA's list; then every CTA takes an equal range
+// of all lists' entries, its warps take them one at a time from a shared
+// counter, and stream their rows through a ring of stages in shared memory
+// filled by asynchronous copies a few batches ahead. Every wait
 // is bounded (STATUS_TIMEOUT).
 #include "lss_kernels.cuh"
 #include "mp_common.cuh"
@@ -99,7 +100,7 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
     extern __shared__ float smem[];
     __shared__ int s_pref[MPB_MAX_GRID + 1];
     __shared__ int s_wcnt[MPB_THREADS / 32];
-    __shared__ int s_cnt, s_total, s_ecnt;
+    __shared__ int s_cnt, s_total, s_ecnt, s_enext;
 
     const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
@@ -108,6 +109,7 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
     const int W = a.cols_per_blk;
     const int lo = min(N, b * W), hi = min(N, lo + W);
     const int64_t ldk = a.ldk, ldb = a.ldb;
+    const int ldb_i = (int)a.ldb;  // < 2^31 (checked at launch): row offsets as one 32x32->64 multiply-add
 
     float* vals = smem;                                       // [W + 2nt]
     int* ivals = reinterpret_cast<int*>(smem + W + 2 * nt);  // [W]
@@ -492,8 +494,13 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
             if (tid == 0) clk.lap(3);
             prefix_counts(a.ment_cnt);
             const int n = s_pref[G];
-            const int e_lo = (int)((int64_t)n * gw / NW), e_hi = (int)((int64_t)n * (gw + 1) / NW);
-            if (e_lo < e_hi) {
+            // this CTA's equal range of all entries, handed to its warps one
+            // entry at a time from a shared counter (each warp starts with one)
+            const int c_lo = (int)((int64_t)n * b / G), c_hi = (int)((int64_t)n * (b + 1) / G);
+            if (tid == 0) s_enext = c_lo + WPB;
+            __syncthreads();
+            const int e_first = c_lo + warp;
+            if (e_first < c_hi) {
                 struct Ent {
                     int4 w0, w1, w2, w3;
                 };
@@ -566,45 +573,51 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
                     const int r0 = S.bb * MPB_ROWS, nr = min(MPB_ROWS, T - r0);
                     const bool act = S.s >= 0;
                     const uint32_t d = ring_s + (uint32_t)(stage * 3 * 8 * 32 + lane) * 4u;
+                    const unsigned m0b = S.m0 >> (rb * 8), m1b = S.m1 >> (rb * 8);
+                    const float* bcol = a.B + S.s;
 #pragma unroll
                     for (int u = 0; u < 8; ++u) {
-                        const int rr = rb * 8 + u;
-                        const bool ld = act && rr < nr;
-                        const int64_t t = r0 + rr;
-                        cp_async4_if(d + (uint32_t)u * 128u, a.B + t * ldb + S.s, ld, pk);
-                        cp_async4_if(d + (uint32_t)(8 + u) * 128u, S.c0p + t * L2, ld && ((S.m0 >> rr) & 1u), ps);
-                        cp_async4_if(d + (uint32_t)(16 + u) * 128u, S.c1p + t * L2, ld && ((S.m1 >> rr) & 1u), ps);
+                        const bool ld = act && rb * 8 + u < nr;
+                        const int t = r0 + rb * 8 + u;
+                        cp_async4_if(d + (uint32_t)u * 128u, bcol + (int64_t)t * ldb_i, ld, pk);
+                        cp_async4_if(d + (uint32_t)(8 + u) * 128u, S.c0p + (int64_t)t * L2, ld && ((m0b >> u) & 1u), ps);
+                        cp_async4_if(d + (uint32_t)(16 + u) * 128u, S.c1p + (int64_t)t * L2, ld && ((m1b >> u) & 1u), ps);
                     }
                 };
                 Ent En;
                 St scur, siss;  // the entry being updated, the entry being fetched
-                ld_ent(e_lo, En);
+                ld_ent(e_first, En);
                 make(En, siss);
                 scur = siss;
-                if (e_lo + 1 < e_hi) ld_ent(e_lo + 1, En);
-                const int nbt = (e_hi - e_lo) * BPB;
+                int n_ent = 1;  // entries this warp has taken so far
                 // flat batch j of the warp's entries into stage j % NST; the
                 // fetch runs NST - 1 batches ahead of the update (less than one
-                // entry, so at most two entries are live)
+                // entry, so at most two entries are live); entering an entry,
+                // it takes the next one and loads its words
                 static_assert(NST - 1 < BPB, "the fetch may run at most one entry ahead");
                 auto fetch_batch = [&](int j) {
                     const int rb = j % BPB;
-                    if (rb == 0 && j > 0) {
-                        make(En, siss);
-                        const int e2 = e_lo + j / BPB + 1;
-                        if (e2 < e_hi) ld_ent(e2, En);
+                    if (rb == 0) {
+                        if (j > 0) make(En, siss);
+                        int e2 = 0;
+                        if (lane == 0) e2 = atomicAdd(&s_enext, 1);
+                        e2 = __shfl_sync(FULL, e2, 0);
+                        if (e2 < c_hi) {
+                            ld_ent(e2, En);
+                            ++n_ent;
+                        }
                     }
                     issue(siss, rb, j % NST);
                 };
 #pragma unroll
                 for (int j = 0; j < NST - 1; ++j) {
-                    if (j < nbt) fetch_batch(j);
+                    if (j < n_ent * BPB) fetch_batch(j);
                     cp_async_commit();
                 }
                 ColMaxRows m;
                 float mn = INFINITY;
-                for (int k = 0; k < nbt; ++k) {
-                    if (k + NST - 1 < nbt) fetch_batch(k + NST - 1);
+                for (int k = 0; k < n_ent * BPB; ++k) {
+                    if (k + NST - 1 < n_ent * BPB) fetch_batch(k + NST - 1);
                     cp_async_commit();
                     cp_async_wait<NST - 1>();  // batch k has landed (this lane's own copies)
                     const int rb = k % BPB;
@@ -616,18 +629,18 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
                     // predicated stores; rows not fetched are never selected),
                     // then the rare Cf candidates
                     float xs[8], ap[8];
+                    const unsigned m0b = scur.m0 >> (rb * 8), m1b = scur.m1 >> (rb * 8);
+                    float* bcol = a.B + scur.s;
 #pragma unroll
                     for (int u = 0; u < 8; ++u) {
-                        const int rr = rb * 8 + u;
-                        const bool okr = act && rr < nr;
-                        const int t = r0 + rr;
+                        const bool okr = act && rb * 8 + u < nr;
+                        const int t = r0 + rb * 8 + u;
                         const float v = stg[u * 32], w0 = stg[(8 + u) * 32], w1 = stg[(16 + u) * 32];
                         const float y0 = __fsub_rn(v, __fmul_rn(scur.a0, w0));
-                        const float xa = ((scur.m0 >> rr) & 1u) ? y0 : v;
+                        const float xa = ((m0b >> u) & 1u) ? y0 : v;
                         const float y1 = __fsub_rn(xa, __fmul_rn(scur.a1, w1));
-                        const float xv = ((scur.m1 >> rr) & 1u) ? y1 : xa;
-                        st_keep_if(a.B + (int64_t)t * ldb + scur.s, xv,
-                                   okr && __float_as_uint(xv) != __float_as_uint(v), pk);
+                        const float xv = ((m1b >> u) & 1u) ? y1 : xa;
+                        st_keep_if(bcol + (int64_t)t * ldb_i, xv, okr && __float_as_uint(xv) != __float_as_uint(v), pk);
                         mn = okr ? fminf(mn, fabsf(xv)) : mn;
                         const float rl = fmaxf(xv, 0.f);
                         ap[u] = okr ? __fmul_rn(__fmul_rn(rl, rl), s_inv[min(t, T - 1)]) : -INFINITY;
@@ -711,7 +724,7 @@ int64_t mp_blocks_list_entries(int64_t N, int nt, int T, int grid) {
 
 cudaError_t launch_mp_blocks(MPArgs a, int grid, cudaStream_t s) {
     if (grid > MPB_MAX_GRID || !a.perm || !a.cmaxr || !a.bkey || !a.bmin || (a.ment && (!a.ment_cnt || a.ment_cap < 0)) ||
-        a.nb != (a.T + MPB_ROWS - 1) / MPB_ROWS)
+        a.nb != (a.T + MPB_ROWS - 1) / MPB_ROWS || a.ldb > INT_MAX || (int64_t)a.T * (2 * a.nt + 1) > INT_MAX)
         return cudaErrorInvalidValue;
     int dev = 0, optin = 0;
     cudaError_t e = cudaGetDevice(&dev);
