@@ -36,7 +36,7 @@ __device__ __forceinline__ float tf32_rna(float x) {
 // so the K values a thread writes per sample land next to its neighbours'
 // and a warp writes 32*K contiguous outputs per sample row.
 template <int KPC, int PC, bool TF32, int NTP>
-__global__ void __launch_bounds__(256, 3) k_pca_proj_t(const float* __restrict__ X, int64_t ldx, int32_t C, int64_t N,
+__global__ void __launch_bounds__(256, KPC <= 6 ? 3 : 2) k_pca_proj_t(const float* __restrict__ X, int64_t ldx, int32_t C, int64_t N,
                                                     const float* __restrict__ wpca, int32_t nt, void* __restrict__ out0,
                                                     void* __restrict__ out_lo, int64_t ldk,
                                                     const int32_t* __restrict__ tiles, const int32_t* __restrict__ ntiles,
