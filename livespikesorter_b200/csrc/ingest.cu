@@ -30,29 +30,65 @@ __device__ __forceinline__ int64_t src_row(int64_t s, const IngestMap& m, int64_
 
 // Per-channel integer sums over the padded batch (exact: raw samples are
 // integers, so the mean is the correctly rounded quotient of an exact sum).
-// Grid: one CTA per 256 columns; threads stride over channels.
-__global__ void k_chan_sums(const int16_t* __restrict__ raw, int32_t ld_raw,
-                            const int32_t* __restrict__ chan_map, int32_t C, int64_t N,
-                            IngestMap map, long long* __restrict__ sums) {
+// Grid: one CTA per 256 columns; a warp per column at a time with channels
+// lane + 32q in registers (all of a column's loads in flight), per-lane int
+// sums combined across the CTA's warps in shared memory, one 64-bit atomic
+// per channel and CTA.
+template <int NQ>
+__global__ void __launch_bounds__(256) k_chan_sums(const int16_t* __restrict__ raw, int32_t ld_raw,
+                                                   const int32_t* __restrict__ chan_map, int32_t C, int64_t N,
+                                                   IngestMap map, long long* __restrict__ sums) {
+    __shared__ int part[8][NQ * 32];
     const int64_t s0 = (int64_t)blockIdx.x * 256;
     const int64_t s1 = min(N, s0 + 256);
     const int64_t base = map.base_dev ? *map.base_dev : 0;
-    for (int c = threadIdx.x; c < C; c += blockDim.x) {
-        const int ch = chan_map ? chan_map[c] : c;
-        int acc = 0;
-        for (int64_t s = s0; s < s1; ++s) {
-            const int64_t r = src_row(s, map, base);
-            if (r >= 0) acc += raw[r * ld_raw + ch];
-        }
-        atomicAdd((unsigned long long*)&sums[c], (unsigned long long)(long long)acc);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int acc[NQ];
+    int ch[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+        const int c = lane + 32 * q;
+        acc[q] = 0;
+        ch[q] = (c < C) ? (chan_map ? chan_map[c] : c) : 0;
     }
+    for (int64_t sc = s0 + warp; sc < s1; sc += 8) {
+        const int64_t r = src_row(sc, map, base);
+        if (r < 0) continue;
+        const int16_t* row = raw + r * ld_raw;
+#pragma unroll
+        for (int q = 0; q < NQ; ++q)
+            if (lane + 32 * q < C) acc[q] += row[ch[q]];
+    }
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) part[warp][lane + 32 * q] = acc[q];
+    __syncthreads();
+    for (int c = threadIdx.x; c < C; c += blockDim.x) {
+        int t = 0;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) t += part[w][c];
+        atomicAdd((unsigned long long*)&sums[c], (unsigned long long)(long long)t);
+    }
+}
+
+template <int NQ>
+static void launch_sums_t(const int16_t* raw, int32_t ld_raw, const int32_t* chan_map, int32_t C, int64_t N,
+                          IngestMap map, long long* sums, cudaStream_t s) {
+    const int grid = (int)((N + 255) / 256);
+    k_chan_sums<NQ><<<grid, 256, 0, s>>>(raw, ld_raw, chan_map, C, N, map, sums);
 }
 
 cudaError_t launch_chan_sums(const int16_t* raw, int32_t ld_raw, const int32_t* chan_map, int32_t C,
                              int64_t N, IngestMap map, long long* sums, cudaStream_t s) {
-    cudaMemsetAsync(sums, 0, sizeof(long long) * C, s);
-    const int grid = (int)((N + 255) / 256);
-    k_chan_sums<<<grid, 256, 0, s>>>(raw, ld_raw, chan_map, C, N, map, sums);
+    cudaError_t e = cudaMemsetAsync(sums, 0, sizeof(long long) * C, s);
+    if (e != cudaSuccess) return e;
+    const int nq = (C + 31) / 32;
+    if (nq <= 2) launch_sums_t<2>(raw, ld_raw, chan_map, C, N, map, sums, s);
+    else if (nq <= 4) launch_sums_t<4>(raw, ld_raw, chan_map, C, N, map, sums, s);
+    else if (nq <= 8) launch_sums_t<8>(raw, ld_raw, chan_map, C, N, map, sums, s);
+    else if (nq <= 12) launch_sums_t<12>(raw, ld_raw, chan_map, C, N, map, sums, s);
+    else if (nq <= 16) launch_sums_t<16>(raw, ld_raw, chan_map, C, N, map, sums, s);
+    else if (nq <= 24) launch_sums_t<24>(raw, ld_raw, chan_map, C, N, map, sums, s);
+    else launch_sums_t<32>(raw, ld_raw, chan_map, C, N, map, sums, s);
     return cudaGetLastError();
 }
 
@@ -81,7 +117,6 @@ __global__ void __launch_bounds__(256) k_car(const int16_t* __restrict__ raw, in
     extern __shared__ float sm[];
     float* tile = sm;                                  // [C][CAR_COLS + 1]
     float* mean = sm + (size_t)C * (CAR_COLS + 1);     // [C]
-    float* med = mean + C;                             // [CAR_COLS]
     const int64_t s0 = (int64_t)blockIdx.x * CAR_COLS;
     const int ncol = (int)min((int64_t)CAR_COLS, N - s0);
     const double invN = 1.0 / (double)N;
@@ -89,28 +124,27 @@ __global__ void __launch_bounds__(256) k_car(const int16_t* __restrict__ raw, in
     for (int c = threadIdx.x; c < C; c += blockDim.x)
         mean[c] = (float)((double)sign * (double)sums[c] * invN);
     __syncthreads();
-    for (int idx = threadIdx.x; idx < C * CAR_COLS; idx += blockDim.x) {
-        const int c = idx % C, j = idx / C;
-        float v = 0.f;
-        if (j < ncol) {
-            const int64_t r = src_row(s0 + j, map, base);
-            const int ch = chan_map ? chan_map[c] : c;
-            const float x = (r >= 0) ? sign * (float)raw[r * ld_raw + ch] : 0.f;
-            v = __fsub_rn(x, mean[c]);
-        }
-        tile[c * (CAR_COLS + 1) + j] = v;
-    }
-    __syncthreads();
+    // a warp per time column: its channels lane + 32q in registers (all loads
+    // of the column in flight at once), mean removed, the lower median found
+    // on the keys, and the referenced values parked in the tile for the
+    // channel-major write below
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (do_car) {
-        const uint32_t kth = (uint32_t)((C - 1) / 2);
-        for (int j = warp; j < ncol; j += blockDim.x >> 5) {
+    const uint32_t kth = (uint32_t)((C - 1) / 2);
+    for (int j = warp; j < CAR_COLS; j += blockDim.x >> 5) {
+        const int64_t r = (j < ncol) ? src_row(s0 + j, map, base) : -1;
+        float v[NQ];
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            const int c = lane + 32 * q;
+            const int ch = (c < C) ? (chan_map ? chan_map[c] : c) : 0;
+            const float x = (c < C && r >= 0) ? sign * (float)raw[r * ld_raw + ch] : 0.f;
+            v[q] = (c < C && j < ncol) ? __fsub_rn(x, mean[c]) : 0.f;
+        }
+        float mj = 0.f;
+        if (do_car && j < ncol) {
             uint32_t key[NQ];
 #pragma unroll
-            for (int q = 0; q < NQ; ++q) {
-                const int c = lane + 32 * q;
-                key[q] = (c < C) ? fkey(tile[c * (CAR_COLS + 1) + j]) : 0xFFFFFFFFu;
-            }
+            for (int q = 0; q < NQ; ++q) key[q] = (lane + 32 * q < C) ? fkey(v[q]) : 0xFFFFFFFFu;
             uint32_t res = 0;
             for (int b = 31; b >= 0; --b) {
                 const uint32_t trial = res | ((1u << b) - 1u);
@@ -120,17 +154,19 @@ __global__ void __launch_bounds__(256) k_car(const int16_t* __restrict__ raw, in
                 cnt = __reduce_add_sync(0xffffffffu, cnt);
                 if (cnt < kth + 1) res |= (1u << b);
             }
-            if (lane == 0) med[j] = unkey(res);
+            mj = unkey(res);
         }
-    } else if (threadIdx.x < CAR_COLS) {
-        med[threadIdx.x] = 0.f;
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            const int c = lane + 32 * q;
+            if (c < C) tile[c * (CAR_COLS + 1) + j] = do_car ? __fsub_rn(v[q], mj) : v[q];
+        }
     }
     __syncthreads();
     for (int idx = threadIdx.x; idx < C * CAR_COLS; idx += blockDim.x) {
         const int j = idx % CAR_COLS, c = idx / CAR_COLS;
         if (j < ncol) {
-            const float v = tile[c * (CAR_COLS + 1) + j];
-            X1[(int64_t)c * ldx + s0 + j] = do_car ? __fsub_rn(v, med[j]) : v;
+            X1[(int64_t)c * ldx + s0 + j] = tile[c * (CAR_COLS + 1) + j];
         }
     }
 }
