@@ -440,6 +440,11 @@ int lss_create(const lss_config* cfg, const lss_tensors* t, lss_handle** out) {
     ALLOC(mp_perm, (size_t)h->mp_nb * MPB_ROWS);
     ALLOC(mp_cmaxr, (size_t)T * T);
     ALLOC(mp_rowof, T);
+    {
+        const int64_t passes = ((T + 15) / 16 * 16 + 255) / 256;  // the score GEMM's template passes
+        ALLOC(sc_part_keys, (size_t)(passes * ld));
+        ALLOC(sc_part, (size_t)(4 * passes * ld));
+    }
     ALLOC(mp_ctcq, (size_t)T * T * L2);
     ALLOC(mp_bkey, (size_t)h->mp_nb * ld);
     ALLOC(mp_phase, 6);
@@ -729,6 +734,9 @@ int lss::run_scores(lss_handle* h, const float* X, int64_t ldx, int64_t N, float
         ex.cf_lo = h->cf_lo.p;
         ex.cf_hi = h->cf_hi.p;
         ex.rowof = rowof;
+        ex.part_keys = h->sc_part_keys.p;
+        ex.part = h->sc_part.p;
+        ex.part_cap = (int64_t)h->sc_part_keys.n;
         CK(launch_score_tc_bf16x3(h->B0T.p, h->B0T16lo.p, h->CKpad, (int)N, folded ? h->Uw16.p : h->Up16.p,
                                   folded ? h->Uw16lo.p : h->Up16lo.p, h->T, h->CKpad, h->nm.p, B, h->ld, h->cfmax.p,
                                   h->imax.p, h->nt, h->status.p, h->sm_count, s, ex));
@@ -759,7 +767,7 @@ int lss::run_scores(lss_handle* h, const float* X, int64_t ldx, int64_t N, float
             h->rc_pending = true;
             h->last_scored = N;
         }
-        h->stats.launches += 7;
+        h->stats.launches += 7 + (h->T > 256 ? 1 : 0);  // + the bounds finalize of a multi-pass GEMM
         h->mark(6, s);
         if (maxima_ready) *maxima_ready = true;
         return LSS_OK;
@@ -772,7 +780,7 @@ int lss::run_scores(lss_handle* h, const float* X, int64_t ldx, int64_t N, float
     CK(launch_score_tc_tf32x3(h->B0T_hi.p, h->B0T_lo.p, h->CKpad, (int)N, folded ? h->Uw_hi.p : h->Up_hi.p,
                               folded ? h->Uw_lo.p : h->Up_lo.p, h->T, h->CKpad, h->nm.p, B, h->ld, h->cfmax.p,
                               h->imax.p, h->nt, h->status.p, h->sm_count, s, ex));
-    h->stats.launches += 2;
+    h->stats.launches += 2 + (h->T > 256 ? 1 : 0);  // + the key maxima of a multi-pass GEMM
     h->mark(6, s);
     if (maxima_ready) *maxima_ready = true;
     return LSS_OK;

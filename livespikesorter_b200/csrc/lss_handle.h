@@ -75,6 +75,8 @@ struct lss_handle {
     DevBuf<int4> mp_ent;                         // block-skipping rounds: per-CTA lists of blocks to process
     DevBuf<int32_t> mp_ent_cnt;                  // [grid] entries per list
     DevBuf<int32_t> mp_rowof;                    // [T] score row of each template in probe order
+    DevBuf<unsigned long long> sc_part_keys;     // [passes, ld] score GEMM: per-pass best keys (error-bound split)
+    DevBuf<float> sc_part;                       // [passes, 4, ld] per-pass bound partials
     DevBuf<float> mp_ctcq;                       // [T, T, 2nt+1] ctc rows in probe order
     // BF16 path (BF16x3 GEMM): projection and templates as bf16 hi / lo splits
     DevBuf<__nv_bfloat16> B0T, B0T16lo, Up16, Up16lo;
@@ -164,7 +166,7 @@ struct lss_handle {
         tF.release(); iCC.release(); iU.release(); cfmax.release(); imax.release(); blk_cnt.release();
         blk_x.release(); blk_y.release(); sp_x.release(); sp_y.release(); sp_round.release();
         round_start.release(); counters.release(); status.release(); sp_amp.release(); blk_amp.release(); colkey.release();
-        mp_perm.release(); mp_cmaxr.release(); mp_phase.release(); mp_ent.release(); mp_ent_cnt.release(); mp_rowof.release(); mp_ctcq.release(); mp_bmin.release(); mp_bkey.release();
+        mp_perm.release(); mp_cmaxr.release(); mp_phase.release(); mp_ent.release(); mp_ent_cnt.release(); mp_rowof.release(); mp_ctcq.release(); sc_part_keys.release(); sc_part.release(); mp_bmin.release(); mp_bkey.release();
         bar.release(); rec_time.release(); rec_count.release(); rec_tmpl.release(); rec_slot.release(); rec_amp.release();
         rec_pc.release(); B0T.release(); B0T16lo.release(); Up16.release(); Up16lo.release();
         B0T_hi.release(); B0T_lo.release(); Up_hi.release(); Up_lo.release();

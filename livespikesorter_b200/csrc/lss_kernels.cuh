@@ -84,6 +84,12 @@ struct TcExtra {
     float eps = 0.f;
     float* cf_lo = nullptr;
     float* cf_hi = nullptr;
+    // error bounds over a full batch in several template passes: scratch for
+    // the per-(pass, column) partials (part_cap = passes x columns it holds);
+    // without it such a batch is scored tile by tile
+    unsigned long long* part_keys = nullptr;
+    float* part = nullptr;  // 4 x part_cap
+    int64_t part_cap = 0;
     // score rows in another order: template t's row of B is rowof[t] (the
     // block-skipping rounds keep rows in probe order); null: row t
     const int32_t* rowof = nullptr;

@@ -86,6 +86,11 @@ struct Args {
     float eps;
     float* cf_lo;
     float* cf_hi;
+    // split mode with error bounds: per (pass, column) partials, finished by
+    // k_bounds_finalize: part_keys [npass][ncols] best key of the pass; part
+    // [npass][4][ncols] lo of the pass's best, largest hi, its template, second hi
+    unsigned long long* part_keys;
+    float* part;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -299,7 +304,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     const int ntiles = (rows + BM - 1) / BM;
     const int PW = a.pass_w;
     const int npass = (a.Tpad + PW - 1) / PW;
-    const bool split = a.keys != nullptr;
+    const bool split = a.keys != nullptr || a.part_keys != nullptr;
     const int items = split ? ntiles * npass : ntiles;
 
     if (warp == 0) {
@@ -472,7 +477,16 @@ __global__ void __launch_bounds__(THREADS, 1)
                 acc = (acc + 1) % a.nacc;
             }
             if (ok && valid) {
-                if (split) {
+                if (split && bounds) {
+                    const int64_t nc = a.ncols;
+                    const float cf = edge ? 0.f : fmaxf(m.best, 0.f);
+                    const uint32_t t = edge ? 0u : (uint32_t)m.bi;
+                    a.part_keys[pb * nc + n] = ((unsigned long long)__float_as_uint(cf) << 32) | (unsigned long long)(~t);
+                    a.part[(pb * 4 + 0) * nc + n] = edge ? 0.f : lo_best;
+                    a.part[(pb * 4 + 1) * nc + n] = edge ? 0.f : hi1;
+                    a.part[(pb * 4 + 2) * nc + n] = __int_as_float(edge ? -1 : thi1);
+                    a.part[(pb * 4 + 3) * nc + n] = edge ? 0.f : hi2;
+                } else if (split) {
                     const float cf = edge ? 0.f : fmaxf(m.best, 0.f);
                     const uint32_t t = edge ? 0u : (uint32_t)m.bi;
                     atomicMax(a.keys + n, ((unsigned long long)__float_as_uint(cf) << 32) | (unsigned long long)(~t));
@@ -506,6 +520,41 @@ __global__ void k_keys_to_maxima(const unsigned long long* __restrict__ keys, in
     const unsigned long long k = keys[n];
     cfmax[n] = __uint_as_float((uint32_t)(k >> 32));
     imax[n] = (int32_t)(~(uint32_t)k);
+}
+
+// Split mode with error bounds: per column, the passes' partials combined into
+// what the unsplit epilogue writes: the best (Cf, first template) over the
+// passes, the lower bound of that template's Cf, the largest upper bound and,
+// in cf2, the largest upper bound of any other template.
+__global__ void k_bounds_finalize(const unsigned long long* __restrict__ part_keys, const float* __restrict__ part,
+                                  int npass, int N, int nt, float* __restrict__ cfmax, int32_t* __restrict__ imax,
+                                  float* __restrict__ cf_lo, float* __restrict__ cf_hi, float* __restrict__ cf2) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    unsigned long long best = 0ull;
+    int pbest = 0;
+    for (int p = 0; p < npass; ++p) {
+        const unsigned long long k = part_keys[(int64_t)p * N + n];
+        if (k > best) {
+            best = k;
+            pbest = p;
+        }
+    }
+    const int tb = (int)(~(uint32_t)best);
+    float hi = 0.f, other = 0.f;
+    for (int p = 0; p < npass; ++p) {
+        const float h1 = part[((int64_t)p * 4 + 1) * N + n];
+        const int t1 = __float_as_int(part[((int64_t)p * 4 + 2) * N + n]);
+        const float h2 = part[((int64_t)p * 4 + 3) * N + n];
+        hi = fmaxf(hi, h1);
+        other = fmaxf(other, (t1 == tb) ? h2 : h1);
+    }
+    const bool edge = (n < nt) || (n >= N - nt);
+    cfmax[n] = edge ? 0.f : __uint_as_float((uint32_t)(best >> 32));
+    imax[n] = edge ? 0 : tb;
+    cf_lo[n] = edge ? 0.f : part[((int64_t)pbest * 4 + 0) * N + n];
+    cf_hi[n] = edge ? 0.f : hi;
+    cf2[n] = edge ? 0.f : other;
 }
 
 // The same for the mapped columns of a re-check (rowmap, count on the device).
@@ -594,15 +643,25 @@ static cudaError_t launch_tc(const void* A, const void* Alo, int64_t ldk, int N,
     // A re-check of mapped rows (rowmap, count on the device) is usually one
     // or two tiles: its templates are split the same way, in narrower passes.
     const int ntiles = (N + tc::BM - 1) / tc::BM;
-    const bool split_map = ex.keys && ex.rowmap && ex.count_dev && !ex.cf2 && !ex.un && T > tc::MAPPED_SPLIT_W;
-    const bool split = split_map || (ex.keys && !ex.cf2 && !ex.rowmap && 2 * ntiles < grid && T > tc::SPLIT_W);
     // templates in passes of at most 256 TMEM columns (equal widths): two
     // accumulators alternate, so one pass's epilogue drains while the next
     // pass's MMAs run, and the smaller stages leave room for four of them
     const int tpad = (T + 15) / 16 * 16;
     const int npass = (tpad + 255) / 256;
     const int even_w = ((tpad + npass - 1) / npass + 15) / 16 * 16;
-    const TcPlan p = tc_plan(T, OP, split_map ? tc::MAPPED_SPLIT_W : (split ? tc::SPLIT_W : even_w));
+    const bool split_map = ex.keys && ex.rowmap && ex.count_dev && !ex.cf2 && !ex.un && T > tc::MAPPED_SPLIT_W;
+    const bool split_short = ex.keys && !ex.cf2 && !ex.un && !ex.rowmap && 2 * ntiles < grid && T > tc::SPLIT_W;
+    // Several passes over a full batch: one work item per (tile, pass), so that
+    // a tile's passes run on consecutive CTAs at the same time and its sample
+    // operand is read from DRAM once (tile by tile the passes would stream it
+    // once per pass, and 148 tiles in flight do not fit the L2); column maxima
+    // through keys, or per-pass partials for the error bounds.
+    const bool bounds_part = ex.un && ex.part_keys && ex.part && (int64_t)npass * N <= ex.part_cap;
+    const bool split_pass = !split_map && !split_short && !ex.rowmap && npass > 1 &&
+                            ((ex.keys && !ex.cf2 && !ex.un) || bounds_part);
+    const bool split = split_map || split_short || split_pass;
+    const bool part_mode = split_pass && bounds_part;
+    const TcPlan p = tc_plan(T, OP, split_map ? tc::MAPPED_SPLIT_W : (split_short ? tc::SPLIT_W : even_w));
     if (p.stages < 2 || CKpad % p.kblock) return cudaErrorInvalidValue;
     CUtensorMap ma, malo, mb, mblo;
     if (!make_map(&ma, A, N, CKpad, ldk, tc::BM, OP) || !make_map(&mb, Bm, p.Tpad, CKpad, CKpad, p.box_rows, OP))
@@ -638,8 +697,10 @@ static cudaError_t launch_tc(const void* A, const void* Alo, int64_t ldk, int N,
     a.ncols = ex.rowmap ? ex.ncols : N;
     a.cf2 = ex.cf2;
     a.pass_w = p.pass_w;
-    a.keys = split ? ex.keys : nullptr;
-    a.un = split ? nullptr : ex.un;
+    a.keys = (split && !part_mode) ? ex.keys : nullptr;
+    a.part_keys = part_mode ? ex.part_keys : nullptr;
+    a.part = part_mode ? ex.part : nullptr;
+    a.un = (split && !part_mode) ? nullptr : ex.un;
     a.pn2 = ex.pn2;
     a.eps = ex.eps;
     a.cf_lo = ex.cf_lo;
@@ -648,12 +709,15 @@ static cudaError_t launch_tc(const void* A, const void* Alo, int64_t ldk, int N,
     cudaError_t e = cudaFuncSetAttribute(tc::k_score_tc<OP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
     if (e != cudaSuccess) return e;
     const int items = split ? ntiles * ((p.Tpad + p.pass_w - 1) / p.pass_w) : ntiles;
-    if (split) {
+    if (split && !part_mode) {
         e = cudaMemsetAsync(ex.keys, 0, (size_t)(split_map ? ex.ncols : N) * sizeof(unsigned long long), s);
         if (e != cudaSuccess) return e;
     }
     tc::k_score_tc<OP><<<std::min(grid, items), tc::THREADS, p.smem, s>>>(ma, malo, mb, mblo, a);
-    if (split_map)
+    if (part_mode)
+        tc::k_bounds_finalize<<<(N + 255) / 256, 256, 0, s>>>(ex.part_keys, ex.part, (p.Tpad + p.pass_w - 1) / p.pass_w, N,
+                                                              nt, cfmax, imax, ex.cf_lo, ex.cf_hi, ex.cf2);
+    else if (split_map)
         tc::k_keys_to_maxima_mapped<<<(N + 255) / 256, 256, 0, s>>>(ex.keys, ex.rowmap, ex.count_dev, ex.map_rows, N,
                                                                     cfmax, imax);
     else if (split)
