@@ -164,6 +164,8 @@ def test_rounds_bit_exact_on_given_scores_at_384ch(T, dup):
     st_o, amps_o, _ = ko.run_matching(X, setup.U, setup.ctc, setup.wPCA, setup.Th, nt, B=B, nm=nm)
     s = Sorter.from_setup(setup, nm=nm)
     assert len(st_o) > 5000
+    # the default: block-skipping rounds from 600 templates up
+    assert s.round_kernel() == (T >= 600)
     for skip in (False, True):
         s.set_round_kernel(skip)
         st, amps = s.match_scores(B.cuda())
