@@ -178,14 +178,14 @@ __global__ void __launch_bounds__(MPB_THREADS, 1) k_mp_blocks(MPArgs a) {
                     v = 0.f;  // Cf[:, :nt] = Cf[:, -nt:] = 0
                     if (own) ivals[s - lo] = 0;
                 } else {
-                    // the block keys of the column, 16 loads in flight at a time
+                    // the block keys of the column, 32 loads in flight at a time
                     unsigned long long k = 0ull;
-                    for (int b0 = 0; b0 < nb; b0 += 16) {
-                        unsigned long long kk[16];
+                    for (int b0 = 0; b0 < nb; b0 += 32) {
+                        unsigned long long kk[32];
 #pragma unroll
-                        for (int u = 0; u < 16; ++u) kk[u] = (b0 + u < nb) ? __ldcg(a.bkey + (b0 + u) * ldk + s) : 0ull;
+                        for (int u = 0; u < 32; ++u) kk[u] = (b0 + u < nb) ? __ldcg(a.bkey + (b0 + u) * ldk + s) : 0ull;
 #pragma unroll
-                        for (int u = 0; u < 16; ++u) k = max(k, kk[u]);
+                        for (int u = 0; u < 32; ++u) k = max(k, kk[u]);
                     }
                     v = __uint_as_float((unsigned)(k >> 32));
                     if (own) ivals[s - lo] = (int)(0xFFFFFFFFu - (unsigned)(k & 0xFFFFFFFFull));
