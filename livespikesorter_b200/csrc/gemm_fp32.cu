@@ -124,7 +124,8 @@ struct StoreFolded {
             const __nv_bfloat16 h = __float2bfloat16_rn(v);
             out16[o] = h;
             if (out16lo) out16lo[o] = __float2bfloat16_rn(__fsub_rn(v, __bfloat162float(h)));
-        } else {
+        }
+        if (hi) {
             uint32_t r;
             asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
             const float h = __uint_as_float(r);

@@ -114,14 +114,21 @@ int lss::rebuild_uw(lss_handle* h) {
     const int C = h->C;
     // templates with the whitening folded in, for lss_sort_batch
     const bool bf16 = h->cfg.precision == LSS_PREC_BF16_RECHECK;
-    CK(launch_build_uw(h->U.p, h->Mw.p, h->T, h->K, C, h->CKpad, nullptr, nullptr, h->Uw_hi.p, h->Uw_lo.p, 0));
+    // one product, stored as the tf32 split (FP32 path, BF16 re-check) and, on
+    // the BF16 path, as the bf16 split too
+    CK(launch_build_uw(h->U.p, h->Mw.p, h->T, h->K, C, h->CKpad, bf16 ? h->Uw16.p : nullptr,
+                       bf16 ? h->Uw16lo.p : nullptr, h->Uw_hi.p, h->Uw_lo.p, 0));
     h->stats.launches += 1;
     if (bf16) {
-        CK(launch_build_uw(h->U.p, h->Mw.p, h->T, h->K, C, h->CKpad, h->Uw16.p, h->Uw16lo.p, nullptr, nullptr, 0));
-        // template norms of the BF16 error bound, for the folded and the plain operand
+        // template norms of the BF16 error bound, for the folded operand and (once
+        // per template set: it does not depend on the drift) the plain one
         CK(launch_row_norms(h->Uw_hi.p, h->Uw_lo.p, h->T, h->CKpad, h->un_w.p, 0));
-        CK(launch_row_norms(h->Up_hi.p, h->Up_lo.p, h->T, h->CKpad, h->un_p.p, 0));
-        h->stats.launches += 3;
+        h->stats.launches += 1;
+        if (h->un_p_stale) {
+            CK(launch_row_norms(h->Up_hi.p, h->Up_lo.p, h->T, h->CKpad, h->un_p.p, 0));
+            h->un_p_stale = false;
+            h->stats.launches += 1;
+        }
     }
     // callers may sort on streams that do not wait for the legacy default
     // stream: the batch entry points wait for this event on their stream

@@ -66,6 +66,7 @@ struct lss_handle {
     DevBuf<unsigned long long> colkey;
     // block-skipping rounds (mp_blocks.cu): template rows in blocks of
     // MPB_ROWS ordered along the probe, |ctc| maxima, per-block column state
+    bool un_p_stale = true;                      // plain-template norms (BF16 bound) need recomputing
     bool mp_skip = false;                        // rounds kernel: block-skipping (mp_blocks.cu) or full (mp.cu)
     int mp_nb = 0;
     DevBuf<int32_t> mp_perm;

@@ -115,7 +115,8 @@ cudaError_t launch_score_tc_tf32x3(const float* B0T_hi, const float* B0T_lo, int
 cudaError_t launch_pca_proj_t_tf32(const float* X, int64_t ldx, int32_t C, int64_t N, const float* wpca, int32_t K,
                                    int32_t nt, float* hi, float* lo, int64_t ldk, cudaStream_t s);
 
-// U_w[t, c'*K + k] = sum_c U[t,k,c] Mw[c,c'] in GEMM layout: bf16 split (out16, out16lo) or tf32 hi/lo
+// U_w[t, c'*K + k] = sum_c U[t,k,c] Mw[c,c'] in GEMM layout: bf16 split (out16, out16lo) and/or tf32
+// hi/lo (a null pointer skips that form)
 cudaError_t launch_build_uw(const float* U, const float* Mw, int32_t T, int32_t K, int32_t C, int64_t ldk,
                             __nv_bfloat16* out16, __nv_bfloat16* out16lo, float* hi, float* lo, cudaStream_t s);
 

@@ -276,6 +276,7 @@ int lss_set_templates(lss_handle* h, const float* U, const float* wPCA) {
     const bool bf16 = h->cfg.precision == LSS_PREC_BF16_RECHECK;
     k_up<<<(unsigned)((nup + 255) / 256), 256, 0, s>>>(h->U.p, T, K, C, h->CKpad, h->Up_hi.p, h->Up_lo.p,
                                                        bf16 ? h->Up16.p : nullptr, bf16 ? h->Up16lo.p : nullptr);
+    h->un_p_stale = true;  // the plain templates changed
     const int64_t nw = (int64_t)T * C * nt;
     k_wave<<<(unsigned)((nw + 255) / 256), 256, 0, s>>>(h->U.p, h->wpca.p, T, K, C, nt, h->wave.p);
     const int M = T * K;
