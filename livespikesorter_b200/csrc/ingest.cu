@@ -360,13 +360,24 @@ __global__ void __launch_bounds__(HF_THREADS, 4) k_highpass_fft(const float* __r
     const int64_t start = (int64_t)blockIdx.x * (HF - 2 * L);
     const float* x1 = X1 + (int64_t)c1 * ldx;
     const float* x2 = X1 + (int64_t)(two ? c2 : c1) * ldx;
-    for (int n = threadIdx.x; n < HF; n += HF_THREADS) {
-        int64_t g = start - L + n;  // circular index (the modulo only near the ends)
-        if (g < 0 || g >= N) {
-            g %= N;
-            if (g < 0) g += N;
+    // 4 samples per thread loaded before they are stored (8 loads in flight)
+    static_assert(HF % (4 * HF_THREADS) == 0, "whole groups of 4 samples per thread");
+#pragma unroll
+    for (int i0 = 0; i0 < HF / HF_THREADS; i0 += 4) {
+        float v1[4], v2[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int n = threadIdx.x + (i0 + u) * HF_THREADS;
+            int64_t g = start - L + n;  // circular index (the modulo only near the ends)
+            if (g < 0 || g >= N) {
+                g %= N;
+                if (g < 0) g += N;
+            }
+            v1[u] = x1[g];
+            v2[u] = two ? x2[g] : 0.f;
         }
-        A[pad16(n)] = make_float2(x1[g], two ? x2[g] : 0.f);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) A[pad16(threadIdx.x + (i0 + u) * HF_THREADS)] = make_float2(v1[u], v2[u]);
     }
     __syncthreads();
     fft16_pass<1>(A, tw);
