@@ -57,11 +57,36 @@ __global__ void __launch_bounds__(256, KPC <= 6 ? 3 : 2) k_pca_proj_t(const floa
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
     for (int k = warp; k < KPC; k += nwarps)
         for (int m = lane; m < ntp; m += 32) ws[k * ntp + m] = (m < nt) ? wpca[k * nt + m] : 0.f;
-    for (int c = warp; c < PC; c += nwarps) {
-        const float* xrow = X + (int64_t)(c0 + c) * ldx;
-        for (int p = lane; p < xw; p += 32) {
-            const int64_t g = s0 - half + p;
-            xs[c * xw + p] = (c < nc && g >= 0 && g < N) ? xrow[g] : 0.f;
+    if constexpr (NTP > 0 && PC % 8 == 0) {
+        // fixed tap count: a warp's channel rows loaded into registers first, so
+        // that all of them are in flight at once, then stored (256 threads)
+        constexpr int XW = PT_S + NTP + 9, NP = (XW + 31) / 32, NCW = PC / 8;
+        float v[NCW][NP];
+#pragma unroll
+        for (int i = 0; i < NCW; ++i) {
+            const int c = warp + 8 * i;
+            const float* xrow = X + (int64_t)(c0 + c) * ldx;
+#pragma unroll
+            for (int j = 0; j < NP; ++j) {
+                const int pp = lane + 32 * j;
+                const int64_t g = s0 - half + pp;
+                v[i][j] = (pp < XW && c < nc && g >= 0 && g < N) ? xrow[g] : 0.f;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < NCW; ++i)
+#pragma unroll
+            for (int j = 0; j < NP; ++j) {
+                const int pp = lane + 32 * j;
+                if (pp < XW) xs[(warp + 8 * i) * XW + pp] = v[i][j];
+            }
+    } else {
+        for (int c = warp; c < PC; c += nwarps) {
+            const float* xrow = X + (int64_t)(c0 + c) * ldx;
+            for (int p = lane; p < xw; p += 32) {
+                const int64_t g = s0 - half + p;
+                xs[c * xw + p] = (c < nc && g >= 0 && g < N) ? xrow[g] : 0.f;
+            }
         }
     }
     __syncthreads();
