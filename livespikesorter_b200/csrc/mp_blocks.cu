@@ -9,8 +9,8 @@
 // the neighbouring floats are at least 2^(e-24) away, so any |d| < 2^(e-25)
 // leaves fl(B - d) == B bit for bit. Templates far apart on the probe have
 // cross-correlations many orders of magnitude below the scores they would
-// change (on a 384-channel probe about three quarters of all (row, spike)
-// updates are such no-ops), so:
+// change (on a 384-channel probe with 800 templates, two thirds of the
+// (spike chunk, row block) updates are such no-ops), so:
 //   * template rows are grouped into blocks of MPB_ROWS templates that lie
 //     close together on the probe (perm: templates ordered by the centre of
 //     mass of their channel energy);
@@ -21,9 +21,10 @@
 //     e's term only if fl(|a_e| * cmaxr[y_e][t_r]) >= thr, thr being a quarter
 //     ulp of the smallest bmin over the warp's columns (cmaxr = max over lags
 //     of |ctc|); a block where no row needs a term is skipped (its scores,
-//     bmin and bkey are provably unchanged); in a processed block the terms
-//     that are no-ops are skipped row by row, the second term only where the
-//     first left the score unchanged;
+//     bmin and bkey are provably unchanged); in a processed block a row's
+//     term is applied where its bound says it may change the score, and a
+//     row's second term also wherever its first was applied (the bound was
+//     taken on the field before the first term);
 //   * the peak phase takes each column's maximum over the block keys.
 // Everything that is computed is computed exactly as in k_mp: single-rounded
 // products and differences (__fmul_rn / __fsub_rn), Cf = fl(fl(r*r)/nm), the
