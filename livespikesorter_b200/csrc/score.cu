@@ -353,8 +353,9 @@ cudaError_t launch_recheck_select(const float* cf_lo, const float* cf_hi, const 
 // arithmetic: every output sums its (zero-padded) taps in ascending order with
 // one fmaf each, so the rows equal the FP32 path's. Column cols[i] goes to row
 // i (scatter = 0) or to row cols[i] (scatter = 1: a batch-sized array). A CTA
-// takes a column at a time and stages its window of PCOL_CH channels x ntp
-// samples in shared memory with coalesced loads before the dot products.
+// takes a (column, chunk of PCOL_CH channels) at a time and stages the chunk's
+// window of PCOL_CH channels x ntp samples in shared memory (coalesced loads,
+// 8 per thread in flight) before the dot products.
 constexpr int PCOL_CH = 64;
 template <int KPC>
 __global__ void __launch_bounds__(256) k_pca_proj_cols(const float* __restrict__ X, int64_t ldx, int32_t C, int64_t N,
@@ -372,16 +373,30 @@ __global__ void __launch_bounds__(256) k_pca_proj_cols(const float* __restrict__
     }
     const int n = *count;
     const int half = nt / 2;
-    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    const int nchunk = (C + PCOL_CH - 1) / PCOL_CH;
+    // one work item per (listed column, chunk of PCOL_CH channels)
+    for (int it = blockIdx.x; it < n * nchunk; it += gridDim.x) {
+        const int i = it / nchunk, c0 = (it - i * nchunk) * PCOL_CH;
         const int64_t s = cols[i];
         const int64_t row = scatter ? s : (int64_t)i;
-        for (int c0 = 0; c0 < C; c0 += PCOL_CH) {
+        {
             const int nc = min(PCOL_CH, C - c0);
             __syncthreads();
-            for (int e = threadIdx.x; e < nc * ntp; e += blockDim.x) {
-                const int c = e / ntp, m = e % ntp;
-                const int64_t g = s - half + m;
-                xs[c * xw + m] = (g >= 0 && g < N) ? X[(int64_t)(c0 + c) * ldx + g] : 0.f;
+            // staged 8 elements per thread at a time (loads before stores)
+            for (int e0 = threadIdx.x; e0 < nc * ntp; e0 += 8 * (int)blockDim.x) {
+                float v[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int e = e0 + u * (int)blockDim.x;
+                    const int c = e / ntp, m = e % ntp;
+                    const int64_t g = s - half + m;
+                    v[u] = (e < nc * ntp && g >= 0 && g < N) ? X[(int64_t)(c0 + c) * ldx + g] : 0.f;
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int e = e0 + u * (int)blockDim.x;
+                    if (e < nc * ntp) xs[(e / ntp) * xw + e % ntp] = v[u];
+                }
             }
             __syncthreads();
             for (int e = threadIdx.x; e < nc * KPC; e += blockDim.x) {
@@ -409,7 +424,8 @@ static cudaError_t launch_cols(const float* X, int64_t ldx, int32_t C, int64_t N
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int grid = std::max(1, std::min(max_cols, 8 * sms));
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)max_cols * ((C + PCOL_CH - 1) / PCOL_CH),
+                                                                   8 * sms));
     k_pca_proj_cols<KPC><<<grid, 256, smem, s>>>(X, ldx, C, N, wpca, nt, ntp, cols, count, hi, lo, ldk, scatter);
     return cudaGetLastError();
 }
